@@ -1,0 +1,188 @@
+/*
+ * shhd_b200.h — C ABI of the B200 step engine for the 2-D spectral
+ * Hohenberg–Halperin / fluctuating-hydrodynamics solver.
+ *
+ * The engine replaces, for one process on one GPU, the reference solver's
+ * per-step hot path: FluidSolver::step (src/fluid_solver.h:97-99) driving a
+ * TimeIntegrator (src/time_integrator.h:141) over the FCalculator RHS
+ * operators (src/fcalculator.h:64-69) on heFFTe transforms
+ * (src/fourier_transform.h:39-51).  State stays in device memory between
+ * calls; host arrays cross the boundary only in set/get calls.
+ *
+ * Conventions
+ *   - Every function returns 0 on success or a negative SHHD_E* code; the
+ *     message of the last failure on the calling thread is shhd_last_error().
+ *   - Host arrays are caller-owned and only read or written during the call.
+ *   - A state array is the reference's State layout (src/state.cc:22-38,
+ *     src/domain.cc:21-30): nfields blocks (rho, psi_0..psi_{N-1}, jx, jy) of
+ *     (nx/2+1)*ny complex values, gx fastest, as interleaved doubles.
+ *   - An engine may hold `batch` independent members (noise realisations or
+ *     jobs of one shape); member m's noise stream is keyed by
+ *     member_offset + m.
+ *   - One host thread at a time per engine; every engine owns a CUDA stream.
+ */
+#ifndef SHHD_B200_H
+#define SHHD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct shhd_engine shhd_engine;
+
+#define SHHD_MAX_ORDER_PARAMETERS 8
+#define SHHD_MAX_FORCES 8
+
+/* error codes */
+#define SHHD_OK 0
+#define SHHD_EINVAL (-1)      /* bad argument or configuration */
+#define SHHD_ECUDA (-2)       /* CUDA runtime failure */
+#define SHHD_ENOMEM (-3)      /* device allocation failed */
+#define SHHD_ENUMERIC (-4)    /* zero density met by v = j / rho (fcalculator_workspace.cc:122-133) */
+#define SHHD_EUNSUPPORTED (-5)/* configuration outside what the engine implements */
+
+enum shhd_mode { SHHD_COMPRESSIBLE = 0, SHHD_INCOMPRESSIBLE = 1, SHHD_QUIESCENT = 2 };
+enum shhd_integrator { SHHD_EULER = 0, SHHD_SRK3 = 1 };
+enum shhd_precision { SHHD_FP64 = 0, SHHD_FP32 = 1 };
+enum shhd_noise_source { SHHD_NOISE_PHILOX = 0, SHHD_NOISE_EXTERNAL = 1 };
+enum shhd_free_energy { SHHD_FE_NONE = 0, SHHD_FE_PHI4 = 1, SHHD_FE_QUADRATIC = 2 };
+
+typedef struct shhd_sine_force {
+    int target;      /* 0 momentum, 1 order parameter */
+    int component;   /* momentum: 0 = x, 1 = y; order parameter: index */
+    int axis;        /* 0 = x, 1 = y */
+    int nk;
+    double amplitude;
+} shhd_sine_force;
+
+typedef struct shhd_gradient_force {
+    int component;   /* order parameter index */
+    int direction;   /* 0 = x, 1 = y */
+    double amplitude;
+} shhd_gradient_force;
+
+/* Solver configuration: the reference's Params fields that shape the step
+ * (src/simulationinfo.h:35-175), with the model plugins given as data. */
+typedef struct shhd_config {
+    int active_nx, active_ny;   /* `grid` (active modes) */
+    int nx, ny;                 /* compute grid after `dealias` */
+    double lx, ly;              /* `length` */
+    double dt;                  /* `timestep` */
+    int mode;                   /* enum shhd_mode   (`time_evolution` */
+    int integrator;             /* enum shhd_integrator  .../...) */
+    int num_order_parameters;   /* `order_parameters` */
+    /* `model free_energy`: mu_a = (k0 + k2 k^2 + k4 k^4) psi_a (spectral) + u3 psi_a^3 (physical) */
+    int free_energy;            /* enum shhd_free_energy */
+    double mu_k0[SHHD_MAX_ORDER_PARAMETERS];
+    double mu_k2[SHHD_MAX_ORDER_PARAMETERS];
+    double mu_k4[SHHD_MAX_ORDER_PARAMETERS];
+    double mu_u3[SHHD_MAX_ORDER_PARAMETERS];
+    /* `model thermo linear_eos`: p = cT^2 rho (spectral only) */
+    double cT;
+    /* `model transport constant` */
+    double eta, zeta;
+    double mobility[SHHD_MAX_ORDER_PARAMETERS];
+    /* `fix ... nonlinear` */
+    int momentum_advection, order_parameter_advection;
+    /* `fix ... noise` */
+    int noise_momentum, noise_order_parameter;
+    int64_t noise_seed;
+    double kBT, chi;
+    /* `fix ... force/sine`, `fix ... force/gradient` */
+    int n_sine_forces;
+    shhd_sine_force sine_forces[SHHD_MAX_FORCES];
+    int n_gradient_forces;
+    shhd_gradient_force gradient_forces[SHHD_MAX_FORCES];
+    /* engine options (no reference counterpart) */
+    int precision;              /* enum shhd_precision */
+    int noise_source;           /* enum shhd_noise_source */
+    int batch;                  /* members advanced together (>= 1) */
+    int member_offset;          /* first member id for the noise key */
+} shhd_config;
+
+typedef struct shhd_info {
+    int nfields;                /* num_order_parameters + 3 */
+    size_t state_doubles;       /* doubles in one member's state array (reference layout) */
+    size_t active_modes;        /* active modes per field: (active_nx/2) * (active_ny - 1) */
+    int n_inverse, n_forward;   /* transforms per stage: C2R fields, R2C product fields */
+    int n_evolved;              /* fields the integrator updates */
+    size_t device_bytes;        /* device memory the engine holds */
+    double bytes_per_stage;     /* HBM bytes the fused kernels must move per stage (all members) */
+    double fft_flops_per_stage; /* 5 n log2 n per complex line equivalent */
+    int64_t step_index;         /* steps taken since creation */
+    double time;                /* simulation time */
+} shhd_info;
+
+/* Thread-local message of the last failure. */
+const char* shhd_last_error(void);
+
+/* Fill *cfg with the reference defaults (src/simulationinfo.h:35-98):
+ * grid 128^2, L = 2 pi, no dealiasing, dt 0.005, srk3/compressible, N = 0,
+ * noise off with seed 12345, kBT 1, chi 1; plus FP64, Philox noise, batch 1. */
+int shhd_config_default(shhd_config* cfg);
+
+/* Parse a reference input script (the hot-path commands of
+ * src/param_parser.cc:42-163,165-339,551-805) into *cfg, applying the same
+ * validation and error messages.  `set`, `measure`, `thermo`, `restart` and
+ * `run` lines are accepted and ignored.  Host only; needs no GPU. */
+int shhd_config_from_script(const char* script_text, shhd_config* cfg);
+
+/* Replaces constructing FluidSolver (src/fluid_solver.h:52-95): allocates
+ * the device state, workspaces and plans for cfg->batch members on the
+ * current CUDA device. */
+int shhd_engine_create(const shhd_config* cfg, shhd_engine** out);
+
+/* Releases all device memory and the stream. */
+void shhd_engine_destroy(shhd_engine* engine);
+
+int shhd_engine_info(const shhd_engine* engine, shhd_info* info);
+
+/* Upload one member's state (reference State layout, n_doubles =
+ * info.state_doubles).  Entries outside the active modes
+ * (src/spectral_mask.cc:45-52) must be zero, as every reference State is
+ * after its mask is applied; anything else is rejected. */
+int shhd_engine_set_state(shhd_engine* engine, int member, const double* state, size_t n_doubles);
+
+/* Download one member's state into the reference layout (inactive entries zero). */
+int shhd_engine_get_state(shhd_engine* engine, int member, double* state, size_t n_doubles);
+
+/* Replaces FluidSolver::step / TimeIntegrator::step (time_integrator.h:141)
+ * called nsteps times (project.h:134-139): enqueues nsteps steps of all
+ * members on the engine's stream and waits for them. */
+int shhd_engine_step(shhd_engine* engine, int nsteps);
+
+/* Same as shhd_engine_step without waiting; errors raised on the device are
+ * reported by the next shhd_engine_synchronize. */
+int shhd_engine_step_async(shhd_engine* engine, int nsteps);
+int shhd_engine_synchronize(shhd_engine* engine);
+
+/* For noise_source == SHHD_NOISE_EXTERNAL: the stochastic right-hand sides
+ * the next step uses, as the reference integrators hold them
+ * (stochastic_rhs_a_ / stochastic_rhs_b_, srk3_compressible.h:23-24; Euler uses
+ * sto_a only).  Reference layout; sto_b may be NULL for Euler. */
+int shhd_engine_set_external_noise(shhd_engine* engine, int member, const double* sto_a, const double* sto_b, size_t n_doubles);
+
+/* Deterministic right-hand side of the current state (rho_det, psi_det,
+ * j_det of src/fcalculator.cc:60-150) in the reference layout. */
+int shhd_engine_rhs(shhd_engine* engine, int member, double* det, size_t n_doubles);
+
+/* Step counter and time (project.h:136-137). */
+int shhd_engine_set_time(shhd_engine* engine, int64_t step_index, double time);
+
+/* CUDA stream the engine launches on (cudaStream_t as void*). */
+void* shhd_engine_stream(shhd_engine* engine);
+
+/* Device pointers of the current state of all members, in the engine's own
+ * active-mode layout [member][field][gx < active_nx/2][j < active_ny-1]
+ * (j = ky for 0 <= ky < active_ny/2, else ky + active_ny - 1), complex
+ * float or double per `precision`.  Valid until the next step call. */
+const void* shhd_engine_state_device(const shhd_engine* engine);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHHD_B200_H */

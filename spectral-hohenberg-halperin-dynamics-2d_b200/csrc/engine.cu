@@ -1,0 +1,823 @@
+// Host side of the step engine: plans, device buffers, launch sequence and
+// the C ABI declared in include/shhd_b200.h.
+//
+// One engine = one configuration (grid, mode, models) and `batch` members.
+// A step of all members is, per right-hand-side stage, one row_pass launch
+// and one col_forward launch (which also produces the next stage's column
+// inverse); each step call starts with one col_inverse launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/shhd_b200.h"
+#include "step_kernels.cuh"
+
+using namespace shhd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Failure : std::runtime_error {
+    int code;
+    Failure(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Failure(SHHD_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return SHHD_OK;
+    } catch (const Failure& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return SHHD_ENOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return SHHD_EINVAL;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FFT plans
+// ---------------------------------------------------------------------------
+FftPlan make_fft_plan(int n) {
+    FftPlan p{};
+    p.n = n;
+    int m = n;
+    std::vector<int> rad;
+    for (int r : {8, 4, 2}) while (m % r == 0) { rad.push_back(r); m /= r; }
+    while (m % 3 == 0) { rad.push_back(3); m /= 3; }
+    while (m % 5 == 0) { rad.push_back(5); m /= 5; }
+    if (m != 1)
+        throw Failure(SHHD_EUNSUPPORTED, "compute grid size " + std::to_string(n) + " has a prime factor other than 2, 3, 5");
+    if (static_cast<int>(rad.size()) > kMaxStages) throw Failure(SHHD_EUNSUPPORTED, "compute grid size too large");
+    p.nstages = static_cast<int>(rad.size());
+    int span = 1;
+    for (int s = 0; s < p.nstages; ++s) {
+        p.radix[s] = rad[s];
+        p.span[s] = span;
+        p.twstride[s] = n / (span * rad[s]);
+        p.div_nr[s] = make_fastdiv(static_cast<uint32_t>(n / rad[s]));
+        p.div_p[s] = make_fastdiv(static_cast<uint32_t>(span));
+        span *= rad[s];
+    }
+    p.tw_hi_count = (n + kTwLo - 1) / kTwLo;
+    return p;
+}
+
+// shared-memory swizzle mask: `slots` complex values make one bank wavefront
+// (16 for float2, 8 for double2) and `width` lines are interleaved; the mask
+// must keep sw() inside aligned blocks the line length is a multiple of.
+int swizzle_mask(int n, int slots, int width) {
+    int m = std::max(1, slots / std::max(1, width)) - 1;
+    while (m > 0 && n % (m + 1) != 0) m >>= 1;
+    return m;
+}
+
+template <typename T>
+std::vector<cplx<T>> twiddle_table(int n) {
+    const int hi = (n + kTwLo - 1) / kTwLo;
+    std::vector<cplx<T>> t(kTwLo + hi);
+    for (int j = 0; j < kTwLo; ++j) {
+        const double a = -2.0 * M_PI * static_cast<double>(j) / n;
+        t[j].x = static_cast<T>(std::cos(a));
+        t[j].y = static_cast<T>(std::sin(a));
+    }
+    for (int i = 0; i < hi; ++i) {
+        const double a = -2.0 * M_PI * static_cast<double>((static_cast<long>(i) * kTwLo) % n) / n;
+        t[kTwLo + i].x = static_cast<T>(std::cos(a));
+        t[kTwLo + i].y = static_cast<T>(std::sin(a));
+    }
+    return t;
+}
+
+}  // namespace
+
+namespace shhd_internal {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace shhd_internal
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+struct shhd_engine {
+    shhd_config cfg{};
+    StepPlan P{};
+    int fp32 = 0;
+    size_t csize = 16;            // bytes per complex element
+    cudaStream_t stream = nullptr;
+    int device = 0;
+
+    void* u = nullptr;
+    void* s1 = nullptr;
+    void* s2 = nullptr;
+    void* i1 = nullptr;
+    void* i2 = nullptr;
+    void* ext_a = nullptr;
+    void* ext_b = nullptr;
+    void* det = nullptr;
+    void* tw_x = nullptr;
+    void* tw_y = nullptr;
+    double* rho0_dev = nullptr;
+    int* err_dev = nullptr;
+    int* static_dev = nullptr;
+    int n_static = 0;
+
+    size_t state_elems = 0;       // complex per member
+    size_t i1_elems = 0, i2_elems = 0;
+    int npos = 16;
+    size_t smem_col = 0, smem_row = 0;
+    int n_evolved = 0;
+    bool need_rho0 = false;
+    std::vector<double> rho0_candidate;
+    std::vector<int> rho0_cached;
+    std::vector<double> rho0_value;
+    size_t device_bytes = 0;
+
+    int64_t step_index = 0;
+    double time = 0.0;
+
+    std::vector<double> host_stage;  // conversion scratch
+};
+
+namespace {
+
+void* dalloc(shhd_engine* e, size_t bytes) {
+    if (bytes == 0) return nullptr;
+    void* p = nullptr;
+    const cudaError_t rc = cudaMalloc(&p, bytes);
+    if (rc != cudaSuccess) {
+        cudaGetLastError();
+        throw Failure(SHHD_ENOMEM, "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(rc));
+    }
+    e->device_bytes += bytes;
+    return p;
+}
+
+void free_engine(shhd_engine* e) {
+    for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y,
+                    static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev)})
+        if (p) cudaFree(p);
+    if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+void validate_config(const shhd_config& c) {
+    if (c.active_nx <= 0 || c.active_ny <= 0) throw Failure(SHHD_EINVAL, "grid sizes must be positive");
+    if (c.active_nx % 2 != 0 || c.active_ny % 2 != 0) throw Failure(SHHD_EINVAL, "grid must be even.");
+    if (c.nx < c.active_nx || c.ny < c.active_ny) throw Failure(SHHD_EINVAL, "active grid cannot exceed compute grid.");
+    if (c.lx <= 0 || c.ly <= 0) throw Failure(SHHD_EINVAL, "domain lengths must be positive");
+    if (c.dt <= 0) throw Failure(SHHD_EINVAL, "timestep must be positive");
+    if (c.mode < 0 || c.mode > 2) throw Failure(SHHD_EINVAL, "unknown time_evolution mode");
+    if (c.integrator < 0 || c.integrator > 1) throw Failure(SHHD_EINVAL, "unknown time_evolution integrator");
+    if (c.num_order_parameters < 0 || c.num_order_parameters > SHHD_MAX_ORDER_PARAMETERS)
+        throw Failure(SHHD_EUNSUPPORTED, "order_parameters must be in [0, " + std::to_string(SHHD_MAX_ORDER_PARAMETERS) + "]");
+    if (c.eta < 0 || c.zeta < 0) throw Failure(SHHD_EINVAL, "transport coefficient requires nonnegative eta and zeta.");
+    if (c.cT < 0) throw Failure(SHHD_EINVAL, "thermodynamics requires nonnegative cT.");
+    for (int a = 0; a < c.num_order_parameters; ++a) {
+        if (c.mobility[a] < 0) throw Failure(SHHD_EINVAL, "transport coefficient requires nonnegative order parameter mobility.");
+        if (c.mu_u3[a] < 0) throw Failure(SHHD_EINVAL, "phi4 free energy requires nonnegative u coefficient.");
+    }
+    if (c.batch < 1) throw Failure(SHHD_EINVAL, "batch must be >= 1");
+    if (c.precision != SHHD_FP64 && c.precision != SHHD_FP32) throw Failure(SHHD_EINVAL, "unknown precision");
+    if (c.n_sine_forces < 0 || c.n_sine_forces > SHHD_MAX_FORCES || c.n_gradient_forces < 0 || c.n_gradient_forces > SHHD_MAX_FORCES)
+        throw Failure(SHHD_EINVAL, "too many forces");
+    const bool quiescent = c.mode == SHHD_QUIESCENT;
+    if (quiescent && (c.momentum_advection || c.order_parameter_advection))
+        throw Failure(SHHD_EINVAL, "quiescent time evolution cannot use nonlinear advection.");
+    if (quiescent && c.n_gradient_forces > 0) throw Failure(SHHD_EINVAL, "force/gradient cannot be used in quiescent mode.");
+    if (c.ny % 2 == 1 && c.ny > 1) {
+        // odd compute rows are handled (the last row pair holds one row)
+    }
+}
+
+void build_plan(shhd_engine* e) {
+    const shhd_config& c = e->cfg;
+    StepPlan& P = e->P;
+    std::memset(&P, 0, sizeof(P));
+    const int nop = c.num_order_parameters;
+    const bool comp = c.mode == SHHD_COMPRESSIBLE, incomp = c.mode == SHHD_INCOMPRESSIBLE, quiet = c.mode == SHHD_QUIESCENT;
+    P.nax = c.active_nx; P.nay = c.active_ny;
+    P.hx = c.active_nx / 2; P.kyn = c.active_ny - 1;
+    P.npx = c.nx; P.npy = c.ny;
+    P.kx_unit = 2.0 * M_PI / c.lx;
+    P.ky_unit = 2.0 * M_PI / c.ly;
+    P.inv_scale = 1.0 / (static_cast<double>(c.nx) * static_cast<double>(c.ny));
+    P.nfields = nop + 3; P.nop = nop; P.mode = c.mode; P.batch = c.batch;
+    const double grid_size = static_cast<double>(c.nx) * static_cast<double>(c.ny);
+    const double volume = c.lx * c.ly;
+    const int f_jx = nop + 1, f_jy = nop + 2;
+
+    // ---- physics flags ----
+    const bool has_phys_mu = c.free_energy == SHHD_FE_PHI4 && [&] {
+        for (int a = 0; a < nop; ++a) if (c.mu_u3[a] != 0.0) return true;
+        return false;
+    }();
+    const bool has_visc = c.eta != 0.0 || c.zeta != 0.0;
+    P.cT2 = c.cT * c.cT; P.eta = c.eta; P.zeta = c.zeta;
+    P.j_zero = quiet || !(P.cT2 != 0.0 || has_visc || c.momentum_advection);
+    P.incomp_visc = incomp && c.eta != 0.0 && !P.j_zero;
+    for (int a = 0; a < nop; ++a) {
+        P.mobility[a] = c.mobility[a];
+        P.mu_k0[a] = c.mu_k0[a]; P.mu_k2[a] = c.mu_k2[a]; P.mu_k4[a] = c.mu_k4[a];
+        P.mu_u3[a] = (c.free_energy == SHHD_FE_PHI4) ? c.mu_u3[a] : 0.0;
+        P.psi_zero[a] = (c.mobility[a] == 0.0 && !c.order_parameter_advection);
+        P.psi_linear[a] = c.mobility[a] != 0.0 && (c.mu_k0[a] != 0.0 || c.mu_k2[a] != 0.0 || c.mu_k4[a] != 0.0);
+    }
+    bool any_grad_incomp = false;
+    for (int g = 0; g < c.n_gradient_forces; ++g) {
+        const shhd_gradient_force& f = c.gradient_forces[g];
+        if (f.component < 0 || f.component >= nop) throw Failure(SHHD_EINVAL, "force/gradient component out of range");
+        if (P.psi_zero[f.component]) continue;
+        if (f.direction == 0) P.grad_ax[f.component] += -f.amplitude;
+        else P.grad_ay[f.component] += -f.amplitude;
+        if (incomp) { P.grad_incomp[f.component] = 1; any_grad_incomp = true; }
+    }
+    // sine sources (fcalculator.cc:702-774)
+    for (int s = 0; s < c.n_sine_forces; ++s) {
+        const shhd_sine_force& f = c.sine_forces[s];
+        int field;
+        if (f.target == 0) {
+            if (quiet) continue;
+            field = f.component == 0 ? f_jx : f_jy;
+        } else {
+            if (f.component < 0 || f.component >= nop) throw Failure(SHHD_EINVAL, "force/sine component out of range");
+            field = 1 + f.component;
+        }
+        const double im = -0.5 * f.amplitude * grid_size;
+        const int gx = f.axis == 0 ? f.nk : 0;
+        const int ky = f.axis == 0 ? 0 : f.nk;
+        auto add = [&](int gxx, int kyy, double re_, double im_) {
+            if (gxx >= P.hx || std::abs(kyy) >= c.active_ny / 2) return;  // only active modes receive the source
+            if (P.n_sine >= kMaxSine) throw Failure(SHHD_EUNSUPPORTED, "too many sine sources");
+            SineSrc& d = P.sine[P.n_sine++];
+            d.field = field; d.gx = gxx; d.ky = kyy; d.re = re_; d.im = im_;
+        };
+        add(gx, ky, 0.0, im);
+        if (f.axis == 1) add(0, -f.nk, 0.0, -im);
+    }
+
+    // ---- outputs and groups ----
+    auto add_out = [&](int kind, int arg) {
+        if (P.n_out >= kMaxOut) throw Failure(SHHD_EUNSUPPORTED, "too many product fields");
+        P.out_kind[P.n_out] = kind;
+        P.out_arg[P.n_out] = arg;
+        return P.n_out++;
+    };
+    auto add_group_out = [&](int g, int o) {
+        if (P.group_nout[g] >= kMaxGroupOut) throw Failure(SHHD_EUNSUPPORTED, "too many products in one group");
+        P.group_out[g][P.group_nout[g]++] = o;
+    };
+    bool need[kMaxFields] = {false};
+    bool need_v = false;
+    for (int a = 0; a < nop; ++a) {
+        const int g = P.n_groups++;
+        P.group_kind[g] = GROUP_PSI;
+        P.group_alpha[g] = a;
+        if (P.psi_zero[a]) continue;
+        if (c.mobility[a] != 0.0 && has_phys_mu && P.mu_u3[a] != 0.0) { add_group_out(g, add_out(OUT_MU, a)); need[1 + a] = true; }
+        if (c.order_parameter_advection) {
+            add_group_out(g, add_out(OUT_PSIVX, a));
+            add_group_out(g, add_out(OUT_PSIVY, a));
+            need[1 + a] = true;
+            need_v = true;
+        }
+        if (comp && (P.grad_ax[a] != 0.0 || P.grad_ay[a] != 0.0 || [&] {
+                for (int q = 0; q < c.n_gradient_forces; ++q) if (c.gradient_forces[q].component == a) return true;
+                return false;
+            }())) {
+            add_group_out(g, add_out(OUT_GRAD, a));
+            need_v = true;
+        }
+    }
+    if (!quiet) {
+        const int g = P.n_groups++;
+        P.group_kind[g] = GROUP_MOMENTUM;
+        P.group_alpha[g] = 0;
+        if (!P.j_zero) {
+            if (comp && has_visc) {
+                add_group_out(g, add_out(OUT_VX, 0));
+                add_group_out(g, add_out(OUT_VY, 0));
+                need_v = true;
+            }
+            if (c.momentum_advection) {
+                add_group_out(g, add_out(OUT_PXX, 0));
+                add_group_out(g, add_out(OUT_PXY, 0));
+                add_group_out(g, add_out(OUT_PYY, 0));
+                need_v = true;
+            }
+        }
+    }
+    if (need_v) { need[f_jx] = need[f_jy] = true; if (comp) need[0] = true; }
+    P.need_v = need_v ? 1 : 0;
+    for (int f = 0; f < kMaxFields; ++f) P.in_slot[f] = -1;
+    // slot order follows the reference's pack order: psi..., rho, jx, jy
+    for (int a = 0; a < nop; ++a) if (need[1 + a]) { P.in_slot[1 + a] = P.n_in; P.in_field[P.n_in++] = 1 + a; }
+    if (need[0]) { P.in_slot[0] = P.n_in; P.in_field[P.n_in++] = 0; }
+    if (need[f_jx]) { P.in_slot[f_jx] = P.n_in; P.in_field[P.n_in++] = f_jx; }
+    if (need[f_jy]) { P.in_slot[f_jy] = P.n_in; P.in_field[P.n_in++] = f_jy; }
+
+    e->n_evolved = comp ? nop + 3 : (incomp ? nop + 2 : nop);
+    e->need_rho0 = incomp && (need_v || P.incomp_visc || any_grad_incomp);
+
+    // ---- noise ----
+    const bool noise_psi_on = c.noise_order_parameter && nop > 0;
+    const double kbt_psi = c.kBT * c.chi;
+    for (int a = 0; a < nop; ++a) {
+        P.noise_psi[a] = noise_psi_on && c.mobility[a] != 0.0 && kbt_psi != 0.0;
+        const double pref = 2.0 * kbt_psi * grid_size * grid_size / volume;
+        P.psi_sig2[a] = 0.5 * pref * c.mobility[a];
+    }
+    P.noise_j = c.noise_momentum && !quiet && c.kBT != 0.0 && has_visc;
+    {
+        const double pref = 2.0 * c.kBT * grid_size * grid_size / volume;
+        P.j_s = std::sqrt(0.5 * pref);
+        P.sqrt_eta = std::sqrt(c.eta);
+        P.sqrt_zeta = std::sqrt(c.zeta);
+    }
+    P.seed = static_cast<uint32_t>(c.noise_seed);
+    P.member_offset = static_cast<uint32_t>(c.member_offset);
+    P.external_noise = c.noise_source == SHHD_NOISE_EXTERNAL;
+
+    // ---- transforms and launch shapes ----
+    P.fy = make_fft_plan(c.ny);
+    P.fx = make_fft_plan(c.nx);
+    const int cs = static_cast<int>(e->csize);
+    // column tile width: largest power of two <= 8 dividing Hx whose ping-pong
+    // tile pair fits ~100 KB (two CTAs per SM) and whose active positions fit
+    // 16 slots per thread.
+    const size_t smem_cap = 227 * 1024;
+    const size_t col_target = 100 * 1024;
+    auto col_bytes = [&](int w) { return static_cast<size_t>(kTwLo + P.fy.tw_hi_count + 2L * w * c.ny) * cs; };
+    // register budget of the epilogue: <= 8 (FP32) / 4 (FP64) positions per thread when the grid allows
+    const long pos_cap = (e->fp32 ? 8L : 4L) * kThreads;
+    int W = 8;
+    while (W > 1 && (P.hx % W != 0 || col_bytes(W) > col_target || static_cast<long>(W) * P.kyn > pos_cap)) W /= 2;
+    if (static_cast<long>(W) * P.kyn > 16L * kThreads || col_bytes(W) > smem_cap)
+        throw Failure(SHHD_EUNSUPPORTED, "compute grid " + std::to_string(c.ny) + " too large for the column kernels");
+    P.W = W;
+    P.ntiles = P.hx / W;
+    P.fy.swz = swizzle_mask(c.ny, e->fp32 ? 16 : 8, W);
+    P.fx.swz = swizzle_mask(c.nx, e->fp32 ? 16 : 8, 1);
+    const long posn = static_cast<long>(W) * P.kyn;
+    e->npos = posn <= 4L * kThreads ? 4 : (posn <= 8L * kThreads ? 8 : 16);
+    e->smem_col = col_bytes(W);
+    // row pass: n_in physical lines + lb product lines + lb ping-pong lines
+    const size_t line_bytes = static_cast<size_t>(c.nx) * cs;
+    const size_t tw_bytes = static_cast<size_t>(kTwLo + P.fx.tw_hi_count) * cs;
+    auto row_bytes = [&](int lb) { return tw_bytes + (P.n_in + 2 * lb) * line_bytes; };
+    int lb = 4;
+    while (lb > 1 && row_bytes(lb) > 113 * 1024) lb /= 2;
+    if (row_bytes(lb) > smem_cap) throw Failure(SHHD_EUNSUPPORTED, "row pass does not fit shared memory at this grid and precision");
+    P.row_lb = lb;
+    P.row_nb = lb;
+    e->smem_row = row_bytes(lb);
+    P.npos = e->npos;
+    P.div_w = make_fastdiv(W);
+    P.div_kyn = make_fastdiv(P.kyn);
+    P.div_npy = make_fastdiv(c.ny);
+    P.div_hx = make_fastdiv(P.hx);
+
+    e->state_elems = static_cast<size_t>(P.nfields) * P.hx * P.kyn;
+    e->i1_elems = static_cast<size_t>(P.n_in) * P.hx * c.ny;
+    e->i2_elems = static_cast<size_t>(P.n_out) * P.hx * c.ny;
+}
+
+// kernel dispatch -------------------------------------------------------------
+template <typename T>
+void set_smem_attrs(shhd_engine* e) {
+    auto setattr = [](const void* fn, size_t bytes) {
+        check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)), "cudaFuncSetAttribute");
+    };
+    setattr(reinterpret_cast<const void*>(col_inverse_kernel<T>), e->smem_col);
+    if (e->npos == 4) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 4>), e->smem_col);
+    else if (e->npos == 8) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 8>), e->smem_col);
+    else setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 16>), e->smem_col);
+    setattr(reinterpret_cast<const void*>(row_pass_kernel<T>), e->smem_row);
+}
+
+template <typename T>
+void launch_col_inverse(shhd_engine* e, const void* state) {
+    const StepPlan& P = e->P;
+    if (P.n_in == 0) return;
+    dim3 grid(P.ntiles, P.n_in, P.batch);
+    auto* st = static_cast<const cplx<T>*>(state);
+    auto* i1 = static_cast<cplx<T>*>(e->i1);
+    auto* tw = static_cast<const cplx<T>*>(e->tw_y);
+    col_inverse_kernel<T><<<grid, kThreads, e->smem_col, e->stream>>>(P, st, i1, tw);
+    check_cuda(cudaGetLastError(), "col_inverse launch");
+}
+
+template <typename T>
+void launch_row(shhd_engine* e) {
+    const StepPlan& P = e->P;
+    if (P.n_out == 0) return;
+    dim3 grid((P.npy + 1) / 2, P.batch);
+    row_pass_kernel<T><<<grid, kThreads, e->smem_row, e->stream>>>(P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2),
+                                                                        static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev, e->err_dev);
+    check_cuda(cudaGetLastError(), "row_pass launch");
+}
+
+template <typename T>
+void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
+    const StepPlan& P = e->P;
+    if (P.n_groups == 0) return;
+    dim3 grid(P.ntiles, P.n_groups, P.batch);
+    auto* tw = static_cast<const cplx<T>*>(e->tw_y);
+    if (e->npos == 4) col_forward_kernel<T, 4><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+    else if (e->npos == 8) col_forward_kernel<T, 8><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+    else col_forward_kernel<T, 16><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+    check_cuda(cudaGetLastError(), "col_forward launch");
+}
+
+void ensure_rho0(shhd_engine* e) {
+    if (!e->need_rho0) return;
+    bool changed = false;
+    for (int m = 0; m < e->cfg.batch; ++m) {
+        if (e->rho0_cached[m]) continue;
+        const double r = e->rho0_candidate[m];
+        if (r == 0.0) throw Failure(SHHD_EINVAL, "reference density must be nonzero.");
+        e->rho0_value[m] = r;
+        e->rho0_cached[m] = 1;
+        changed = true;
+    }
+    if (changed)
+        check_cuda(cudaMemcpyAsync(e->rho0_dev, e->rho0_value.data(), sizeof(double) * e->cfg.batch, cudaMemcpyHostToDevice, e->stream),
+                   "rho0 upload");
+}
+
+template <typename T>
+void prepare_static(shhd_engine* e) {
+    if (e->n_static == 0) return;
+    dim3 grid(e->n_static, e->P.batch);
+    prepare_static_kernel<T><<<grid, kThreads, 0, e->stream>>>(e->P, e->static_dev, static_cast<cplx<T>*>(e->u), static_cast<cplx<T>*>(e->s1),
+                                                             static_cast<cplx<T>*>(e->s2));
+    check_cuda(cudaGetLastError(), "prepare_static launch");
+}
+
+constexpr double kSqrt2 = 1.41421356237309504880;
+constexpr double kSqrt3 = 1.73205080756887729352;
+// time_integrator_srk3_compressible.h:10-21
+const double kBeta[3] = {(2.0 * kSqrt2 + kSqrt3) / 5.0, (-4.0 * kSqrt2 + 3.0 * kSqrt3) / 5.0, (kSqrt2 - 2.0 * kSqrt3) / 10.0};
+const double kWb[3] = {0.0, 3.0 / 4.0, 1.0 / 3.0};
+const double kWc[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
+
+template <typename T>
+StageArgs<T> stage_args(shhd_engine* e, const void* cur, const void* base, void* next, double wb, double wc, double beta, int srk3, int fused) {
+    StageArgs<T> A{};
+    A.cur = static_cast<const cplx<T>*>(cur);
+    A.base = static_cast<const cplx<T>*>(base);
+    A.next = static_cast<cplx<T>*>(next);
+    A.i2 = static_cast<const cplx<T>*>(e->i2);
+    A.i1_next = static_cast<cplx<T>*>(e->i1);
+    A.ext_a = static_cast<const cplx<T>*>(e->ext_a);
+    A.ext_b = static_cast<const cplx<T>*>(e->ext_b);
+    A.rho0 = e->rho0_dev;
+    A.err = e->err_dev;
+    A.wb = wb; A.wc = wc; A.beta = beta;
+    A.dt = e->cfg.dt;
+    A.sdt = std::sqrt(e->cfg.dt);
+    A.step = static_cast<uint64_t>(e->step_index);
+    A.srk3 = srk3;
+    A.fused_inverse = fused;
+    A.det_mode = 0;
+    return A;
+}
+
+template <typename T>
+void enqueue_steps(shhd_engine* e, int nsteps) {
+    ensure_rho0(e);
+    prepare_static<T>(e);
+    launch_col_inverse<T>(e, e->u);
+    const bool srk3 = e->cfg.integrator == SHHD_SRK3;
+    for (int s = 0; s < nsteps; ++s) {
+        const bool last_step = (s + 1 == nsteps);
+        if (srk3) {
+            void* cur[3] = {e->u, e->s1, e->s2};
+            void* nxt[3] = {e->s1, e->s2, e->u};
+            for (int k = 0; k < 3; ++k) {
+                launch_row<T>(e);
+                const int fused = !(last_step && k == 2);
+                launch_col_forward<T>(e, stage_args<T>(e, cur[k], e->u, nxt[k], kWb[k], kWc[k], kBeta[k], 1, fused));
+            }
+        } else {
+            launch_row<T>(e);
+            launch_col_forward<T>(e, stage_args<T>(e, e->u, e->u, e->s1, 0.0, 1.0, 0.0, 0, last_step ? 0 : 1));
+            std::swap(e->u, e->s1);
+        }
+        e->step_index += 1;
+        e->time += e->cfg.dt;
+    }
+}
+
+void enqueue(shhd_engine* e, int nsteps) {
+    if (nsteps < 0) throw Failure(SHHD_EINVAL, "nsteps must be nonnegative");
+    if (nsteps == 0) return;
+    if (e->cfg.noise_source == SHHD_NOISE_EXTERNAL && nsteps != 1)
+        throw Failure(SHHD_EINVAL, "external noise supplies one step at a time: call step with nsteps = 1");
+    check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+    if (e->fp32) enqueue_steps<float>(e, nsteps);
+    else enqueue_steps<double>(e, nsteps);
+}
+
+void sync_and_check(shhd_engine* e) {
+    check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+    int err = 0;
+    check_cuda(cudaMemcpy(&err, e->err_dev, sizeof(int), cudaMemcpyDeviceToHost), "error flag read");
+    if (err != 0) {
+        check_cuda(cudaMemset(e->err_dev, 0, sizeof(int)), "error flag reset");
+        if (err & ERR_ZERO_DENSITY) throw Failure(SHHD_ENUMERIC, "compressible velocity encountered zero density.");
+    }
+}
+
+// reference layout <-> active layout (host side) -----------------------------
+size_t ref_doubles(const shhd_engine* e) {
+    return static_cast<size_t>(e->P.nfields) * (e->cfg.nx / 2 + 1) * e->cfg.ny * 2;
+}
+
+template <typename T>
+void upload_ref(shhd_engine* e, const double* ref, void* dst_base, int member, bool check_inactive) {
+    const StepPlan& P = e->P;
+    const int hxr = e->cfg.nx / 2 + 1, ny = e->cfg.ny;
+    std::vector<cplx<T>> act(e->state_elems);
+    for (int f = 0; f < P.nfields; ++f) {
+        const double* rf = ref + static_cast<size_t>(f) * hxr * ny * 2;
+        if (check_inactive) {
+            for (int gy = 0; gy < ny; ++gy) {
+                const int sgy = gy <= ny / 2 ? gy : gy - ny;
+                const bool row_active = std::abs(sgy) < P.nay / 2;
+                for (int gx = 0; gx < hxr; ++gx) {
+                    if (row_active && gx < P.hx) continue;
+                    const double* v = rf + (static_cast<size_t>(gy) * hxr + gx) * 2;
+                    if (v[0] != 0.0 || v[1] != 0.0)
+                        throw Failure(SHHD_EINVAL, "state has a nonzero entry outside the active modes (field " + std::to_string(f) + ", gx " +
+                                                       std::to_string(gx) + ", gy " + std::to_string(gy) + ")");
+                }
+            }
+        }
+        for (int gx = 0; gx < P.hx; ++gx)
+            for (int j = 0; j < P.kyn; ++j) {
+                const int ky = j < P.nay / 2 ? j : j - P.kyn;
+                const int gy = ky >= 0 ? ky : ky + ny;
+                const double* v = rf + (static_cast<size_t>(gy) * hxr + gx) * 2;
+                cplx<T>& o = act[(static_cast<size_t>(f) * P.hx + gx) * P.kyn + j];
+                o.x = static_cast<T>(v[0]);
+                o.y = static_cast<T>(v[1]);
+            }
+    }
+    char* dst = static_cast<char*>(dst_base) + static_cast<size_t>(member) * e->state_elems * sizeof(cplx<T>);
+    check_cuda(cudaMemcpyAsync(dst, act.data(), act.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice, e->stream), "state upload");
+    check_cuda(cudaStreamSynchronize(e->stream), "state upload sync");
+}
+
+template <typename T>
+void download_ref(shhd_engine* e, const void* src_base, int member, double* ref) {
+    const StepPlan& P = e->P;
+    const int hxr = e->cfg.nx / 2 + 1, ny = e->cfg.ny;
+    std::vector<cplx<T>> act(e->state_elems);
+    const char* src = static_cast<const char*>(src_base) + static_cast<size_t>(member) * e->state_elems * sizeof(cplx<T>);
+    check_cuda(cudaMemcpyAsync(act.data(), src, act.size() * sizeof(cplx<T>), cudaMemcpyDeviceToHost, e->stream), "state download");
+    check_cuda(cudaStreamSynchronize(e->stream), "state download sync");
+    std::memset(ref, 0, ref_doubles(e) * sizeof(double));
+    for (int f = 0; f < P.nfields; ++f) {
+        double* rf = ref + static_cast<size_t>(f) * hxr * ny * 2;
+        for (int gx = 0; gx < P.hx; ++gx)
+            for (int j = 0; j < P.kyn; ++j) {
+                const int ky = j < P.nay / 2 ? j : j - P.kyn;
+                const int gy = ky >= 0 ? ky : ky + ny;
+                const cplx<T>& v = act[(static_cast<size_t>(f) * P.hx + gx) * P.kyn + j];
+                rf[(static_cast<size_t>(gy) * hxr + gx) * 2] = static_cast<double>(v.x);
+                rf[(static_cast<size_t>(gy) * hxr + gx) * 2 + 1] = static_cast<double>(v.y);
+            }
+    }
+}
+
+template <typename T>
+void run_rhs(shhd_engine* e, int member, double* out) {
+    const size_t bytes = e->state_elems * e->cfg.batch * sizeof(cplx<T>);
+    if (!e->det) e->det = dalloc(e, bytes);
+    ensure_rho0(e);
+    check_cuda(cudaMemsetAsync(e->det, 0, bytes, e->stream), "det clear");
+    launch_col_inverse<T>(e, e->u);
+    launch_row<T>(e);
+    StageArgs<T> A = stage_args<T>(e, e->u, e->u, e->det, 0.0, 1.0, 0.0, 0, 0);
+    A.det_mode = 1;
+    launch_col_forward<T>(e, A);
+    sync_and_check(e);
+    download_ref<T>(e, e->det, member, out);
+}
+
+template <typename T>
+void init_device(shhd_engine* e) {
+    const size_t cs = sizeof(cplx<T>);
+    const size_t B = e->cfg.batch;
+    e->u = dalloc(e, e->state_elems * B * cs);
+    e->s1 = dalloc(e, e->state_elems * B * cs);
+    e->s2 = dalloc(e, e->state_elems * B * cs);
+    check_cuda(cudaMemsetAsync(e->u, 0, e->state_elems * B * cs, e->stream), "memset");
+    check_cuda(cudaMemsetAsync(e->s1, 0, e->state_elems * B * cs, e->stream), "memset");
+    check_cuda(cudaMemsetAsync(e->s2, 0, e->state_elems * B * cs, e->stream), "memset");
+    e->i1 = dalloc(e, std::max<size_t>(1, e->i1_elems) * B * cs);
+    e->i2 = dalloc(e, std::max<size_t>(1, e->i2_elems) * B * cs);
+    if (e->cfg.noise_source == SHHD_NOISE_EXTERNAL) {
+        e->ext_a = dalloc(e, e->state_elems * B * cs);
+        e->ext_b = dalloc(e, e->state_elems * B * cs);
+        check_cuda(cudaMemsetAsync(e->ext_a, 0, e->state_elems * B * cs, e->stream), "memset");
+        check_cuda(cudaMemsetAsync(e->ext_b, 0, e->state_elems * B * cs, e->stream), "memset");
+    }
+    const auto twx = twiddle_table<T>(e->cfg.nx);
+    const auto twy = twiddle_table<T>(e->cfg.ny);
+    e->tw_x = dalloc(e, twx.size() * cs);
+    e->tw_y = dalloc(e, twy.size() * cs);
+    check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    e->rho0_dev = static_cast<double*>(dalloc(e, sizeof(double) * B));
+    check_cuda(cudaMemsetAsync(e->rho0_dev, 0, sizeof(double) * B, e->stream), "memset");
+    e->err_dev = static_cast<int*>(dalloc(e, sizeof(int)));
+    check_cuda(cudaMemsetAsync(e->err_dev, 0, sizeof(int), e->stream), "memset");
+    // fields the integrator does not evolve
+    std::vector<int> st;
+    const int nop = e->cfg.num_order_parameters;
+    if (e->cfg.mode == SHHD_INCOMPRESSIBLE) st = {0};
+    if (e->cfg.mode == SHHD_QUIESCENT) st = {0, nop + 1, nop + 2};
+    e->n_static = static_cast<int>(st.size());
+    if (!st.empty()) {
+        e->static_dev = static_cast<int*>(dalloc(e, sizeof(int) * st.size()));
+        check_cuda(cudaMemcpyAsync(e->static_dev, st.data(), sizeof(int) * st.size(), cudaMemcpyHostToDevice, e->stream), "static fields upload");
+    }
+    set_smem_attrs<T>(e);
+    check_cuda(cudaStreamSynchronize(e->stream), "init sync");
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* shhd_last_error(void) { return g_last_error.c_str(); }
+
+int shhd_engine_create(const shhd_config* cfg, shhd_engine** out) {
+    if (!cfg || !out) {
+        g_last_error = "null argument";
+        return SHHD_EINVAL;
+    }
+    *out = nullptr;
+    shhd_engine* e = new shhd_engine();
+    const int rc = guarded([&] {
+        e->cfg = *cfg;
+        validate_config(e->cfg);
+        e->fp32 = cfg->precision == SHHD_FP32;
+        e->csize = e->fp32 ? sizeof(float2) : sizeof(double2);
+        build_plan(e);
+        check_cuda(cudaGetDevice(&e->device), "cudaGetDevice");
+        check_cuda(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        e->rho0_candidate.assign(cfg->batch, 0.0);
+        e->rho0_cached.assign(cfg->batch, 0);
+        e->rho0_value.assign(cfg->batch, 0.0);
+        if (e->fp32) init_device<float>(e);
+        else init_device<double>(e);
+    });
+    if (rc != SHHD_OK) {
+        free_engine(e);
+        delete e;
+        return rc;
+    }
+    *out = e;
+    return SHHD_OK;
+}
+
+void shhd_engine_destroy(shhd_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_engine(e);
+    delete e;
+}
+
+int shhd_engine_info(const shhd_engine* e, shhd_info* info) {
+    if (!e || !info) { g_last_error = "null argument"; return SHHD_EINVAL; }
+    const StepPlan& P = e->P;
+    std::memset(info, 0, sizeof(*info));
+    info->nfields = P.nfields;
+    info->state_doubles = ref_doubles(e);
+    info->active_modes = static_cast<size_t>(P.hx) * P.kyn;
+    info->n_inverse = P.n_in;
+    info->n_forward = P.n_out;
+    info->n_evolved = e->n_evolved;
+    info->device_bytes = e->device_bytes;
+    const double s = static_cast<double>(e->csize);
+    const double I = static_cast<double>(P.hx) * P.npy;
+    const double Ma = static_cast<double>(P.hx) * P.kyn;
+    const double nev = e->n_evolved;
+    // steady-state fused stage: row reads F_in*I, writes F_out*I; column forward reads F_out*I,
+    // current (and base on stages 2, 3 of SRK3), writes the evolved fields and F_in*I
+    const double base_reads = e->cfg.integrator == SHHD_SRK3 ? nev * 2.0 / 3.0 : 0.0;
+    info->bytes_per_stage = s * P.batch * (2.0 * P.n_in * I + 2.0 * P.n_out * I + (nev + base_reads + nev) * Ma);
+    auto flops = [](double n) { return 5.0 * n * std::log2(n); };
+    info->fft_flops_per_stage = P.batch * ((P.n_in + P.n_out) * (P.hx * flops(P.npy) + 0.5 * P.npy * flops(P.npx)));
+    info->step_index = e->step_index;
+    info->time = e->time;
+    return SHHD_OK;
+}
+
+int shhd_engine_set_state(shhd_engine* e, int member, const double* state, size_t n) {
+    return guarded([&] {
+        if (!e || !state) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (n != ref_doubles(e)) throw Failure(SHHD_EINVAL, "state size mismatch: expected " + std::to_string(ref_doubles(e)) + " doubles");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) upload_ref<float>(e, state, e->u, member, true);
+        else upload_ref<double>(e, state, e->u, member, true);
+        e->rho0_candidate[member] = state[0] / (static_cast<double>(e->cfg.nx) * e->cfg.ny);
+    });
+}
+
+int shhd_engine_get_state(shhd_engine* e, int member, double* state, size_t n) {
+    return guarded([&] {
+        if (!e || !state) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (n != ref_doubles(e)) throw Failure(SHHD_EINVAL, "state size mismatch");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) download_ref<float>(e, e->u, member, state);
+        else download_ref<double>(e, e->u, member, state);
+    });
+}
+
+int shhd_engine_set_external_noise(shhd_engine* e, int member, const double* sto_a, const double* sto_b, size_t n) {
+    return guarded([&] {
+        if (!e || !sto_a) throw Failure(SHHD_EINVAL, "null argument");
+        if (e->cfg.noise_source != SHHD_NOISE_EXTERNAL) throw Failure(SHHD_EINVAL, "engine was created with Philox noise");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (n != ref_doubles(e)) throw Failure(SHHD_EINVAL, "noise size mismatch");
+        if (e->cfg.integrator == SHHD_SRK3 && !sto_b) throw Failure(SHHD_EINVAL, "srk3 needs both noise draws");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) {
+            upload_ref<float>(e, sto_a, e->ext_a, member, false);
+            if (sto_b) upload_ref<float>(e, sto_b, e->ext_b, member, false);
+        } else {
+            upload_ref<double>(e, sto_a, e->ext_a, member, false);
+            if (sto_b) upload_ref<double>(e, sto_b, e->ext_b, member, false);
+        }
+    });
+}
+
+int shhd_engine_step(shhd_engine* e, int nsteps) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        enqueue(e, nsteps);
+        sync_and_check(e);
+    });
+}
+
+int shhd_engine_step_async(shhd_engine* e, int nsteps) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        enqueue(e, nsteps);
+    });
+}
+
+int shhd_engine_synchronize(shhd_engine* e) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        sync_and_check(e);
+    });
+}
+
+int shhd_engine_rhs(shhd_engine* e, int member, double* det, size_t n) {
+    return guarded([&] {
+        if (!e || !det) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (n != ref_doubles(e)) throw Failure(SHHD_EINVAL, "size mismatch");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) run_rhs<float>(e, member, det);
+        else run_rhs<double>(e, member, det);
+    });
+}
+
+int shhd_engine_set_time(shhd_engine* e, int64_t step_index, double time) {
+    if (!e) { g_last_error = "null engine"; return SHHD_EINVAL; }
+    e->step_index = step_index;
+    e->time = time;
+    return SHHD_OK;
+}
+
+void* shhd_engine_stream(shhd_engine* e) { return e ? static_cast<void*>(e->stream) : nullptr; }
+
+const void* shhd_engine_state_device(const shhd_engine* e) { return e ? e->u : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,624 @@
+// The three fused kernels of one right-hand-side stage.
+//
+// Notation: Na = active grid, Np = compute (padded) grid, Hx = Na_x/2 active
+// kx columns, Ky = Na_y - 1 active ky values.  Memory (per member):
+//   state  [field][gx < Hx][j < Ky]          complex, j = ky (ky >= 0) or ky + Ky
+//   I1/I2  [slot][tile][y < Np_y][w < W]     complex, gx = tile*W + w
+// I1 holds the y-inverse of the transformed state fields ("x-spectral,
+// y-physical"), I2 the x-forward of the product fields.  Tiles make the
+// column passes read and write whole contiguous blocks.
+//
+//   col_inverse   state -> I1          (first stage of a step call only)
+//   row_pass      I1 -> C2R -> products (j v, psi v, mu, v) -> R2C -> I2
+//   col_forward   I2 -> y-forward -> RHS epilogue -> stage update -> state
+//                 [-> y-inverse of the new state -> I1 for the next stage]
+//
+// The 3/2 padding is never stored: column loads zero-fill |ky| >= Na/2 and
+// row loads zero-fill kx >= Na/2; the forward transforms keep only the active
+// modes.  References to the solver this replaces are given per term.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_core.cuh"
+#include "philox.cuh"
+
+namespace shhd {
+
+constexpr int kThreads = 256;
+constexpr int kMaxOp = 8;
+constexpr int kMaxFields = kMaxOp + 3;
+constexpr int kMaxIn = kMaxOp + 3;
+constexpr int kMaxOut = 4 * kMaxOp + 5;
+constexpr int kMaxGroupOut = 8;
+constexpr int kMaxGroups = kMaxOp + 1;
+constexpr int kMaxSine = 8;
+
+enum OutKind : int { OUT_MU = 0, OUT_PSIVX, OUT_PSIVY, OUT_GRAD, OUT_VX, OUT_VY, OUT_PXX, OUT_PXY, OUT_PYY };
+enum GroupKind : int { GROUP_PSI = 0, GROUP_MOMENTUM = 1 };
+enum ErrBits : int { ERR_ZERO_DENSITY = 1 };
+
+struct SineSrc {
+    int field;     // state field index
+    int gx, ky;    // active mode receiving the source
+    double re, im; // source value
+};
+
+struct StepPlan {
+    // geometry
+    int nax, nay, hx, kyn, npx, npy, W, ntiles;
+    double kx_unit, ky_unit, inv_scale;
+    int nfields, nop, mode, batch;
+    // C2R inputs
+    int n_in;
+    int in_field[kMaxIn];
+    int in_slot[kMaxFields];
+    int need_v;
+    // R2C outputs
+    int n_out;
+    int out_kind[kMaxOut];
+    int out_arg[kMaxOut];
+    // column-forward groups
+    int n_groups;
+    int group_kind[kMaxGroups];
+    int group_alpha[kMaxGroups];
+    int group_nout[kMaxGroups];
+    int group_out[kMaxGroups][kMaxGroupOut];
+    // physics
+    double mobility[kMaxOp], mu_k0[kMaxOp], mu_k2[kMaxOp], mu_k4[kMaxOp], mu_u3[kMaxOp];
+    int psi_zero[kMaxOp];          // psi_det early return (fcalculator.cc:93-95)
+    int psi_linear[kMaxOp];        // linear mu term present (fcalculator.cc:158-160)
+    double grad_ax[kMaxOp], grad_ay[kMaxOp];  // summed -A per direction (gradient forces)
+    int grad_incomp[kMaxOp];
+    double cT2, eta, zeta;
+    int j_zero;                    // j_det early return (fcalculator.cc:131-133)
+    int incomp_visc;               // add_incompressible_viscous_term with eta != 0
+    int n_sine;
+    SineSrc sine[kMaxSine];
+    // noise
+    int noise_psi[kMaxOp];
+    double psi_sig2[kMaxOp];       // 0.5 * prefactor * M  (sigma^2 / k^2)
+    int noise_j;
+    double j_s, sqrt_eta, sqrt_zeta;
+    uint32_t seed, member_offset;
+    int external_noise;
+    // transforms
+    FftPlan fy, fx;
+    FastDiv div_w, div_kyn, div_npy, div_hx;
+    int row_lb;                    // max lines per row transform call
+    int row_nb;                    // work lines for outputs
+    int npos;                      // position slots per thread in col_forward
+};
+
+template <typename T>
+struct StageArgs {
+    const cplx<T>* cur;
+    const cplx<T>* base;
+    cplx<T>* next;
+    const cplx<T>* i2;
+    cplx<T>* i1_next;
+    const cplx<T>* ext_a;
+    const cplx<T>* ext_b;
+    const double* rho0;            // per member
+    int* err;
+    double wb, wc, dt, sdt, beta;
+    uint64_t step;
+    int srk3;                      // draw b exists
+    int fused_inverse;
+    int det_mode;                  // write det instead of the stage update
+};
+
+__device__ __forceinline__ int ky_of_j(int j, int nay) { return j < nay / 2 ? j : j - (nay - 1); }
+
+// ---------------------------------------------------------------------------
+// column inverse: state -> I1   (grid: tiles x n_in x batch)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kThreads) col_inverse_kernel(const StepPlan P, const cplx<T>* __restrict__ state,
+                                                               cplx<T>* __restrict__ i1, const cplx<T>* __restrict__ tw) {
+    using C = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s_lo = reinterpret_cast<C*>(smem_raw);
+    C* s_hi = s_lo + kTwLo;
+    C* buf = s_hi + P.fy.tw_hi_count;
+    C* scr = buf + P.W * P.npy;
+
+    const int tile = blockIdx.x, slot = blockIdx.y, b = blockIdx.z;
+    const int W = P.W, npy = P.npy, kyn = P.kyn, half = P.nay / 2;
+    const uint32_t mask = P.fy.swz;
+    const int field = P.in_field[slot];
+    load_twiddles(s_lo, s_hi, tw, P.fy.tw_hi_count);
+
+    const C* src = state + (static_cast<size_t>(b) * P.nfields + field) * P.hx * kyn + static_cast<size_t>(tile) * W * kyn;
+    C* in = fft_input(buf, scr, P.fy);
+    const int total = W * npy;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int w = fdiv(e, P.div_npy);
+        const int y = e - w * npy;
+        int j = -1;
+        if (y < half) j = y;
+        else if (y > npy - half) j = y - npy + kyn;
+        in[sw(y, mask) * W + w] = (j >= 0) ? src[w * kyn + j] : czero<C>();
+    }
+    __syncthreads();
+    fft_lines<+1, true>(buf, scr, P.fy, W, P.div_w, 1, W, s_lo, s_hi);
+    const T sc = static_cast<T>(P.inv_scale);
+    C* dst = i1 + ((static_cast<size_t>(b) * P.n_in + slot) * P.ntiles + tile) * static_cast<size_t>(npy) * W;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        const int y = fdiv(e, P.div_w);
+        const int w = e - y * W;
+        dst[e] = cscale(buf[sw(y, mask) * W + w], sc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// row pass: I1 -> C2R -> products -> R2C -> I2   (grid: row pairs x batch)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T product_value(const StepPlan& P, int kind, int arg, T psi, T jx, T jy, T vx, T vy) {
+    switch (kind) {
+        case OUT_MU: return static_cast<T>(P.mu_u3[arg]) * psi * psi * psi;   // model_free_energy_phi4.cc:47-55
+        case OUT_PSIVX: return psi * vx;                                       // fcalculator.cc:226-239
+        case OUT_PSIVY: return psi * vy;
+        case OUT_GRAD: return static_cast<T>(P.grad_ax[arg]) * vx + static_cast<T>(P.grad_ay[arg]) * vy;  // fcalculator.cc:814-826
+        case OUT_VX: return vx;                                                // fcalculator.cc:366-367
+        case OUT_VY: return vy;
+        case OUT_PXX: return jx * vx;                                          // fcalculator.cc:447-451
+        case OUT_PXY: return jx * vy;
+        default: return jy * vy;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
+                                                            const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
+                                                            int* __restrict__ err) {
+    using C = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s_lo = reinterpret_cast<C*>(smem_raw);
+    C* s_hi = s_lo + kTwLo;
+    const int npx = P.npx, npy = P.npy, W = P.W, hx = P.hx;
+    C* lines = s_hi + P.fx.tw_hi_count;                     // n_in physical row pairs
+    C* work = lines + static_cast<size_t>(P.n_in) * npx;     // row_lb product lines
+    C* scr = work + static_cast<size_t>(P.row_lb) * npx;     // row_lb ping-pong lines
+    const uint32_t mask = P.fx.swz;
+
+    const int pair = blockIdx.x, b = blockIdx.y;
+    const int y0 = 2 * pair;
+    const bool has1 = (y0 + 1) < npy;
+    load_twiddles(s_lo, s_hi, tw, P.fx.tw_hi_count);
+    __syncthreads();
+
+    // 1. inputs, lb lines at a time: Z[k] = X0[k] + i X1[k] with the Hermitian
+    //    mirror (rows y0, y0+1), zero outside |kx| < Na/2; inverse transform
+    const size_t i1_member = static_cast<size_t>(b) * P.n_in * P.ntiles * npy * W;
+    for (int s0 = 0; s0 < P.n_in; s0 += P.row_lb) {
+        const int nl = min(P.row_lb, P.n_in - s0);
+        C* in = fft_input(lines + static_cast<size_t>(s0) * npx, scr, P.fx);
+        for (int l = 0; l < nl; ++l) {
+            C* z = in + static_cast<size_t>(l) * npx;
+            const C* src = i1 + i1_member + static_cast<size_t>(s0 + l) * P.ntiles * npy * W;
+            for (int k = threadIdx.x; k < npx; k += blockDim.x) {
+                if (k < hx) {
+                    const int t = fdiv(k, P.div_w), w = k - t * W;
+                    const C* p0 = src + (static_cast<size_t>(t) * npy + y0) * W + w;
+                    C a = p0[0];
+                    C c = has1 ? p0[W] : czero<C>();
+                    if (k == 0) { a.y = 0; c.y = 0; }  // C2R uses the real part of the kx = 0 entry
+                    z[sw(k, mask)] = mk(a.x - c.y, a.y + c.x);
+                    if (k > 0) z[sw(npx - k, mask)] = mk(a.x + c.y, c.x - a.y);
+                } else if (k <= npx - hx) {
+                    z[sw(k, mask)] = czero<C>();
+                }
+            }
+        }
+        __syncthreads();
+        fft_lines<+1, false>(lines + static_cast<size_t>(s0) * npx, scr, P.fx, nl, P.div_w, npx, 1, s_lo, s_hi);
+    }
+
+    // 2. velocity: v = j / rho (compressible) or j / rho0 (fcalculator_workspace.cc:115-142),
+    //    formed where a product needs it; the zero-density check runs once per row pair.
+    //    Pointwise work runs over shared-memory slots: every line uses the same swizzle.
+    const int s_rho = P.in_slot[0];
+    const int s_jx = P.in_slot[P.nop + 1];
+    const int s_jy = P.in_slot[P.nop + 2];
+    const bool comp = (P.mode == 0);
+    const T inv_rho0 = (P.need_v && !comp) ? static_cast<T>(1.0 / rho0_member[b]) : T(0);
+    if (P.need_v && comp) {
+        int bad = 0;
+        for (int x = threadIdx.x; x < npx; x += blockDim.x) {
+            const C rho = lines[static_cast<size_t>(s_rho) * npx + x];
+            if (rho.x == T(0) || (has1 && rho.y == T(0))) bad = 1;
+        }
+        if (bad) atomicOr(err, ERR_ZERO_DENSITY);
+    }
+
+    // 3. products -> forward transforms -> keep kx < Hx
+    const size_t i2_member = static_cast<size_t>(b) * P.n_out * P.ntiles * npy * W;
+    for (int o0 = 0; o0 < P.n_out; o0 += P.row_lb) {
+        const int nl = min(P.row_lb, P.n_out - o0);
+        C* in = fft_input(work, scr, P.fx);
+        for (int l = 0; l < nl; ++l) {
+            const int kind = P.out_kind[o0 + l], arg = P.out_arg[o0 + l];
+            C* dst = in + static_cast<size_t>(l) * npx;
+            const int s_psi = (kind == OUT_MU || kind == OUT_PSIVX || kind == OUT_PSIVY) ? P.in_slot[1 + arg] : -1;
+            const bool use_v = (kind != OUT_MU);
+            for (int x = threadIdx.x; x < npx; x += blockDim.x) {
+                const C psi = s_psi >= 0 ? lines[static_cast<size_t>(s_psi) * npx + x] : czero<C>();
+                C jx = czero<C>(), jy = czero<C>(), vx = czero<C>(), vy = czero<C>();
+                if (use_v) {
+                    jx = lines[static_cast<size_t>(s_jx) * npx + x];
+                    jy = lines[static_cast<size_t>(s_jy) * npx + x];
+                    if (comp) {
+                        const C rho = lines[static_cast<size_t>(s_rho) * npx + x];
+                        vx = mk(jx.x / rho.x, jx.y / rho.y);
+                        vy = mk(jy.x / rho.x, jy.y / rho.y);
+                    } else {
+                        vx = mk(jx.x * inv_rho0, jx.y * inv_rho0);
+                        vy = mk(jy.x * inv_rho0, jy.y * inv_rho0);
+                    }
+                }
+                C val = mk(product_value<T>(P, kind, arg, psi.x, jx.x, jy.x, vx.x, vy.x),
+                           product_value<T>(P, kind, arg, psi.y, jx.y, jy.y, vx.y, vy.y));
+                if (!has1) val.y = T(0);  // odd row count: the last pair holds one row
+                dst[x] = val;
+            }
+        }
+        __syncthreads();
+        fft_lines<-1, false>(work, scr, P.fx, nl, P.div_w, npx, 1, s_lo, s_hi);
+        for (int l = 0; l < nl; ++l) {
+            const C* z = work + static_cast<size_t>(l) * npx;
+            C* dst = i2 + i2_member + static_cast<size_t>(o0 + l) * P.ntiles * npy * W;
+            for (int k = threadIdx.x; k < hx; k += blockDim.x) {
+                const C zk = z[sw(k, mask)];
+                const C zn = cconj(z[sw(k == 0 ? 0 : npx - k, mask)]);
+                const C g0 = mk(static_cast<T>(0.5) * (zk.x + zn.x), static_cast<T>(0.5) * (zk.y + zn.y));
+                const C d = csub(zk, zn);
+                const C g1 = mk(static_cast<T>(0.5) * d.y, static_cast<T>(-0.5) * d.x);
+                const int t = fdiv(k, P.div_w), w = k - t * W;
+                C* q = dst + (static_cast<size_t>(t) * npy + y0) * W + w;
+                q[0] = g0;
+                if (has1) q[W] = g1;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// column forward + epilogue   (grid: tiles x groups x batch)
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ cplx<T> psi_noise(const StepPlan& P, int alpha, int draw, uint64_t step, uint32_t member, uint32_t mode_id,
+                                             bool conj_line, T sigma) {
+    cplx<T> xi = complex_normal<T>(P.seed, member, step, psi_stream(alpha, draw), mode_id);
+    if (conj_line) xi = cconj(xi);
+    return cscale(xi, sigma);
+}
+
+// j_sto for one draw (fcalculator.cc:587-700): out = -i k . pi(xi)
+template <typename T>
+__device__ __forceinline__ void j_noise(const StepPlan& P, int draw, uint64_t step, uint32_t member, uint32_t mode_id, bool conj_line,
+                                        T kx, T ky, cplx<T>& ox, cplx<T>& oy) {
+    using C = cplx<T>;
+    C x1 = complex_normal<T>(P.seed, member, step, j_stream(0, draw), mode_id);
+    C x2 = complex_normal<T>(P.seed, member, step, j_stream(1, draw), mode_id);
+    C x3 = complex_normal<T>(P.seed, member, step, j_stream(2, draw), mode_id);
+    if (conj_line) { x1 = cconj(x1); x2 = cconj(x2); x3 = cconj(x3); }
+    const T s = static_cast<T>(P.j_s), se = static_cast<T>(P.sqrt_eta), sz = static_cast<T>(P.sqrt_zeta);
+    const C pxx = mk(-s * (sz * x1.x + se * x2.x), -s * (sz * x1.y + se * x2.y));
+    const C pyy = mk(-s * (sz * x1.x - se * x2.x), -s * (sz * x1.y - se * x2.y));
+    const C pxy = mk(-s * se * x3.x, -s * se * x3.y);
+    ox = cmulmi(cadd(cscale(pxx, kx), cscale(pxy, ky)));
+    oy = cmulmi(cadd(cscale(pxy, kx), cscale(pyy, ky)));
+}
+
+template <typename T, int NPOS>
+__global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P, const StageArgs<T> A, const cplx<T>* __restrict__ tw) {
+    using C = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s_lo = reinterpret_cast<C*>(smem_raw);
+    C* s_hi = s_lo + kTwLo;
+    C* buf = s_hi + P.fy.tw_hi_count;
+    C* scr = buf + P.W * P.npy;
+    const uint32_t mask = P.fy.swz;
+
+    const int tile = blockIdx.x, grp = blockIdx.y, b = blockIdx.z;
+    const int W = P.W, npy = P.npy, kyn = P.kyn, nay = P.nay;
+    const int gkind = P.group_kind[grp];
+    const int alpha = P.group_alpha[grp];
+    const int nop = P.nop;
+    const bool comp = (P.mode == 0), incomp = (P.mode == 1);
+    const uint32_t member = P.member_offset + b;
+    load_twiddles(s_lo, s_hi, tw, P.fy.tw_hi_count);
+
+    const int npos_total = W * kyn;
+    const size_t fstride = static_cast<size_t>(P.hx) * kyn;
+    const size_t mbase = static_cast<size_t>(b) * P.nfields * fstride + static_cast<size_t>(tile) * W * kyn;
+
+    // accumulators: psi group -> acc0 = psi_alpha; momentum group -> acc0 = jx, acc1 = jy
+    C acc0[NPOS], acc1[NPOS];
+#pragma unroll
+    for (int i = 0; i < NPOS; ++i) { acc0[i] = czero<C>(); acc1[i] = czero<C>(); }
+
+    const T kxu = static_cast<T>(P.kx_unit), kyu = static_cast<T>(P.ky_unit);
+    const int ngo = P.group_nout[grp];
+    for (int go = 0; go < ngo; ++go) {
+        const int o = P.group_out[grp][go];
+        const C* src = A.i2 + ((static_cast<size_t>(b) * P.n_out + o) * P.ntiles + tile) * static_cast<size_t>(npy) * W;
+        const int total = W * npy;
+        C* in = fft_input(buf, scr, P.fy);
+        for (int e = threadIdx.x; e < total; e += blockDim.x) {
+            const int y = fdiv(e, P.div_w);
+            const int w = e - y * W;
+            in[sw(y, mask) * W + w] = src[e];
+        }
+        __syncthreads();
+        fft_lines<-1, true>(buf, scr, P.fy, W, P.div_w, 1, W, s_lo, s_hi);
+        const int kind = P.out_kind[o];
+#pragma unroll
+        for (int i = 0; i < NPOS; ++i) {
+            const int p = threadIdx.x + i * kThreads;
+            if (p < npos_total) {
+                const int w = fdiv(p, P.div_kyn);
+                const int j = p - w * kyn;
+                const int ky = ky_of_j(j, nay);
+                const int y = ky >= 0 ? ky : ky + npy;
+                const C v = buf[sw(y, mask) * W + w];
+                const T kx = kxu * static_cast<T>(tile * W + w);
+                const T kyv = kyu * static_cast<T>(ky);
+                switch (kind) {
+                    case OUT_MU: {  // -M k^2 mu_hat (fcalculator.cc:244-257)
+                        const T m = static_cast<T>(P.mobility[alpha]);
+                        acc0[i] = cadd(acc0[i], cscale(v, -m * (kx * kx + kyv * kyv)));
+                        break;
+                    }
+                    case OUT_PSIVX: acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kx))); break;   // fcalculator.cc:260-272
+                    case OUT_PSIVY: acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kyv))); break;
+                    case OUT_GRAD: acc0[i] = cadd(acc0[i], v); break;                         // fcalculator.cc:831-833
+                    case OUT_VX: {  // compressible viscous stress (fcalculator.cc:374-396)
+                        const T eta = static_cast<T>(P.eta), zeta = static_cast<T>(P.zeta);
+                        acc0[i] = cadd(acc0[i], cscale(v, -((eta + zeta) * kx * kx + eta * kyv * kyv)));
+                        acc1[i] = cadd(acc1[i], cscale(v, -(zeta * kx * kyv)));
+                        break;
+                    }
+                    case OUT_VY: {
+                        const T eta = static_cast<T>(P.eta), zeta = static_cast<T>(P.zeta);
+                        acc0[i] = cadd(acc0[i], cscale(v, -(zeta * kx * kyv)));
+                        acc1[i] = cadd(acc1[i], cscale(v, -(eta * kx * kx + (eta + zeta) * kyv * kyv)));
+                        break;
+                    }
+                    case OUT_PXX: acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kx))); break;     // fcalculator.cc:475-492
+                    case OUT_PXY:
+                        acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kyv)));
+                        acc1[i] = cadd(acc1[i], cmulmi(cscale(v, kx)));
+                        break;
+                    default: acc1[i] = cadd(acc1[i], cmulmi(cscale(v, kyv))); break;
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- epilogue: spectral terms, noise, stage update; results replace acc0/acc1 ----
+    const T dt = static_cast<T>(A.dt), sdt = static_cast<T>(A.sdt), wb = static_cast<T>(A.wb), wc = static_cast<T>(A.wc);
+    const T beta = static_cast<T>(A.beta);
+    const int f_jx = nop + 1, f_jy = nop + 2;
+#pragma unroll
+    for (int i = 0; i < NPOS; ++i) {
+        const int p = threadIdx.x + i * kThreads;
+        if (p >= npos_total) continue;
+        const int w = fdiv(p, P.div_kyn);
+        const int j = p - w * kyn;
+        const int ky = ky_of_j(j, nay);
+        const int gx = tile * W + w;
+        const T kx = kxu * static_cast<T>(gx);
+        const T kyv = kyu * static_cast<T>(ky);
+        const T k2 = kx * kx + kyv * kyv;
+        const size_t pos = mbase + static_cast<size_t>(w) * kyn + j;
+        const bool conj_line = (gx == 0 && ky < 0);
+        const uint32_t mode_id = static_cast<uint32_t>(gx) * static_cast<uint32_t>(nay) + static_cast<uint32_t>(((conj_line ? -ky : ky) % nay + nay) % nay);
+        const bool k_nonzero = !(gx == 0 && ky == 0);
+
+        if (gkind == GROUP_PSI) {
+            const int f = 1 + alpha;
+            const C cur = A.cur[pos + f * fstride];
+            C det = czero<C>();
+            if (!P.psi_zero[alpha]) {
+                det = acc0[i];
+                if (P.psi_linear[alpha]) {  // fcalculator.cc:152-187
+                    const T m = static_cast<T>(P.mobility[alpha]);
+                    const T mu = static_cast<T>(P.mu_k0[alpha]) + static_cast<T>(P.mu_k2[alpha]) * k2 + static_cast<T>(P.mu_k4[alpha]) * k2 * k2;
+                    det = cadd(det, cscale(cur, -m * k2 * mu));
+                }
+                for (int s = 0; s < P.n_sine; ++s)
+                    if (P.sine[s].field == f && P.sine[s].gx == gx && P.sine[s].ky == ky)
+                        det = cadd(det, mk(static_cast<T>(P.sine[s].re), static_cast<T>(P.sine[s].im)));
+                if (P.grad_incomp[alpha]) {  // fcalculator.cc:790-806
+                    const T r0 = static_cast<T>(1.0 / A.rho0[b]);
+                    const C jxv = A.cur[pos + f_jx * fstride];
+                    const C jyv = A.cur[pos + f_jy * fstride];
+                    det = cadd(det, cadd(cscale(jxv, static_cast<T>(P.grad_ax[alpha]) * r0), cscale(jyv, static_cast<T>(P.grad_ay[alpha]) * r0)));
+                }
+            }
+            if (A.det_mode) { acc0[i] = det; continue; }
+            C sto = czero<C>();
+            if (P.external_noise) {
+                sto = A.ext_a[pos + f * fstride];
+                if (A.srk3) sto = cadd(sto, cscale(A.ext_b[pos + f * fstride], beta));
+            } else if (P.noise_psi[alpha] && k_nonzero) {
+                const T sigma = sqrt(static_cast<T>(P.psi_sig2[alpha]) * k2);
+                sto = psi_noise<T>(P, alpha, 0, A.step, member, mode_id, conj_line, sigma);
+                if (A.srk3) sto = cadd(sto, cscale(psi_noise<T>(P, alpha, 1, A.step, member, mode_id, conj_line, sigma), beta));
+            }
+            const C base = (A.wb != 0.0) ? A.base[pos + f * fstride] : czero<C>();
+            const C inner = cadd(cadd(cur, cscale(det, dt)), cscale(sto, sdt));
+            acc0[i] = cadd(cscale(base, wb), cscale(inner, wc));
+        } else {
+            const C cjx = A.cur[pos + f_jx * fstride];
+            const C cjy = A.cur[pos + f_jy * fstride];
+            C djx = czero<C>(), djy = czero<C>();
+            if (!P.j_zero) {
+                djx = acc0[i];
+                djy = acc1[i];
+                if (P.cT2 != 0.0) {  // fcalculator.cc:276-300
+                    const C ph = cscale(A.cur[pos], static_cast<T>(P.cT2));
+                    djx = cadd(djx, cmulmi(cscale(ph, kx)));
+                    djy = cadd(djy, cmulmi(cscale(ph, kyv)));
+                }
+                if (P.incomp_visc) {  // fcalculator.cc:302-341
+                    const T r0 = static_cast<T>(1.0 / A.rho0[b]);
+                    const T eta = static_cast<T>(P.eta);
+                    const C vx = cscale(cjx, r0), vy = cscale(cjy, r0);
+                    djx = csub(djx, cscale(cadd(cscale(vx, 2 * kx * kx + kyv * kyv), cscale(vy, kx * kyv)), eta));
+                    djy = csub(djy, cscale(cadd(cscale(vx, kx * kyv), cscale(vy, kx * kx + 2 * kyv * kyv)), eta));
+                }
+                for (int s = 0; s < P.n_sine; ++s)
+                    if (P.sine[s].gx == gx && P.sine[s].ky == ky) {
+                        const C src = mk(static_cast<T>(P.sine[s].re), static_cast<T>(P.sine[s].im));
+                        if (P.sine[s].field == f_jx) djx = cadd(djx, src);
+                        else if (P.sine[s].field == f_jy) djy = cadd(djy, src);
+                    }
+            }
+            if (A.det_mode) { acc0[i] = djx; acc1[i] = djy; continue; }
+            C sx = czero<C>(), sy = czero<C>();
+            if (P.external_noise) {
+                sx = A.ext_a[pos + f_jx * fstride];
+                sy = A.ext_a[pos + f_jy * fstride];
+                if (A.srk3) {
+                    sx = cadd(sx, cscale(A.ext_b[pos + f_jx * fstride], beta));
+                    sy = cadd(sy, cscale(A.ext_b[pos + f_jy * fstride], beta));
+                }
+            } else if (P.noise_j && k_nonzero) {
+                j_noise<T>(P, 0, A.step, member, mode_id, conj_line, kx, kyv, sx, sy);
+                if (A.srk3) {
+                    C bx, by;
+                    j_noise<T>(P, 1, A.step, member, mode_id, conj_line, kx, kyv, bx, by);
+                    sx = cadd(sx, cscale(bx, beta));
+                    sy = cadd(sy, cscale(by, beta));
+                }
+            }
+            const C bjx = (A.wb != 0.0) ? A.base[pos + f_jx * fstride] : czero<C>();
+            const C bjy = (A.wb != 0.0) ? A.base[pos + f_jy * fstride] : czero<C>();
+            C incx = cadd(cscale(djx, dt), cscale(sx, sdt));
+            C incy = cadd(cscale(djy, dt), cscale(sy, sdt));
+            if (incomp && k2 != T(0)) {  // transverse projection (srk3_incompressible.h:81-96)
+                const C tr = cadd(cscale(incx, -kyv), cscale(incy, kx));
+                incx = cscale(cscale(tr, -kyv), T(1) / k2);
+                incy = cscale(cscale(tr, kx), T(1) / k2);
+            }
+            acc0[i] = cadd(cscale(bjx, wb), cscale(cadd(cjx, incx), wc));
+            acc1[i] = cadd(cscale(bjy, wb), cscale(cadd(cjy, incy), wc));
+        }
+    }
+
+    // ---- which fields this CTA writes, in order: psi | (rho), jx, jy ----
+    int nwf = 0;
+    int wfield[3];
+    if (gkind == GROUP_PSI) { wfield[nwf++] = 1 + alpha; }
+    else { if (comp) wfield[nwf++] = 0; wfield[nwf++] = f_jx; wfield[nwf++] = f_jy; }
+
+    C* stage_buf = fft_input(buf, scr, P.fy);  // new values, zero-padded, ready for the y-inverse
+    for (int q = 0; q < nwf; ++q) {
+        const int f = wfield[q];
+        const int total = W * npy;
+        for (int e = threadIdx.x; e < total; e += blockDim.x) stage_buf[e] = czero<C>();
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < NPOS; ++i) {
+            const int p = threadIdx.x + i * kThreads;
+            if (p < npos_total) {
+                const int w = fdiv(p, P.div_kyn);
+                const int j = p - w * kyn;
+                const int ky = ky_of_j(j, nay);
+                const int y = ky >= 0 ? ky : ky + npy;
+                C v;
+                if (f == 0) {  // rho: rho_det (fcalculator.cc:60-84) and its stage update
+                    const size_t pos = mbase + static_cast<size_t>(w) * kyn + j;
+                    const T kx = kxu * static_cast<T>(tile * W + w);
+                    const T kyv = kyu * static_cast<T>(ky);
+                    const C drho = cmulmi(cadd(cscale(A.cur[pos + f_jx * fstride], kx), cscale(A.cur[pos + f_jy * fstride], kyv)));
+                    if (A.det_mode) v = drho;
+                    else v = cadd(cscale((A.wb != 0.0) ? A.base[pos] : czero<C>(), wb), cscale(cadd(A.cur[pos], cscale(drho, dt)), wc));
+                } else {
+                    v = (f == f_jy) ? acc1[i] : acc0[i];
+                }
+                stage_buf[sw(y, mask) * W + w] = v;
+            }
+        }
+        __syncthreads();
+        // real-symmetry projection of the kx = 0 line (time_integrator.h:70-109)
+        if (tile == 0 && !A.det_mode) {
+            for (int ky = threadIdx.x; ky < nay / 2; ky += blockDim.x) {
+                if (ky == 0) {
+                    stage_buf[0].y = T(0);
+                } else {
+                    C* pa = stage_buf + sw(ky, mask) * W;
+                    C* pc = stage_buf + sw(npy - ky, mask) * W;
+                    const C a = *pa, c = *pc;
+                    const C pj = mk(static_cast<T>(0.5) * (a.x + c.x), static_cast<T>(0.5) * (a.y - c.y));
+                    *pa = pj;
+                    *pc = cconj(pj);
+                }
+            }
+            __syncthreads();
+        }
+        // write the state
+        C* dst = A.next + mbase + f * fstride;
+        for (int p = threadIdx.x; p < npos_total; p += blockDim.x) {
+            const int w = fdiv(p, P.div_kyn);
+            const int j = p - w * kyn;
+            const int ky = ky_of_j(j, nay);
+            const int y = ky >= 0 ? ky : ky + npy;
+            dst[static_cast<size_t>(w) * kyn + j] = stage_buf[sw(y, mask) * W + w];
+        }
+        // y-inverse of the new field for the next stage (scaled by 1/(Nx Ny) on the way out)
+        const int slot = P.in_slot[f];
+        if (A.fused_inverse && slot >= 0) {
+            __syncthreads();
+            fft_lines<+1, true>(buf, scr, P.fy, W, P.div_w, 1, W, s_lo, s_hi);
+            const T sc = static_cast<T>(P.inv_scale);
+            C* o1 = A.i1_next + ((static_cast<size_t>(b) * P.n_in + slot) * P.ntiles + tile) * static_cast<size_t>(npy) * W;
+            for (int e = threadIdx.x; e < total; e += blockDim.x) {
+                const int y = fdiv(e, P.div_w);
+                const int w = e - y * W;
+                o1[e] = cscale(buf[sw(y, mask) * W + w], sc);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fields the integrator only copies: symmetrise the kx = 0 line once and
+// mirror them into the stage buffers   (grid: fields x batch)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kThreads) prepare_static_kernel(const StepPlan P, const int* __restrict__ fields, cplx<T>* u, cplx<T>* s1,
+                                                                 cplx<T>* s2) {
+    using C = cplx<T>;
+    const int f = fields[blockIdx.x], b = blockIdx.y;
+    const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
+    C* uf = u + (static_cast<size_t>(b) * P.nfields + f) * fstride;
+    const int half = P.nay / 2;
+    if (threadIdx.x == 0) uf[0].y = T(0);
+    for (int ky = 1 + threadIdx.x; ky < half; ky += blockDim.x) {
+        const int jn = P.kyn - ky;  // j of -ky
+        const C a = uf[ky];
+        const C c = uf[jn];
+        const C pj = mk(static_cast<T>(0.5) * (a.x + c.x), static_cast<T>(0.5) * (a.y - c.y));
+        uf[ky] = pj;
+        uf[jn] = cconj(pj);
+    }
+    __syncthreads();
+    C* a1 = s1 + (static_cast<size_t>(b) * P.nfields + f) * fstride;
+    C* a2 = s2 + (static_cast<size_t>(b) * P.nfields + f) * fstride;
+    for (size_t e = threadIdx.x; e < fstride; e += blockDim.x) {
+        const C v = uf[e];
+        a1[e] = v;
+        a2[e] = v;
+    }
+}
+
+}  // namespace shhd

@@ -1,0 +1,235 @@
+"""Python binding of the B200 step engine (ctypes over lib/libshhd_b200.so).
+
+The engine is the CUDA path; this module only moves arguments across the C
+ABI declared in include/shhd_b200.h.  Importing it loads the library and
+fails loudly if it has not been built (there is no CPU fallback).
+
+Typical use mirrors the reference's driver loop (src/project.h:128-145)::
+
+    cfg = config_from_script(open("input.script").read())
+    eng = Engine(cfg)
+    eng.set_state(state)          # reference State layout, complex128
+    eng.step(100)                 # FluidSolver::step x 100
+    state = eng.get_state()
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libshhd_b200.so")
+
+MAX_OP = 8
+MAX_FORCES = 8
+
+SHHD_OK = 0
+SHHD_EINVAL = -1
+SHHD_ECUDA = -2
+SHHD_ENOMEM = -3
+SHHD_ENUMERIC = -4
+SHHD_EUNSUPPORTED = -5
+
+COMPRESSIBLE, INCOMPRESSIBLE, QUIESCENT = 0, 1, 2
+EULER, SRK3 = 0, 1
+FP64, FP32 = 0, 1
+NOISE_PHILOX, NOISE_EXTERNAL = 0, 1
+
+
+class SineForce(ctypes.Structure):
+    _fields_ = [("target", ctypes.c_int), ("component", ctypes.c_int), ("axis", ctypes.c_int), ("nk", ctypes.c_int),
+                ("amplitude", ctypes.c_double)]
+
+
+class GradientForce(ctypes.Structure):
+    _fields_ = [("component", ctypes.c_int), ("direction", ctypes.c_int), ("amplitude", ctypes.c_double)]
+
+
+class Config(ctypes.Structure):
+    """Mirror of shhd_config."""
+    _fields_ = [
+        ("active_nx", ctypes.c_int), ("active_ny", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("lx", ctypes.c_double), ("ly", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("mode", ctypes.c_int), ("integrator", ctypes.c_int),
+        ("num_order_parameters", ctypes.c_int),
+        ("free_energy", ctypes.c_int),
+        ("mu_k0", ctypes.c_double * MAX_OP), ("mu_k2", ctypes.c_double * MAX_OP),
+        ("mu_k4", ctypes.c_double * MAX_OP), ("mu_u3", ctypes.c_double * MAX_OP),
+        ("cT", ctypes.c_double),
+        ("eta", ctypes.c_double), ("zeta", ctypes.c_double),
+        ("mobility", ctypes.c_double * MAX_OP),
+        ("momentum_advection", ctypes.c_int), ("order_parameter_advection", ctypes.c_int),
+        ("noise_momentum", ctypes.c_int), ("noise_order_parameter", ctypes.c_int),
+        ("noise_seed", ctypes.c_int64),
+        ("kBT", ctypes.c_double), ("chi", ctypes.c_double),
+        ("n_sine_forces", ctypes.c_int), ("sine_forces", SineForce * MAX_FORCES),
+        ("n_gradient_forces", ctypes.c_int), ("gradient_forces", GradientForce * MAX_FORCES),
+        ("precision", ctypes.c_int), ("noise_source", ctypes.c_int),
+        ("batch", ctypes.c_int), ("member_offset", ctypes.c_int),
+    ]
+
+    def copy(self) -> "Config":
+        c = Config()
+        ctypes.memmove(ctypes.byref(c), ctypes.byref(self), ctypes.sizeof(Config))
+        return c
+
+
+class Info(ctypes.Structure):
+    _fields_ = [
+        ("nfields", ctypes.c_int), ("state_doubles", ctypes.c_size_t), ("active_modes", ctypes.c_size_t),
+        ("n_inverse", ctypes.c_int), ("n_forward", ctypes.c_int), ("n_evolved", ctypes.c_int),
+        ("device_bytes", ctypes.c_size_t), ("bytes_per_stage", ctypes.c_double), ("fft_flops_per_stage", ctypes.c_double),
+        ("step_index", ctypes.c_int64), ("time", ctypes.c_double),
+    ]
+
+
+class ShhdError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+# every symbol include/shhd_b200.h declares
+EXPORTED = (
+    "shhd_last_error", "shhd_config_default", "shhd_config_from_script", "shhd_engine_create", "shhd_engine_destroy",
+    "shhd_engine_info", "shhd_engine_set_state", "shhd_engine_get_state", "shhd_engine_step", "shhd_engine_step_async",
+    "shhd_engine_synchronize", "shhd_engine_set_external_noise", "shhd_engine_rhs", "shhd_engine_set_time",
+    "shhd_engine_stream", "shhd_engine_state_device",
+)
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run `make -C {os.path.dirname(LIB_PATH)}/..` (the engine has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, dp, sz, i = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_size_t, ctypes.c_int
+    lib.shhd_last_error.restype = ctypes.c_char_p
+    lib.shhd_config_default.argtypes = [ctypes.POINTER(Config)]
+    lib.shhd_config_from_script.argtypes = [ctypes.c_char_p, ctypes.POINTER(Config)]
+    lib.shhd_engine_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(vp)]
+    lib.shhd_engine_destroy.argtypes = [vp]
+    lib.shhd_engine_destroy.restype = None
+    lib.shhd_engine_info.argtypes = [vp, ctypes.POINTER(Info)]
+    lib.shhd_engine_set_state.argtypes = [vp, i, dp, sz]
+    lib.shhd_engine_get_state.argtypes = [vp, i, dp, sz]
+    lib.shhd_engine_step.argtypes = [vp, i]
+    lib.shhd_engine_step_async.argtypes = [vp, i]
+    lib.shhd_engine_synchronize.argtypes = [vp]
+    lib.shhd_engine_set_external_noise.argtypes = [vp, i, dp, dp, sz]
+    lib.shhd_engine_rhs.argtypes = [vp, i, dp, sz]
+    lib.shhd_engine_set_time.argtypes = [vp, ctypes.c_int64, ctypes.c_double]
+    lib.shhd_engine_stream.argtypes = [vp]
+    lib.shhd_engine_stream.restype = vp
+    lib.shhd_engine_state_device.argtypes = [vp]
+    lib.shhd_engine_state_device.restype = vp
+    return lib
+
+
+lib = _load()
+
+
+def _check(rc: int) -> None:
+    if rc != SHHD_OK:
+        raise ShhdError(rc, lib.shhd_last_error().decode())
+
+
+def default_config() -> Config:
+    c = Config()
+    _check(lib.shhd_config_default(ctypes.byref(c)))
+    return c
+
+
+def config_from_script(text: str) -> Config:
+    """Parse a reference input script into a Config (host only)."""
+    c = Config()
+    _check(lib.shhd_config_from_script(text.encode(), ctypes.byref(c)))
+    return c
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Engine:
+    """One engine: `cfg.batch` members of one configuration on the current GPU."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg.copy()
+        h = ctypes.c_void_p()
+        _check(lib.shhd_engine_create(ctypes.byref(self.cfg), ctypes.byref(h)))
+        self._h = h
+        self.info = self.get_info()
+        self.shape = (self.info.nfields, cfg.ny, cfg.nx // 2 + 1)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.shhd_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def get_info(self) -> Info:
+        inf = Info()
+        _check(lib.shhd_engine_info(self._h, ctypes.byref(inf)))
+        return inf
+
+    def _as_ref(self, state: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(state, dtype=np.complex128)
+        if a.shape != self.shape:
+            raise ValueError(f"state shape {a.shape} != {self.shape}")
+        return a
+
+    def set_state(self, state: np.ndarray, member: int = 0) -> None:
+        a = self._as_ref(state)
+        _check(lib.shhd_engine_set_state(self._h, member, _dptr(a.view(np.float64)), a.size * 2))
+
+    def get_state(self, member: int = 0) -> np.ndarray:
+        out = np.zeros(self.shape, dtype=np.complex128)
+        _check(lib.shhd_engine_get_state(self._h, member, _dptr(out.view(np.float64)), out.size * 2))
+        return out
+
+    def step(self, nsteps: int = 1) -> None:
+        _check(lib.shhd_engine_step(self._h, nsteps))
+
+    def step_async(self, nsteps: int = 1) -> None:
+        _check(lib.shhd_engine_step_async(self._h, nsteps))
+
+    def synchronize(self) -> None:
+        _check(lib.shhd_engine_synchronize(self._h))
+
+    def set_external_noise(self, sto_a: np.ndarray, sto_b: Optional[np.ndarray] = None, member: int = 0) -> None:
+        a = self._as_ref(sto_a)
+        b = self._as_ref(sto_b) if sto_b is not None else None
+        _check(lib.shhd_engine_set_external_noise(self._h, member, _dptr(a.view(np.float64)),
+                                                  _dptr(b.view(np.float64)) if b is not None else None, a.size * 2))
+
+    def rhs(self, member: int = 0) -> np.ndarray:
+        out = np.zeros(self.shape, dtype=np.complex128)
+        _check(lib.shhd_engine_rhs(self._h, member, _dptr(out.view(np.float64)), out.size * 2))
+        return out
+
+    def set_time(self, step_index: int, time: float) -> None:
+        _check(lib.shhd_engine_set_time(self._h, int(step_index), float(time)))
+
+    @property
+    def stream(self) -> int:
+        return lib.shhd_engine_stream(self._h) or 0
+
+    @property
+    def state_device_ptr(self) -> int:
+        return lib.shhd_engine_state_device(self._h) or 0

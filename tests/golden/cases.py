@@ -1,0 +1,156 @@
+"""Input scripts of the golden cases (reference grammar).
+
+Small grids so the fixtures stay a few hundred KB; together they reach every
+term of the step: the three modes under Euler and SRK3, phi4 and quadratic
+free energies, advection of psi and j, compressible and incompressible
+viscosity, linear pressure, sine and gradient forces, the three dealias rules,
+a rectangular box with an odd padded row count, and conservative noise.
+"""
+
+_HEAD = """dimension 2
+boundary p p
+"""
+
+CASES = {
+    # 1024^2 N=2 configuration shrunk to 16^2: compressible, phi4, advection, noise
+    "srk3_compressible_n2": _HEAD + """grid 16 16
+length 16 16
+dealias 3/2
+order_parameters 2
+timestep 0.01
+time_evolution srk3/compressible
+model thermo linear_eos cT 1
+model free_energy phi4 a[0] -1 b[0] 1 u[0] 1 a[1] -1 b[1] 1 u[1] 1
+model transport constant eta 1 zeta 1 M[0,0] 1 M[1,1] 1
+fix 1 all nonlinear on
+fix 2 all noise on seed 3 kBT 1e-3
+set density equilibrium/gaussian kBT 1e-3 rho0 1 cT 1 seed 1
+set momentum all equilibrium/gaussian/compressible kBT 1e-3 seed 2
+set order_parameter all equilibrium/gaussian seed 7 kBT 1 k0 4 k2 0
+run 2
+""",
+    "euler_compressible_n2": _HEAD + """grid 16 16
+length 16 16
+dealias 3/2
+order_parameters 2
+timestep 0.005
+time_evolution euler/compressible
+model thermo linear_eos cT 1
+model free_energy phi4 a[0] -1 b[0] 1 u[0] 1 a[1] 0.5 b[1] 2 u[1] 0
+model transport constant eta 0.5 zeta 2 M[0,0] 1 M[1,1] 0.5
+fix 1 all nonlinear on
+fix 2 all noise on seed 11 kBT 1e-3 chi 2
+set density equilibrium/gaussian kBT 1e-3 rho0 1 cT 1 seed 4
+set momentum all equilibrium/gaussian/compressible kBT 1e-3 seed 5
+set order_parameter all equilibrium/gaussian seed 9 kBT 1 k0 4 k2 0
+run 2
+""",
+    "srk3_incompressible_n1_forces": _HEAD + """grid 16 16
+length 12 12
+dealias 3/2
+order_parameters 1
+timestep 0.01
+time_evolution srk3/incompressible
+model transport constant eta 0.3 zeta 0 M[0,0] 0.7
+model free_energy phi4 a[0] 1 b[0] 0.5 u[0] 0.2
+fix 1 all nonlinear on
+fix 2 all noise on seed 5 kBT 1e-3
+fix 3 momentum force/sine on component x axis y nk 2 amplitude 0.05
+fix 4 order_parameter force/gradient on component 0 direction x amplitude 0.3
+set density uniform value 1.3
+set momentum all equilibrium/gaussian/incompressible kBT 1e-3 seed 3
+set order_parameter all equilibrium/gaussian seed 2 kBT 1 k0 4 k2 0
+run 2
+""",
+    "euler_incompressible_n0": _HEAD + """grid 16 16
+length 16 16
+dealias 3/2
+order_parameters 0
+timestep 0.01
+time_evolution euler/incompressible
+model transport constant eta 0.1 zeta 0
+fix 1 momentum nonlinear on
+fix 2 all noise on seed 8 kBT 1e-4
+fix 3 momentum force/sine on component y axis x nk 3 amplitude 0.02
+set density uniform value 1.0
+set momentum all random_vorticity n0 3 sigma 2 urms 0.5 seed 11
+run 2
+""",
+    # ensemble member shrunk to 16^2: quiescent phi4 quench with noise
+    "srk3_quiescent_n1": _HEAD + """grid 16 16
+length 16 16
+dealias 3/2
+order_parameters 1
+timestep 0.02
+time_evolution srk3/quiescent
+model free_energy phi4 a[0] -1 b[0] 1 u[0] 1
+model transport constant eta 0 zeta 0 M[0,0] 1
+fix 1 order_parameter noise on seed 0 kBT 0.05
+set density uniform value 1.0
+set order_parameter all equilibrium/gaussian seed 0 kBT 0.01 k0 1 k2 0
+run 2
+""",
+    "euler_quiescent_n2_quadratic": _HEAD + """grid 16 16
+length 10 10
+dealias 3/2
+order_parameters 2
+timestep 0.01
+time_evolution euler/quiescent
+model free_energy quadratic a[0] 1 a[1] 2.5
+model transport constant eta 0 zeta 0 M[0,0] 1 M[1,1] 0.25
+fix 1 order_parameter noise on seed 21 kBT 0.1
+set density uniform value 1.0
+set order_parameter all equilibrium/gaussian seed 4 kBT 0.1 k0 1 k2 1
+run 2
+""",
+    # plain-method configuration shrunk: N=0 compressible, no dealiasing, rectangular box
+    "srk3_compressible_n0_rect_nodealias": _HEAD + """grid 16 12
+length 16 10
+dealias none
+order_parameters 0
+timestep 0.02
+time_evolution srk3/compressible
+model thermo linear_eos cT 1
+model transport constant eta 1 zeta 1
+fix 1 all nonlinear on
+fix 2 all noise on seed 1 kBT 1e-4
+set density equilibrium/gaussian kBT 1e-4 rho0 1 cT 1 seed 1
+set momentum all equilibrium/gaussian/compressible kBT 1e-4 seed 1
+run 2
+""",
+    # dealias two, compressible gradient force, order-parameter sine force, odd padded rows (6 -> 9)
+    "srk3_compressible_n1_two_gradient": _HEAD + """grid 12 6
+length 9 7
+dealias 3/2
+order_parameters 1
+timestep 0.005
+time_evolution srk3/compressible
+model thermo linear_eos cT 0.8
+model free_energy phi4 a[0] 0.5 b[0] 0.3 u[0] 0.4
+model transport constant eta 0.4 zeta 0.1 M[0,0] 0.6
+fix 1 all nonlinear on
+fix 2 all noise on seed 17 kBT 1e-3
+fix 3 order_parameter force/gradient on component 0 direction y amplitude 0.2
+fix 4 order_parameter force/sine on component 0 axis x nk 2 amplitude 0.1
+set density equilibrium/gaussian kBT 1e-3 rho0 1 cT 0.8 seed 6
+set momentum all equilibrium/gaussian/compressible kBT 1e-3 seed 7
+set order_parameter all equilibrium/gaussian seed 8 kBT 1 k0 2 k2 0
+run 2
+""",
+    "srk3_compressible_two_dealias": _HEAD + """grid 8 8
+length 8 8
+dealias two
+order_parameters 1
+timestep 0.01
+time_evolution srk3/compressible
+model thermo linear_eos cT 1
+model free_energy phi4 a[0] -1 b[0] 1 u[0] 1
+model transport constant eta 1 zeta 0.5 M[0,0] 1
+fix 1 all nonlinear on
+fix 2 all noise on seed 2 kBT 1e-3
+set density equilibrium/gaussian kBT 1e-3 rho0 1 cT 1 seed 3
+set momentum all equilibrium/gaussian/compressible kBT 1e-3 seed 4
+set order_parameter all equilibrium/gaussian seed 5 kBT 1 k0 4 k2 0
+run 2
+""",
+}

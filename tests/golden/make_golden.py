@@ -1,0 +1,62 @@
+"""Generate the golden fixtures from the reference's own code.
+
+Runs in the build container, where the reference sources exist: it loads
+oracle/_ref/libshhd_ref.so (the reference's src .cc files compiled against the
+single-rank MPI / heFFTe shims, see oracle/Makefile) and records, per case:
+the input script, the initial state the reference's initial-condition styles
+produce, the deterministic RHS at that state, and two steps of the reference
+integrator with the stochastic right-hand sides it drew.
+
+    python tests/golden/make_golden.py      # writes tests/golden/ref_cases.npz
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, HERE)
+from cases import CASES  # noqa: E402
+
+NSTEPS = 2
+
+
+def main() -> None:
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libshhd_ref.so"))
+    lib.shref_create.restype = ctypes.c_void_p
+    lib.shref_last_error.restype = ctypes.c_char_p
+    out = {}
+    for name, script in CASES.items():
+        h = ctypes.c_void_p(lib.shref_create(script.encode()))
+        if not h.value:
+            raise RuntimeError(f"{name}: {lib.shref_last_error().decode()}")
+        info = (ctypes.c_long * 10)()
+        dinfo = (ctypes.c_double * 4)()
+        lib.shref_info(h, info, dinfo)
+        nf, ny, hx = info[4], info[1], info[0] // 2 + 1
+        shape = (nf, ny, hx)
+        P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        u0 = np.zeros(shape, complex)
+        lib.shref_get_state(h, P(u0))
+        det = np.zeros(shape, complex)
+        assert lib.shref_rhs(h, ctypes.c_double(0.0), P(det)) == 0
+        noise = np.zeros((NSTEPS, 2) + shape, complex)
+        states = np.zeros((NSTEPS,) + shape, complex)
+        for s in range(NSTEPS):
+            rc = lib.shref_step(h, 1, P(noise[s]))
+            if rc != 0:
+                raise RuntimeError(f"{name}: {lib.shref_last_error().decode()}")
+            lib.shref_get_state(h, P(states[s]))
+        lib.shref_destroy(h)
+        out[f"{name}/u0"] = u0
+        out[f"{name}/det"] = det
+        out[f"{name}/noise"] = noise
+        out[f"{name}/states"] = states
+        print(f"{name}: shape {shape}, |u0| {np.abs(u0).max():.3g}, |noise| {np.abs(noise).max():.3g}")
+    np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **out)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,236 @@
+"""CUDA engine vs the oracle, through the C ABI (GPU).
+
+Tolerances (relative L2 over the whole state):
+  FP64 engine  <= 1e-12 against the FP64 oracle / reference fixtures
+  FP32 engine  <= 1e-5  (deterministic, few steps), per the FP32-bulk target
+"""
+import numpy as np
+import pytest
+
+import shhd_oracle as so
+from helpers import load_golden, random_state, script
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 1e-5
+CASES = load_golden()
+
+
+@pytest.fixture(scope="module")
+def sb():
+    import torch
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    import shhd_b200
+    return shhd_b200
+
+
+def make_engine(sb, text, precision=0, noise_source=0, batch=1, member_offset=0):
+    cfg = sb.config_from_script(text)
+    cfg.precision = precision
+    cfg.noise_source = noise_source
+    cfg.batch = batch
+    cfg.member_offset = member_offset
+    return sb.Engine(cfg)
+
+
+# ---------------------------------------------------------------------------
+# reference fixtures (states and noise produced by the reference's own code)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("precision", [0, 1])
+def test_rhs_matches_reference(sb, name, precision):
+    c = CASES[name]
+    with make_engine(sb, c["script"], precision) as eng:
+        eng.set_state(c["u0"])
+        det = eng.rhs()
+    assert so.rel_l2(det, c["det"]) < (TOL64 if precision == 0 else TOL32)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("precision", [0, 1])
+def test_steps_with_reference_noise(sb, name, precision):
+    c = CASES[name]
+    with make_engine(sb, c["script"], precision, noise_source=1) as eng:
+        eng.set_state(c["u0"])
+        for s in range(c["states"].shape[0]):
+            eng.set_external_noise(c["noise"][s, 0], c["noise"][s, 1])
+            eng.step(1)
+            u = eng.get_state()
+            assert so.rel_l2(u, c["states"][s]) < (TOL64 if precision == 0 else TOL32), f"step {s}"
+
+
+# ---------------------------------------------------------------------------
+# seeded inputs against the oracle at larger sizes
+# ---------------------------------------------------------------------------
+SCRIPTS = {
+    "srk3_comp_n2_64": script(grid=(64, 64), length=(64.0, 64.0), nop=2, dt=0.01),
+    "euler_comp_n1_48x32": script(grid=(48, 32), length=(40.0, 30.0), nop=1, dt=0.005, eta=0.5, zeta=2.0),
+    "srk3_incomp_n1_64": script(grid=(64, 64), length=(100.0, 100.0), nop=1, dt=0.01, te="srk3/incompressible", cT=None, eta=0.2, zeta=0.0),
+    "srk3_incomp_n0_128": script(grid=(128, 128), length=(128.0, 128.0), nop=0, dt=0.01, te="srk3/incompressible", cT=None, eta=0.05,
+                                 zeta=0.0, nonlinear="momentum"),
+    "srk3_quiescent_n1_128": script(grid=(128, 128), length=(256.0, 256.0), nop=1, dt=0.02, te="srk3/quiescent", cT=None, eta=0.0,
+                                    zeta=0.0, nonlinear=None),
+    "euler_quiescent_n3_64": script(grid=(64, 64), length=(64.0, 64.0), nop=3, dt=0.01, te="euler/quiescent", cT=None, eta=0.0,
+                                    zeta=0.0, nonlinear=None, fe="quadratic", a=0.7),
+    "srk3_comp_n0_128_none": script(grid=(128, 128), length=(128.0, 128.0), nop=0, dt=0.05, dealias="none"),
+    "srk3_comp_n1_two_40": script(grid=(40, 40), length=(40.0, 40.0), nop=1, dt=0.01, dealias="two"),
+}
+
+
+def _state_for(cfg):
+    return random_state(cfg, seed=hash(cfg.time_evolution) % 1000, amp=0.05, transverse=(cfg.mode == "incompressible"))
+
+
+@pytest.mark.parametrize("name", sorted(SCRIPTS))
+def test_deterministic_trajectory_fp64(sb, name):
+    text = SCRIPTS[name]
+    cfg = so.parse_script(text)
+    u0 = _state_for(cfg)
+    o = so.Oracle(cfg)
+    ref = u0
+    nsteps = 5
+    for _ in range(nsteps):
+        ref = o.step(ref)
+    with make_engine(sb, text, 0) as eng:
+        eng.set_state(u0)
+        eng.step(nsteps)
+        u = eng.get_state()
+    assert so.rel_l2(u, ref) < TOL64
+
+
+@pytest.mark.parametrize("name", sorted(SCRIPTS))
+def test_deterministic_trajectory_fp32(sb, name):
+    text = SCRIPTS[name]
+    cfg = so.parse_script(text)
+    u0 = _state_for(cfg)
+    o = so.Oracle(cfg)
+    ref = u0
+    for _ in range(3):
+        ref = o.step(ref)
+    with make_engine(sb, text, 1) as eng:
+        eng.set_state(u0)
+        eng.step(3)
+        u = eng.get_state()
+    assert so.rel_l2(u, ref) < TOL32
+
+
+@pytest.mark.parametrize("name", ["srk3_comp_n2_64", "srk3_incomp_n1_64", "srk3_quiescent_n1_128", "euler_comp_n1_48x32"])
+def test_philox_noise_matches_oracle(sb, name):
+    """The engine's in-kernel Philox noise equals the oracle's restatement."""
+    text = SCRIPTS[name].replace("run 1", "fix 9 all noise on seed 77 kBT 0.003\nrun 1")
+    cfg = so.parse_script(text)
+    u0 = _state_for(cfg)
+    o = so.Oracle(cfg)
+    ref = u0
+    for _ in range(3):
+        ref = o.step(ref, "philox")
+    with make_engine(sb, text, 0) as eng:
+        eng.set_state(u0)
+        eng.step(3)
+        u = eng.get_state()
+    assert so.rel_l2(u, ref) < TOL64
+
+
+def test_batch_members_are_independent_and_keyed(sb):
+    text = SCRIPTS["srk3_comp_n2_64"].replace("run 1", "fix 9 all noise on seed 5 kBT 0.002\nrun 1")
+    cfg = so.parse_script(text)
+    states = [random_state(cfg, seed=s, amp=0.04) for s in range(3)]
+    with make_engine(sb, text, 0, batch=3, member_offset=10) as eng:
+        for m, st in enumerate(states):
+            eng.set_state(st, member=m)
+        eng.step(2)
+        got = [eng.get_state(m) for m in range(3)]
+    for m in range(3):
+        o = so.Oracle(cfg, member=10 + m)
+        ref = states[m]
+        for _ in range(2):
+            ref = o.step(ref, "philox")
+        assert so.rel_l2(got[m], ref) < TOL64
+
+
+def test_step_calls_compose(sb):
+    """step(a) then step(b) equals step(a + b) (noise keyed by absolute step)."""
+    text = SCRIPTS["srk3_comp_n2_64"].replace("run 1", "fix 9 all noise on seed 3 kBT 0.001\nrun 1")
+    cfg = so.parse_script(text)
+    u0 = random_state(cfg, seed=1)
+    with make_engine(sb, text, 0) as e1, make_engine(sb, text, 0) as e2:
+        e1.set_state(u0)
+        e2.set_state(u0)
+        e1.step(4)
+        e2.step(1)
+        e2.step(3)
+        assert so.rel_l2(e1.get_state(), e2.get_state()) < 1e-15
+
+
+def test_fp32_tracks_fp64(sb):
+    text = script(grid=(128, 128), length=(256.0, 256.0), nop=2, dt=0.01)
+    cfg = so.parse_script(text)
+    u0 = random_state(cfg, seed=4)
+    with make_engine(sb, text, 0) as e64, make_engine(sb, text, 1) as e32:
+        e64.set_state(u0)
+        e32.set_state(u0)
+        e64.step(20)
+        e32.step(20)
+        assert so.rel_l2(e32.get_state(), e64.get_state()) < TOL32
+
+
+def test_conservation_and_symmetry_full_size(sb):
+    """1024^2, N = 2 compressible (the headline workload) in FP32: mass and
+    momentum (k = 0 modes) are conserved, the kx = 0 line stays Hermitian, and
+    FP32 stays within tolerance of FP64 over a few steps."""
+    text = script(grid=(1024, 1024), length=(1024.0, 1024.0), nop=2, dt=0.01, noise="kBT 0.001 seed 7")
+    cfg = so.parse_script(text)
+    u0 = random_state(cfg, seed=9, amp=0.05)
+    with make_engine(sb, text, 1) as e32, make_engine(sb, text, 0) as e64:
+        e32.set_state(u0)
+        e64.set_state(u0)
+        e32.step(5)
+        e64.step(5)
+        u32, u64 = e32.get_state(), e64.get_state()
+    n = cfg.num_order_parameters
+    for u, tol in ((u64, 1e-13), (u32, 1e-6)):
+        assert abs(u[0, 0, 0] - u0[0, 0, 0]) <= tol * abs(u0[0, 0, 0])
+        for f in (n + 1, n + 2):
+            assert abs(u[f, 0, 0]) <= tol * abs(u0[0, 0, 0])
+        line = u[:, :, 0]
+        ny = u.shape[1]
+        assert np.allclose(line[:, 1:ny // 2], np.conj(line[:, ny - 1:ny // 2:-1]), rtol=0, atol=0)
+    assert so.rel_l2(u32, u64) < TOL32
+
+
+def test_incompressible_stays_transverse(sb):
+    text = script(grid=(256, 256), length=(256.0, 256.0), nop=0, dt=0.01, te="srk3/incompressible", cT=None, eta=0.01, zeta=0.0,
+                  nonlinear="momentum", noise="kBT 1e-4 seed 3")
+    cfg = so.parse_script(text)
+    u0 = random_state(cfg, seed=2, transverse=True)
+    with make_engine(sb, text, 1) as eng:
+        eng.set_state(u0)
+        eng.step(10)
+        u = eng.get_state()
+    g = so.Geometry(cfg)
+    kdotj = g.kx * u[1] + g.ky * u[2]
+    scale = np.sqrt(g.k2) * np.sqrt(np.abs(u[1]) ** 2 + np.abs(u[2]) ** 2)
+    assert np.all(np.abs(kdotj) <= 1e-5 * scale + 1e-6)
+
+
+def test_zero_density_is_reported(sb):
+    text = script(grid=(16, 16), length=(16.0, 16.0), nop=0, dt=0.01)
+    cfg = so.parse_script(text)
+    u0 = np.zeros((3, cfg.grid[1], cfg.grid[0] // 2 + 1), complex)
+    with make_engine(sb, text, 0) as eng:
+        eng.set_state(u0)
+        with pytest.raises(sb.ShhdError) as ei:
+            eng.step(1)
+        assert ei.value.code == sb.SHHD_ENUMERIC
+        assert "zero density" in str(ei.value)
+
+
+def test_set_state_rejects_inactive_modes(sb):
+    c = CASES["srk3_compressible_n2"]
+    bad = c["u0"].copy()
+    bad[1, 12, 12] = 1.0  # Nyquist row, outside the active set
+    with make_engine(sb, c["script"], 0) as eng:
+        with pytest.raises(sb.ShhdError) as ei:
+            eng.set_state(bad)
+        assert ei.value.code == sb.SHHD_EINVAL
