@@ -1,0 +1,485 @@
+#!/usr/bin/env python
+"""Benchmark of the step engine on the headline workload.
+
+Workload (the reference's Hohenberg-Halperin compressible configuration):
+1024x1024 active grid (3/2 rule -> 1536^2 compute grid), Lx = Ly = 1024,
+N = 2 order parameters with phi4 free energy (mu_a = -psi_a + psi_a^3 -
+lap psi_a), M_a = 1, rho0 = 1, eta = zeta = 1, linear EOS cT = 1, advection of
+psi and j, conservative noise kBT = 1e-3, psi initial state equilibrium
+Gaussian (seed 7, real-space std ~0.1), SRK3 with dt = 0.01.  Synthetic
+inputs of that shape (no dataset is involved).
+
+One "step" = one SRK3 step of one trajectory.  `value` = trajectory steps/s
+over all ranks (each rank advances its own replica: the single-grid path has
+no data-path collective), timed on the device with CUDA events on the
+engine's stream, max over ranks.  `e2e` = the same metric through the C ABI
+with host buffers: every step uploads the host State (reference layout,
+pinned), steps, and downloads the host State, as a drop-in
+FluidSolver::step(State&) must.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "spectral-hohenberg-halperin-dynamics-2d_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "SRK3 steps/s (1024^2, N=2)"
+UNIT = "steps/s"
+L2_BYTES = 126 * 1024 * 1024
+
+WORKLOAD = """dimension 2
+boundary p p
+grid 1024 1024
+length 1024 1024
+dealias 3/2
+order_parameters 2
+timestep 0.01
+time_evolution srk3/compressible
+model thermo linear_eos cT 1
+model free_energy phi4 a[0] -1 b[0] 1 u[0] 1 a[1] -1 b[1] 1 u[1] 1
+model transport constant eta 1 zeta 1 M[0,0] 1 M[1,1] 1
+fix 1 all nonlinear on
+fix 2 all noise on seed 7 kBT 1e-3
+set density uniform value 1.0
+set order_parameter all equilibrium/gaussian seed 7 kBT 0.010019559897527924 k0 1 k2 0
+run 10000
+"""
+
+# ensemble configuration: 256 members, 256^2 (3/2 -> 384^2), quiescent phi4 quench
+ENSEMBLE = """dimension 2
+grid 256 256
+length 256 256
+dealias 3/2
+order_parameters 1
+timestep 0.02
+time_evolution srk3/quiescent
+model free_energy phi4 a[0] -1 b[0] 1 u[0] 1
+model transport constant eta 0 zeta 0 M[0,0] 1
+fix 1 order_parameter noise on seed 0 kBT 0.05
+set density uniform value 1.0
+set order_parameter all equilibrium/gaussian seed 0 kBT 0.010078585159554018 k0 1 k2 0
+run 5000
+"""
+
+CONFIG = {
+    "workload": "HH compressible 1024^2 (3/2 -> 1536^2), N=2 phi4, advection + noise, SRK3 dt=0.01",
+    "grid": [1024, 1024],
+    "compute_grid": [1536, 1536],
+    "order_parameters": 2,
+    "mode": "srk3/compressible",
+    "l2": "no flush: per-step working set (3 states + 16 transform planes) exceeds the 126 MB L2",
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# process group (one rank per GPU)
+# ---------------------------------------------------------------------------
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_group(world, local, backend):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
+    return dist
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="shhd_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            if self.uuid and parts[0] != self.uuid:
+                continue
+            rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the reference's own code; the numpy port if that is absent)
+# ---------------------------------------------------------------------------
+def reference_lib():
+    path = os.path.join(ROOT, "oracle", "_ref", "libshhd_ref.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    lib.shref_create.restype = ctypes.c_void_p
+    lib.shref_last_error.restype = ctypes.c_char_p
+    lib.shref_time_steps.restype = ctypes.c_double
+    lib.shref_threads.restype = ctypes.c_int
+    return lib
+
+
+def time_reference(nsteps_max: int, budget_s: float):
+    """Time the reference's own step on the workload; returns (steps/s, steps, cores, kind, note)."""
+    lib = reference_lib()
+    if lib is not None:
+        h = ctypes.c_void_p(lib.shref_create(WORKLOAD.encode()))
+        if not h.value:
+            raise RuntimeError(lib.shref_last_error().decode())
+        first = lib.shref_time_steps(h, 1)
+        n = max(1, min(nsteps_max, int(budget_s / max(first, 1e-3))))
+        t = lib.shref_time_steps(h, n)
+        cores = lib.shref_threads()
+        lib.shref_destroy(h)
+        return n / t, n, cores, "reference", "reference src .cc files (unmodified) on single-rank MPI/heFFTe shims, threaded shim FFT"
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import shhd_oracle as so
+    import shhd_b200 as sb
+    from shhd_b200.initial import initial_state
+    cfg = so.parse_script(WORKLOAD)
+    o = so.Oracle(cfg)
+    u = initial_state(sb.config_from_script(WORKLOAD), WORKLOAD)
+    t0 = time.perf_counter()
+    u = o.step(u, "philox")
+    t = time.perf_counter() - t0
+    return 1.0 / t, 1, 1, "port", "numpy FP64 restatement (reference checker not built)"
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    budget = float(os.environ.get("SHHD_REF_BUDGET_S", "120"))
+    # warm-up steps (untimed), then the timed steps, capped to a bounded sample
+    lib = reference_lib()
+    if lib is None:
+        sps, n, cores, kind, note = time_reference(args.steps, budget)
+    else:
+        h = ctypes.c_void_p(lib.shref_create(WORKLOAD.encode()))
+        if not h.value:
+            print(json.dumps({"impl": "reference", "unavailable": lib.shref_last_error().decode()}))
+            return
+        first = lib.shref_time_steps(h, 1)
+        wsteps = max(0, min(args.warmup - 1, int(0.25 * budget / max(first, 1e-3))))
+        if wsteps:
+            lib.shref_time_steps(h, wsteps)
+        n = max(1, min(args.steps, int(budget / max(first, 1e-3))))
+        t = lib.shref_time_steps(h, n)
+        cores = lib.shref_threads()
+        lib.shref_destroy(h)
+        sps, kind = n / t, "reference"
+        note = "reference src .cc files (unmodified) on single-rank MPI/heFFTe shims, threaded shim FFT"
+    sample = f"{n} SRK3 steps of the 1024^2 N=2 workload ({note})"
+    line = {
+        "metric": METRIC, "value": sps, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": n, "warmup": args.warmup,
+        "ms_per_step": 1e3 / sps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": CONFIG,
+        "cpu_baseline": {"value": sps, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": sps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def dram_traffic_from_profiles():
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    out = {}
+    if os.path.exists(path):
+        for line in open(path):
+            t = line.split("#", 1)[0].split()
+            if len(t) == 2:
+                try:
+                    out[t[0]] = float(t[1])
+                except ValueError:
+                    pass
+    return out
+
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        try:
+            return float(json.load(open(path))["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def run_b200(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup()
+    dist = init_group(world, local, "nccl")
+    torch.cuda.set_device(local)
+    import shhd_b200 as sb
+    from shhd_b200.initial import initial_state
+
+    cfg = sb.config_from_script(WORKLOAD)
+    cfg.precision = sb.FP32 if args.precision == "fp32" else sb.FP64
+    cfg.member_offset = rank
+    u0 = initial_state(cfg, WORKLOAD)
+    eng = sb.Engine(cfg)
+    eng.set_state(u0)
+    stream = torch.cuda.ExternalStream(eng.stream)
+
+    # warm-up
+    eng.step(args.warmup)
+
+    props = torch.cuda.get_device_properties(local)
+    uuid = "GPU-" + str(getattr(props, "uuid", "")) if getattr(props, "uuid", None) else ""
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    eng.reset_stats()
+    ev0.record(stream)
+    eng.step_async(args.steps)
+    ev1.record(stream)
+    eng.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    stats = eng.kernel_stats()
+    launches = int(sum(v[1] for v in stats.values()))
+    ms_max = max_over_ranks(ms, world)
+    value = world * args.steps / (ms_max / 1e3)
+
+    # per-kernel device time (CUDA events around each launch on the engine stream)
+    kprof_steps = max(10, min(args.steps, 100))
+    eng.reset_stats()
+    eng.set_profiling(True)
+    eng.step(kprof_steps)
+    eng.set_profiling(False)
+    kst = eng.kernel_stats()
+    dom = max(("row_pass", "col_forward"), key=lambda k: kst[k][0])
+    t_ms, n_l, by = kst[dom]
+    achieved = (by / n_l) / (t_ms / n_l * 1e-3) / 1e9
+    peak, peak_kind = measured_peak_gbs()
+    traffic = dram_traffic_from_profiles().get(dom)
+    step_bytes = sum(v[2] for v in kst.values()) / kprof_steps
+    step_ms_profiled = sum(v[0] for v in kst.values()) / kprof_steps
+    kernels = {k: {"ms_per_launch": (v[0] / v[1]) if v[1] else None, "launches_per_step": v[1] / kprof_steps,
+                   "GBps": ((v[2] / v[1]) / (v[0] / v[1] * 1e-3) / 1e9) if v[1] and v[0] > 0 else None} for k, v in kst.items() if v[1]}
+
+    # e2e: host State (pinned) -> device, one step, device -> host State, every step
+    e2e_steps = max(3, min(args.steps, 20))
+    shape = eng.shape
+    nbytes = int(np.prod(shape)) * 16
+    hin_t = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    hout_t = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+    hin = hin_t.numpy().view(np.complex128).reshape(shape)
+    hout = hout_t.numpy().view(np.complex128).reshape(shape)
+    eng.get_state(out=hin)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.set_state(hin)
+        eng.step(1)
+        eng.get_state(out=hout)
+        hin, hout = hout, hin
+    t_e2e = time.perf_counter() - t0
+    t_e2e = max_over_ranks(t_e2e, world)
+    e2e_value = world * e2e_steps / t_e2e
+    # resident variant: state stays on the device, one host call for many steps
+    t0 = time.perf_counter()
+    eng.set_state(hin)
+    eng.step(args.steps)
+    eng.get_state(out=hout)
+    t_res = max_over_ranks(time.perf_counter() - t0, world)
+    resident_value = world * args.steps / t_res
+    eng.close()
+
+    extras = {}
+    if not args.no_extras:
+        extras = run_extras(args, world, rank, local, sb, initial_state, torch)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sps, n, cores, kind, note = time_reference(5, float(os.environ.get("SHHD_CPU_BASELINE_S", "20")))
+        cpu = {"value": sps, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{n} SRK3 steps of the same 1024^2 N=2 workload ({note})"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": by / n_l, "step_GBps": step_bytes / (step_ms_profiled * 1e-3) / 1e9},
+            "kernels": kernels,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                    "what": "set_state(host pinned) + step(1) + get_state(host) through the C ABI every step"},
+            "e2e_resident": {"value": resident_value, "unit": UNIT, "what": f"set_state + step({args.steps}) + get_state, one host call"},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        line.update(extras)
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_extras(args, world, rank, local, sb, initial_state, torch):
+    out = {}
+    # the plain one-job-at-a-time FP64 path on the same workload
+    cfg = sb.config_from_script(WORKLOAD)
+    cfg.precision = sb.FP64
+    cfg.member_offset = rank
+    eng = sb.Engine(cfg)
+    eng.set_state(initial_state(cfg, WORKLOAD))
+    eng.step(2)
+    n64 = max(3, min(args.steps, 50))
+    stream = torch.cuda.ExternalStream(eng.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.step_async(n64)
+    e1.record(stream)
+    eng.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    out["fp64_plain"] = {"value": world * n64 / (ms / 1e3), "unit": UNIT, "steps": n64}
+    eng.close()
+
+    # batched ensemble: 256 members advanced together
+    cfg = sb.config_from_script(ENSEMBLE)
+    cfg.precision = sb.FP32
+    cfg.batch = 256
+    cfg.member_offset = rank * 256
+    eng = sb.Engine(cfg)
+    base = initial_state(cfg, ENSEMBLE)
+    for m in range(cfg.batch):
+        # member m: seed m (the ensemble draws psi0 per member seed)
+        eng.set_state(initial_state(cfg, ENSEMBLE.replace("all equilibrium/gaussian seed 0 ", f"all equilibrium/gaussian seed {m} ")) if m else base, member=m)
+    eng.step(2)
+    nb = max(3, min(args.steps, 50))
+    stream = torch.cuda.ExternalStream(eng.stream)
+    e0.record(stream)
+    eng.step_async(nb)
+    e1.record(stream)
+    eng.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    out["batched"] = {"value": world * nb * cfg.batch / (ms / 1e3), "unit": "member-steps/s", "members": cfg.batch * world,
+                      "ensemble_steps_per_s": world * nb / (ms / 1e3) / world, "workload": "256 x 256^2 (3/2), quiescent N=1 phi4, SRK3, FP32"}
+    eng.close()
+
+    # cuFFT beside it: the same transforms per stage (5 C2R + 11 R2C at 1536^2, FP32)
+    x = torch.randn(11, 1536, 1536, device="cuda", dtype=torch.float32)
+    X = torch.fft.rfft2(x[:5])
+    for _ in range(3):
+        torch.fft.irfft2(X, s=(1536, 1536))
+        torch.fft.rfft2(x)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(10):
+        torch.fft.irfft2(X, s=(1536, 1536))
+        torch.fft.rfft2(x)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_stage = e0.elapsed_time(e1) / 10
+    out["cufft_reference"] = {"ms_per_stage": ms_stage, "steps_per_s_transforms_only": 1e3 / (3 * ms_stage),
+                              "what": "torch.fft (cuFFT) 5 irfft2 + 11 rfft2 at 1536^2 FP32 per stage, unfused, no products or RHS"}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--precision", choices=("fp32", "fp64"), default="fp32")
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

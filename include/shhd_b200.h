@@ -172,6 +172,14 @@ int shhd_engine_rhs(shhd_engine* engine, int member, double* det, size_t n_doubl
 /* Step counter and time (project.h:136-137). */
 int shhd_engine_set_time(shhd_engine* engine, int64_t step_index, double time);
 
+/* Kernel statistics (no reference counterpart).  Kinds: 0 column inverse,
+ * 1 row pass, 2 column forward + epilogue, 3 other.  Launch counts and
+ * algorithmic HBM bytes accumulate always; per-kernel device time (CUDA
+ * events around each launch on the engine stream) only while profiling is on. */
+int shhd_engine_set_profiling(shhd_engine* engine, int on);
+int shhd_engine_kernel_stats(shhd_engine* engine, double* total_ms, int64_t* launches, double* bytes);
+int shhd_engine_reset_stats(shhd_engine* engine);
+
 /* CUDA stream the engine launches on (cudaStream_t as void*). */
 void* shhd_engine_stream(shhd_engine* engine);
 

@@ -290,6 +290,9 @@ int shref_rhs(void* h, double t, double* out) {
     });
 }
 
+/* Host threads the shim transforms use. */
+int shref_threads() { return shimfft::num_threads(); }
+
 /* Wall time of nsteps steps (seconds), for the CPU baseline. */
 double shref_time_steps(void* h, int nsteps) {
     RefRun* r = static_cast<RefRun*>(h);

@@ -14,23 +14,61 @@
  *   - forward is unnormalised, backward with scale::full divides by Nx*Ny;
  *   - batch fields are contiguous, one after another;
  *   - a C2R ignores the imaginary parts of the kx = 0 and kx = Nx/2 entries
- *     (FFTW's c2r convention for Hermitian input).
+ *     (FFTW's c2r convention for Hermitian input);
+ *   - rows and columns are split over host threads (SHHD_REF_THREADS, default
+ *     all hardware threads), the shared-memory counterpart of heFFTe's rank
+ *     decomposition.
  */
 #ifndef SHHD_ORACLE_SHIM_HEFFTE_H
 #define SHHD_ORACLE_SHIM_HEFFTE_H
 
 #include <mpi.h>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <complex>
 #include <cstddef>
+#include <cstdlib>
 #include <stdexcept>
+#include <thread>
 #include <vector>
 
 namespace shimfft {
 
 using cplx = std::complex<double>;
+
+// Threads for the transforms: SHHD_REF_THREADS, else all hardware threads.
+inline int num_threads() {
+    static const int n = [] {
+        if (const char* e = std::getenv("SHHD_REF_THREADS")) {
+            const int v = std::atoi(e);
+            if (v > 0) return v;
+        }
+        const unsigned h = std::thread::hardware_concurrency();
+        return h > 0 ? static_cast<int>(h) : 1;
+    }();
+    return n;
+}
+
+// fn(begin, end) over [0, n) split into contiguous chunks, one per thread.
+template <typename F>
+void parallel_for(int n, F&& fn) {
+    const int t = std::min(num_threads(), std::max(1, n));
+    if (t <= 1) {
+        fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(static_cast<std::size_t>(t - 1));
+    const int chunk = (n + t - 1) / t;
+    for (int i = 1; i < t; ++i) {
+        const int b = i * chunk, e = std::min(n, b + chunk);
+        if (b < e) pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    fn(0, std::min(n, chunk));
+    for (auto& th : pool) th.join();
+}
 
 // One complex FFT plan of length n (Stockham autosort, out of place ping-pong).
 class Plan {
@@ -203,62 +241,73 @@ private:
         for (int i = 0; i < hx_ * ny_; ++i) x[i] *= f;
     }
 
-    // rows (x) real->complex two at a time, then columns (y) complex forward
+    // rows (x) real->complex two at a time, then columns (y) complex forward;
+    // rows and columns are independent, so OpenMP threads split them
     void forward_one(const double* in, std::complex<double>* out) const {
-        std::vector<shimfft::cplx> z(nx_), w(nx_), col(ny_), wc(ny_);
-        for (int y = 0; y < ny_; y += 2) {
-            const bool pair = (y + 1 < ny_);
-            for (int x = 0; x < nx_; ++x)
-                z[x] = shimfft::cplx(in[y * nx_ + x], pair ? in[(y + 1) * nx_ + x] : 0.0);
-            px_.execute(z.data(), w.data(), -1);
-            for (int k = 0; k < hx_; ++k) {
-                const shimfft::cplx a = z[k];
-                const shimfft::cplx b = std::conj(z[(nx_ - k) % nx_]);
-                out[y * hx_ + k] = 0.5 * (a + b);
-                if (pair) out[(y + 1) * hx_ + k] = shimfft::cplx(0.0, -0.5) * (a - b);
+        shimfft::parallel_for((ny_ + 1) / 2, [&](int p0, int p1) {
+            std::vector<shimfft::cplx> z(nx_), w(nx_);
+            for (int y = 2 * p0; y < std::min(ny_, 2 * p1); y += 2) {
+                const bool pair = (y + 1 < ny_);
+                for (int x = 0; x < nx_; ++x)
+                    z[x] = shimfft::cplx(in[y * nx_ + x], pair ? in[(y + 1) * nx_ + x] : 0.0);
+                px_.execute(z.data(), w.data(), -1);
+                for (int k = 0; k < hx_; ++k) {
+                    const shimfft::cplx a = z[k];
+                    const shimfft::cplx b = std::conj(z[(nx_ - k) % nx_]);
+                    out[y * hx_ + k] = 0.5 * (a + b);
+                    if (pair) out[(y + 1) * hx_ + k] = shimfft::cplx(0.0, -0.5) * (a - b);
+                }
             }
-        }
-        for (int k = 0; k < hx_; ++k) {
-            for (int y = 0; y < ny_; ++y) col[y] = out[y * hx_ + k];
-            py_.execute(col.data(), wc.data(), -1);
-            for (int y = 0; y < ny_; ++y) out[y * hx_ + k] = col[y];
-        }
+        });
+        shimfft::parallel_for(hx_, [&](int k0, int k1) {
+            std::vector<shimfft::cplx> col(ny_), wc(ny_);
+            for (int k = k0; k < k1; ++k) {
+                for (int y = 0; y < ny_; ++y) col[y] = out[y * hx_ + k];
+                py_.execute(col.data(), wc.data(), -1);
+                for (int y = 0; y < ny_; ++y) out[y * hx_ + k] = col[y];
+            }
+        });
     }
 
     // columns (y) complex backward, then rows (x) complex->real two at a time
     void backward_one(const std::complex<double>* in, double* out) const {
         std::vector<shimfft::cplx> mid(static_cast<std::size_t>(hx_) * ny_);
-        std::vector<shimfft::cplx> col(ny_), wc(ny_), z(nx_), w(nx_);
-        for (int k = 0; k < hx_; ++k) {
-            for (int y = 0; y < ny_; ++y) col[y] = in[y * hx_ + k];
-            py_.execute(col.data(), wc.data(), +1);
-            for (int y = 0; y < ny_; ++y) mid[static_cast<std::size_t>(y) * hx_ + k] = col[y];
-        }
         const bool even = (nx_ % 2 == 0);
-        for (int y = 0; y < ny_; y += 2) {
-            const bool pair = (y + 1 < ny_);
-            const shimfft::cplx* r0 = &mid[static_cast<std::size_t>(y) * hx_];
-            const shimfft::cplx* r1 = pair ? &mid[static_cast<std::size_t>(y + 1) * hx_] : nullptr;
-            for (int k = 0; k < nx_; ++k) z[k] = 0.0;
-            for (int k = 0; k < hx_; ++k) {
-                shimfft::cplx a = r0[k];
-                shimfft::cplx b = pair ? r1[k] : shimfft::cplx(0.0, 0.0);
-                const bool self_conjugate = (k == 0) || (even && k == nx_ / 2);
-                if (self_conjugate) {
-                    a = shimfft::cplx(a.real(), 0.0);
-                    b = shimfft::cplx(b.real(), 0.0);
-                    z[k] = a + shimfft::cplx(0.0, 1.0) * b;
-                } else {
-                    z[k] = a + shimfft::cplx(0.0, 1.0) * b;
-                    z[nx_ - k] = std::conj(a) + shimfft::cplx(0.0, 1.0) * std::conj(b);
+        shimfft::parallel_for(hx_, [&](int k0, int k1) {
+            std::vector<shimfft::cplx> col(ny_), wc(ny_);
+            for (int k = k0; k < k1; ++k) {
+                for (int y = 0; y < ny_; ++y) col[y] = in[y * hx_ + k];
+                py_.execute(col.data(), wc.data(), +1);
+                for (int y = 0; y < ny_; ++y) mid[static_cast<std::size_t>(y) * hx_ + k] = col[y];
+            }
+        });
+        shimfft::parallel_for((ny_ + 1) / 2, [&](int p0, int p1) {
+            std::vector<shimfft::cplx> z(nx_), w(nx_);
+            for (int y = 2 * p0; y < std::min(ny_, 2 * p1); y += 2) {
+                const bool pair = (y + 1 < ny_);
+                const shimfft::cplx* r0 = &mid[static_cast<std::size_t>(y) * hx_];
+                const shimfft::cplx* r1 = pair ? &mid[static_cast<std::size_t>(y + 1) * hx_] : nullptr;
+                for (int k = 0; k < nx_; ++k) z[k] = 0.0;
+                for (int k = 0; k < hx_; ++k) {
+                    shimfft::cplx a = r0[k];
+                    shimfft::cplx b = pair ? r1[k] : shimfft::cplx(0.0, 0.0);
+                    const bool self_conjugate = (k == 0) || (even && k == nx_ / 2);
+                    if (self_conjugate) {
+                        a = shimfft::cplx(a.real(), 0.0);
+                        b = shimfft::cplx(b.real(), 0.0);
+                        z[k] = a + shimfft::cplx(0.0, 1.0) * b;
+                    } else {
+                        z[k] = a + shimfft::cplx(0.0, 1.0) * b;
+                        z[nx_ - k] = std::conj(a) + shimfft::cplx(0.0, 1.0) * std::conj(b);
+                    }
+                }
+                px_.execute(z.data(), w.data(), +1);
+                for (int x = 0; x < nx_; ++x) {
+                    out[y * nx_ + x] = z[x].real();
+                    if (pair) out[(y + 1) * nx_ + x] = z[x].imag();
                 }
             }
-            px_.execute(z.data(), w.data(), +1);
-            for (int x = 0; x < nx_; ++x) {
-                out[y * nx_ + x] = z[x].real();
-                if (pair) out[(y + 1) * nx_ + x] = z[x].imag();
-            }
-        }
+        });
     }
 };
 

@@ -150,7 +150,17 @@ struct shhd_engine {
     int64_t step_index = 0;
     double time = 0.0;
 
-    std::vector<double> host_stage;  // conversion scratch
+    void* ref_stage = nullptr;       // one member's reference-layout state (FP64) on the device
+    int* flag_dev = nullptr;
+
+    // per-kernel statistics: 0 col_inverse, 1 row_pass, 2 col_forward, 3 other
+    bool profiling = false;
+    struct Pending { int kind; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double kernel_ms[4] = {0, 0, 0, 0};
+    int64_t kernel_launches[4] = {0, 0, 0, 0};
+    double kernel_bytes[4] = {0, 0, 0, 0};
 };
 
 namespace {
@@ -168,10 +178,57 @@ void* dalloc(shhd_engine* e, size_t bytes) {
 }
 
 void free_engine(shhd_engine* e) {
-    for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y,
-                    static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev)})
+    for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->ref_stage,
+                    static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
+                    static_cast<void*>(e->flag_dev)})
         if (p) cudaFree(p);
+    for (auto& pe : e->pending) { e->event_pool.push_back(pe.a); e->event_pool.push_back(pe.b); }
+    for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
     if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+// --- per-kernel timing (CUDA events around each launch while profiling) ---
+cudaEvent_t take_event(shhd_engine* e) {
+    if (!e->event_pool.empty()) {
+        cudaEvent_t ev = e->event_pool.back();
+        e->event_pool.pop_back();
+        return ev;
+    }
+    cudaEvent_t ev;
+    check_cuda(cudaEventCreate(&ev), "cudaEventCreate");
+    return ev;
+}
+
+struct LaunchScope {
+    shhd_engine* e;
+    int kind;
+    cudaEvent_t a = nullptr, b = nullptr;
+    LaunchScope(shhd_engine* eng, int k, double bytes) : e(eng), kind(k) {
+        e->kernel_launches[kind] += 1;
+        e->kernel_bytes[kind] += bytes;
+        if (e->profiling) {
+            a = take_event(e);
+            b = take_event(e);
+            check_cuda(cudaEventRecord(a, e->stream), "cudaEventRecord");
+        }
+    }
+    ~LaunchScope() {
+        if (a) {
+            cudaEventRecord(b, e->stream);
+            e->pending.push_back({kind, a, b});
+        }
+    }
+};
+
+void resolve_timings(shhd_engine* e) {
+    for (auto& pe : e->pending) {
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, pe.a, pe.b), "cudaEventElapsedTime");
+        e->kernel_ms[pe.kind] += ms;
+        e->event_pool.push_back(pe.a);
+        e->event_pool.push_back(pe.b);
+    }
+    e->pending.clear();
 }
 
 void validate_config(const shhd_config& c) {
@@ -413,6 +470,8 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
     const StepPlan& P = e->P;
     if (P.n_in == 0) return;
     dim3 grid(P.ntiles, P.n_in, P.batch);
+    const double s = sizeof(cplx<T>);
+    LaunchScope scope(e, 0, s * P.batch * P.n_in * (static_cast<double>(P.hx) * P.kyn + static_cast<double>(P.hx) * P.npy));
     auto* st = static_cast<const cplx<T>*>(state);
     auto* i1 = static_cast<cplx<T>*>(e->i1);
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
@@ -425,6 +484,7 @@ void launch_row(shhd_engine* e) {
     const StepPlan& P = e->P;
     if (P.n_out == 0) return;
     dim3 grid((P.npy + 1) / 2, P.batch);
+    LaunchScope scope(e, 1, static_cast<double>(sizeof(cplx<T>)) * P.batch * (P.n_in + P.n_out) * static_cast<double>(P.hx) * P.npy);
     row_pass_kernel<T><<<grid, kThreads, e->smem_row, e->stream>>>(P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2),
                                                                         static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev, e->err_dev);
     check_cuda(cudaGetLastError(), "row_pass launch");
@@ -435,6 +495,12 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
     const StepPlan& P = e->P;
     if (P.n_groups == 0) return;
     dim3 grid(P.ntiles, P.n_groups, P.batch);
+    // algorithmic bytes: I2 tiles read; current (and base) read, next written per evolved field;
+    // next stage's I1 written when fused
+    LaunchScope scope(e, 2, static_cast<double>(sizeof(cplx<T>)) * P.batch *
+                                (P.n_out * static_cast<double>(P.hx) * P.npy +
+                                 e->n_evolved * static_cast<double>(P.hx) * P.kyn * (A.det_mode ? 1.0 : (2.0 + (A.wb != 0.0 ? 1.0 : 0.0))) +
+                                 (A.fused_inverse ? P.n_in * static_cast<double>(P.hx) * P.npy : 0.0)));
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
     if (e->npos == 4) col_forward_kernel<T, 4><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
     else if (e->npos == 8) col_forward_kernel<T, 8><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
@@ -462,6 +528,7 @@ template <typename T>
 void prepare_static(shhd_engine* e) {
     if (e->n_static == 0) return;
     dim3 grid(e->n_static, e->P.batch);
+    LaunchScope scope(e, 3, static_cast<double>(sizeof(cplx<T>)) * e->P.batch * e->n_static * 3.0 * e->P.hx * e->P.kyn);
     prepare_static_kernel<T><<<grid, kThreads, 0, e->stream>>>(e->P, e->static_dev, static_cast<cplx<T>*>(e->u), static_cast<cplx<T>*>(e->s1),
                                                              static_cast<cplx<T>*>(e->s2));
     check_cuda(cudaGetLastError(), "prepare_static launch");
@@ -534,6 +601,7 @@ void enqueue(shhd_engine* e, int nsteps) {
 
 void sync_and_check(shhd_engine* e) {
     check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+    resolve_timings(e);
     int err = 0;
     check_cuda(cudaMemcpy(&err, e->err_dev, sizeof(int), cudaMemcpyDeviceToHost), "error flag read");
     if (err != 0) {
@@ -547,61 +615,46 @@ size_t ref_doubles(const shhd_engine* e) {
     return static_cast<size_t>(e->P.nfields) * (e->cfg.nx / 2 + 1) * e->cfg.ny * 2;
 }
 
+// host array (reference layout) -> device staging buffer -> engine layout; the
+// inactive-mode check runs on the device over the staged copy
 template <typename T>
 void upload_ref(shhd_engine* e, const double* ref, void* dst_base, int member, bool check_inactive) {
     const StepPlan& P = e->P;
-    const int hxr = e->cfg.nx / 2 + 1, ny = e->cfg.ny;
-    std::vector<cplx<T>> act(e->state_elems);
-    for (int f = 0; f < P.nfields; ++f) {
-        const double* rf = ref + static_cast<size_t>(f) * hxr * ny * 2;
-        if (check_inactive) {
-            for (int gy = 0; gy < ny; ++gy) {
-                const int sgy = gy <= ny / 2 ? gy : gy - ny;
-                const bool row_active = std::abs(sgy) < P.nay / 2;
-                for (int gx = 0; gx < hxr; ++gx) {
-                    if (row_active && gx < P.hx) continue;
-                    const double* v = rf + (static_cast<size_t>(gy) * hxr + gx) * 2;
-                    if (v[0] != 0.0 || v[1] != 0.0)
-                        throw Failure(SHHD_EINVAL, "state has a nonzero entry outside the active modes (field " + std::to_string(f) + ", gx " +
-                                                       std::to_string(gx) + ", gy " + std::to_string(gy) + ")");
-                }
-            }
-        }
-        for (int gx = 0; gx < P.hx; ++gx)
-            for (int j = 0; j < P.kyn; ++j) {
-                const int ky = j < P.nay / 2 ? j : j - P.kyn;
-                const int gy = ky >= 0 ? ky : ky + ny;
-                const double* v = rf + (static_cast<size_t>(gy) * hxr + gx) * 2;
-                cplx<T>& o = act[(static_cast<size_t>(f) * P.hx + gx) * P.kyn + j];
-                o.x = static_cast<T>(v[0]);
-                o.y = static_cast<T>(v[1]);
-            }
+    const int ref_hx = e->cfg.nx / 2 + 1;
+    const size_t bytes = ref_doubles(e) * sizeof(double);
+    if (!e->ref_stage) e->ref_stage = dalloc(e, bytes);
+    if (!e->flag_dev) e->flag_dev = static_cast<int*>(dalloc(e, sizeof(int)));
+    check_cuda(cudaMemcpyAsync(e->ref_stage, ref, bytes, cudaMemcpyHostToDevice, e->stream), "state upload");
+    const double2* st = static_cast<const double2*>(e->ref_stage);
+    if (check_inactive) {
+        check_cuda(cudaMemsetAsync(e->flag_dev, 0, sizeof(int), e->stream), "flag clear");
+        dim3 g((P.npy * ref_hx + kThreads - 1) / kThreads, P.nfields);
+        check_inactive_kernel<<<g, kThreads, 0, e->stream>>>(P, ref_hx, st, e->flag_dev);
+        check_cuda(cudaGetLastError(), "check_inactive launch");
+        int bad = 0;
+        check_cuda(cudaMemcpyAsync(&bad, e->flag_dev, sizeof(int), cudaMemcpyDeviceToHost, e->stream), "flag read");
+        check_cuda(cudaStreamSynchronize(e->stream), "upload sync");
+        if (bad) throw Failure(SHHD_EINVAL, "state has a nonzero entry outside the active modes");
     }
-    char* dst = static_cast<char*>(dst_base) + static_cast<size_t>(member) * e->state_elems * sizeof(cplx<T>);
-    check_cuda(cudaMemcpyAsync(dst, act.data(), act.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice, e->stream), "state upload");
+    cplx<T>* dst = static_cast<cplx<T>*>(dst_base) + static_cast<size_t>(member) * e->state_elems;
+    dim3 g((P.hx * P.kyn + kThreads - 1) / kThreads, P.nfields);
+    ref_to_active_kernel<T><<<g, kThreads, 0, e->stream>>>(P, ref_hx, st, dst);
+    check_cuda(cudaGetLastError(), "ref_to_active launch");
     check_cuda(cudaStreamSynchronize(e->stream), "state upload sync");
 }
 
 template <typename T>
 void download_ref(shhd_engine* e, const void* src_base, int member, double* ref) {
     const StepPlan& P = e->P;
-    const int hxr = e->cfg.nx / 2 + 1, ny = e->cfg.ny;
-    std::vector<cplx<T>> act(e->state_elems);
-    const char* src = static_cast<const char*>(src_base) + static_cast<size_t>(member) * e->state_elems * sizeof(cplx<T>);
-    check_cuda(cudaMemcpyAsync(act.data(), src, act.size() * sizeof(cplx<T>), cudaMemcpyDeviceToHost, e->stream), "state download");
+    const int ref_hx = e->cfg.nx / 2 + 1;
+    const size_t bytes = ref_doubles(e) * sizeof(double);
+    if (!e->ref_stage) e->ref_stage = dalloc(e, bytes);
+    const cplx<T>* src = static_cast<const cplx<T>*>(src_base) + static_cast<size_t>(member) * e->state_elems;
+    dim3 g((P.npy * ref_hx + kThreads - 1) / kThreads, P.nfields);
+    active_to_ref_kernel<T><<<g, kThreads, 0, e->stream>>>(P, ref_hx, src, static_cast<double2*>(e->ref_stage));
+    check_cuda(cudaGetLastError(), "active_to_ref launch");
+    check_cuda(cudaMemcpyAsync(ref, e->ref_stage, bytes, cudaMemcpyDeviceToHost, e->stream), "state download");
     check_cuda(cudaStreamSynchronize(e->stream), "state download sync");
-    std::memset(ref, 0, ref_doubles(e) * sizeof(double));
-    for (int f = 0; f < P.nfields; ++f) {
-        double* rf = ref + static_cast<size_t>(f) * hxr * ny * 2;
-        for (int gx = 0; gx < P.hx; ++gx)
-            for (int j = 0; j < P.kyn; ++j) {
-                const int ky = j < P.nay / 2 ? j : j - P.kyn;
-                const int gy = ky >= 0 ? ky : ky + ny;
-                const cplx<T>& v = act[(static_cast<size_t>(f) * P.hx + gx) * P.kyn + j];
-                rf[(static_cast<size_t>(gy) * hxr + gx) * 2] = static_cast<double>(v.x);
-                rf[(static_cast<size_t>(gy) * hxr + gx) * 2 + 1] = static_cast<double>(v.y);
-            }
-    }
 }
 
 template <typename T>
@@ -817,6 +870,37 @@ int shhd_engine_set_time(shhd_engine* e, int64_t step_index, double time) {
 }
 
 void* shhd_engine_stream(shhd_engine* e) { return e ? static_cast<void*>(e->stream) : nullptr; }
+
+int shhd_engine_set_profiling(shhd_engine* e, int on) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+        resolve_timings(e);
+        e->profiling = on != 0;
+    });
+}
+
+int shhd_engine_kernel_stats(shhd_engine* e, double* total_ms, int64_t* launches, double* bytes) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+        resolve_timings(e);
+        for (int k = 0; k < 4; ++k) {
+            if (total_ms) total_ms[k] = e->kernel_ms[k];
+            if (launches) launches[k] = e->kernel_launches[k];
+            if (bytes) bytes[k] = e->kernel_bytes[k];
+        }
+    });
+}
+
+int shhd_engine_reset_stats(shhd_engine* e) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+        resolve_timings(e);
+        for (int k = 0; k < 4; ++k) { e->kernel_ms[k] = 0; e->kernel_launches[k] = 0; e->kernel_bytes[k] = 0; }
+    });
+}
 
 const void* shhd_engine_state_device(const shhd_engine* e) { return e ? e->u : nullptr; }
 

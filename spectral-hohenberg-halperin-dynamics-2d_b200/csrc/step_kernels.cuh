@@ -621,4 +621,53 @@ __global__ void __launch_bounds__(kThreads) prepare_static_kernel(const StepPlan
     }
 }
 
+// ---------------------------------------------------------------------------
+// reference State layout (FP64, [field][gy][gx <= nx/2]) <-> engine layout
+// ---------------------------------------------------------------------------
+// grid: (ceil(hx*kyn / 256), nfields); one thread per active mode
+template <typename T>
+__global__ void __launch_bounds__(kThreads) ref_to_active_kernel(const StepPlan P, int ref_hx, const double2* __restrict__ ref,
+                                                                cplx<T>* __restrict__ act) {
+    const int f = blockIdx.y;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= P.hx * P.kyn) return;
+    const int gx = e / P.kyn, j = e - gx * P.kyn;
+    const int ky = ky_of_j(j, P.nay);
+    const int gy = ky >= 0 ? ky : ky + P.npy;
+    const double2 v = ref[(static_cast<size_t>(f) * P.npy + gy) * ref_hx + gx];
+    act[static_cast<size_t>(f) * P.hx * P.kyn + e] = mk(static_cast<T>(v.x), static_cast<T>(v.y));
+}
+
+// flags a nonzero entry outside the active modes; grid: (ceil(npy*ref_hx / 256), nfields)
+__global__ void __launch_bounds__(kThreads) check_inactive_kernel(const StepPlan P, int ref_hx, const double2* __restrict__ ref,
+                                                                  int* __restrict__ bad) {
+    const int f = blockIdx.y;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= P.npy * ref_hx) return;
+    const int gy = e / ref_hx, gx = e - gy * ref_hx;
+    const int sgy = gy <= P.npy / 2 ? gy : gy - P.npy;
+    const bool active = gx < P.hx && (sgy < 0 ? -sgy : sgy) < P.nay / 2;
+    if (active) return;
+    const double2 v = ref[static_cast<size_t>(f) * P.npy * ref_hx + e];
+    if (v.x != 0.0 || v.y != 0.0) atomicOr(bad, 1);
+}
+
+// grid: (ceil(npy*ref_hx / 256), nfields); writes every entry (zeros outside the active modes)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) active_to_ref_kernel(const StepPlan P, int ref_hx, const cplx<T>* __restrict__ act,
+                                                                double2* __restrict__ ref) {
+    const int f = blockIdx.y;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= P.npy * ref_hx) return;
+    const int gy = e / ref_hx, gx = e - gy * ref_hx;
+    const int sgy = gy <= P.npy / 2 ? gy : gy - P.npy;
+    double2 v = make_double2(0.0, 0.0);
+    if (gx < P.hx && (sgy < 0 ? -sgy : sgy) < P.nay / 2) {
+        const int j = sgy >= 0 ? sgy : sgy + P.kyn;
+        const cplx<T> a = act[(static_cast<size_t>(f) * P.hx + gx) * P.kyn + j];
+        v = make_double2(static_cast<double>(a.x), static_cast<double>(a.y));
+    }
+    ref[static_cast<size_t>(f) * P.npy * ref_hx + e] = v;
+}
+
 }  // namespace shhd

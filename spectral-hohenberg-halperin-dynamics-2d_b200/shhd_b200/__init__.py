@@ -99,8 +99,11 @@ EXPORTED = (
     "shhd_last_error", "shhd_config_default", "shhd_config_from_script", "shhd_engine_create", "shhd_engine_destroy",
     "shhd_engine_info", "shhd_engine_set_state", "shhd_engine_get_state", "shhd_engine_step", "shhd_engine_step_async",
     "shhd_engine_synchronize", "shhd_engine_set_external_noise", "shhd_engine_rhs", "shhd_engine_set_time",
-    "shhd_engine_stream", "shhd_engine_state_device",
+    "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
+    "shhd_engine_reset_stats",
 )
+
+KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
 
 
 def _load() -> ctypes.CDLL:
@@ -127,6 +130,9 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_stream.restype = vp
     lib.shhd_engine_state_device.argtypes = [vp]
     lib.shhd_engine_state_device.restype = vp
+    lib.shhd_engine_set_profiling.argtypes = [vp, i]
+    lib.shhd_engine_kernel_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
+    lib.shhd_engine_reset_stats.argtypes = [vp]
     return lib
 
 
@@ -198,8 +204,11 @@ class Engine:
         a = self._as_ref(state)
         _check(lib.shhd_engine_set_state(self._h, member, _dptr(a.view(np.float64)), a.size * 2))
 
-    def get_state(self, member: int = 0) -> np.ndarray:
-        out = np.zeros(self.shape, dtype=np.complex128)
+    def get_state(self, member: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.complex128)
+        elif out.shape != self.shape or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous complex128 array of the state shape")
         _check(lib.shhd_engine_get_state(self._h, member, _dptr(out.view(np.float64)), out.size * 2))
         return out
 
@@ -225,6 +234,20 @@ class Engine:
 
     def set_time(self, step_index: int, time: float) -> None:
         _check(lib.shhd_engine_set_time(self._h, int(step_index), float(time)))
+
+    def set_profiling(self, on: bool) -> None:
+        _check(lib.shhd_engine_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_stats(self) -> dict:
+        """{kind: (total_ms, launches, algorithmic_bytes)} since the last reset."""
+        ms = (ctypes.c_double * 4)()
+        n = (ctypes.c_int64 * 4)()
+        by = (ctypes.c_double * 4)()
+        _check(lib.shhd_engine_kernel_stats(self._h, ms, n, by))
+        return {KERNEL_KINDS[k]: (ms[k], n[k], by[k]) for k in range(4)}
+
+    def reset_stats(self) -> None:
+        _check(lib.shhd_engine_reset_stats(self._h))
 
     @property
     def stream(self) -> int:
