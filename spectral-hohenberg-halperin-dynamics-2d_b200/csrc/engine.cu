@@ -13,6 +13,7 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/shhd_b200.h"
@@ -102,6 +103,48 @@ std::vector<cplx<T>> twiddle_table(int n) {
         t[kTwLo + i].y = static_cast<T>(std::sin(a));
     }
     return t;
+}
+
+// per-stage twiddle rows of a compile-time plan (forward sign)
+template <typename T>
+std::vector<cplx<T>> stage_table(int n) {
+    const CPlan c = make_cplan(n);
+    std::vector<cplx<T>> t(std::max(c.twsz, 2));
+    for (auto& z : t) { z.x = 0; z.y = 0; }
+    for (int s = 0; s < c.ns; ++s) {
+        const int R = c.r[s], p = c.p[s];
+        if (p == 1) continue;
+        for (int k = 0; k < p; ++k)
+            for (int q = 1; q < R; ++q) {
+                const double a = -2.0 * M_PI * static_cast<double>(q) * k / (static_cast<double>(p) * R);
+                cplx<T>& z = t[c.twoff[s] + k * tw_row(R) + (q - 1)];
+                z.x = static_cast<T>(std::cos(a));
+                z.y = static_cast<T>(std::sin(a));
+            }
+    }
+    return t;
+}
+
+template <typename T>
+std::vector<cplx<T>> shared_table(int n) {
+    return is_fixed_size(n) ? stage_table<T>(n) : twiddle_table<T>(n);
+}
+
+int fixed_of(int n) { return is_fixed_size(n) ? n : 0; }
+
+// call f(std::integral_constant<int, N>) for the compile-time size N (0 = runtime plan)
+template <typename F>
+void with_size(int n, F&& f) {
+    switch (fixed_of(n)) {
+        case 96: f(std::integral_constant<int, 96>{}); break;
+        case 192: f(std::integral_constant<int, 192>{}); break;
+        case 384: f(std::integral_constant<int, 384>{}); break;
+        case 768: f(std::integral_constant<int, 768>{}); break;
+        case 1536: f(std::integral_constant<int, 1536>{}); break;
+        case 3072: f(std::integral_constant<int, 3072>{}); break;
+        case 6144: f(std::integral_constant<int, 6144>{}); break;
+        default: f(std::integral_constant<int, 0>{}); break;
+    }
 }
 
 }  // namespace
@@ -417,7 +460,9 @@ void build_plan(shhd_engine* e) {
     // 16 slots per thread.
     const size_t smem_cap = 227 * 1024;
     const size_t col_target = 100 * 1024;
-    auto col_bytes = [&](int w) { return static_cast<size_t>(kTwLo + P.fy.tw_hi_count + 2L * w * c.ny) * cs; };
+    P.twy_count = is_fixed_size(c.ny) ? std::max(make_cplan(c.ny).twsz, 2) : kTwLo + P.fy.tw_hi_count;
+    P.twx_count = is_fixed_size(c.nx) ? std::max(make_cplan(c.nx).twsz, 2) : kTwLo + P.fx.tw_hi_count;
+    auto col_bytes = [&](int w) { return static_cast<size_t>(P.twy_count + 2L * w * c.ny) * cs; };
     // register budget of the epilogue: <= 8 (FP32) / 4 (FP64) positions per thread when the grid allows
     const long pos_cap = (e->fp32 ? 8L : 4L) * kThreads;
     int W = 8;
@@ -425,15 +470,20 @@ void build_plan(shhd_engine* e) {
     if (static_cast<long>(W) * P.kyn > 16L * kThreads || col_bytes(W) > smem_cap)
         throw Failure(SHHD_EUNSUPPORTED, "compute grid " + std::to_string(c.ny) + " too large for the column kernels");
     P.W = W;
+    P.logw = W == 8 ? 3 : (W == 4 ? 2 : (W == 2 ? 1 : 0));
     P.ntiles = P.hx / W;
     P.fy.swz = swizzle_mask(c.ny, e->fp32 ? 16 : 8, W);
     P.fx.swz = swizzle_mask(c.nx, e->fp32 ? 16 : 8, 1);
+    // compile-time sizes add q * N/R (a multiple of 64) to a swizzled base, which
+    // commutes with sw() only while the mask reads bits 3..5
+    if (is_fixed_size(c.ny)) P.fy.swz = std::min(P.fy.swz, 7);
+    if (is_fixed_size(c.nx)) P.fx.swz = std::min(P.fx.swz, 7);
     const long posn = static_cast<long>(W) * P.kyn;
     e->npos = posn <= 4L * kThreads ? 4 : (posn <= 8L * kThreads ? 8 : 16);
     e->smem_col = col_bytes(W);
     // row pass: n_in physical lines + lb product lines + lb ping-pong lines
     const size_t line_bytes = static_cast<size_t>(c.nx) * cs;
-    const size_t tw_bytes = static_cast<size_t>(kTwLo + P.fx.tw_hi_count) * cs;
+    const size_t tw_bytes = static_cast<size_t>(P.twx_count) * cs;
     auto row_bytes = [&](int lb) { return tw_bytes + (P.n_in + 2 * lb) * line_bytes; };
     int lb = 4;
     while (lb > 1 && row_bytes(lb) > 113 * 1024) lb /= 2;
@@ -458,11 +508,17 @@ void set_smem_attrs(shhd_engine* e) {
     auto setattr = [](const void* fn, size_t bytes) {
         check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)), "cudaFuncSetAttribute");
     };
-    setattr(reinterpret_cast<const void*>(col_inverse_kernel<T>), e->smem_col);
-    if (e->npos == 4) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 4>), e->smem_col);
-    else if (e->npos == 8) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 8>), e->smem_col);
-    else setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 16>), e->smem_col);
-    setattr(reinterpret_cast<const void*>(row_pass_kernel<T>), e->smem_row);
+    with_size(e->P.npy, [&](auto fy) {
+        constexpr int FY = decltype(fy)::value;
+        setattr(reinterpret_cast<const void*>(col_inverse_kernel<T, FY>), e->smem_col);
+        if (e->npos == 4) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 4, FY>), e->smem_col);
+        else if (e->npos == 8) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 8, FY>), e->smem_col);
+        else setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 16, FY>), e->smem_col);
+    });
+    with_size(e->P.npx, [&](auto fx) {
+        constexpr int FX = decltype(fx)::value;
+        setattr(reinterpret_cast<const void*>(row_pass_kernel<T, FX>), e->smem_row);
+    });
 }
 
 template <typename T>
@@ -475,7 +531,9 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
     auto* st = static_cast<const cplx<T>*>(state);
     auto* i1 = static_cast<cplx<T>*>(e->i1);
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
-    col_inverse_kernel<T><<<grid, kThreads, e->smem_col, e->stream>>>(P, st, i1, tw);
+    with_size(P.npy, [&](auto fy) {
+        col_inverse_kernel<T, decltype(fy)::value><<<grid, kThreads, e->smem_col, e->stream>>>(P, st, i1, tw);
+    });
     check_cuda(cudaGetLastError(), "col_inverse launch");
 }
 
@@ -485,8 +543,11 @@ void launch_row(shhd_engine* e) {
     if (P.n_out == 0) return;
     dim3 grid((P.npy + 1) / 2, P.batch);
     LaunchScope scope(e, 1, static_cast<double>(sizeof(cplx<T>)) * P.batch * (P.n_in + P.n_out) * static_cast<double>(P.hx) * P.npy);
-    row_pass_kernel<T><<<grid, kThreads, e->smem_row, e->stream>>>(P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2),
-                                                                        static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev, e->err_dev);
+    with_size(P.npx, [&](auto fx) {
+        row_pass_kernel<T, decltype(fx)::value><<<grid, kThreads, e->smem_row, e->stream>>>(
+            P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
+            e->err_dev);
+    });
     check_cuda(cudaGetLastError(), "row_pass launch");
 }
 
@@ -502,9 +563,12 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
                                  e->n_evolved * static_cast<double>(P.hx) * P.kyn * (A.det_mode ? 1.0 : (2.0 + (A.wb != 0.0 ? 1.0 : 0.0))) +
                                  (A.fused_inverse ? P.n_in * static_cast<double>(P.hx) * P.npy : 0.0)));
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
-    if (e->npos == 4) col_forward_kernel<T, 4><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
-    else if (e->npos == 8) col_forward_kernel<T, 8><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
-    else col_forward_kernel<T, 16><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+    with_size(P.npy, [&](auto fy) {
+        constexpr int FY = decltype(fy)::value;
+        if (e->npos == 4) col_forward_kernel<T, 4, FY><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+        else if (e->npos == 8) col_forward_kernel<T, 8, FY><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+        else col_forward_kernel<T, 16, FY><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+    });
     check_cuda(cudaGetLastError(), "col_forward launch");
 }
 
@@ -690,8 +754,8 @@ void init_device(shhd_engine* e) {
         check_cuda(cudaMemsetAsync(e->ext_a, 0, e->state_elems * B * cs, e->stream), "memset");
         check_cuda(cudaMemsetAsync(e->ext_b, 0, e->state_elems * B * cs, e->stream), "memset");
     }
-    const auto twx = twiddle_table<T>(e->cfg.nx);
-    const auto twy = twiddle_table<T>(e->cfg.ny);
+    const auto twx = shared_table<T>(e->cfg.nx);
+    const auto twy = shared_table<T>(e->cfg.ny);
     e->tw_x = dalloc(e, twx.size() * cs);
     e->tw_y = dalloc(e, twy.size() * cs);
     check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");

@@ -276,6 +276,142 @@ __device__ __forceinline__ void fft_lines(C* buf, C* scratch, const FftPlan& pla
     }
 }
 
+// ---------------------------------------------------------------------------
+// compile-time sizes: radix plan, spans and per-stage twiddle rows resolved by
+// the compiler, so every index is shifts and immediate offsets
+// ---------------------------------------------------------------------------
+constexpr int kMaxFixedStages = 12;
+
+// twiddle row length per butterfly for radix R: R - 1 entries padded so a
+// float2 row starts on a 16-byte boundary
+__host__ __device__ constexpr int tw_row(int R) { return R == 8 ? 8 : (R == 4 ? 4 : (R == 5 ? 4 : 2)); }
+
+struct CPlan {
+    int ns;
+    int r[kMaxFixedStages];
+    int p[kMaxFixedStages];
+    int twoff[kMaxFixedStages];  // offset of the stage's twiddle rows (span > 1 only)
+    int twsz;                    // total twiddle entries
+};
+
+__host__ __device__ constexpr CPlan make_cplan(int n) {
+    CPlan c{};
+    int m = n, ns = 0;
+    while (m % 8 == 0) { c.r[ns++] = 8; m /= 8; }
+    if (m % 4 == 0) { c.r[ns++] = 4; m /= 4; }
+    if (m % 2 == 0) { c.r[ns++] = 2; m /= 2; }
+    while (m % 3 == 0) { c.r[ns++] = 3; m /= 3; }
+    while (m % 5 == 0) { c.r[ns++] = 5; m /= 5; }
+    c.ns = ns;
+    int p = 1, off = 0;
+    for (int s = 0; s < ns; ++s) {
+        c.p[s] = p;
+        c.twoff[s] = off;
+        if (p > 1) off += p * tw_row(c.r[s]);
+        p *= c.r[s];
+    }
+    c.twsz = off;
+    return c;
+}
+
+template <int N> struct FixedPlan { static constexpr CPlan c = make_cplan(N); };
+
+// sizes with a compile-time path (3 * 2^k padded grids of the 3/2 rule)
+__host__ __device__ constexpr bool is_fixed_size(int n) {
+    return n == 96 || n == 192 || n == 384 || n == 768 || n == 1536 || n == 3072 || n == 6144;
+}
+
+// One stage of a compile-time transform; lines interleave with width 2^logw
+// (LF) or sit N apart (rows).  Twiddles w^q (q = 1..R-1) for span index k
+// come from row k of the stage's table.  Requires mask <= 7: then
+// sw(y + m) = sw(y) + m for every multiple m of 64.
+template <int N, int R, int P, int TWOFF, int DIR, bool LF, typename C>
+__device__ __forceinline__ void fixed_stage(const C* __restrict__ src, C* __restrict__ dst, int lines, int logw, uint32_t mask,
+                                            const C* __restrict__ tw) {
+    constexpr int NR = N / R;
+    constexpr int ROW = tw_row(R);
+    const int total = lines * NR;
+#pragma unroll 2
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        int l, bi;
+        if constexpr (LF) { l = b & ((1 << logw) - 1); bi = b >> logw; }
+        else { l = b / NR; bi = b - l * NR; }
+        const C* in = LF ? src + l : src + l * N;
+        C v[R];
+        if constexpr (NR % 64 == 0) {
+            const uint32_t s0 = sw(bi, mask);
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[q] = in[(s0 + q * NR) << (LF ? logw : 0)];
+        } else {
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[q] = in[sw(bi + q * NR, mask) << (LF ? logw : 0)];
+        }
+        const int k = bi % P;
+        if constexpr (P > 1) {
+            const C* t = tw + TWOFF + k * ROW;
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                const C w = t[q - 1];
+                v[q] = DIR < 0 ? cmul(v[q], w) : cmulc(v[q], w);
+            }
+        }
+        bfly<R, DIR>(v);
+        const int j = (bi - k) * R + k;
+        C* out = LF ? dst + l : dst + l * N;
+        if constexpr (P % 64 == 0) {
+            const uint32_t s0 = sw(j, mask);
+#pragma unroll
+            for (int q = 0; q < R; ++q) out[(s0 + q * P) << (LF ? logw : 0)] = v[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < R; ++q) out[sw(j + q * P, mask) << (LF ? logw : 0)] = v[q];
+        }
+    }
+    __syncthreads();
+}
+
+template <int N, int S, int DIR, bool LF, typename C>
+__device__ __forceinline__ void fixed_stages(C* a, C* b, int lines, int logw, uint32_t mask, const C* tw) {
+    constexpr CPlan cp = FixedPlan<N>::c;
+    if constexpr (S < cp.ns) {
+        fixed_stage<N, cp.r[S], cp.p[S], cp.twoff[S], DIR, LF>(a, b, lines, logw, mask, tw);
+        fixed_stages<N, S + 1, DIR, LF>(b, a, lines, logw, mask, tw);
+    }
+}
+
+template <int N, typename C>
+__device__ __forceinline__ C* fixed_input(C* buf, C* scratch) {
+    return (FixedPlan<N>::c.ns & 1) ? scratch : buf;
+}
+
+// Transform `lines` lines; input at fixed_input(buf, scratch), result in buf.
+template <int N, int DIR, bool LF, typename C>
+__device__ __forceinline__ void fixed_fft(C* buf, C* scratch, int lines, int logw, uint32_t mask, const C* tw) {
+    fixed_stages<N, 0, DIR, LF>(fixed_input<N>(buf, scratch), (fixed_input<N>(buf, scratch) == buf) ? scratch : buf, lines, logw, mask, tw);
+}
+
+// ---------------------------------------------------------------------------
+// dispatch: FN = compile-time size, or 0 for the runtime plan.  `tw` is the
+// shared-memory table (per-stage rows for FN > 0, the two-level table else).
+// ---------------------------------------------------------------------------
+template <int FN, typename C>
+__device__ __forceinline__ C* xform_input(C* buf, C* scratch, const FftPlan& plan) {
+    if constexpr (FN == 0) return fft_input(buf, scratch, plan);
+    else return fixed_input<FN>(buf, scratch);
+}
+
+template <int FN, int DIR, bool LF, typename C>
+__device__ __forceinline__ void xform(C* buf, C* scratch, const FftPlan& plan, int nlines, const FastDiv& div_lines, int line_stride,
+                                      int elem_stride, int logw, const C* tw) {
+    if constexpr (FN == 0) fft_lines<DIR, LF>(buf, scratch, plan, nlines, div_lines, line_stride, elem_stride, tw, tw + kTwLo);
+    else fixed_fft<FN, DIR, LF>(buf, scratch, nlines, logw, static_cast<uint32_t>(plan.swz), tw);
+}
+
+template <typename C>
+__device__ __forceinline__ void load_table(C* dst, const C* __restrict__ src, int count) {
+    for (int i = threadIdx.x; i < count; i += blockDim.x) dst[i] = src[i];
+}
+
 // copy the plan's twiddle tables (global, forward sign) into shared memory
 template <typename C>
 __device__ __forceinline__ void load_twiddles(C* s_lo, C* s_hi, const C* g_tw, int hi_count) {

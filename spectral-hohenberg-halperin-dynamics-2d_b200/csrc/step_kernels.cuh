@@ -86,6 +86,8 @@ struct StepPlan {
     // transforms
     FftPlan fy, fx;
     FastDiv div_w, div_kyn, div_npy, div_hx;
+    int twx_count, twy_count;      // shared-memory twiddle entries for the row / column transforms
+    int logw;                      // log2(W)
     int row_lb;                    // max lines per row transform call
     int row_nb;                    // work lines for outputs
     int npos;                      // position slots per thread in col_forward
@@ -114,24 +116,23 @@ __device__ __forceinline__ int ky_of_j(int j, int nay) { return j < nay / 2 ? j 
 // ---------------------------------------------------------------------------
 // column inverse: state -> I1   (grid: tiles x n_in x batch)
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, int FY>
 __global__ void __launch_bounds__(kThreads) col_inverse_kernel(const StepPlan P, const cplx<T>* __restrict__ state,
                                                                cplx<T>* __restrict__ i1, const cplx<T>* __restrict__ tw) {
     using C = cplx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* s_lo = reinterpret_cast<C*>(smem_raw);
-    C* s_hi = s_lo + kTwLo;
-    C* buf = s_hi + P.fy.tw_hi_count;
+    C* s_tw = reinterpret_cast<C*>(smem_raw);
+    C* buf = s_tw + P.twy_count;
     C* scr = buf + P.W * P.npy;
 
     const int tile = blockIdx.x, slot = blockIdx.y, b = blockIdx.z;
     const int W = P.W, npy = P.npy, kyn = P.kyn, half = P.nay / 2;
     const uint32_t mask = P.fy.swz;
     const int field = P.in_field[slot];
-    load_twiddles(s_lo, s_hi, tw, P.fy.tw_hi_count);
+    load_table(s_tw, tw, P.twy_count);
 
     const C* src = state + (static_cast<size_t>(b) * P.nfields + field) * P.hx * kyn + static_cast<size_t>(tile) * W * kyn;
-    C* in = fft_input(buf, scr, P.fy);
+    C* in = xform_input<FY>(buf, scr, P.fy);
     const int total = W * npy;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
         const int w = fdiv(e, P.div_npy);
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kThreads) col_inverse_kernel(const StepPlan P,
         in[sw(y, mask) * W + w] = (j >= 0) ? src[w * kyn + j] : czero<C>();
     }
     __syncthreads();
-    fft_lines<+1, true>(buf, scr, P.fy, W, P.div_w, 1, W, s_lo, s_hi);
+    xform<FY, +1, true>(buf, scr, P.fy, W, P.div_w, 1, W, P.logw, s_tw);
     const T sc = static_cast<T>(P.inv_scale);
     C* dst = i1 + ((static_cast<size_t>(b) * P.n_in + slot) * P.ntiles + tile) * static_cast<size_t>(npy) * W;
     for (int e = threadIdx.x; e < total; e += blockDim.x) {
@@ -170,16 +171,15 @@ __device__ __forceinline__ T product_value(const StepPlan& P, int kind, int arg,
     }
 }
 
-template <typename T>
+template <typename T, int FX>
 __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
                                                             const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
                                                             int* __restrict__ err) {
     using C = cplx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* s_lo = reinterpret_cast<C*>(smem_raw);
-    C* s_hi = s_lo + kTwLo;
+    C* s_tw = reinterpret_cast<C*>(smem_raw);
     const int npx = P.npx, npy = P.npy, W = P.W, hx = P.hx;
-    C* lines = s_hi + P.fx.tw_hi_count;                     // n_in physical row pairs
+    C* lines = s_tw + P.twx_count;                           // n_in physical row pairs
     C* work = lines + static_cast<size_t>(P.n_in) * npx;     // row_lb product lines
     C* scr = work + static_cast<size_t>(P.row_lb) * npx;     // row_lb ping-pong lines
     const uint32_t mask = P.fx.swz;
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
     const int pair = blockIdx.x, b = blockIdx.y;
     const int y0 = 2 * pair;
     const bool has1 = (y0 + 1) < npy;
-    load_twiddles(s_lo, s_hi, tw, P.fx.tw_hi_count);
+    load_table(s_tw, tw, P.twx_count);
     __syncthreads();
 
     // 1. inputs, lb lines at a time: Z[k] = X0[k] + i X1[k] with the Hermitian
@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
     const size_t i1_member = static_cast<size_t>(b) * P.n_in * P.ntiles * npy * W;
     for (int s0 = 0; s0 < P.n_in; s0 += P.row_lb) {
         const int nl = min(P.row_lb, P.n_in - s0);
-        C* in = fft_input(lines + static_cast<size_t>(s0) * npx, scr, P.fx);
+        C* in = xform_input<FX>(lines + static_cast<size_t>(s0) * npx, scr, P.fx);
         for (int l = 0; l < nl; ++l) {
             C* z = in + static_cast<size_t>(l) * npx;
             const C* src = i1 + i1_member + static_cast<size_t>(s0 + l) * P.ntiles * npy * W;
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
             }
         }
         __syncthreads();
-        fft_lines<+1, false>(lines + static_cast<size_t>(s0) * npx, scr, P.fx, nl, P.div_w, npx, 1, s_lo, s_hi);
+        xform<FX, +1, false>(lines + static_cast<size_t>(s0) * npx, scr, P.fx, nl, P.div_w, npx, 1, 0, s_tw);
     }
 
     // 2. velocity: v = j / rho (compressible) or j / rho0 (fcalculator_workspace.cc:115-142),
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
     const size_t i2_member = static_cast<size_t>(b) * P.n_out * P.ntiles * npy * W;
     for (int o0 = 0; o0 < P.n_out; o0 += P.row_lb) {
         const int nl = min(P.row_lb, P.n_out - o0);
-        C* in = fft_input(work, scr, P.fx);
+        C* in = xform_input<FX>(work, scr, P.fx);
         for (int l = 0; l < nl; ++l) {
             const int kind = P.out_kind[o0 + l], arg = P.out_arg[o0 + l];
             C* dst = in + static_cast<size_t>(l) * npx;
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
             }
         }
         __syncthreads();
-        fft_lines<-1, false>(work, scr, P.fx, nl, P.div_w, npx, 1, s_lo, s_hi);
+        xform<FX, -1, false>(work, scr, P.fx, nl, P.div_w, npx, 1, 0, s_tw);
         for (int l = 0; l < nl; ++l) {
             const C* z = work + static_cast<size_t>(l) * npx;
             C* dst = i2 + i2_member + static_cast<size_t>(o0 + l) * P.ntiles * npy * W;
@@ -314,13 +314,12 @@ __device__ __forceinline__ void j_noise(const StepPlan& P, int draw, uint64_t st
     oy = cmulmi(cadd(cscale(pxy, kx), cscale(pyy, ky)));
 }
 
-template <typename T, int NPOS>
+template <typename T, int NPOS, int FY>
 __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P, const StageArgs<T> A, const cplx<T>* __restrict__ tw) {
     using C = cplx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* s_lo = reinterpret_cast<C*>(smem_raw);
-    C* s_hi = s_lo + kTwLo;
-    C* buf = s_hi + P.fy.tw_hi_count;
+    C* s_tw = reinterpret_cast<C*>(smem_raw);
+    C* buf = s_tw + P.twy_count;
     C* scr = buf + P.W * P.npy;
     const uint32_t mask = P.fy.swz;
 
@@ -331,7 +330,7 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
     const int nop = P.nop;
     const bool comp = (P.mode == 0), incomp = (P.mode == 1);
     const uint32_t member = P.member_offset + b;
-    load_twiddles(s_lo, s_hi, tw, P.fy.tw_hi_count);
+    load_table(s_tw, tw, P.twy_count);
 
     const int npos_total = W * kyn;
     const size_t fstride = static_cast<size_t>(P.hx) * kyn;
@@ -348,14 +347,14 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
         const int o = P.group_out[grp][go];
         const C* src = A.i2 + ((static_cast<size_t>(b) * P.n_out + o) * P.ntiles + tile) * static_cast<size_t>(npy) * W;
         const int total = W * npy;
-        C* in = fft_input(buf, scr, P.fy);
+        C* in = xform_input<FY>(buf, scr, P.fy);
         for (int e = threadIdx.x; e < total; e += blockDim.x) {
             const int y = fdiv(e, P.div_w);
             const int w = e - y * W;
             in[sw(y, mask) * W + w] = src[e];
         }
         __syncthreads();
-        fft_lines<-1, true>(buf, scr, P.fy, W, P.div_w, 1, W, s_lo, s_hi);
+        xform<FY, -1, true>(buf, scr, P.fy, W, P.div_w, 1, W, P.logw, s_tw);
         const int kind = P.out_kind[o];
 #pragma unroll
         for (int i = 0; i < NPOS; ++i) {
@@ -519,7 +518,7 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
     if (gkind == GROUP_PSI) { wfield[nwf++] = 1 + alpha; }
     else { if (comp) wfield[nwf++] = 0; wfield[nwf++] = f_jx; wfield[nwf++] = f_jy; }
 
-    C* stage_buf = fft_input(buf, scr, P.fy);  // new values, zero-padded, ready for the y-inverse
+    C* stage_buf = xform_input<FY>(buf, scr, P.fy);  // new values, zero-padded, ready for the y-inverse
     for (int q = 0; q < nwf; ++q) {
         const int f = wfield[q];
         const int total = W * npy;
@@ -577,7 +576,7 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
         const int slot = P.in_slot[f];
         if (A.fused_inverse && slot >= 0) {
             __syncthreads();
-            fft_lines<+1, true>(buf, scr, P.fy, W, P.div_w, 1, W, s_lo, s_hi);
+            xform<FY, +1, true>(buf, scr, P.fy, W, P.div_w, 1, W, P.logw, s_tw);
             const T sc = static_cast<T>(P.inv_scale);
             C* o1 = A.i1_next + ((static_cast<size_t>(b) * P.n_in + slot) * P.ntiles + tile) * static_cast<size_t>(npy) * W;
             for (int e = threadIdx.x; e < total; e += blockDim.x) {

@@ -75,6 +75,10 @@ SCRIPTS = {
                                     zeta=0.0, nonlinear=None, fe="quadratic", a=0.7),
     "srk3_comp_n0_128_none": script(grid=(128, 128), length=(128.0, 128.0), nop=0, dt=0.05, dealias="none"),
     "srk3_comp_n1_two_40": script(grid=(40, 40), length=(40.0, 40.0), nop=1, dt=0.01, dealias="two"),
+    # compile-time transform sizes (3/2 rule): 256 -> 384, 512 -> 768
+    "srk3_comp_n2_256": script(grid=(256, 256), length=(512.0, 512.0), nop=2, dt=0.01),
+    "srk3_incomp_n1_512x256": script(grid=(512, 256), length=(1024.0, 512.0), nop=1, dt=0.01, te="srk3/incompressible", cT=None,
+                                     eta=0.1, zeta=0.0),
 }
 
 
