@@ -18,6 +18,7 @@
 
 #include "../../include/shhd_b200.h"
 #include "step_kernels.cuh"
+#include "step_kernels_fixed.cuh"
 
 using namespace shhd;
 
@@ -125,11 +126,6 @@ std::vector<cplx<T>> stage_table(int n) {
     return t;
 }
 
-template <typename T>
-std::vector<cplx<T>> shared_table(int n) {
-    return is_fixed_size(n) ? stage_table<T>(n) : twiddle_table<T>(n);
-}
-
 int fixed_of(int n) { return is_fixed_size(n) ? n : 0; }
 
 // call f(std::integral_constant<int, N>) for the compile-time size N (0 = runtime plan)
@@ -182,6 +178,9 @@ struct shhd_engine {
     size_t state_elems = 0;       // complex per member
     size_t i1_elems = 0, i2_elems = 0;
     int npos = 16;
+    bool col_fixed = false;       // compile-time column kernels (group per column)
+    bool row_fixed = false;       // compile-time row kernel (group per line)
+    size_t smem_col_inv = 0;
     size_t smem_col = 0, smem_row = 0;
     int n_evolved = 0;
     bool need_rho0 = false;
@@ -455,42 +454,70 @@ void build_plan(shhd_engine* e) {
     P.fy = make_fft_plan(c.ny);
     P.fx = make_fft_plan(c.nx);
     const int cs = static_cast<int>(e->csize);
-    // column tile width: largest power of two <= 8 dividing Hx whose ping-pong
-    // tile pair fits ~100 KB (two CTAs per SM) and whose active positions fit
-    // 16 slots per thread.
     const size_t smem_cap = 227 * 1024;
-    const size_t col_target = 100 * 1024;
-    P.twy_count = is_fixed_size(c.ny) ? std::max(make_cplan(c.ny).twsz, 2) : kTwLo + P.fy.tw_hi_count;
-    P.twx_count = is_fixed_size(c.nx) ? std::max(make_cplan(c.nx).twsz, 2) : kTwLo + P.fx.tw_hi_count;
-    auto col_bytes = [&](int w) { return static_cast<size_t>(P.twy_count + 2L * w * c.ny) * cs; };
-    // register budget of the epilogue: <= 8 (FP32) / 4 (FP64) positions per thread when the grid allows
-    const long pos_cap = (e->fp32 ? 8L : 4L) * kThreads;
-    int W = 8;
-    while (W > 1 && (P.hx % W != 0 || col_bytes(W) > col_target || static_cast<long>(W) * P.kyn > pos_cap)) W /= 2;
-    if (static_cast<long>(W) * P.kyn > 16L * kThreads || col_bytes(W) > smem_cap)
-        throw Failure(SHHD_EUNSUPPORTED, "compute grid " + std::to_string(c.ny) + " too large for the column kernels");
+    int W = 1;
+    // compile-time kernels: fixed column width per (precision, NY) with one
+    // thread group per column; fixed row groups per (precision, NX)
+    with_size(c.ny, [&](auto fy) {
+        constexpr int FY = decltype(fy)::value;
+        if constexpr (FY != 0) {
+            const int wf = e->fp32 ? col_width<float, FY>() : col_width<double, FY>();
+            const size_t fwd_b = (static_cast<size_t>(wf) * FY + 2ull * wf * P.kyn) * cs;
+            if (P.hx % wf == 0 && fwd_b <= smem_cap) {
+                e->col_fixed = true;
+                W = wf;
+                e->smem_col = fwd_b;
+                e->smem_col_inv = static_cast<size_t>(wf) * FY * cs;
+            }
+        }
+    });
+    with_size(c.nx, [&](auto fx) {
+        constexpr int FX = decltype(fx)::value;
+        if constexpr (FX != 0) {
+            const int gsz = e->fp32 ? row_group<float, FX>() : row_group<double, FX>();
+            const size_t rb = static_cast<size_t>(P.n_in + kThreads / gsz) * FX * cs;
+            if (rb <= smem_cap) {
+                e->row_fixed = true;
+                e->smem_row = rb;
+            }
+        }
+    });
+    // shared-memory twiddle tables of the runtime-plan kernels (the compile-time
+    // kernels read per-stage rows from global memory)
+    P.twy_count = e->col_fixed ? 0 : kTwLo + P.fy.tw_hi_count;
+    P.twx_count = e->row_fixed ? 0 : kTwLo + P.fx.tw_hi_count;
+    if (!e->col_fixed) {
+        // runtime-plan column tile: largest power of two <= 8 dividing Hx whose
+        // ping-pong tile pair fits ~100 KB and whose positions fit the register budget
+        const size_t col_target = 100 * 1024;
+        auto col_bytes = [&](int w) { return static_cast<size_t>(P.twy_count + 2L * w * c.ny) * cs; };
+        const long pos_cap = (e->fp32 ? 8L : 4L) * kThreads;
+        W = 8;
+        while (W > 1 && (P.hx % W != 0 || col_bytes(W) > col_target || static_cast<long>(W) * P.kyn > pos_cap)) W /= 2;
+        if (static_cast<long>(W) * P.kyn > 16L * kThreads || col_bytes(W) > smem_cap)
+            throw Failure(SHHD_EUNSUPPORTED, "compute grid " + std::to_string(c.ny) + " too large for the column kernels");
+        e->smem_col = col_bytes(W);
+        e->smem_col_inv = e->smem_col;
+        const long posn = static_cast<long>(W) * P.kyn;
+        e->npos = posn <= 4L * kThreads ? 4 : (posn <= 8L * kThreads ? 8 : 16);
+    }
     P.W = W;
     P.logw = W == 8 ? 3 : (W == 4 ? 2 : (W == 2 ? 1 : 0));
     P.ntiles = P.hx / W;
     P.fy.swz = swizzle_mask(c.ny, e->fp32 ? 16 : 8, W);
     P.fx.swz = swizzle_mask(c.nx, e->fp32 ? 16 : 8, 1);
-    // compile-time sizes add q * N/R (a multiple of 64) to a swizzled base, which
-    // commutes with sw() only while the mask reads bits 3..5
-    if (is_fixed_size(c.ny)) P.fy.swz = std::min(P.fy.swz, 7);
-    if (is_fixed_size(c.nx)) P.fx.swz = std::min(P.fx.swz, 7);
-    const long posn = static_cast<long>(W) * P.kyn;
-    e->npos = posn <= 4L * kThreads ? 4 : (posn <= 8L * kThreads ? 8 : 16);
-    e->smem_col = col_bytes(W);
-    // row pass: n_in physical lines + lb product lines + lb ping-pong lines
-    const size_t line_bytes = static_cast<size_t>(c.nx) * cs;
-    const size_t tw_bytes = static_cast<size_t>(P.twx_count) * cs;
-    auto row_bytes = [&](int lb) { return tw_bytes + (P.n_in + 2 * lb) * line_bytes; };
-    int lb = 4;
-    while (lb > 1 && row_bytes(lb) > 113 * 1024) lb /= 2;
-    if (row_bytes(lb) > smem_cap) throw Failure(SHHD_EUNSUPPORTED, "row pass does not fit shared memory at this grid and precision");
-    P.row_lb = lb;
-    P.row_nb = lb;
-    e->smem_row = row_bytes(lb);
+    if (!e->row_fixed) {
+        // runtime-plan row pass: n_in physical lines + lb product lines + lb ping-pong lines
+        const size_t line_bytes = static_cast<size_t>(c.nx) * cs;
+        const size_t tw_bytes = static_cast<size_t>(P.twx_count) * cs;
+        auto row_bytes = [&](int lb) { return tw_bytes + (P.n_in + 2 * lb) * line_bytes; };
+        int lb = 4;
+        while (lb > 1 && row_bytes(lb) > 113 * 1024) lb /= 2;
+        if (row_bytes(lb) > smem_cap) throw Failure(SHHD_EUNSUPPORTED, "row pass does not fit shared memory at this grid and precision");
+        P.row_lb = lb;
+        P.row_nb = lb;
+        e->smem_row = row_bytes(lb);
+    }
     P.npos = e->npos;
     P.div_w = make_fastdiv(W);
     P.div_kyn = make_fastdiv(P.kyn);
@@ -510,14 +537,27 @@ void set_smem_attrs(shhd_engine* e) {
     };
     with_size(e->P.npy, [&](auto fy) {
         constexpr int FY = decltype(fy)::value;
-        setattr(reinterpret_cast<const void*>(col_inverse_kernel<T, FY>), e->smem_col);
-        if (e->npos == 4) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 4, FY>), e->smem_col);
-        else if (e->npos == 8) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 8, FY>), e->smem_col);
-        else setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 16, FY>), e->smem_col);
+        if constexpr (FY != 0) {
+            if (e->col_fixed) {
+                setattr(reinterpret_cast<const void*>(col_inverse_fixed<T, FY>), e->smem_col_inv);
+                setattr(reinterpret_cast<const void*>(col_forward_fixed<T, FY>), e->smem_col);
+                return;
+            }
+        }
+        setattr(reinterpret_cast<const void*>(col_inverse_kernel<T, 0>), e->smem_col);
+        if (e->npos == 4) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 4, 0>), e->smem_col);
+        else if (e->npos == 8) setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 8, 0>), e->smem_col);
+        else setattr(reinterpret_cast<const void*>(col_forward_kernel<T, 16, 0>), e->smem_col);
     });
     with_size(e->P.npx, [&](auto fx) {
         constexpr int FX = decltype(fx)::value;
-        setattr(reinterpret_cast<const void*>(row_pass_kernel<T, FX>), e->smem_row);
+        if constexpr (FX != 0) {
+            if (e->row_fixed) {
+                setattr(reinterpret_cast<const void*>(row_pass_fixed<T, FX>), e->smem_row);
+                return;
+            }
+        }
+        setattr(reinterpret_cast<const void*>(row_pass_kernel<T, 0>), e->smem_row);
     });
 }
 
@@ -532,7 +572,14 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
     auto* i1 = static_cast<cplx<T>*>(e->i1);
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
     with_size(P.npy, [&](auto fy) {
-        col_inverse_kernel<T, decltype(fy)::value><<<grid, kThreads, e->smem_col, e->stream>>>(P, st, i1, tw);
+        constexpr int FY = decltype(fy)::value;
+        if constexpr (FY != 0) {
+            if (e->col_fixed) {
+                col_inverse_fixed<T, FY><<<grid, kThreads, e->smem_col_inv, e->stream>>>(P, st, i1, tw);
+                return;
+            }
+        }
+        col_inverse_kernel<T, 0><<<grid, kThreads, e->smem_col, e->stream>>>(P, st, i1, tw);
     });
     check_cuda(cudaGetLastError(), "col_inverse launch");
 }
@@ -544,7 +591,16 @@ void launch_row(shhd_engine* e) {
     dim3 grid((P.npy + 1) / 2, P.batch);
     LaunchScope scope(e, 1, static_cast<double>(sizeof(cplx<T>)) * P.batch * (P.n_in + P.n_out) * static_cast<double>(P.hx) * P.npy);
     with_size(P.npx, [&](auto fx) {
-        row_pass_kernel<T, decltype(fx)::value><<<grid, kThreads, e->smem_row, e->stream>>>(
+        constexpr int FX = decltype(fx)::value;
+        if constexpr (FX != 0) {
+            if (e->row_fixed) {
+                row_pass_fixed<T, FX><<<grid, kThreads, e->smem_row, e->stream>>>(
+                    P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
+                    e->err_dev);
+                return;
+            }
+        }
+        row_pass_kernel<T, 0><<<grid, kThreads, e->smem_row, e->stream>>>(
             P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
             e->err_dev);
     });
@@ -565,9 +621,15 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
     with_size(P.npy, [&](auto fy) {
         constexpr int FY = decltype(fy)::value;
-        if (e->npos == 4) col_forward_kernel<T, 4, FY><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
-        else if (e->npos == 8) col_forward_kernel<T, 8, FY><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
-        else col_forward_kernel<T, 16, FY><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+        if constexpr (FY != 0) {
+            if (e->col_fixed) {
+                col_forward_fixed<T, FY><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+                return;
+            }
+        }
+        if (e->npos == 4) col_forward_kernel<T, 4, 0><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+        else if (e->npos == 8) col_forward_kernel<T, 8, 0><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
+        else col_forward_kernel<T, 16, 0><<<grid, kThreads, e->smem_col, e->stream>>>(P, A, tw);
     });
     check_cuda(cudaGetLastError(), "col_forward launch");
 }
@@ -754,8 +816,8 @@ void init_device(shhd_engine* e) {
         check_cuda(cudaMemsetAsync(e->ext_a, 0, e->state_elems * B * cs, e->stream), "memset");
         check_cuda(cudaMemsetAsync(e->ext_b, 0, e->state_elems * B * cs, e->stream), "memset");
     }
-    const auto twx = shared_table<T>(e->cfg.nx);
-    const auto twy = shared_table<T>(e->cfg.ny);
+    const auto twx = e->row_fixed ? stage_table<T>(e->cfg.nx) : twiddle_table<T>(e->cfg.nx);
+    const auto twy = e->col_fixed ? stage_table<T>(e->cfg.ny) : twiddle_table<T>(e->cfg.ny);
     e->tw_x = dalloc(e, twx.size() * cs);
     e->tw_y = dalloc(e, twy.size() * cs);
     check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");

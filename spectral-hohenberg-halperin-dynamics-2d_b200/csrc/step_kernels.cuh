@@ -314,6 +314,184 @@ __device__ __forceinline__ void j_noise(const StepPlan& P, int draw, uint64_t st
     oy = cmulmi(cadd(cscale(pxy, kx), cscale(pyy, ky)));
 }
 
+// ---------------------------------------------------------------------------
+// epilogue math shared by the column-forward kernels: one active mode at a time
+// ---------------------------------------------------------------------------
+struct ModeCtx {
+    int gx, ky;            // integer wave numbers
+    size_t pos;            // index of (field 0, gx, j) in the state arrays
+    uint32_t mode_id;      // Philox counter word
+    bool conj_line;        // kx = 0, ky < 0: conjugate of the |ky| draw
+    bool k_nonzero;
+};
+
+template <typename T>
+__device__ __forceinline__ ModeCtx mode_ctx(const StepPlan& P, size_t mbase, int tile, int w, int j) {
+    ModeCtx m;
+    m.ky = ky_of_j(j, P.nay);
+    m.gx = tile * P.W + w;
+    m.pos = mbase + static_cast<size_t>(w) * P.kyn + j;
+    m.conj_line = (m.gx == 0 && m.ky < 0);
+    const int aky = m.conj_line ? -m.ky : m.ky;
+    m.mode_id = static_cast<uint32_t>(m.gx) * static_cast<uint32_t>(P.nay) + static_cast<uint32_t>((aky % P.nay + P.nay) % P.nay);
+    m.k_nonzero = !(m.gx == 0 && m.ky == 0);
+    return m;
+}
+
+// accumulate one transformed product field into the group's RHS (coefficients
+// of the reference's spectral divergences, fcalculator.cc:244-272, 374-396, 475-492)
+template <typename T>
+__device__ __forceinline__ void accumulate_product(const StepPlan& P, int kind, int alpha, T kx, T kyv, cplx<T> v, cplx<T>& a0, cplx<T>& a1) {
+    switch (kind) {
+        case OUT_MU: {
+            const T m = static_cast<T>(P.mobility[alpha]);
+            a0 = cadd(a0, cscale(v, -m * (kx * kx + kyv * kyv)));
+            break;
+        }
+        case OUT_PSIVX: a0 = cadd(a0, cmulmi(cscale(v, kx))); break;
+        case OUT_PSIVY: a0 = cadd(a0, cmulmi(cscale(v, kyv))); break;
+        case OUT_GRAD: a0 = cadd(a0, v); break;
+        case OUT_VX: {
+            const T eta = static_cast<T>(P.eta), zeta = static_cast<T>(P.zeta);
+            a0 = cadd(a0, cscale(v, -((eta + zeta) * kx * kx + eta * kyv * kyv)));
+            a1 = cadd(a1, cscale(v, -(zeta * kx * kyv)));
+            break;
+        }
+        case OUT_VY: {
+            const T eta = static_cast<T>(P.eta), zeta = static_cast<T>(P.zeta);
+            a0 = cadd(a0, cscale(v, -(zeta * kx * kyv)));
+            a1 = cadd(a1, cscale(v, -(eta * kx * kx + (eta + zeta) * kyv * kyv)));
+            break;
+        }
+        case OUT_PXX: a0 = cadd(a0, cmulmi(cscale(v, kx))); break;
+        case OUT_PXY:
+            a0 = cadd(a0, cmulmi(cscale(v, kyv)));
+            a1 = cadd(a1, cmulmi(cscale(v, kx)));
+            break;
+        default: a1 = cadd(a1, cmulmi(cscale(v, kyv))); break;
+    }
+}
+
+// psi_alpha: det from the accumulated products plus the spectral terms, then
+// (unless det_mode) the stage update with noise; returns next (or det)
+template <typename T>
+__device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageArgs<T>& A, int alpha, const ModeCtx& m, T kx, T kyv,
+                                                cplx<T> acc, uint32_t member, size_t fstride, int b) {
+    using C = cplx<T>;
+    const int f = 1 + alpha;
+    const T k2 = kx * kx + kyv * kyv;
+    const C cur = A.cur[m.pos + f * fstride];
+    C det = czero<C>();
+    if (!P.psi_zero[alpha]) {
+        det = acc;
+        if (P.psi_linear[alpha]) {  // fcalculator.cc:152-187
+            const T mob = static_cast<T>(P.mobility[alpha]);
+            const T mu = static_cast<T>(P.mu_k0[alpha]) + static_cast<T>(P.mu_k2[alpha]) * k2 + static_cast<T>(P.mu_k4[alpha]) * k2 * k2;
+            det = cadd(det, cscale(cur, -mob * k2 * mu));
+        }
+        for (int s = 0; s < P.n_sine; ++s)
+            if (P.sine[s].field == f && P.sine[s].gx == m.gx && P.sine[s].ky == m.ky)
+                det = cadd(det, mk(static_cast<T>(P.sine[s].re), static_cast<T>(P.sine[s].im)));
+        if (P.grad_incomp[alpha]) {  // fcalculator.cc:790-806
+            const T r0 = static_cast<T>(1.0 / A.rho0[b]);
+            const C jxv = A.cur[m.pos + (P.nop + 1) * fstride];
+            const C jyv = A.cur[m.pos + (P.nop + 2) * fstride];
+            det = cadd(det, cadd(cscale(jxv, static_cast<T>(P.grad_ax[alpha]) * r0), cscale(jyv, static_cast<T>(P.grad_ay[alpha]) * r0)));
+        }
+    }
+    if (A.det_mode) return det;
+    const T beta = static_cast<T>(A.beta);
+    C sto = czero<C>();
+    if (P.external_noise) {
+        sto = A.ext_a[m.pos + f * fstride];
+        if (A.srk3) sto = cadd(sto, cscale(A.ext_b[m.pos + f * fstride], beta));
+    } else if (P.noise_psi[alpha] && m.k_nonzero) {
+        const T sigma = sqrt(static_cast<T>(P.psi_sig2[alpha]) * k2);
+        sto = psi_noise<T>(P, alpha, 0, A.step, member, m.mode_id, m.conj_line, sigma);
+        if (A.srk3) sto = cadd(sto, cscale(psi_noise<T>(P, alpha, 1, A.step, member, m.mode_id, m.conj_line, sigma), beta));
+    }
+    const C base = (A.wb != 0.0) ? A.base[m.pos + f * fstride] : czero<C>();
+    const C inner = cadd(cadd(cur, cscale(det, static_cast<T>(A.dt))), cscale(sto, static_cast<T>(A.sdt)));
+    return cadd(cscale(base, static_cast<T>(A.wb)), cscale(inner, static_cast<T>(A.wc)));
+}
+
+// momentum: det_j from the accumulated products plus pressure, incompressible
+// viscosity and sine forces; stage update with noise and (incompressible)
+// transverse projection.  Results replace a0 (jx) and a1 (jy).
+template <typename T>
+__device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const StageArgs<T>& A, const ModeCtx& m, T kx, T kyv, cplx<T>& a0,
+                                                  cplx<T>& a1, uint32_t member, size_t fstride, int b) {
+    using C = cplx<T>;
+    const int f_jx = P.nop + 1, f_jy = P.nop + 2;
+    const T k2 = kx * kx + kyv * kyv;
+    const C cjx = A.cur[m.pos + f_jx * fstride];
+    const C cjy = A.cur[m.pos + f_jy * fstride];
+    C djx = czero<C>(), djy = czero<C>();
+    if (!P.j_zero) {
+        djx = a0;
+        djy = a1;
+        if (P.cT2 != 0.0) {  // fcalculator.cc:276-300
+            const C ph = cscale(A.cur[m.pos], static_cast<T>(P.cT2));
+            djx = cadd(djx, cmulmi(cscale(ph, kx)));
+            djy = cadd(djy, cmulmi(cscale(ph, kyv)));
+        }
+        if (P.incomp_visc) {  // fcalculator.cc:302-341
+            const T r0 = static_cast<T>(1.0 / A.rho0[b]);
+            const T eta = static_cast<T>(P.eta);
+            const C vx = cscale(cjx, r0), vy = cscale(cjy, r0);
+            djx = csub(djx, cscale(cadd(cscale(vx, 2 * kx * kx + kyv * kyv), cscale(vy, kx * kyv)), eta));
+            djy = csub(djy, cscale(cadd(cscale(vx, kx * kyv), cscale(vy, kx * kx + 2 * kyv * kyv)), eta));
+        }
+        for (int s = 0; s < P.n_sine; ++s)
+            if (P.sine[s].gx == m.gx && P.sine[s].ky == m.ky) {
+                const C src = mk(static_cast<T>(P.sine[s].re), static_cast<T>(P.sine[s].im));
+                if (P.sine[s].field == f_jx) djx = cadd(djx, src);
+                else if (P.sine[s].field == f_jy) djy = cadd(djy, src);
+            }
+    }
+    if (A.det_mode) { a0 = djx; a1 = djy; return; }
+    const T beta = static_cast<T>(A.beta);
+    C sx = czero<C>(), sy = czero<C>();
+    if (P.external_noise) {
+        sx = A.ext_a[m.pos + f_jx * fstride];
+        sy = A.ext_a[m.pos + f_jy * fstride];
+        if (A.srk3) {
+            sx = cadd(sx, cscale(A.ext_b[m.pos + f_jx * fstride], beta));
+            sy = cadd(sy, cscale(A.ext_b[m.pos + f_jy * fstride], beta));
+        }
+    } else if (P.noise_j && m.k_nonzero) {
+        j_noise<T>(P, 0, A.step, member, m.mode_id, m.conj_line, kx, kyv, sx, sy);
+        if (A.srk3) {
+            C bx, by;
+            j_noise<T>(P, 1, A.step, member, m.mode_id, m.conj_line, kx, kyv, bx, by);
+            sx = cadd(sx, cscale(bx, beta));
+            sy = cadd(sy, cscale(by, beta));
+        }
+    }
+    const T dt = static_cast<T>(A.dt), sdt = static_cast<T>(A.sdt), wb = static_cast<T>(A.wb), wc = static_cast<T>(A.wc);
+    const C bjx = (A.wb != 0.0) ? A.base[m.pos + f_jx * fstride] : czero<C>();
+    const C bjy = (A.wb != 0.0) ? A.base[m.pos + f_jy * fstride] : czero<C>();
+    C incx = cadd(cscale(djx, dt), cscale(sx, sdt));
+    C incy = cadd(cscale(djy, dt), cscale(sy, sdt));
+    if (P.mode == 1 && k2 != T(0)) {  // transverse projection (srk3_incompressible.h:81-96)
+        const C tr = cadd(cscale(incx, -kyv), cscale(incy, kx));
+        incx = cscale(cscale(tr, -kyv), T(1) / k2);
+        incy = cscale(cscale(tr, kx), T(1) / k2);
+    }
+    a0 = cadd(cscale(bjx, wb), cscale(cadd(cjx, incx), wc));
+    a1 = cadd(cscale(bjy, wb), cscale(cadd(cjy, incy), wc));
+}
+
+// rho: rho_det (fcalculator.cc:60-84) and its stage update
+template <typename T>
+__device__ __forceinline__ cplx<T> rho_epilogue(const StepPlan& P, const StageArgs<T>& A, size_t pos, T kx, T kyv, size_t fstride) {
+    using C = cplx<T>;
+    const C drho = cmulmi(cadd(cscale(A.cur[pos + (P.nop + 1) * fstride], kx), cscale(A.cur[pos + (P.nop + 2) * fstride], kyv)));
+    if (A.det_mode) return drho;
+    const C base = (A.wb != 0.0) ? A.base[pos] : czero<C>();
+    return cadd(cscale(base, static_cast<T>(A.wb)), cscale(cadd(A.cur[pos], cscale(drho, static_cast<T>(A.dt))), static_cast<T>(A.wc)));
+}
+
 template <typename T, int NPOS, int FY>
 __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P, const StageArgs<T> A, const cplx<T>* __restrict__ tw) {
     using C = cplx<T>;
@@ -328,7 +506,7 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
     const int gkind = P.group_kind[grp];
     const int alpha = P.group_alpha[grp];
     const int nop = P.nop;
-    const bool comp = (P.mode == 0), incomp = (P.mode == 1);
+    const bool comp = (P.mode == 0);
     const uint32_t member = P.member_offset + b;
     load_table(s_tw, tw, P.twy_count);
 
@@ -367,42 +545,13 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
                 const C v = buf[sw(y, mask) * W + w];
                 const T kx = kxu * static_cast<T>(tile * W + w);
                 const T kyv = kyu * static_cast<T>(ky);
-                switch (kind) {
-                    case OUT_MU: {  // -M k^2 mu_hat (fcalculator.cc:244-257)
-                        const T m = static_cast<T>(P.mobility[alpha]);
-                        acc0[i] = cadd(acc0[i], cscale(v, -m * (kx * kx + kyv * kyv)));
-                        break;
-                    }
-                    case OUT_PSIVX: acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kx))); break;   // fcalculator.cc:260-272
-                    case OUT_PSIVY: acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kyv))); break;
-                    case OUT_GRAD: acc0[i] = cadd(acc0[i], v); break;                         // fcalculator.cc:831-833
-                    case OUT_VX: {  // compressible viscous stress (fcalculator.cc:374-396)
-                        const T eta = static_cast<T>(P.eta), zeta = static_cast<T>(P.zeta);
-                        acc0[i] = cadd(acc0[i], cscale(v, -((eta + zeta) * kx * kx + eta * kyv * kyv)));
-                        acc1[i] = cadd(acc1[i], cscale(v, -(zeta * kx * kyv)));
-                        break;
-                    }
-                    case OUT_VY: {
-                        const T eta = static_cast<T>(P.eta), zeta = static_cast<T>(P.zeta);
-                        acc0[i] = cadd(acc0[i], cscale(v, -(zeta * kx * kyv)));
-                        acc1[i] = cadd(acc1[i], cscale(v, -(eta * kx * kx + (eta + zeta) * kyv * kyv)));
-                        break;
-                    }
-                    case OUT_PXX: acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kx))); break;     // fcalculator.cc:475-492
-                    case OUT_PXY:
-                        acc0[i] = cadd(acc0[i], cmulmi(cscale(v, kyv)));
-                        acc1[i] = cadd(acc1[i], cmulmi(cscale(v, kx)));
-                        break;
-                    default: acc1[i] = cadd(acc1[i], cmulmi(cscale(v, kyv))); break;
-                }
+                accumulate_product<T>(P, kind, alpha, kx, kyv, v, acc0[i], acc1[i]);
             }
         }
         __syncthreads();
     }
 
     // ---- epilogue: spectral terms, noise, stage update; results replace acc0/acc1 ----
-    const T dt = static_cast<T>(A.dt), sdt = static_cast<T>(A.sdt), wb = static_cast<T>(A.wb), wc = static_cast<T>(A.wc);
-    const T beta = static_cast<T>(A.beta);
     const int f_jx = nop + 1, f_jy = nop + 2;
 #pragma unroll
     for (int i = 0; i < NPOS; ++i) {
@@ -410,106 +559,11 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
         if (p >= npos_total) continue;
         const int w = fdiv(p, P.div_kyn);
         const int j = p - w * kyn;
-        const int ky = ky_of_j(j, nay);
-        const int gx = tile * W + w;
-        const T kx = kxu * static_cast<T>(gx);
-        const T kyv = kyu * static_cast<T>(ky);
-        const T k2 = kx * kx + kyv * kyv;
-        const size_t pos = mbase + static_cast<size_t>(w) * kyn + j;
-        const bool conj_line = (gx == 0 && ky < 0);
-        const uint32_t mode_id = static_cast<uint32_t>(gx) * static_cast<uint32_t>(nay) + static_cast<uint32_t>(((conj_line ? -ky : ky) % nay + nay) % nay);
-        const bool k_nonzero = !(gx == 0 && ky == 0);
-
-        if (gkind == GROUP_PSI) {
-            const int f = 1 + alpha;
-            const C cur = A.cur[pos + f * fstride];
-            C det = czero<C>();
-            if (!P.psi_zero[alpha]) {
-                det = acc0[i];
-                if (P.psi_linear[alpha]) {  // fcalculator.cc:152-187
-                    const T m = static_cast<T>(P.mobility[alpha]);
-                    const T mu = static_cast<T>(P.mu_k0[alpha]) + static_cast<T>(P.mu_k2[alpha]) * k2 + static_cast<T>(P.mu_k4[alpha]) * k2 * k2;
-                    det = cadd(det, cscale(cur, -m * k2 * mu));
-                }
-                for (int s = 0; s < P.n_sine; ++s)
-                    if (P.sine[s].field == f && P.sine[s].gx == gx && P.sine[s].ky == ky)
-                        det = cadd(det, mk(static_cast<T>(P.sine[s].re), static_cast<T>(P.sine[s].im)));
-                if (P.grad_incomp[alpha]) {  // fcalculator.cc:790-806
-                    const T r0 = static_cast<T>(1.0 / A.rho0[b]);
-                    const C jxv = A.cur[pos + f_jx * fstride];
-                    const C jyv = A.cur[pos + f_jy * fstride];
-                    det = cadd(det, cadd(cscale(jxv, static_cast<T>(P.grad_ax[alpha]) * r0), cscale(jyv, static_cast<T>(P.grad_ay[alpha]) * r0)));
-                }
-            }
-            if (A.det_mode) { acc0[i] = det; continue; }
-            C sto = czero<C>();
-            if (P.external_noise) {
-                sto = A.ext_a[pos + f * fstride];
-                if (A.srk3) sto = cadd(sto, cscale(A.ext_b[pos + f * fstride], beta));
-            } else if (P.noise_psi[alpha] && k_nonzero) {
-                const T sigma = sqrt(static_cast<T>(P.psi_sig2[alpha]) * k2);
-                sto = psi_noise<T>(P, alpha, 0, A.step, member, mode_id, conj_line, sigma);
-                if (A.srk3) sto = cadd(sto, cscale(psi_noise<T>(P, alpha, 1, A.step, member, mode_id, conj_line, sigma), beta));
-            }
-            const C base = (A.wb != 0.0) ? A.base[pos + f * fstride] : czero<C>();
-            const C inner = cadd(cadd(cur, cscale(det, dt)), cscale(sto, sdt));
-            acc0[i] = cadd(cscale(base, wb), cscale(inner, wc));
-        } else {
-            const C cjx = A.cur[pos + f_jx * fstride];
-            const C cjy = A.cur[pos + f_jy * fstride];
-            C djx = czero<C>(), djy = czero<C>();
-            if (!P.j_zero) {
-                djx = acc0[i];
-                djy = acc1[i];
-                if (P.cT2 != 0.0) {  // fcalculator.cc:276-300
-                    const C ph = cscale(A.cur[pos], static_cast<T>(P.cT2));
-                    djx = cadd(djx, cmulmi(cscale(ph, kx)));
-                    djy = cadd(djy, cmulmi(cscale(ph, kyv)));
-                }
-                if (P.incomp_visc) {  // fcalculator.cc:302-341
-                    const T r0 = static_cast<T>(1.0 / A.rho0[b]);
-                    const T eta = static_cast<T>(P.eta);
-                    const C vx = cscale(cjx, r0), vy = cscale(cjy, r0);
-                    djx = csub(djx, cscale(cadd(cscale(vx, 2 * kx * kx + kyv * kyv), cscale(vy, kx * kyv)), eta));
-                    djy = csub(djy, cscale(cadd(cscale(vx, kx * kyv), cscale(vy, kx * kx + 2 * kyv * kyv)), eta));
-                }
-                for (int s = 0; s < P.n_sine; ++s)
-                    if (P.sine[s].gx == gx && P.sine[s].ky == ky) {
-                        const C src = mk(static_cast<T>(P.sine[s].re), static_cast<T>(P.sine[s].im));
-                        if (P.sine[s].field == f_jx) djx = cadd(djx, src);
-                        else if (P.sine[s].field == f_jy) djy = cadd(djy, src);
-                    }
-            }
-            if (A.det_mode) { acc0[i] = djx; acc1[i] = djy; continue; }
-            C sx = czero<C>(), sy = czero<C>();
-            if (P.external_noise) {
-                sx = A.ext_a[pos + f_jx * fstride];
-                sy = A.ext_a[pos + f_jy * fstride];
-                if (A.srk3) {
-                    sx = cadd(sx, cscale(A.ext_b[pos + f_jx * fstride], beta));
-                    sy = cadd(sy, cscale(A.ext_b[pos + f_jy * fstride], beta));
-                }
-            } else if (P.noise_j && k_nonzero) {
-                j_noise<T>(P, 0, A.step, member, mode_id, conj_line, kx, kyv, sx, sy);
-                if (A.srk3) {
-                    C bx, by;
-                    j_noise<T>(P, 1, A.step, member, mode_id, conj_line, kx, kyv, bx, by);
-                    sx = cadd(sx, cscale(bx, beta));
-                    sy = cadd(sy, cscale(by, beta));
-                }
-            }
-            const C bjx = (A.wb != 0.0) ? A.base[pos + f_jx * fstride] : czero<C>();
-            const C bjy = (A.wb != 0.0) ? A.base[pos + f_jy * fstride] : czero<C>();
-            C incx = cadd(cscale(djx, dt), cscale(sx, sdt));
-            C incy = cadd(cscale(djy, dt), cscale(sy, sdt));
-            if (incomp && k2 != T(0)) {  // transverse projection (srk3_incompressible.h:81-96)
-                const C tr = cadd(cscale(incx, -kyv), cscale(incy, kx));
-                incx = cscale(cscale(tr, -kyv), T(1) / k2);
-                incy = cscale(cscale(tr, kx), T(1) / k2);
-            }
-            acc0[i] = cadd(cscale(bjx, wb), cscale(cadd(cjx, incx), wc));
-            acc1[i] = cadd(cscale(bjy, wb), cscale(cadd(cjy, incy), wc));
-        }
+        const ModeCtx m = mode_ctx<T>(P, mbase, tile, w, j);
+        const T kx = kxu * static_cast<T>(m.gx);
+        const T kyv = kyu * static_cast<T>(m.ky);
+        if (gkind == GROUP_PSI) acc0[i] = psi_epilogue<T>(P, A, alpha, m, kx, kyv, acc0[i], member, fstride, b);
+        else momentum_epilogue<T>(P, A, m, kx, kyv, acc0[i], acc1[i], member, fstride, b);
     }
 
     // ---- which fields this CTA writes, in order: psi | (rho), jx, jy ----
@@ -533,13 +587,9 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
                 const int ky = ky_of_j(j, nay);
                 const int y = ky >= 0 ? ky : ky + npy;
                 C v;
-                if (f == 0) {  // rho: rho_det (fcalculator.cc:60-84) and its stage update
+                if (f == 0) {
                     const size_t pos = mbase + static_cast<size_t>(w) * kyn + j;
-                    const T kx = kxu * static_cast<T>(tile * W + w);
-                    const T kyv = kyu * static_cast<T>(ky);
-                    const C drho = cmulmi(cadd(cscale(A.cur[pos + f_jx * fstride], kx), cscale(A.cur[pos + f_jy * fstride], kyv)));
-                    if (A.det_mode) v = drho;
-                    else v = cadd(cscale((A.wb != 0.0) ? A.base[pos] : czero<C>(), wb), cscale(cadd(A.cur[pos], cscale(drho, dt)), wc));
+                    v = rho_epilogue<T>(P, A, pos, kxu * static_cast<T>(tile * W + w), kyu * static_cast<T>(ky), fstride);
                 } else {
                     v = (f == f_jy) ? acc1[i] : acc0[i];
                 }

@@ -1,0 +1,362 @@
+// Step kernels for the compile-time transform sizes (3 * 2^k padded grids).
+//
+// Same three passes and the same epilogue math as step_kernels.cuh, organised
+// for throughput: a transform line belongs to one group of G threads (one or
+// more warps) that synchronises on its own named barrier, stages its
+// butterflies in registers and transforms the line in place (no ping-pong
+// buffer).  The row pass keeps one line per group in flight; the column pass
+// gives each of the tile's W columns to one group and keeps the RHS
+// accumulators in shared memory.  Twiddles are read through the read-only
+// cache from the per-stage rows in global memory.
+#pragma once
+
+#include "step_kernels.cuh"
+
+namespace shhd {
+
+// threads per transform group for a line of N complex values: about 24 staged
+// values per thread in the widest stage
+template <typename T, int N>
+__host__ __device__ constexpr int row_group() {
+    constexpr int g = (sizeof(T) == 4 ? N / 24 : N / 12);
+    return g <= 32 ? 32 : (g <= 64 ? 64 : (g <= 128 ? 128 : 256));
+}
+// column tile width for the compile-time column kernels (columns per CTA, one group each)
+template <typename T, int N>
+__host__ __device__ constexpr int col_width() {
+    constexpr int w = (sizeof(T) == 4 ? 4096 : 2048) / N;
+    return w >= 8 ? 8 : (w >= 4 ? 4 : (w >= 2 ? 2 : 1));
+}
+
+__device__ __forceinline__ uint32_t sw7(uint32_t y) { return y ^ ((y >> 3) & 7u); }
+
+template <int G>
+__device__ __forceinline__ void group_sync(int bid) {
+    if constexpr (G == 32) __syncwarp();
+    else if constexpr (G == kThreads) __syncthreads();
+    else asm volatile("bar.sync %0, %1;" ::"r"(bid), "n"(G) : "memory");
+}
+
+// one in-place stage of a group transform of a line (element y at sw7(y))
+template <int N, int R, int P, int TWOFF, int G, int DIR, typename C>
+__device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt, int bid) {
+    constexpr int NR = N / R;
+    constexpr int B = (NR + G - 1) / G;
+    constexpr int ROW = tw_row(R);
+    C v[B][R];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int bi = gt + i * G;
+        if (NR % G == 0 || bi < NR) {
+            if constexpr (NR % 64 == 0) {
+                const uint32_t s0 = sw7(bi);
+#pragma unroll
+                for (int q = 0; q < R; ++q) v[i][q] = line[s0 + q * NR];
+            } else {
+#pragma unroll
+                for (int q = 0; q < R; ++q) v[i][q] = line[sw7(bi + q * NR)];
+            }
+        }
+    }
+    group_sync<G>(bid);
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int bi = gt + i * G;
+        if (NR % G == 0 || bi < NR) {
+            const int k = bi % P;
+            if constexpr (P > 1) {
+                const C* t = tw + TWOFF + k * ROW;
+#pragma unroll
+                for (int q = 1; q < R; ++q) {
+                    const C w = __ldg(t + q - 1);
+                    v[i][q] = DIR < 0 ? cmul(v[i][q], w) : cmulc(v[i][q], w);
+                }
+            }
+            bfly<R, DIR>(v[i]);
+            const int j = (bi - k) * R + k;
+            if constexpr (P % 64 == 0) {
+                const uint32_t s0 = sw7(j);
+#pragma unroll
+                for (int q = 0; q < R; ++q) line[s0 + q * P] = v[i][q];
+            } else {
+#pragma unroll
+                for (int q = 0; q < R; ++q) line[sw7(j + q * P)] = v[i][q];
+            }
+        }
+    }
+    group_sync<G>(bid);
+}
+
+template <int N, int G, int DIR, int S, typename C>
+__device__ __forceinline__ void gstages(C* line, const C* tw, int gt, int bid) {
+    constexpr CPlan cp = FixedPlan<N>::c;
+    if constexpr (S < cp.ns) {
+        gstage<N, cp.r[S], cp.p[S], cp.twoff[S], G, DIR>(line, tw, gt, bid);
+        gstages<N, G, DIR, S + 1>(line, tw, gt, bid);
+    }
+}
+
+// in-place transform of one line by the calling group; the caller has
+// synchronised the group (or CTA) after writing the line
+template <int N, int G, int DIR, typename C>
+__device__ __forceinline__ void gfft(C* line, const C* tw, int gt, int bid) {
+    gstages<N, G, DIR, 0>(line, tw, gt, bid);
+}
+
+// ---------------------------------------------------------------------------
+// column inverse (compile-time NY): state -> I1   (grid: tiles x n_in x batch)
+// ---------------------------------------------------------------------------
+template <typename T, int NY>
+__global__ void __launch_bounds__(kThreads) col_inverse_fixed(const StepPlan P, const cplx<T>* __restrict__ state, cplx<T>* __restrict__ i1,
+                                                              const cplx<T>* __restrict__ tw) {
+    using C = cplx<T>;
+    constexpr int W = col_width<T, NY>();
+    constexpr int G = kThreads / W;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tile = reinterpret_cast<C*>(smem_raw);  // [W][NY]
+    const int g = threadIdx.x / G, gt = threadIdx.x - g * G, bid = 1 + g;
+    const int t = blockIdx.x, slot = blockIdx.y, b = blockIdx.z;
+    const int kyn = P.kyn, half = P.nay / 2;
+    const int field = P.in_field[slot];
+    const C* src = state + (static_cast<size_t>(b) * P.nfields + field) * P.hx * kyn + static_cast<size_t>(t) * W * kyn;
+    // column g: zero-padded copy (|ky| < Na/2 only)
+    C* line = tile + g * NY;
+    for (int y = gt; y < NY; y += G) {
+        int j = -1;
+        if (y < half) j = y;
+        else if (y > NY - half) j = y - NY + kyn;
+        line[sw7(y)] = (j >= 0) ? src[g * kyn + j] : czero<C>();
+    }
+    group_sync<G>(bid);
+    gfft<NY, G, +1>(line, tw, gt, bid);
+    __syncthreads();
+    const T sc = static_cast<T>(P.inv_scale);
+    C* dst = i1 + ((static_cast<size_t>(b) * P.n_in + slot) * P.ntiles + t) * static_cast<size_t>(NY) * W;
+    for (int e = threadIdx.x; e < W * NY; e += kThreads) {
+        const int y = e / W, w = e - y * W;
+        dst[e] = cscale(tile[w * NY + sw7(y)], sc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// row pass (compile-time NX): I1 -> C2R -> products -> R2C -> I2   (grid: row pairs x batch)
+// ---------------------------------------------------------------------------
+template <typename T, int NX>
+__global__ void __launch_bounds__(kThreads) row_pass_fixed(const StepPlan P, const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
+                                                           const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
+                                                           int* __restrict__ err) {
+    using C = cplx<T>;
+    constexpr int G = row_group<T, NX>();
+    constexpr int NG = kThreads / G;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* lines = reinterpret_cast<C*>(smem_raw);          // [n_in][NX] physical row pairs
+    C* work = lines + static_cast<size_t>(P.n_in) * NX;  // [NG][NX] one product line per group
+    const int g = threadIdx.x / G, gt = threadIdx.x - g * G, bid = 1 + g;
+    const int npy = P.npy, W = P.W, hx = P.hx;
+    const int pair = blockIdx.x, b = blockIdx.y;
+    const int y0 = 2 * pair;
+    const bool has1 = (y0 + 1) < npy;
+
+    // 1. inputs: Z[k] = X0[k] + i X1[k] with the Hermitian mirror, zero outside |kx| < Na/2
+    const size_t i1_member = static_cast<size_t>(b) * P.n_in * P.ntiles * npy * W;
+    for (int e = threadIdx.x; e < P.n_in * NX; e += kThreads) {
+        const int s = e / NX, k = e - s * NX;
+        C* z = lines + static_cast<size_t>(s) * NX;
+        if (k < hx) {
+            const C* src = i1 + i1_member + static_cast<size_t>(s) * P.ntiles * npy * W;
+            const int t = k >> P.logw, w = k & (W - 1);
+            const C* p0 = src + (static_cast<size_t>(t) * npy + y0) * W + w;
+            C a = p0[0];
+            C c = has1 ? p0[W] : czero<C>();
+            if (k == 0) { a.y = 0; c.y = 0; }  // C2R uses the real part of the kx = 0 entry
+            z[sw7(k)] = mk(a.x - c.y, a.y + c.x);
+            if (k > 0) z[sw7(NX - k)] = mk(a.x + c.y, c.x - a.y);
+        } else if (k <= NX - hx) {
+            z[sw7(k)] = czero<C>();
+        }
+    }
+    __syncthreads();
+    for (int s = g; s < P.n_in; s += NG) gfft<NX, G, +1>(lines + static_cast<size_t>(s) * NX, tw, gt, bid);
+    __syncthreads();
+
+    // 2. velocity: v = j / rho (compressible) or j / rho0 (fcalculator_workspace.cc:115-142);
+    //    pointwise work runs over swizzled slots (every line shares the permutation)
+    const int s_rho = P.in_slot[0];
+    const int s_jx = P.in_slot[P.nop + 1];
+    const int s_jy = P.in_slot[P.nop + 2];
+    const bool comp = (P.mode == 0);
+    const T inv_rho0 = (P.need_v && !comp) ? static_cast<T>(1.0 / rho0_member[b]) : T(0);
+    if (P.need_v && comp) {
+        int bad = 0;
+        for (int x = threadIdx.x; x < NX; x += kThreads) {
+            const C rho = lines[static_cast<size_t>(s_rho) * NX + x];
+            if (rho.x == T(0) || (has1 && rho.y == T(0))) bad = 1;
+        }
+        if (bad) atomicOr(err, ERR_ZERO_DENSITY);
+    }
+
+    // 3. products -> forward transform -> keep kx < Hx; output o belongs to group o % NG
+    const size_t i2_member = static_cast<size_t>(b) * P.n_out * P.ntiles * npy * W;
+    C* z = work + static_cast<size_t>(g) * NX;
+    for (int o = g; o < P.n_out; o += NG) {
+        const int kind = P.out_kind[o], arg = P.out_arg[o];
+        const int s_psi = (kind == OUT_MU || kind == OUT_PSIVX || kind == OUT_PSIVY) ? P.in_slot[1 + arg] : -1;
+        const bool use_v = (kind != OUT_MU);
+        for (int x = gt; x < NX; x += G) {
+            const C psi = s_psi >= 0 ? lines[static_cast<size_t>(s_psi) * NX + x] : czero<C>();
+            C jx = czero<C>(), jy = czero<C>(), vx = czero<C>(), vy = czero<C>();
+            if (use_v) {
+                jx = lines[static_cast<size_t>(s_jx) * NX + x];
+                jy = lines[static_cast<size_t>(s_jy) * NX + x];
+                if (comp) {
+                    const C rho = lines[static_cast<size_t>(s_rho) * NX + x];
+                    vx = mk(jx.x / rho.x, jx.y / rho.y);
+                    vy = mk(jy.x / rho.x, jy.y / rho.y);
+                } else {
+                    vx = mk(jx.x * inv_rho0, jx.y * inv_rho0);
+                    vy = mk(jy.x * inv_rho0, jy.y * inv_rho0);
+                }
+            }
+            C val = mk(product_value<T>(P, kind, arg, psi.x, jx.x, jy.x, vx.x, vy.x),
+                       product_value<T>(P, kind, arg, psi.y, jx.y, jy.y, vx.y, vy.y));
+            if (!has1) val.y = T(0);
+            z[x] = val;
+        }
+        group_sync<G>(bid);
+        gfft<NX, G, -1>(z, tw, gt, bid);
+        C* dst = i2 + i2_member + static_cast<size_t>(o) * P.ntiles * npy * W;
+        for (int k = gt; k < hx; k += G) {
+            const C zk = z[sw7(k)];
+            const C zn = cconj(z[sw7(k == 0 ? 0 : NX - k)]);
+            const C g0 = mk(static_cast<T>(0.5) * (zk.x + zn.x), static_cast<T>(0.5) * (zk.y + zn.y));
+            const C d = csub(zk, zn);
+            const C g1 = mk(static_cast<T>(0.5) * d.y, static_cast<T>(-0.5) * d.x);
+            const int t = k >> P.logw, w = k & (W - 1);
+            C* q = dst + (static_cast<size_t>(t) * npy + y0) * W + w;
+            q[0] = g0;
+            if (has1) q[W] = g1;
+        }
+        group_sync<G>(bid);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// column forward + epilogue (compile-time NY)   (grid: tiles x groups x batch)
+// ---------------------------------------------------------------------------
+template <typename T, int NY>
+__global__ void __launch_bounds__(kThreads) col_forward_fixed(const StepPlan P, const StageArgs<T> A, const cplx<T>* __restrict__ tw) {
+    using C = cplx<T>;
+    constexpr int W = col_width<T, NY>();
+    constexpr int G = kThreads / W;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int kyn = P.kyn, nay = P.nay;
+    C* tile = reinterpret_cast<C*>(smem_raw);   // [W][NY]
+    C* acc0 = tile + W * NY;                     // [W][Ky]
+    C* acc1 = acc0 + W * kyn;                    // [W][Ky]
+    const int g = threadIdx.x / G, gt = threadIdx.x - g * G, bid = 1 + g;
+    const int t = blockIdx.x, grp = blockIdx.y, b = blockIdx.z;
+    const int gkind = P.group_kind[grp];
+    const int alpha = P.group_alpha[grp];
+    const bool comp = (P.mode == 0);
+    const uint32_t member = P.member_offset + b;
+    const size_t fstride = static_cast<size_t>(P.hx) * kyn;
+    const size_t mbase = static_cast<size_t>(b) * P.nfields * fstride + static_cast<size_t>(t) * W * kyn;
+    const T kxu = static_cast<T>(P.kx_unit), kyu = static_cast<T>(P.ky_unit);
+    C* line = tile + g * NY;
+    C* a0 = acc0 + g * kyn;
+    C* a1 = acc1 + g * kyn;
+    const T kx = kxu * static_cast<T>(t * W + g);
+
+    for (int j = gt; j < kyn; j += G) { a0[j] = czero<C>(); a1[j] = czero<C>(); }
+
+    const int ngo = P.group_nout[grp];
+    for (int go = 0; go < ngo; ++go) {
+        const int o = P.group_out[grp][go];
+        const C* src = A.i2 + ((static_cast<size_t>(b) * P.n_out + o) * P.ntiles + t) * static_cast<size_t>(NY) * W;
+        __syncthreads();  // every group is done with the previous tile
+        for (int e = threadIdx.x; e < W * NY; e += kThreads) {
+            const int y = e / W, w = e - y * W;
+            tile[w * NY + sw7(y)] = src[e];
+        }
+        __syncthreads();
+        gfft<NY, G, -1>(line, tw, gt, bid);
+        const int kind = P.out_kind[o];
+        for (int j = gt; j < kyn; j += G) {
+            const int ky = ky_of_j(j, nay);
+            const int y = ky >= 0 ? ky : ky + NY;
+            C u0 = a0[j], u1 = a1[j];
+            accumulate_product<T>(P, kind, alpha, kx, kyu * static_cast<T>(ky), line[sw7(y)], u0, u1);
+            a0[j] = u0;
+            a1[j] = u1;
+        }
+    }
+
+    // epilogue for column g: results replace a0 (psi or jx) and a1 (jy)
+    for (int j = gt; j < kyn; j += G) {
+        const ModeCtx m = mode_ctx<T>(P, mbase, t, g, j);
+        const T kyv = kyu * static_cast<T>(m.ky);
+        if (gkind == GROUP_PSI) {
+            a0[j] = psi_epilogue<T>(P, A, alpha, m, kx, kyv, a0[j], member, fstride, b);
+        } else {
+            C u0 = a0[j], u1 = a1[j];
+            momentum_epilogue<T>(P, A, m, kx, kyv, u0, u1, member, fstride, b);
+            a0[j] = u0;
+            a1[j] = u1;
+        }
+    }
+
+    int nwf = 0;
+    int wfield[3];
+    if (gkind == GROUP_PSI) { wfield[nwf++] = 1 + alpha; }
+    else { if (comp) wfield[nwf++] = 0; wfield[nwf++] = P.nop + 1; wfield[nwf++] = P.nop + 2; }
+    for (int q = 0; q < nwf; ++q) {
+        const int f = wfield[q];
+        __syncthreads();  // previous field's I1 copy-out is done
+        for (int y = gt; y < NY; y += G) line[y] = czero<C>();
+        group_sync<G>(bid);
+        C* dst = A.next + mbase + static_cast<size_t>(f) * fstride + static_cast<size_t>(g) * kyn;
+        for (int j = gt; j < kyn; j += G) {
+            const int ky = ky_of_j(j, nay);
+            const int y = ky >= 0 ? ky : ky + NY;
+            C v;
+            if (f == 0) v = rho_epilogue<T>(P, A, mbase + static_cast<size_t>(g) * kyn + j, kx, kyu * static_cast<T>(ky), fstride);
+            else v = (f == P.nop + 2) ? a1[j] : a0[j];
+            line[sw7(y)] = v;
+        }
+        group_sync<G>(bid);
+        // real-symmetry projection of the kx = 0 line (time_integrator.h:70-109)
+        if (t == 0 && g == 0 && !A.det_mode) {
+            for (int ky = gt; ky < nay / 2; ky += G) {
+                if (ky == 0) {
+                    line[0].y = T(0);
+                } else {
+                    C* pa = line + sw7(ky);
+                    C* pc = line + sw7(NY - ky);
+                    const C av = *pa, cv = *pc;
+                    const C pj = mk(static_cast<T>(0.5) * (av.x + cv.x), static_cast<T>(0.5) * (av.y - cv.y));
+                    *pa = pj;
+                    *pc = cconj(pj);
+                }
+            }
+            group_sync<G>(bid);
+        }
+        for (int j = gt; j < kyn; j += G) {
+            const int ky = ky_of_j(j, nay);
+            dst[j] = line[sw7(ky >= 0 ? ky : ky + NY)];
+        }
+        const int slot = P.in_slot[f];
+        if (A.fused_inverse && slot >= 0) {
+            group_sync<G>(bid);
+            gfft<NY, G, +1>(line, tw, gt, bid);
+            __syncthreads();
+            const T sc = static_cast<T>(P.inv_scale);
+            C* o1 = A.i1_next + ((static_cast<size_t>(b) * P.n_in + slot) * P.ntiles + t) * static_cast<size_t>(NY) * W;
+            for (int e = threadIdx.x; e < W * NY; e += kThreads) {
+                const int y = e / W, w = e - y * W;
+                o1[e] = cscale(tile[w * NY + sw7(y)], sc);
+            }
+        }
+    }
+}
+
+}  // namespace shhd
