@@ -57,13 +57,14 @@ template <> struct BoxMuller<double> {
 
 template <> struct BoxMuller<float> {
     __device__ __forceinline__ static float2 apply(const Philox4& r) {
-        const uint64_t a = ((static_cast<uint64_t>(r.w1) << 32) | r.w0) >> 11;
-        const uint64_t b = ((static_cast<uint64_t>(r.w3) << 32) | r.w2) >> 11;
-        const float u1 = static_cast<float>((static_cast<double>(a) + 0.5) * (1.0 / 9007199254740992.0));
-        const float u2 = static_cast<float>((static_cast<double>(b) + 0.5) * (1.0 / 9007199254740992.0));
-        const float rad = sqrtf(-2.0f * logf(u1));
+        // the FP64 path's 53-bit uniforms to FP32 accuracy: their top 32 bits
+        // are w1 and w3; fast hardware log / sin / cos (absolute error ~1e-6,
+        // far below the FP32 path's tolerance) keep the draw cheap
+        const float u1 = __uint2float_rn(r.w1) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
+        const float u2 = __uint2float_rn(r.w3) * 2.3283064365386963e-10f + 1.1641532182693481e-10f;
+        const float rad = sqrtf(-2.0f * __logf(u1));
         float s, c;
-        sincospif(2.0f * u2, &s, &c);
+        __sincosf(6.28318530717958647692f * u2, &s, &c);
         return make_float2(rad * c, rad * s);
     }
 };

@@ -78,6 +78,17 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
                 const uint32_t s0 = sw7(j);
 #pragma unroll
                 for (int q = 0; q < R; ++q) line[s0 + q * P] = v[i][q];
+            } else if constexpr (R == 8 && P == 1) {
+                // j = 8 bi: sw7(j + q) = 8 bi + (q ^ (bi & 7))
+                C* o = line + 8 * bi;
+                const uint32_t m = bi & 7;
+#pragma unroll
+                for (int q = 0; q < R; ++q) o[q ^ m] = v[i][q];
+            } else if constexpr (R == 8 && P == 8) {
+                // j = 64 (bi >> 3) + k: sw7(j + 8 q) = 64 (bi >> 3) + 8 q + (k ^ q)
+                C* o = line + 64 * (bi >> 3);
+#pragma unroll
+                for (int q = 0; q < R; ++q) o[8 * q + (k ^ q)] = v[i][q];
             } else {
 #pragma unroll
                 for (int q = 0; q < R; ++q) line[sw7(j + q * P)] = v[i][q];
@@ -101,6 +112,30 @@ __device__ __forceinline__ void gstages(C* line, const C* tw, int gt, int bid) {
 template <int N, int G, int DIR, typename C>
 __device__ __forceinline__ void gfft(C* line, const C* tw, int gt, int bid) {
     gstages<N, G, DIR, 0>(line, tw, gt, bid);
+}
+
+// contiguous [y][w] tile (global) -> [w][sw7(y)] lines (shared); all loads of a
+// thread are issued before its stores so they overlap in flight
+template <int W, int NY, typename C>
+__device__ __forceinline__ void load_tile(C* tile, const C* __restrict__ src) {
+    constexpr int PER = (W * NY + kThreads - 1) / kThreads;
+    constexpr int CH = PER < 12 ? PER : 12;
+    for (int e0 = 0; e0 < PER; e0 += CH) {
+        C v[CH];
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int e = threadIdx.x + (e0 + u) * kThreads;
+            if ((W * NY) % kThreads == 0 || e < W * NY) v[u] = src[e];
+        }
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int e = threadIdx.x + (e0 + u) * kThreads;
+            if ((W * NY) % kThreads == 0 || e < W * NY) {
+                const int y = e / W, w = e - y * W;
+                tile[w * NY + sw7(y)] = v[u];
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -142,7 +177,7 @@ __global__ void __launch_bounds__(kThreads) col_inverse_fixed(const StepPlan P, 
 // row pass (compile-time NX): I1 -> C2R -> products -> R2C -> I2   (grid: row pairs x batch)
 // ---------------------------------------------------------------------------
 template <typename T, int NX>
-__global__ void __launch_bounds__(kThreads) row_pass_fixed(const StepPlan P, const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
+__global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
                                                            const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
                                                            int* __restrict__ err) {
     using C = cplx<T>;
@@ -157,23 +192,42 @@ __global__ void __launch_bounds__(kThreads) row_pass_fixed(const StepPlan P, con
     const int y0 = 2 * pair;
     const bool has1 = (y0 + 1) < npy;
 
-    // 1. inputs: Z[k] = X0[k] + i X1[k] with the Hermitian mirror, zero outside |kx| < Na/2
+    // 1. inputs: Z[k] = X0[k] + i X1[k] with the Hermitian mirror, zero outside |kx| < Na/2;
+    //    loads are issued in batches of 4 per thread so several are in flight
     const size_t i1_member = static_cast<size_t>(b) * P.n_in * P.ntiles * npy * W;
-    for (int e = threadIdx.x; e < P.n_in * NX; e += kThreads) {
-        const int s = e / NX, k = e - s * NX;
-        C* z = lines + static_cast<size_t>(s) * NX;
-        if (k < hx) {
-            const C* src = i1 + i1_member + static_cast<size_t>(s) * P.ntiles * npy * W;
-            const int t = k >> P.logw, w = k & (W - 1);
-            const C* p0 = src + (static_cast<size_t>(t) * npy + y0) * W + w;
-            C a = p0[0];
-            C c = has1 ? p0[W] : czero<C>();
-            if (k == 0) { a.y = 0; c.y = 0; }  // C2R uses the real part of the kx = 0 entry
-            z[sw7(k)] = mk(a.x - c.y, a.y + c.x);
-            if (k > 0) z[sw7(NX - k)] = mk(a.x + c.y, c.x - a.y);
-        } else if (k <= NX - hx) {
-            z[sw7(k)] = czero<C>();
+    const size_t slot_stride = static_cast<size_t>(P.ntiles) * npy * W;
+    const int nload = P.n_in * hx;
+    constexpr int U = 4;
+    for (int e0 = threadIdx.x; e0 < nload; e0 += kThreads * U) {
+        C a[U], c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * kThreads;
+            if (e < nload) {
+                const int s = e / hx, k = e - s * hx;
+                const int t = k >> P.logw, w = k & (W - 1);
+                const C* p0 = i1 + i1_member + s * slot_stride + (static_cast<size_t>(t) * npy + y0) * W + w;
+                a[u] = p0[0];
+                c[u] = has1 ? p0[W] : czero<C>();
+            }
         }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + u * kThreads;
+            if (e < nload) {
+                const int s = e / hx, k = e - s * hx;
+                C* z = lines + static_cast<size_t>(s) * NX;
+                C av = a[u], cv = c[u];
+                if (k == 0) { av.y = 0; cv.y = 0; }  // C2R uses the real part of the kx = 0 entry
+                z[sw7(k)] = mk(av.x - cv.y, av.y + cv.x);
+                if (k > 0) z[sw7(NX - k)] = mk(av.x + cv.y, cv.x - av.y);
+            }
+        }
+    }
+    const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
+    for (int e = threadIdx.x; e < P.n_in * nzero; e += kThreads) {
+        const int s = e / nzero, k = hx + (e - s * nzero);
+        lines[static_cast<size_t>(s) * NX + sw7(k)] = czero<C>();
     }
     __syncthreads();
     for (int s = g; s < P.n_in; s += NG) gfft<NX, G, +1>(lines + static_cast<size_t>(s) * NX, tw, gt, bid);
@@ -187,12 +241,16 @@ __global__ void __launch_bounds__(kThreads) row_pass_fixed(const StepPlan P, con
     const bool comp = (P.mode == 0);
     const T inv_rho0 = (P.need_v && !comp) ? static_cast<T>(1.0 / rho0_member[b]) : T(0);
     if (P.need_v && comp) {
+        // zero-density check, then rho is replaced by 1/rho (its only use is v = j / rho)
         int bad = 0;
         for (int x = threadIdx.x; x < NX; x += kThreads) {
-            const C rho = lines[static_cast<size_t>(s_rho) * NX + x];
+            C* pr = lines + static_cast<size_t>(s_rho) * NX + x;
+            const C rho = *pr;
             if (rho.x == T(0) || (has1 && rho.y == T(0))) bad = 1;
+            *pr = mk(T(1) / rho.x, has1 ? T(1) / rho.y : T(0));
         }
         if (bad) atomicOr(err, ERR_ZERO_DENSITY);
+        __syncthreads();
     }
 
     // 3. products -> forward transform -> keep kx < Hx; output o belongs to group o % NG
@@ -209,9 +267,9 @@ __global__ void __launch_bounds__(kThreads) row_pass_fixed(const StepPlan P, con
                 jx = lines[static_cast<size_t>(s_jx) * NX + x];
                 jy = lines[static_cast<size_t>(s_jy) * NX + x];
                 if (comp) {
-                    const C rho = lines[static_cast<size_t>(s_rho) * NX + x];
-                    vx = mk(jx.x / rho.x, jx.y / rho.y);
-                    vy = mk(jy.x / rho.x, jy.y / rho.y);
+                    const C ir = lines[static_cast<size_t>(s_rho) * NX + x];  // 1/rho
+                    vx = mk(jx.x * ir.x, jx.y * ir.y);
+                    vy = mk(jy.x * ir.x, jy.y * ir.y);
                 } else {
                     vx = mk(jx.x * inv_rho0, jx.y * inv_rho0);
                     vy = mk(jy.x * inv_rho0, jy.y * inv_rho0);
@@ -244,7 +302,7 @@ __global__ void __launch_bounds__(kThreads) row_pass_fixed(const StepPlan P, con
 // column forward + epilogue (compile-time NY)   (grid: tiles x groups x batch)
 // ---------------------------------------------------------------------------
 template <typename T, int NY>
-__global__ void __launch_bounds__(kThreads) col_forward_fixed(const StepPlan P, const StageArgs<T> A, const cplx<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(kThreads, 2) col_forward_fixed(const StepPlan P, const StageArgs<T> A, const cplx<T>* __restrict__ tw) {
     using C = cplx<T>;
     constexpr int W = col_width<T, NY>();
     constexpr int G = kThreads / W;
@@ -274,10 +332,7 @@ __global__ void __launch_bounds__(kThreads) col_forward_fixed(const StepPlan P, 
         const int o = P.group_out[grp][go];
         const C* src = A.i2 + ((static_cast<size_t>(b) * P.n_out + o) * P.ntiles + t) * static_cast<size_t>(NY) * W;
         __syncthreads();  // every group is done with the previous tile
-        for (int e = threadIdx.x; e < W * NY; e += kThreads) {
-            const int y = e / W, w = e - y * W;
-            tile[w * NY + sw7(y)] = src[e];
-        }
+        load_tile<W, NY>(tile, src);
         __syncthreads();
         gfft<NY, G, -1>(line, tw, gt, bid);
         const int kind = P.out_kind[o];
