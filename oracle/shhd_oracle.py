@@ -283,31 +283,32 @@ def philox4x32_10(c0, c1, c2, c3, k0: int, k1: int):
     return c0, c1, c2, c3
 
 
-def philox_normals(seed: int, member: int, step: int, stream: int, mode_id) -> np.ndarray:
-    """One complex standard normal per mode id (real and imaginary parts N(0,1)).
+def philox_normals(seed: int, member: int, step: int, stream: int, mode_id):
+    """The two complex standard normals (draws a and b) of one noise component per mode id.
 
     counter = (mode_id, stream, step_lo, step_hi), key = (seed, member);
-    u = (((w_hi << 32) | w_lo) >> 11 + 0.5) * 2^-53 for two 53-bit uniforms;
+    draw a from words (w0, w1), draw b from (w2, w3); u = (w + 1/2) 2^-32;
     Box-Muller: r = sqrt(-2 ln u1), theta = 2 pi u2.
     """
     step = int(step)
     w0, w1, w2, w3 = philox4x32_10(mode_id, stream, step & 0xFFFFFFFF, (step >> 32) & 0xFFFFFFFF, seed, member)
-    a = ((w1 << np.uint64(32)) | w0) >> np.uint64(11)
-    b = ((w3 << np.uint64(32)) | w2) >> np.uint64(11)
-    u1 = (a.astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
-    u2 = (b.astype(np.float64) + 0.5) * (1.0 / 9007199254740992.0)
-    r = np.sqrt(-2.0 * np.log(u1))
-    return r * np.cos(2.0 * math.pi * u2) + 1j * r * np.sin(2.0 * math.pi * u2)
+
+    def bm(wr, wt):
+        u1 = (wr.astype(np.float64) + 0.5) * 2.3283064365386963e-10
+        u2 = (wt.astype(np.float64) + 0.5) * 2.3283064365386963e-10
+        r = np.sqrt(-2.0 * np.log(u1))
+        return r * np.cos(2.0 * math.pi * u2) + 1j * r * np.sin(2.0 * math.pi * u2)
+
+    return bm(w0, w1), bm(w2, w3)
 
 
-# stream ids: bit 0 = draw (0 = a, 1 = b); psi component alpha -> alpha << 1,
-# momentum stress draws xi_1..xi_3 -> (4096 + m) << 1
-def psi_stream(alpha: int, draw: int) -> int:
-    return (alpha << 1) | draw
+# stream ids: psi component alpha -> alpha; momentum stress draws xi_1..xi_3 -> 4096 + m
+def psi_stream(alpha: int) -> int:
+    return alpha
 
 
-def j_stream(m: int, draw: int) -> int:
-    return ((4096 + m) << 1) | draw
+def j_stream(m: int) -> int:
+    return 4096 + m
 
 
 class PhysicalFields:
@@ -587,12 +588,15 @@ class Oracle:
         ky = np.where(g.gx == 0, np.abs(g.sgy), g.sgy)
         return (g.gx.astype(np.int64) * g.nay + np.mod(ky, g.nay)).astype(np.uint64)
 
-    def philox_noise(self, step: int, draw: int) -> np.ndarray:
+    def philox_noise(self, step: int):
+        """(sto_a, sto_b) of one step from the Philox scheme of the CUDA path."""
         cfg = self.cfg
         ids = self.mode_ids()
-        xp = [philox_normals(cfg.noise_seed, self.member, step, psi_stream(a, draw), ids) for a in range(cfg.num_order_parameters)]
-        xj = [philox_normals(cfg.noise_seed, self.member, step, j_stream(m, draw), ids) for m in range(3)]
-        return self.noise_from_normals(xp, xj)
+        xp = [philox_normals(cfg.noise_seed, self.member, step, psi_stream(a), ids) for a in range(cfg.num_order_parameters)]
+        xj = [philox_normals(cfg.noise_seed, self.member, step, j_stream(m), ids) for m in range(3)]
+        sa = self.noise_from_normals([x[0] for x in xp], [x[0] for x in xj])
+        sb = self.noise_from_normals([x[1] for x in xp], [x[1] for x in xj])
+        return sa, sb
 
     # --- symmetry (time_integrator.h:70-109) --------------------------------
     def enforce_real_symmetry(self, u: np.ndarray) -> np.ndarray:
@@ -655,8 +659,7 @@ class Oracle:
             zero = np.zeros(self.shape, dtype=np.complex128)
             sa, sb = zero, zero
         elif isinstance(noise, str):
-            sa = self.philox_noise(self.step_index, 0)
-            sb = self.philox_noise(self.step_index, 1) if cfg.integrator == "srk3" else None
+            sa, sb = self.philox_noise(self.step_index)
         else:
             sa = noise[0]
             sb = noise[1] if cfg.integrator == "srk3" else None

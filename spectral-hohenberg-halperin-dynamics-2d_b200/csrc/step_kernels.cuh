@@ -289,27 +289,34 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
 // ---------------------------------------------------------------------------
 // column forward + epilogue   (grid: tiles x groups x batch)
 // ---------------------------------------------------------------------------
+// psi_sto for both draws (fcalculator.cc:496-585): sigma * xi (conjugated on the kx = 0, ky < 0 half)
 template <typename T>
-__device__ __forceinline__ cplx<T> psi_noise(const StepPlan& P, int alpha, int draw, uint64_t step, uint32_t member, uint32_t mode_id,
-                                             bool conj_line, T sigma) {
-    cplx<T> xi = complex_normal<T>(P.seed, member, step, psi_stream(alpha, draw), mode_id);
-    if (conj_line) xi = cconj(xi);
-    return cscale(xi, sigma);
+__device__ __forceinline__ cplx<T> psi_noise(const StepPlan& P, int alpha, uint64_t step, uint32_t member, uint32_t mode_id, bool conj_line,
+                                             T sigma, bool srk3, T beta) {
+    cplx<T> xa, xb;
+    complex_normals<T>(P.seed, member, step, psi_stream(alpha), mode_id, srk3, xa, xb);
+    cplx<T> x = srk3 ? cadd(xa, cscale(xb, beta)) : xa;
+    if (conj_line) x = cconj(x);
+    return cscale(x, sigma);
 }
 
-// j_sto for one draw (fcalculator.cc:587-700): out = -i k . pi(xi)
+// j_sto for both draws (fcalculator.cc:587-700): out = -i k . pi(xi_a + beta xi_b)
 template <typename T>
-__device__ __forceinline__ void j_noise(const StepPlan& P, int draw, uint64_t step, uint32_t member, uint32_t mode_id, bool conj_line,
-                                        T kx, T ky, cplx<T>& ox, cplx<T>& oy) {
+__device__ __forceinline__ void j_noise(const StepPlan& P, uint64_t step, uint32_t member, uint32_t mode_id, bool conj_line, T kx, T ky,
+                                        bool srk3, T beta, cplx<T>& ox, cplx<T>& oy) {
     using C = cplx<T>;
-    C x1 = complex_normal<T>(P.seed, member, step, j_stream(0, draw), mode_id);
-    C x2 = complex_normal<T>(P.seed, member, step, j_stream(1, draw), mode_id);
-    C x3 = complex_normal<T>(P.seed, member, step, j_stream(2, draw), mode_id);
-    if (conj_line) { x1 = cconj(x1); x2 = cconj(x2); x3 = cconj(x3); }
+    C x[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        C xa, xb;
+        complex_normals<T>(P.seed, member, step, j_stream(m), mode_id, srk3, xa, xb);
+        x[m] = srk3 ? cadd(xa, cscale(xb, beta)) : xa;
+        if (conj_line) x[m] = cconj(x[m]);
+    }
     const T s = static_cast<T>(P.j_s), se = static_cast<T>(P.sqrt_eta), sz = static_cast<T>(P.sqrt_zeta);
-    const C pxx = mk(-s * (sz * x1.x + se * x2.x), -s * (sz * x1.y + se * x2.y));
-    const C pyy = mk(-s * (sz * x1.x - se * x2.x), -s * (sz * x1.y - se * x2.y));
-    const C pxy = mk(-s * se * x3.x, -s * se * x3.y);
+    const C pxx = mk(-s * (sz * x[0].x + se * x[1].x), -s * (sz * x[0].y + se * x[1].y));
+    const C pyy = mk(-s * (sz * x[0].x - se * x[1].x), -s * (sz * x[0].y - se * x[1].y));
+    const C pxy = mk(-s * se * x[2].x, -s * se * x[2].y);
     ox = cmulmi(cadd(cscale(pxx, kx), cscale(pxy, ky)));
     oy = cmulmi(cadd(cscale(pxy, kx), cscale(pyy, ky)));
 }
@@ -372,15 +379,41 @@ __device__ __forceinline__ void accumulate_product(const StepPlan& P, int kind, 
     }
 }
 
+// global inputs of one mode's epilogue, loaded ahead of the math so the next
+// mode's loads can be in flight while the current one is computed
+template <typename T>
+struct PsiLoads {
+    cplx<T> cur, base, ea, eb, jx, jy;
+};
+
+template <typename T>
+__device__ __forceinline__ PsiLoads<T> psi_loads(const StepPlan& P, const StageArgs<T>& A, int alpha, size_t pos, size_t fstride) {
+    using C = cplx<T>;
+    const int f = 1 + alpha;
+    PsiLoads<T> L;
+    L.cur = A.cur[pos + f * fstride];
+    L.base = (A.wb != 0.0 && !A.det_mode) ? A.base[pos + f * fstride] : czero<C>();
+    L.ea = (P.external_noise && !A.det_mode) ? A.ext_a[pos + f * fstride] : czero<C>();
+    L.eb = (P.external_noise && A.srk3 && !A.det_mode) ? A.ext_b[pos + f * fstride] : czero<C>();
+    if (P.grad_incomp[alpha] && !P.psi_zero[alpha]) {
+        L.jx = A.cur[pos + (P.nop + 1) * fstride];
+        L.jy = A.cur[pos + (P.nop + 2) * fstride];
+    } else {
+        L.jx = czero<C>();
+        L.jy = czero<C>();
+    }
+    return L;
+}
+
 // psi_alpha: det from the accumulated products plus the spectral terms, then
 // (unless det_mode) the stage update with noise; returns next (or det)
 template <typename T>
 __device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageArgs<T>& A, int alpha, const ModeCtx& m, T kx, T kyv,
-                                                cplx<T> acc, uint32_t member, size_t fstride, int b) {
+                                                cplx<T> acc, uint32_t member, const PsiLoads<T>& L, int b) {
     using C = cplx<T>;
     const int f = 1 + alpha;
     const T k2 = kx * kx + kyv * kyv;
-    const C cur = A.cur[m.pos + f * fstride];
+    const C cur = L.cur;
     C det = czero<C>();
     if (!P.psi_zero[alpha]) {
         det = acc;
@@ -394,25 +427,46 @@ __device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageAr
                 det = cadd(det, mk(static_cast<T>(P.sine[s].re), static_cast<T>(P.sine[s].im)));
         if (P.grad_incomp[alpha]) {  // fcalculator.cc:790-806
             const T r0 = static_cast<T>(1.0 / A.rho0[b]);
-            const C jxv = A.cur[m.pos + (P.nop + 1) * fstride];
-            const C jyv = A.cur[m.pos + (P.nop + 2) * fstride];
-            det = cadd(det, cadd(cscale(jxv, static_cast<T>(P.grad_ax[alpha]) * r0), cscale(jyv, static_cast<T>(P.grad_ay[alpha]) * r0)));
+            det = cadd(det, cadd(cscale(L.jx, static_cast<T>(P.grad_ax[alpha]) * r0), cscale(L.jy, static_cast<T>(P.grad_ay[alpha]) * r0)));
         }
     }
     if (A.det_mode) return det;
     const T beta = static_cast<T>(A.beta);
     C sto = czero<C>();
     if (P.external_noise) {
-        sto = A.ext_a[m.pos + f * fstride];
-        if (A.srk3) sto = cadd(sto, cscale(A.ext_b[m.pos + f * fstride], beta));
+        sto = L.ea;
+        if (A.srk3) sto = cadd(sto, cscale(L.eb, beta));
     } else if (P.noise_psi[alpha] && m.k_nonzero) {
         const T sigma = sqrt(static_cast<T>(P.psi_sig2[alpha]) * k2);
-        sto = psi_noise<T>(P, alpha, 0, A.step, member, m.mode_id, m.conj_line, sigma);
-        if (A.srk3) sto = cadd(sto, cscale(psi_noise<T>(P, alpha, 1, A.step, member, m.mode_id, m.conj_line, sigma), beta));
+        sto = psi_noise<T>(P, alpha, A.step, member, m.mode_id, m.conj_line, sigma, A.srk3 != 0, beta);
     }
-    const C base = (A.wb != 0.0) ? A.base[m.pos + f * fstride] : czero<C>();
     const C inner = cadd(cadd(cur, cscale(det, static_cast<T>(A.dt))), cscale(sto, static_cast<T>(A.sdt)));
-    return cadd(cscale(base, static_cast<T>(A.wb)), cscale(inner, static_cast<T>(A.wc)));
+    return cadd(cscale(L.base, static_cast<T>(A.wb)), cscale(inner, static_cast<T>(A.wc)));
+}
+
+template <typename T>
+struct MomLoads {
+    cplx<T> cjx, cjy, crho, bjx, bjy, eax, eay, ebx, eby;
+};
+
+template <typename T>
+__device__ __forceinline__ MomLoads<T> momentum_loads(const StepPlan& P, const StageArgs<T>& A, size_t pos, size_t fstride) {
+    using C = cplx<T>;
+    const int f_jx = P.nop + 1, f_jy = P.nop + 2;
+    const bool upd = !A.det_mode;
+    MomLoads<T> L;
+    L.cjx = A.cur[pos + f_jx * fstride];
+    L.cjy = A.cur[pos + f_jy * fstride];
+    L.crho = (P.cT2 != 0.0 && !P.j_zero) ? A.cur[pos] : czero<C>();
+    const bool wb = upd && A.wb != 0.0;
+    L.bjx = wb ? A.base[pos + f_jx * fstride] : czero<C>();
+    L.bjy = wb ? A.base[pos + f_jy * fstride] : czero<C>();
+    const bool ext = upd && P.external_noise;
+    L.eax = ext ? A.ext_a[pos + f_jx * fstride] : czero<C>();
+    L.eay = ext ? A.ext_a[pos + f_jy * fstride] : czero<C>();
+    L.ebx = (ext && A.srk3) ? A.ext_b[pos + f_jx * fstride] : czero<C>();
+    L.eby = (ext && A.srk3) ? A.ext_b[pos + f_jy * fstride] : czero<C>();
+    return L;
 }
 
 // momentum: det_j from the accumulated products plus pressure, incompressible
@@ -420,18 +474,17 @@ __device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageAr
 // transverse projection.  Results replace a0 (jx) and a1 (jy).
 template <typename T>
 __device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const StageArgs<T>& A, const ModeCtx& m, T kx, T kyv, cplx<T>& a0,
-                                                  cplx<T>& a1, uint32_t member, size_t fstride, int b) {
+                                                  cplx<T>& a1, uint32_t member, const MomLoads<T>& L, int b) {
     using C = cplx<T>;
     const int f_jx = P.nop + 1, f_jy = P.nop + 2;
     const T k2 = kx * kx + kyv * kyv;
-    const C cjx = A.cur[m.pos + f_jx * fstride];
-    const C cjy = A.cur[m.pos + f_jy * fstride];
+    const C cjx = L.cjx, cjy = L.cjy;
     C djx = czero<C>(), djy = czero<C>();
     if (!P.j_zero) {
         djx = a0;
         djy = a1;
         if (P.cT2 != 0.0) {  // fcalculator.cc:276-300
-            const C ph = cscale(A.cur[m.pos], static_cast<T>(P.cT2));
+            const C ph = cscale(L.crho, static_cast<T>(P.cT2));
             djx = cadd(djx, cmulmi(cscale(ph, kx)));
             djy = cadd(djy, cmulmi(cscale(ph, kyv)));
         }
@@ -453,24 +506,16 @@ __device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const Stage
     const T beta = static_cast<T>(A.beta);
     C sx = czero<C>(), sy = czero<C>();
     if (P.external_noise) {
-        sx = A.ext_a[m.pos + f_jx * fstride];
-        sy = A.ext_a[m.pos + f_jy * fstride];
+        sx = L.eax;
+        sy = L.eay;
         if (A.srk3) {
-            sx = cadd(sx, cscale(A.ext_b[m.pos + f_jx * fstride], beta));
-            sy = cadd(sy, cscale(A.ext_b[m.pos + f_jy * fstride], beta));
+            sx = cadd(sx, cscale(L.ebx, beta));
+            sy = cadd(sy, cscale(L.eby, beta));
         }
     } else if (P.noise_j && m.k_nonzero) {
-        j_noise<T>(P, 0, A.step, member, m.mode_id, m.conj_line, kx, kyv, sx, sy);
-        if (A.srk3) {
-            C bx, by;
-            j_noise<T>(P, 1, A.step, member, m.mode_id, m.conj_line, kx, kyv, bx, by);
-            sx = cadd(sx, cscale(bx, beta));
-            sy = cadd(sy, cscale(by, beta));
-        }
+        j_noise<T>(P, A.step, member, m.mode_id, m.conj_line, kx, kyv, A.srk3 != 0, beta, sx, sy);
     }
     const T dt = static_cast<T>(A.dt), sdt = static_cast<T>(A.sdt), wb = static_cast<T>(A.wb), wc = static_cast<T>(A.wc);
-    const C bjx = (A.wb != 0.0) ? A.base[m.pos + f_jx * fstride] : czero<C>();
-    const C bjy = (A.wb != 0.0) ? A.base[m.pos + f_jy * fstride] : czero<C>();
     C incx = cadd(cscale(djx, dt), cscale(sx, sdt));
     C incy = cadd(cscale(djy, dt), cscale(sy, sdt));
     if (P.mode == 1 && k2 != T(0)) {  // transverse projection (srk3_incompressible.h:81-96)
@@ -478,8 +523,8 @@ __device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const Stage
         incx = cscale(cscale(tr, -kyv), T(1) / k2);
         incy = cscale(cscale(tr, kx), T(1) / k2);
     }
-    a0 = cadd(cscale(bjx, wb), cscale(cadd(cjx, incx), wc));
-    a1 = cadd(cscale(bjy, wb), cscale(cadd(cjy, incy), wc));
+    a0 = cadd(cscale(L.bjx, wb), cscale(cadd(cjx, incx), wc));
+    a1 = cadd(cscale(L.bjy, wb), cscale(cadd(cjy, incy), wc));
 }
 
 // rho: rho_det (fcalculator.cc:60-84) and its stage update
@@ -562,8 +607,8 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
         const ModeCtx m = mode_ctx<T>(P, mbase, tile, w, j);
         const T kx = kxu * static_cast<T>(m.gx);
         const T kyv = kyu * static_cast<T>(m.ky);
-        if (gkind == GROUP_PSI) acc0[i] = psi_epilogue<T>(P, A, alpha, m, kx, kyv, acc0[i], member, fstride, b);
-        else momentum_epilogue<T>(P, A, m, kx, kyv, acc0[i], acc1[i], member, fstride, b);
+        if (gkind == GROUP_PSI) acc0[i] = psi_epilogue<T>(P, A, alpha, m, kx, kyv, acc0[i], member, psi_loads<T>(P, A, alpha, m.pos, fstride), b);
+        else momentum_epilogue<T>(P, A, m, kx, kyv, acc0[i], acc1[i], member, momentum_loads<T>(P, A, m.pos, fstride), b);
     }
 
     // ---- which fields this CTA writes, in order: psi | (rho), jx, jy ----

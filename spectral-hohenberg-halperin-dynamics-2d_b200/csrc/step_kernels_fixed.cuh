@@ -346,17 +346,28 @@ __global__ void __launch_bounds__(kThreads, 2) col_forward_fixed(const StepPlan 
         }
     }
 
-    // epilogue for column g: results replace a0 (psi or jx) and a1 (jy)
-    for (int j = gt; j < kyn; j += G) {
-        const ModeCtx m = mode_ctx<T>(P, mbase, t, g, j);
-        const T kyv = kyu * static_cast<T>(m.ky);
-        if (gkind == GROUP_PSI) {
-            a0[j] = psi_epilogue<T>(P, A, alpha, m, kx, kyv, a0[j], member, fstride, b);
-        } else {
+    // epilogue for column g: results replace a0 (psi or jx) and a1 (jy); the
+    // next mode's global loads are issued before the current mode's math
+    if (gkind == GROUP_PSI) {
+        PsiLoads<T> L = psi_loads<T>(P, A, alpha, mode_ctx<T>(P, mbase, t, g, gt < kyn ? gt : 0).pos, fstride);
+        for (int j = gt; j < kyn; j += G) {
+            const ModeCtx m = mode_ctx<T>(P, mbase, t, g, j);
+            const int jn = j + G < kyn ? j + G : j;
+            const PsiLoads<T> Ln = psi_loads<T>(P, A, alpha, mode_ctx<T>(P, mbase, t, g, jn).pos, fstride);
+            a0[j] = psi_epilogue<T>(P, A, alpha, m, kx, kyu * static_cast<T>(m.ky), a0[j], member, L, b);
+            L = Ln;
+        }
+    } else {
+        MomLoads<T> L = momentum_loads<T>(P, A, mode_ctx<T>(P, mbase, t, g, gt < kyn ? gt : 0).pos, fstride);
+        for (int j = gt; j < kyn; j += G) {
+            const ModeCtx m = mode_ctx<T>(P, mbase, t, g, j);
+            const int jn = j + G < kyn ? j + G : j;
+            const MomLoads<T> Ln = momentum_loads<T>(P, A, mode_ctx<T>(P, mbase, t, g, jn).pos, fstride);
             C u0 = a0[j], u1 = a1[j];
-            momentum_epilogue<T>(P, A, m, kx, kyv, u0, u1, member, fstride, b);
+            momentum_epilogue<T>(P, A, m, kx, kyu * static_cast<T>(m.ky), u0, u1, member, L, b);
             a0[j] = u0;
             a1[j] = u1;
+            L = Ln;
         }
     }
 

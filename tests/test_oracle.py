@@ -65,14 +65,16 @@ def test_reference_noise_has_the_restated_structure(name):
 
 def test_philox_normals_statistics():
     ids = np.arange(200000, dtype=np.uint64)
-    z = so.philox_normals(1234, 0, 7, so.psi_stream(0, 0), ids)
-    assert abs(z.real.mean()) < 0.01 and abs(z.imag.mean()) < 0.01
-    assert abs(z.real.var() - 1) < 0.01 and abs(z.imag.var() - 1) < 0.01
-    assert abs(np.mean(z.real * z.imag)) < 0.01
+    za, zb = so.philox_normals(1234, 0, 7, so.psi_stream(0), ids)
+    for z in (za, zb):
+        assert abs(z.real.mean()) < 0.01 and abs(z.imag.mean()) < 0.01
+        assert abs(z.real.var() - 1) < 0.01 and abs(z.imag.var() - 1) < 0.01
+        assert abs(np.mean(z.real * z.imag)) < 0.01
+    assert abs(np.mean(za.real * zb.real)) < 0.01
     # different streams, steps, members and seeds are different realisations
-    for other in (so.philox_normals(1234, 0, 7, so.psi_stream(0, 1), ids), so.philox_normals(1234, 0, 8, so.psi_stream(0, 0), ids),
-                  so.philox_normals(1234, 1, 7, so.psi_stream(0, 0), ids), so.philox_normals(99, 0, 7, so.psi_stream(0, 0), ids)):
-        assert abs(np.mean(z.real * other.real)) < 0.01
+    for other in (so.philox_normals(1234, 0, 7, so.psi_stream(1), ids)[0], so.philox_normals(1234, 0, 8, so.psi_stream(0), ids)[0],
+                  so.philox_normals(1234, 1, 7, so.psi_stream(0), ids)[0], so.philox_normals(99, 0, 7, so.psi_stream(0), ids)[0]):
+        assert abs(np.mean(za.real * other.real)) < 0.01
 
 
 def test_philox4x32_known_answer():
