@@ -169,6 +169,15 @@ int shhd_engine_set_external_noise(shhd_engine* engine, int member, const double
  * j_det of src/fcalculator.cc:60-150) in the reference layout. */
 int shhd_engine_rhs(shhd_engine* engine, int member, double* det, size_t n_doubles);
 
+/* Per-member controls of a batched engine (no reference counterpart; used by
+ * the serving loop).  Member m draws its noise with key (seed, key) at step
+ * (engine step index - step_origin), scaled by noise_scale (the factor
+ * sqrt(kBT_m / kBT) for a member whose temperature differs from the
+ * configuration's); inactive members are skipped by every kernel.  Defaults:
+ * key = member_offset + m, step_origin 0, noise_scale 1, active.  Resets the
+ * member's cached reference density (a new trajectory). */
+int shhd_engine_set_member(shhd_engine* engine, int member, uint32_t key, int64_t step_origin, double noise_scale, int active);
+
 /* Step counter and time (project.h:136-137). */
 int shhd_engine_set_time(shhd_engine* engine, int64_t step_index, double time);
 

@@ -172,6 +172,9 @@ struct shhd_engine {
     void* tw_y = nullptr;
     double* rho0_dev = nullptr;
     int* err_dev = nullptr;
+    MemberInfo* members_dev = nullptr;
+    std::vector<MemberInfo> members;
+    bool members_dirty = true;
     int* static_dev = nullptr;
     int n_static = 0;
 
@@ -222,6 +225,7 @@ void* dalloc(shhd_engine* e, size_t bytes) {
 void free_engine(shhd_engine* e) {
     for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->ref_stage,
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
+                    static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev)})
         if (p) cudaFree(p);
     for (auto& pe : e->pending) { e->event_pool.push_back(pe.a); e->event_pool.push_back(pe.b); }
@@ -575,11 +579,11 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
         constexpr int FY = decltype(fy)::value;
         if constexpr (FY != 0) {
             if (e->col_fixed) {
-                col_inverse_fixed<T, FY><<<grid, kThreads, e->smem_col_inv, e->stream>>>(P, st, i1, tw);
+                col_inverse_fixed<T, FY><<<grid, kThreads, e->smem_col_inv, e->stream>>>(P, e->members_dev, st, i1, tw);
                 return;
             }
         }
-        col_inverse_kernel<T, 0><<<grid, kThreads, e->smem_col, e->stream>>>(P, st, i1, tw);
+        col_inverse_kernel<T, 0><<<grid, kThreads, e->smem_col, e->stream>>>(P, e->members_dev, st, i1, tw);
     });
     check_cuda(cudaGetLastError(), "col_inverse launch");
 }
@@ -595,13 +599,13 @@ void launch_row(shhd_engine* e) {
         if constexpr (FX != 0) {
             if (e->row_fixed) {
                 row_pass_fixed<T, FX><<<grid, kThreads, e->smem_row, e->stream>>>(
-                    P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
+                    P, e->members_dev, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
                     e->err_dev);
                 return;
             }
         }
         row_pass_kernel<T, 0><<<grid, kThreads, e->smem_row, e->stream>>>(
-            P, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
+            P, e->members_dev, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
             e->err_dev);
     });
     check_cuda(cudaGetLastError(), "row_pass launch");
@@ -634,11 +638,20 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
     check_cuda(cudaGetLastError(), "col_forward launch");
 }
 
+void upload_members(shhd_engine* e) {
+    if (!e->members_dirty) return;
+    check_cuda(cudaMemcpyAsync(e->members_dev, e->members.data(), sizeof(MemberInfo) * e->members.size(), cudaMemcpyHostToDevice, e->stream),
+               "member info upload");
+    check_cuda(cudaStreamSynchronize(e->stream), "member info sync");
+    e->members_dirty = false;
+}
+
 void ensure_rho0(shhd_engine* e) {
+    upload_members(e);
     if (!e->need_rho0) return;
     bool changed = false;
     for (int m = 0; m < e->cfg.batch; ++m) {
-        if (e->rho0_cached[m]) continue;
+        if (e->rho0_cached[m] || !e->members[m].active) continue;
         const double r = e->rho0_candidate[m];
         if (r == 0.0) throw Failure(SHHD_EINVAL, "reference density must be nonzero.");
         e->rho0_value[m] = r;
@@ -670,6 +683,7 @@ const double kWc[3] = {1.0, 1.0 / 4.0, 2.0 / 3.0};
 template <typename T>
 StageArgs<T> stage_args(shhd_engine* e, const void* cur, const void* base, void* next, double wb, double wc, double beta, int srk3, int fused) {
     StageArgs<T> A{};
+    A.members = e->members_dev;
     A.cur = static_cast<const cplx<T>*>(cur);
     A.base = static_cast<const cplx<T>*>(base);
     A.next = static_cast<cplx<T>*>(next);
@@ -825,6 +839,15 @@ void init_device(shhd_engine* e) {
     e->rho0_dev = static_cast<double*>(dalloc(e, sizeof(double) * B));
     check_cuda(cudaMemsetAsync(e->rho0_dev, 0, sizeof(double) * B, e->stream), "memset");
     e->err_dev = static_cast<int*>(dalloc(e, sizeof(int)));
+    e->members_dev = static_cast<MemberInfo*>(dalloc(e, sizeof(MemberInfo) * B));
+    e->members.resize(B);
+    for (size_t m = 0; m < B; ++m) {
+        e->members[m].key = static_cast<uint32_t>(e->cfg.member_offset + static_cast<int>(m));
+        e->members[m].active = 1;
+        e->members[m].step0 = 0;
+        e->members[m].noise_scale = 1.0;
+    }
+    e->members_dirty = true;
     check_cuda(cudaMemsetAsync(e->err_dev, 0, sizeof(int), e->stream), "memset");
     // fields the integrator does not evolve
     std::vector<int> st;
@@ -985,6 +1008,21 @@ int shhd_engine_rhs(shhd_engine* e, int member, double* det, size_t n) {
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         if (e->fp32) run_rhs<float>(e, member, det);
         else run_rhs<double>(e, member, det);
+    });
+}
+
+int shhd_engine_set_member(shhd_engine* e, int member, uint32_t key, int64_t step_origin, double noise_scale, int active) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (!(noise_scale >= 0.0)) throw Failure(SHHD_EINVAL, "noise_scale must be nonnegative");
+        MemberInfo& mi = e->members[member];
+        mi.key = key;
+        mi.step0 = step_origin;
+        mi.noise_scale = noise_scale;
+        mi.active = active ? 1 : 0;
+        e->rho0_cached[member] = 0;  // a new trajectory: rho0 is taken again at its first use
+        e->members_dirty = true;
     });
 }
 

@@ -93,8 +93,18 @@ struct StepPlan {
     int npos;                      // position slots per thread in col_forward
 };
 
+// per-member controls of a batched engine (serving): noise key, step origin
+// of the member's own step count, noise amplitude factor, active flag
+struct MemberInfo {
+    uint32_t key;
+    int32_t active;
+    int64_t step0;
+    double noise_scale;
+};
+
 template <typename T>
 struct StageArgs {
+    const MemberInfo* members;
     const cplx<T>* cur;
     const cplx<T>* base;
     cplx<T>* next;
@@ -117,8 +127,10 @@ __device__ __forceinline__ int ky_of_j(int j, int nay) { return j < nay / 2 ? j 
 // column inverse: state -> I1   (grid: tiles x n_in x batch)
 // ---------------------------------------------------------------------------
 template <typename T, int FY>
-__global__ void __launch_bounds__(kThreads) col_inverse_kernel(const StepPlan P, const cplx<T>* __restrict__ state,
-                                                               cplx<T>* __restrict__ i1, const cplx<T>* __restrict__ tw) {
+__global__ void __launch_bounds__(kThreads) col_inverse_kernel(const StepPlan P, const MemberInfo* __restrict__ members,
+                                                               const cplx<T>* __restrict__ state, cplx<T>* __restrict__ i1,
+                                                               const cplx<T>* __restrict__ tw) {
+    if (!members[blockIdx.z].active) return;
     using C = cplx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s_tw = reinterpret_cast<C*>(smem_raw);
@@ -172,9 +184,11 @@ __device__ __forceinline__ T product_value(const StepPlan& P, int kind, int arg,
 }
 
 template <typename T, int FX>
-__global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
+__global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, const MemberInfo* __restrict__ members,
+                                                            const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
                                                             const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
                                                             int* __restrict__ err) {
+    if (!members[blockIdx.y].active) return;
     using C = cplx<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s_tw = reinterpret_cast<C*>(smem_raw);
@@ -293,6 +307,7 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
 template <typename T>
 __device__ __forceinline__ cplx<T> psi_noise(const StepPlan& P, int alpha, uint64_t step, uint32_t member, uint32_t mode_id, bool conj_line,
                                              T sigma, bool srk3, T beta) {
+    // sigma already carries the member's amplitude factor
     cplx<T> xa, xb;
     complex_normals<T>(P.seed, member, step, psi_stream(alpha), mode_id, srk3, xa, xb);
     cplx<T> x = srk3 ? cadd(xa, cscale(xb, beta)) : xa;
@@ -303,7 +318,7 @@ __device__ __forceinline__ cplx<T> psi_noise(const StepPlan& P, int alpha, uint6
 // j_sto for both draws (fcalculator.cc:587-700): out = -i k . pi(xi_a + beta xi_b)
 template <typename T>
 __device__ __forceinline__ void j_noise(const StepPlan& P, uint64_t step, uint32_t member, uint32_t mode_id, bool conj_line, T kx, T ky,
-                                        bool srk3, T beta, cplx<T>& ox, cplx<T>& oy) {
+                                        bool srk3, T beta, T jscale, cplx<T>& ox, cplx<T>& oy) {
     using C = cplx<T>;
     C x[3];
 #pragma unroll
@@ -313,7 +328,7 @@ __device__ __forceinline__ void j_noise(const StepPlan& P, uint64_t step, uint32
         x[m] = srk3 ? cadd(xa, cscale(xb, beta)) : xa;
         if (conj_line) x[m] = cconj(x[m]);
     }
-    const T s = static_cast<T>(P.j_s), se = static_cast<T>(P.sqrt_eta), sz = static_cast<T>(P.sqrt_zeta);
+    const T s = static_cast<T>(P.j_s) * jscale, se = static_cast<T>(P.sqrt_eta), sz = static_cast<T>(P.sqrt_zeta);
     const C pxx = mk(-s * (sz * x[0].x + se * x[1].x), -s * (sz * x[0].y + se * x[1].y));
     const C pyy = mk(-s * (sz * x[0].x - se * x[1].x), -s * (sz * x[0].y - se * x[1].y));
     const C pxy = mk(-s * se * x[2].x, -s * se * x[2].y);
@@ -409,7 +424,7 @@ __device__ __forceinline__ PsiLoads<T> psi_loads(const StepPlan& P, const StageA
 // (unless det_mode) the stage update with noise; returns next (or det)
 template <typename T>
 __device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageArgs<T>& A, int alpha, const ModeCtx& m, T kx, T kyv,
-                                                cplx<T> acc, uint32_t member, const PsiLoads<T>& L, int b) {
+                                                cplx<T> acc, const MemberInfo& mi, const PsiLoads<T>& L, int b) {
     using C = cplx<T>;
     const int f = 1 + alpha;
     const T k2 = kx * kx + kyv * kyv;
@@ -437,8 +452,8 @@ __device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageAr
         sto = L.ea;
         if (A.srk3) sto = cadd(sto, cscale(L.eb, beta));
     } else if (P.noise_psi[alpha] && m.k_nonzero) {
-        const T sigma = sqrt(static_cast<T>(P.psi_sig2[alpha]) * k2);
-        sto = psi_noise<T>(P, alpha, A.step, member, m.mode_id, m.conj_line, sigma, A.srk3 != 0, beta);
+        const T sigma = sqrt(static_cast<T>(P.psi_sig2[alpha]) * k2) * static_cast<T>(mi.noise_scale);
+        sto = psi_noise<T>(P, alpha, A.step - static_cast<uint64_t>(mi.step0), mi.key, m.mode_id, m.conj_line, sigma, A.srk3 != 0, beta);
     }
     const C inner = cadd(cadd(cur, cscale(det, static_cast<T>(A.dt))), cscale(sto, static_cast<T>(A.sdt)));
     return cadd(cscale(L.base, static_cast<T>(A.wb)), cscale(inner, static_cast<T>(A.wc)));
@@ -474,7 +489,7 @@ __device__ __forceinline__ MomLoads<T> momentum_loads(const StepPlan& P, const S
 // transverse projection.  Results replace a0 (jx) and a1 (jy).
 template <typename T>
 __device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const StageArgs<T>& A, const ModeCtx& m, T kx, T kyv, cplx<T>& a0,
-                                                  cplx<T>& a1, uint32_t member, const MomLoads<T>& L, int b) {
+                                                  cplx<T>& a1, const MemberInfo& mi, const MomLoads<T>& L, int b) {
     using C = cplx<T>;
     const int f_jx = P.nop + 1, f_jy = P.nop + 2;
     const T k2 = kx * kx + kyv * kyv;
@@ -513,7 +528,8 @@ __device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const Stage
             sy = cadd(sy, cscale(L.eby, beta));
         }
     } else if (P.noise_j && m.k_nonzero) {
-        j_noise<T>(P, A.step, member, m.mode_id, m.conj_line, kx, kyv, A.srk3 != 0, beta, sx, sy);
+        j_noise<T>(P, A.step - static_cast<uint64_t>(mi.step0), mi.key, m.mode_id, m.conj_line, kx, kyv, A.srk3 != 0, beta,
+                   static_cast<T>(mi.noise_scale), sx, sy);
     }
     const T dt = static_cast<T>(A.dt), sdt = static_cast<T>(A.sdt), wb = static_cast<T>(A.wb), wc = static_cast<T>(A.wc);
     C incx = cadd(cscale(djx, dt), cscale(sx, sdt));
@@ -552,7 +568,8 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
     const int alpha = P.group_alpha[grp];
     const int nop = P.nop;
     const bool comp = (P.mode == 0);
-    const uint32_t member = P.member_offset + b;
+    const MemberInfo mi = A.members[b];
+    if (!mi.active) return;
     load_table(s_tw, tw, P.twy_count);
 
     const int npos_total = W * kyn;
@@ -607,8 +624,8 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
         const ModeCtx m = mode_ctx<T>(P, mbase, tile, w, j);
         const T kx = kxu * static_cast<T>(m.gx);
         const T kyv = kyu * static_cast<T>(m.ky);
-        if (gkind == GROUP_PSI) acc0[i] = psi_epilogue<T>(P, A, alpha, m, kx, kyv, acc0[i], member, psi_loads<T>(P, A, alpha, m.pos, fstride), b);
-        else momentum_epilogue<T>(P, A, m, kx, kyv, acc0[i], acc1[i], member, momentum_loads<T>(P, A, m.pos, fstride), b);
+        if (gkind == GROUP_PSI) acc0[i] = psi_epilogue<T>(P, A, alpha, m, kx, kyv, acc0[i], mi, psi_loads<T>(P, A, alpha, m.pos, fstride), b);
+        else momentum_epilogue<T>(P, A, m, kx, kyv, acc0[i], acc1[i], mi, momentum_loads<T>(P, A, m.pos, fstride), b);
     }
 
     // ---- which fields this CTA writes, in order: psi | (rho), jx, jy ----

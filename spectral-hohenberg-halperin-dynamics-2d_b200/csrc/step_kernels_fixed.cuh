@@ -142,8 +142,10 @@ __device__ __forceinline__ void load_tile(C* tile, const C* __restrict__ src) {
 // column inverse (compile-time NY): state -> I1   (grid: tiles x n_in x batch)
 // ---------------------------------------------------------------------------
 template <typename T, int NY>
-__global__ void __launch_bounds__(kThreads) col_inverse_fixed(const StepPlan P, const cplx<T>* __restrict__ state, cplx<T>* __restrict__ i1,
+__global__ void __launch_bounds__(kThreads) col_inverse_fixed(const StepPlan P, const MemberInfo* __restrict__ members,
+                                                              const cplx<T>* __restrict__ state, cplx<T>* __restrict__ i1,
                                                               const cplx<T>* __restrict__ tw) {
+    if (!members[blockIdx.z].active) return;
     using C = cplx<T>;
     constexpr int W = col_width<T, NY>();
     constexpr int G = kThreads / W;
@@ -177,9 +179,11 @@ __global__ void __launch_bounds__(kThreads) col_inverse_fixed(const StepPlan P, 
 // row pass (compile-time NX): I1 -> C2R -> products -> R2C -> I2   (grid: row pairs x batch)
 // ---------------------------------------------------------------------------
 template <typename T, int NX>
-__global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
+__global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, const MemberInfo* __restrict__ members,
+                                                           const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
                                                            const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
                                                            int* __restrict__ err) {
+    if (!members[blockIdx.y].active) return;
     using C = cplx<T>;
     constexpr int G = row_group<T, NX>();
     constexpr int NG = kThreads / G;
@@ -316,7 +320,8 @@ __global__ void __launch_bounds__(kThreads, 2) col_forward_fixed(const StepPlan 
     const int gkind = P.group_kind[grp];
     const int alpha = P.group_alpha[grp];
     const bool comp = (P.mode == 0);
-    const uint32_t member = P.member_offset + b;
+    const MemberInfo mi = A.members[b];
+    if (!mi.active) return;
     const size_t fstride = static_cast<size_t>(P.hx) * kyn;
     const size_t mbase = static_cast<size_t>(b) * P.nfields * fstride + static_cast<size_t>(t) * W * kyn;
     const T kxu = static_cast<T>(P.kx_unit), kyu = static_cast<T>(P.ky_unit);
@@ -354,7 +359,7 @@ __global__ void __launch_bounds__(kThreads, 2) col_forward_fixed(const StepPlan 
             const ModeCtx m = mode_ctx<T>(P, mbase, t, g, j);
             const int jn = j + G < kyn ? j + G : j;
             const PsiLoads<T> Ln = psi_loads<T>(P, A, alpha, mode_ctx<T>(P, mbase, t, g, jn).pos, fstride);
-            a0[j] = psi_epilogue<T>(P, A, alpha, m, kx, kyu * static_cast<T>(m.ky), a0[j], member, L, b);
+            a0[j] = psi_epilogue<T>(P, A, alpha, m, kx, kyu * static_cast<T>(m.ky), a0[j], mi, L, b);
             L = Ln;
         }
     } else {
@@ -364,7 +369,7 @@ __global__ void __launch_bounds__(kThreads, 2) col_forward_fixed(const StepPlan 
             const int jn = j + G < kyn ? j + G : j;
             const MomLoads<T> Ln = momentum_loads<T>(P, A, mode_ctx<T>(P, mbase, t, g, jn).pos, fstride);
             C u0 = a0[j], u1 = a1[j];
-            momentum_epilogue<T>(P, A, m, kx, kyu * static_cast<T>(m.ky), u0, u1, member, L, b);
+            momentum_epilogue<T>(P, A, m, kx, kyu * static_cast<T>(m.ky), u0, u1, mi, L, b);
             a0[j] = u0;
             a1[j] = u1;
             L = Ln;

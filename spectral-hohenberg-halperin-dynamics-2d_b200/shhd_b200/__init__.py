@@ -100,7 +100,7 @@ EXPORTED = (
     "shhd_engine_info", "shhd_engine_set_state", "shhd_engine_get_state", "shhd_engine_step", "shhd_engine_step_async",
     "shhd_engine_synchronize", "shhd_engine_set_external_noise", "shhd_engine_rhs", "shhd_engine_set_time",
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
-    "shhd_engine_reset_stats",
+    "shhd_engine_reset_stats", "shhd_engine_set_member",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -133,6 +133,7 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_set_profiling.argtypes = [vp, i]
     lib.shhd_engine_kernel_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
     lib.shhd_engine_reset_stats.argtypes = [vp]
+    lib.shhd_engine_set_member.argtypes = [vp, i, ctypes.c_uint32, ctypes.c_int64, ctypes.c_double, i]
     return lib
 
 
@@ -234,6 +235,10 @@ class Engine:
 
     def set_time(self, step_index: int, time: float) -> None:
         _check(lib.shhd_engine_set_time(self._h, int(step_index), float(time)))
+
+    def set_member(self, member: int, key: int, step_origin: int = 0, noise_scale: float = 1.0, active: bool = True) -> None:
+        """Per-member noise key, step origin, amplitude factor and active flag (serving)."""
+        _check(lib.shhd_engine_set_member(self._h, member, int(key) & 0xFFFFFFFF, int(step_origin), float(noise_scale), 1 if active else 0))
 
     def set_profiling(self, on: bool) -> None:
         _check(lib.shhd_engine_set_profiling(self._h, 1 if on else 0))

@@ -1,0 +1,62 @@
+"""Serving loop: continuous batching of mixed jobs; each result equals the job run alone (GPU)."""
+import numpy as np
+import pytest
+
+import shhd_oracle as so
+from helpers import random_state, script
+
+pytestmark = pytest.mark.gpu
+
+
+def _jobs(sb, serve):
+    specs = [
+        (script(grid=(64, 64), length=(128.0, 128.0), nop=2, dt=0.01, noise="kBT 0.002 seed 1"), 40, 0.000),
+        (script(grid=(64, 64), length=(128.0, 128.0), nop=2, dt=0.01, noise="kBT 0.0005 seed 9"), 65, 0.005),
+        (script(grid=(128, 128), length=(256.0, 256.0), nop=1, dt=0.02, te="srk3/quiescent", cT=None, eta=0.0, zeta=0.0,
+                nonlinear=None, noise="kBT 0.01 seed 2"), 30, 0.010),
+        (script(grid=(64, 64), length=(128.0, 128.0), nop=2, dt=0.01, noise="kBT 0.004 seed 3"), 25, 0.020),
+        (script(grid=(128, 128), length=(256.0, 256.0), nop=1, dt=0.02, te="srk3/quiescent", cT=None, eta=0.0, zeta=0.0,
+                nonlinear=None, noise="kBT 0.03 seed 4"), 55, 0.030),
+        (script(grid=(64, 64), length=(128.0, 128.0), nop=0, dt=0.01, te="srk3/incompressible", cT=None, eta=0.05, zeta=0.0,
+                nonlinear="momentum", noise="kBT 0.001 seed 5"), 35, 0.040),
+    ]
+    jobs = []
+    for k, (text, n, t) in enumerate(specs):
+        cfg = sb.config_from_script(text)
+        ocfg = so.parse_script(text)
+        st = random_state(ocfg, seed=100 + k, amp=0.03, transverse=(ocfg.mode == "incompressible"))
+        jobs.append(serve.Job(key=1000 + k, config=cfg, state=st, nsteps=n, arrival=t))
+    return jobs
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_served_results_equal_alone(precision):
+    import shhd_b200 as sb
+    from shhd_b200 import serve
+    jobs = _jobs(sb, serve)
+    srv = serve.Server(precision=precision, seed=77, max_slots=4, chunk=10)
+    stats = srv.run(jobs)
+    srv.close()
+    assert stats["jobs"] == len(jobs)
+    assert stats["p50_s"] <= stats["p99_s"]
+    assert stats["buckets"] >= 3  # three distinct configurations
+    for job in jobs:
+        alone = serve.run_alone(job, precision, seed=77)
+        assert job.result is not None
+        assert so.rel_l2(job.result, alone) < 1e-13, job.key
+
+
+def test_inactive_members_are_untouched():
+    import shhd_b200 as sb
+    text = script(grid=(64, 64), length=(128.0, 128.0), nop=1, dt=0.01, noise="kBT 0.002 seed 1")
+    cfg = sb.config_from_script(text)
+    cfg.batch = 2
+    ocfg = so.parse_script(text)
+    a, b = random_state(ocfg, seed=1), random_state(ocfg, seed=2)
+    with sb.Engine(cfg) as eng:
+        eng.set_state(a, member=0)
+        eng.set_state(b, member=1)
+        eng.set_member(1, key=5, active=False)
+        eng.step(3)
+        assert np.array_equal(eng.get_state(1), b)
+        assert not np.array_equal(eng.get_state(0), a)
