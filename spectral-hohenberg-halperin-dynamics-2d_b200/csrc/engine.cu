@@ -11,6 +11,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -534,11 +536,24 @@ void build_plan(shhd_engine* e) {
 }
 
 // kernel dispatch -------------------------------------------------------------
+// The dynamic shared-memory limit is a property of the kernel on a device, shared
+// by every engine that launches it: only ever raise it, so that an engine with a
+// smaller need never lowers the limit below what another engine launches with.
+void raise_smem_limit(const void* fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> limit;
+    int dev = 0;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = limit[{dev, fn}];
+    if (bytes <= cur) return;
+    check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)), "cudaFuncSetAttribute");
+    cur = bytes;
+}
+
 template <typename T>
 void set_smem_attrs(shhd_engine* e) {
-    auto setattr = [](const void* fn, size_t bytes) {
-        check_cuda(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)), "cudaFuncSetAttribute");
-    };
+    auto setattr = [](const void* fn, size_t bytes) { raise_smem_limit(fn, bytes); };
     with_size(e->P.npy, [&](auto fy) {
         constexpr int FY = decltype(fy)::value;
         if constexpr (FY != 0) {

@@ -60,3 +60,24 @@ def test_inactive_members_are_untouched():
         eng.step(3)
         assert np.array_equal(eng.get_state(1), b)
         assert not np.array_equal(eng.get_state(0), a)
+
+
+def test_engines_sharing_a_kernel_size_coexist():
+    """Two engines of one compute size but different shared-memory needs (5 and 2 transformed
+    fields at 96^2): creating the smaller one must not break launches of the larger one."""
+    import shhd_b200 as sb
+    big = script(grid=(64, 64), length=(128.0, 128.0), nop=2, dt=0.01)
+    small = script(grid=(64, 64), length=(128.0, 128.0), nop=0, dt=0.01, te="srk3/incompressible", cT=None, eta=0.05,
+                   zeta=0.0, nonlinear="momentum")
+    ob, osm = so.parse_script(big), so.parse_script(small)
+    ub, us = random_state(ob, seed=3), random_state(osm, seed=4, transverse=True)
+    with sb.Engine(sb.config_from_script(big)) as eb, sb.Engine(sb.config_from_script(small)) as es:
+        eb.set_state(ub)
+        es.set_state(us)
+        eb.step(2)
+        es.step(2)
+        ref = so.Oracle(ob)
+        u = ub
+        for _ in range(2):
+            u = ref.step(u, "philox")
+        assert so.rel_l2(eb.get_state(), u) < 1e-12
