@@ -198,6 +198,29 @@ void* shhd_engine_stream(shhd_engine* engine);
  * float or double per `precision`.  Valid until the next step call. */
 const void* shhd_engine_state_device(const shhd_engine* engine);
 
+/* Deterministic right-hand side of one state without any device allocation.
+ * No counterpart in the reference: it exists for hosts that must not call
+ * cudaMalloc, such as a solver running inside a framework whose caching
+ * allocator already owns the GPU's memory, or a plugin loaded into a process
+ * that reserved its device memory up front.  Such a caller passes device
+ * buffers it owns: state_dev (the input State, reference layout, FP64) and
+ * rhs_dev (same layout; receives what shhd_engine_rhs would return for that
+ * state), n_doubles = info.state_doubles, cfg->batch = 1.  The work is
+ * enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream) and
+ * the call returns once it has finished.
+ *
+ * Every intermediate lives in one array of SHHD_NOALLOC_SCRATCH_BYTES compiled
+ * into the library, which each GPU that loads the library holds until the
+ * process exits.  A configuration that needs more is rejected with SHHD_EINVAL
+ * and a message giving the size it needs (32 MiB covers, for example, a 256^2
+ * grid with 3/2 padding, two order parameters and advection in FP64).  The
+ * first call on a device looks up that device's address of the array; make
+ * that first call before any stream capture.  All calls share the one array,
+ * so calls whose work overlaps on the GPU (other streams or host threads)
+ * race: serialise them. */
+#define SHHD_NOALLOC_SCRATCH_BYTES (32u << 20)
+int shhd_rhs_noalloc(const shhd_config* cfg, const double* state_dev, double* rhs_dev, size_t n_doubles, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1084,3 +1084,166 @@ int shhd_engine_reset_stats(shhd_engine* e) {
 const void* shhd_engine_state_device(const shhd_engine* e) { return e ? e->u : nullptr; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Right-hand side without device allocation
+//
+// For hosts that may not call cudaMalloc themselves: a solver embedded in a
+// framework whose caching allocator owns the device memory (a second
+// allocator would fragment it or exceed its budget), or a plugin loaded into
+// a process whose memory was reserved up front.  They hand in device buffers
+// they already own; every intermediate (column-inverse and product planes,
+// the active-mode copies of input and output, twiddles, flags) lives in one
+// fixed array compiled into this library.  That array is held on every GPU
+// the library is loaded on, until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocAlign = 256;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SHHD_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// device address of the scratch array on the current device; the first call on
+// a device looks it up (the array's host-side name is not a device address)
+unsigned char* noalloc_base(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) throw Failure(SHHD_EUNSUPPORTED, "device ordinal beyond the supported range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[device]) {
+        void* p = nullptr;
+        check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress of the static scratch");
+        g_noalloc_base[device] = static_cast<unsigned char*>(p);
+    }
+    return g_noalloc_base[device];
+}
+
+// carves aligned regions out of the scratch array; sizes only, when base is null
+struct ScratchCarver {
+    unsigned char* base;
+    size_t used = 0;
+    void* take(size_t bytes) {
+        void* p = base ? base + used : nullptr;
+        used += (std::max<size_t>(bytes, 1) + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign;
+        return p;
+    }
+};
+
+void check_device_buffer(const void* p, int device, const char* what) {
+    if (!p) throw Failure(SHHD_EINVAL, std::string(what) + " is null");
+    if (reinterpret_cast<uintptr_t>(p) % 16 != 0) throw Failure(SHHD_EINVAL, std::string(what) + " must be 16-byte aligned");
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        throw Failure(SHHD_EINVAL, std::string(what) + " is not a CUDA pointer");
+    }
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
+        throw Failure(SHHD_EINVAL, std::string(what) + " must be device memory");
+    if (a.type == cudaMemoryTypeDevice && a.device != device)
+        throw Failure(SHHD_EINVAL, std::string(what) + " belongs to another device than the current one");
+}
+
+template <typename T>
+void rhs_noalloc(shhd_engine* e, const double* state_dev, double* rhs_dev, unsigned char* base) {
+    const StepPlan& P = e->P;
+    const size_t cs = sizeof(cplx<T>);
+    const auto twx = e->row_fixed ? stage_table<T>(e->cfg.nx) : twiddle_table<T>(e->cfg.nx);
+    const auto twy = e->col_fixed ? stage_table<T>(e->cfg.ny) : twiddle_table<T>(e->cfg.ny);
+    ScratchCarver sc{base};
+    void* act_in = sc.take(e->state_elems * cs);
+    void* act_out = sc.take(e->state_elems * cs);
+    e->i1 = sc.take(e->i1_elems * cs);
+    e->i2 = sc.take(e->i2_elems * cs);
+    e->tw_x = sc.take(twx.size() * cs);
+    e->tw_y = sc.take(twy.size() * cs);
+    e->rho0_dev = static_cast<double*>(sc.take(sizeof(double)));
+    e->err_dev = static_cast<int*>(sc.take(sizeof(int)));
+    e->flag_dev = static_cast<int*>(sc.take(sizeof(int)));
+    e->members_dev = static_cast<MemberInfo*>(sc.take(sizeof(MemberInfo)));
+    if (sc.used > SHHD_NOALLOC_SCRATCH_BYTES)
+        throw Failure(SHHD_EINVAL, "shhd_rhs_noalloc: this configuration needs " + std::to_string(sc.used) +
+                                       " bytes of scratch but the static scratch holds " + std::to_string(SHHD_NOALLOC_SCRATCH_BYTES) +
+                                       " bytes; use an engine (shhd_engine_create) for it");
+    cudaStream_t s = e->stream;
+    MemberInfo mi{};
+    mi.key = static_cast<uint32_t>(e->cfg.member_offset);
+    mi.active = 1;
+    mi.step0 = 0;
+    mi.noise_scale = 1.0;
+    // the array keeps the previous call's contents: rewrite or clear everything read before written
+    check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, s), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size() * cs, cudaMemcpyHostToDevice, s), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(e->members_dev, &mi, sizeof(mi), cudaMemcpyHostToDevice, s), "member upload");
+    check_cuda(cudaMemsetAsync(e->err_dev, 0, sizeof(int), s), "error word clear");
+    check_cuda(cudaMemsetAsync(e->flag_dev, 0, sizeof(int), s), "flag clear");
+    check_cuda(cudaMemsetAsync(act_out, 0, e->state_elems * cs, s), "rhs clear");
+
+    // input checks of shhd_engine_set_state: nothing outside the active modes
+    const int ref_hx = e->cfg.nx / 2 + 1;
+    const double2* ref_in = reinterpret_cast<const double2*>(state_dev);
+    {
+        dim3 g((P.npy * ref_hx + kThreads - 1) / kThreads, P.nfields);
+        check_inactive_kernel<<<g, kThreads, 0, s>>>(P, ref_hx, ref_in, e->flag_dev);
+        check_cuda(cudaGetLastError(), "check_inactive launch");
+    }
+    int bad = 0;
+    double rho00 = 0.0;
+    check_cuda(cudaMemcpyAsync(&bad, e->flag_dev, sizeof(int), cudaMemcpyDeviceToHost, s), "flag read");
+    check_cuda(cudaMemcpyAsync(&rho00, state_dev, sizeof(double), cudaMemcpyDeviceToHost, s), "density mode read");
+    check_cuda(cudaStreamSynchronize(s), "input check sync");
+    if (bad) throw Failure(SHHD_EINVAL, "state has a nonzero entry outside the active modes");
+    // reference density of the incompressible terms (fcalculator_workspace.cc:41-66)
+    double rho0 = rho00 / (static_cast<double>(e->cfg.nx) * e->cfg.ny);
+    if (e->need_rho0 && rho0 == 0.0) throw Failure(SHHD_EINVAL, "reference density must be nonzero.");
+    check_cuda(cudaMemcpyAsync(e->rho0_dev, &rho0, sizeof(double), cudaMemcpyHostToDevice, s), "rho0 upload");
+    {
+        dim3 g((P.hx * P.kyn + kThreads - 1) / kThreads, P.nfields);
+        ref_to_active_kernel<T><<<g, kThreads, 0, s>>>(P, ref_hx, ref_in, static_cast<cplx<T>*>(act_in));
+        check_cuda(cudaGetLastError(), "ref_to_active launch");
+    }
+    launch_col_inverse<T>(e, act_in);
+    launch_row<T>(e);
+    StageArgs<T> A = stage_args<T>(e, act_in, act_in, act_out, 0.0, 1.0, 0.0, 0, 0);
+    A.det_mode = 1;
+    launch_col_forward<T>(e, A);
+    {
+        dim3 g((P.npy * ref_hx + kThreads - 1) / kThreads, P.nfields);
+        active_to_ref_kernel<T><<<g, kThreads, 0, s>>>(P, ref_hx, static_cast<const cplx<T>*>(act_out), reinterpret_cast<double2*>(rhs_dev));
+        check_cuda(cudaGetLastError(), "active_to_ref launch");
+    }
+    int err = 0;
+    check_cuda(cudaMemcpyAsync(&err, e->err_dev, sizeof(int), cudaMemcpyDeviceToHost, s), "error word read");
+    check_cuda(cudaStreamSynchronize(s), "rhs sync");
+    if (err & ERR_ZERO_DENSITY) throw Failure(SHHD_ENUMERIC, "compressible velocity encountered zero density.");
+}
+
+}  // namespace
+
+extern "C" int shhd_rhs_noalloc(const shhd_config* cfg, const double* state_dev, double* rhs_dev, size_t n_doubles, void* stream) {
+    return guarded([&] {
+        if (!cfg) throw Failure(SHHD_EINVAL, "null configuration");
+        if (cfg->batch != 1) throw Failure(SHHD_EINVAL, "shhd_rhs_noalloc evaluates one state: cfg->batch must be 1");
+        // a host-side engine record only: its device pointers are set into the static scratch
+        shhd_engine e;
+        e.cfg = *cfg;
+        validate_config(e.cfg);
+        e.fp32 = cfg->precision == SHHD_FP32;
+        e.csize = e.fp32 ? sizeof(float2) : sizeof(double2);
+        build_plan(&e);
+        if (n_doubles != ref_doubles(&e))
+            throw Failure(SHHD_EINVAL, "state size mismatch: expected " + std::to_string(ref_doubles(&e)) + " doubles");
+        check_cuda(cudaGetDevice(&e.device), "cudaGetDevice");
+        check_device_buffer(state_dev, e.device, "state_dev");
+        check_device_buffer(rhs_dev, e.device, "rhs_dev");
+        e.stream = static_cast<cudaStream_t>(stream);
+        unsigned char* base = noalloc_base(e.device);
+        if (e.fp32) {
+            set_smem_attrs<float>(&e);
+            rhs_noalloc<float>(&e, state_dev, rhs_dev, base);
+        } else {
+            set_smem_attrs<double>(&e);
+            rhs_noalloc<double>(&e, state_dev, rhs_dev, base);
+        }
+    });
+}

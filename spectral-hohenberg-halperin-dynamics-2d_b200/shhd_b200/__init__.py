@@ -100,7 +100,7 @@ EXPORTED = (
     "shhd_engine_info", "shhd_engine_set_state", "shhd_engine_get_state", "shhd_engine_step", "shhd_engine_step_async",
     "shhd_engine_synchronize", "shhd_engine_set_external_noise", "shhd_engine_rhs", "shhd_engine_set_time",
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
-    "shhd_engine_reset_stats", "shhd_engine_set_member",
+    "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -134,6 +134,7 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_kernel_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]
     lib.shhd_engine_reset_stats.argtypes = [vp]
     lib.shhd_engine_set_member.argtypes = [vp, i, ctypes.c_uint32, ctypes.c_int64, ctypes.c_double, i]
+    lib.shhd_rhs_noalloc.argtypes = [ctypes.POINTER(Config), vp, vp, sz, vp]
     return lib
 
 
