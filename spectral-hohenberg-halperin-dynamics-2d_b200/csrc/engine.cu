@@ -21,6 +21,7 @@
 #include "../../include/shhd_b200.h"
 #include "step_kernels.cuh"
 #include "step_kernels_fixed.cuh"
+#include "step_kernels_pair.cuh"
 
 using namespace shhd;
 
@@ -145,6 +146,19 @@ void with_size(int n, F&& f) {
     }
 }
 
+// call f(std::integral_constant<int, N>) for a pair-path size N (0 = none)
+template <typename F>
+void with_pair_size(int n, F&& f) {
+    switch (n) {
+        case 96: f(std::integral_constant<int, 96>{}); break;
+        case 192: f(std::integral_constant<int, 192>{}); break;
+        case 384: f(std::integral_constant<int, 384>{}); break;
+        case 768: f(std::integral_constant<int, 768>{}); break;
+        case 1536: f(std::integral_constant<int, 1536>{}); break;
+        default: f(std::integral_constant<int, 0>{}); break;
+    }
+}
+
 }  // namespace
 
 namespace shhd_internal {
@@ -185,6 +199,7 @@ struct shhd_engine {
     int npos = 16;
     bool col_fixed = false;       // compile-time column kernels (group per column)
     bool row_fixed = false;       // compile-time row kernel (group per line)
+    bool pair_path = false;       // FP32 pair-line kernels (compile-time sizes up to 1536)
     size_t smem_col_inv = 0;
     size_t smem_col = 0, smem_row = 0;
     int n_evolved = 0;
@@ -305,6 +320,86 @@ void validate_config(const shhd_config& c) {
     if (quiescent && c.n_gradient_forces > 0) throw Failure(SHHD_EINVAL, "force/gradient cannot be used in quiescent mode.");
     if (c.ny % 2 == 1 && c.ny > 1) {
         // odd compute rows are handled (the last row pair holds one row)
+    }
+}
+
+// Row pass of the pair path: outputs are transformed two at a time; pairing
+// outputs of one kind (mu_0 with mu_1, psi_0 vx with psi_1 vx, vx with vy, ...)
+// keeps the packed product arithmetic uniform.  Each product is written as a
+// combination of the terms psi^3, psi vx, psi vy, vx, vy, jx vx, jx vy, jy vy.
+void plan_row_pairs(StepPlan& P) {
+    std::vector<int> order(P.n_out);
+    for (int o = 0; o < P.n_out; ++o) order[o] = o;
+    // pairing order: same kinds together, (vx, vy) and (jx vx, jy vy) adjacent
+    auto rank = [](int kind) {
+        switch (kind) {
+            case OUT_MU: return 0;
+            case OUT_PSIVX: return 1;
+            case OUT_PSIVY: return 2;
+            case OUT_VX: return 3;
+            case OUT_VY: return 4;
+            case OUT_PXX: return 5;
+            case OUT_PYY: return 6;
+            case OUT_PXY: return 7;
+            default: return 8;
+        }
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return rank(P.out_kind[a]) != rank(P.out_kind[b]) ? rank(P.out_kind[a]) < rank(P.out_kind[b]) : P.out_arg[a] < P.out_arg[b];
+    });
+    auto coef = [&](int o, float* c) {
+        for (int q = 0; q < 8; ++q) c[q] = 0.f;
+        const int a = P.out_arg[o];
+        switch (P.out_kind[o]) {
+            case OUT_MU: c[0] = static_cast<float>(P.mu_u3[a]); break;
+            case OUT_PSIVX: c[1] = 1.f; break;
+            case OUT_PSIVY: c[2] = 1.f; break;
+            case OUT_GRAD: c[3] = static_cast<float>(P.grad_ax[a]); c[4] = static_cast<float>(P.grad_ay[a]); break;
+            case OUT_VX: c[3] = 1.f; break;
+            case OUT_VY: c[4] = 1.f; break;
+            case OUT_PXX: c[5] = 1.f; break;
+            case OUT_PXY: c[6] = 1.f; break;
+            default: c[7] = 1.f; break;
+        }
+    };
+    P.rp_n = 0;
+    for (size_t i = 0; i < order.size(); i += 2) {
+        const int pi = P.rp_n++;
+        P.rp_a[pi] = order[i];
+        P.rp_b[pi] = i + 1 < order.size() ? order[i + 1] : -1;
+        float ca[8], cb[8];
+        coef(P.rp_a[pi], ca);
+        if (P.rp_b[pi] >= 0) coef(P.rp_b[pi], cb);
+        else for (int q = 0; q < 8; ++q) cb[q] = 0.f;
+        for (int q = 0; q < 8; ++q) { P.rp_coef[pi][q][0] = ca[q]; P.rp_coef[pi][q][1] = cb[q]; }
+    }
+    // canonical input roles after the x-inverse
+    const int s_rho = P.in_slot[0], s_jx = P.in_slot[P.nop + 1], s_jy = P.in_slot[P.nop + 2];
+    P.rp_canon = 0; P.rp_prep = 0; P.rp_jline = -1; P.rp_vline = -1;
+    if (!P.need_v) {
+        P.rp_canon = 1;
+    } else if (P.mode == SHHD_COMPRESSIBLE) {
+        if (s_rho >= 0 && s_rho % 2 == 0 && s_jx == s_rho + 1 && s_jy == s_rho + 2 && P.n_in == s_rho + 3) {
+            P.rp_canon = 1; P.rp_prep = 1; P.rp_jline = s_rho / 2; P.rp_vline = s_rho / 2 + 1;
+        }
+    } else if (s_jx >= 0 && s_jx % 2 == 0 && s_jy == s_jx + 1) {
+        P.rp_canon = 1; P.rp_jline = s_jx / 2;
+    }
+    // pairs whose two products are elementwise products of whole input lines
+    for (int pi = 0; pi < P.rp_n; ++pi) {
+        P.rp_mode[pi] = 0;
+        if (!P.rp_canon) continue;
+        const int a = P.rp_a[pi], b = P.rp_b[pi];
+        const int ka = P.out_kind[a], kb = b >= 0 ? P.out_kind[b] : -1;
+        if (ka == OUT_VX && kb == OUT_VY) { P.rp_mode[pi] = 1; continue; }
+        if (ka == OUT_PXX && kb == OUT_PYY) { P.rp_mode[pi] = 2; continue; }
+        // psi of A in the low half of a line and psi of B (if any) in its high half
+        const int sa = P.in_slot[1 + P.out_arg[a]];
+        const bool packed = sa >= 0 && sa % 2 == 0 && (b < 0 || (kb == ka && P.in_slot[1 + P.out_arg[b]] == sa + 1));
+        if (!packed) continue;
+        if (ka == OUT_MU) P.rp_mode[pi] = 3;
+        else if (ka == OUT_PSIVX && P.need_v) P.rp_mode[pi] = 4;
+        else if (ka == OUT_PSIVY && P.need_v) P.rp_mode[pi] = 5;
     }
 }
 
@@ -530,6 +625,29 @@ void build_plan(shhd_engine* e) {
     P.div_npy = make_fastdiv(c.ny);
     P.div_hx = make_fastdiv(P.hx);
 
+    // FP32 pair-line kernels: both compute sizes in 96 ... 1536, column pairs
+    // that tile the active kx range, row pairs that tile the compute rows
+    if (e->fp32 && is_pair_size(c.nx) && is_pair_size(c.ny) && P.hx % 2 == 0) {
+        const int cp = kPairMaxN / c.ny, rp = kPairMaxN / c.nx;
+        const int nip = (P.n_in + 1) / 2;
+        const size_t row_b = static_cast<size_t>(rp) * (nip + 1) * c.nx * 16;
+        const size_t col_b = static_cast<size_t>(cp) * c.ny * 16 + 3ull * cp * P.kyn * 16;  // lines, 3 per-mode arrays
+        if ((P.hx / 2) % cp == 0 && (c.ny / 2) % rp == 0 && row_b <= smem_cap && col_b <= smem_cap) {
+            e->pair_path = true;
+            e->col_fixed = e->row_fixed = false;
+            W = 2;
+            P.W = 2;
+            P.logw = 1;
+            P.ntiles = P.hx / 2;
+            P.div_w = make_fastdiv(2);
+            P.twx_count = P.twy_count = 0;
+            e->smem_col_inv = static_cast<size_t>(cp) * c.ny * 16;
+            e->smem_row = row_b;
+            e->smem_col = col_b;
+            plan_row_pairs(P);
+        }
+    }
+
     e->state_elems = static_cast<size_t>(P.nfields) * P.hx * P.kyn;
     e->i1_elems = static_cast<size_t>(P.n_in) * P.hx * c.ny;
     e->i2_elems = static_cast<size_t>(P.n_out) * P.hx * c.ny;
@@ -554,6 +672,22 @@ void raise_smem_limit(const void* fn, size_t bytes) {
 template <typename T>
 void set_smem_attrs(shhd_engine* e) {
     auto setattr = [](const void* fn, size_t bytes) { raise_smem_limit(fn, bytes); };
+    if constexpr (std::is_same<T, float>::value) {
+        if (e->pair_path) {
+            with_pair_size(e->P.npy, [&](auto fy) {
+                constexpr int FY = decltype(fy)::value;
+                if constexpr (FY != 0) {
+                    setattr(reinterpret_cast<const void*>(pcol_inverse<FY>), e->smem_col_inv);
+                    setattr(reinterpret_cast<const void*>(pcol_forward<FY>), e->smem_col);
+                }
+            });
+            with_pair_size(e->P.npx, [&](auto fx) {
+                constexpr int FX = decltype(fx)::value;
+                if constexpr (FX != 0) setattr(reinterpret_cast<const void*>(prow_pass<FX>), e->smem_row);
+            });
+            return;
+        }
+    }
     with_size(e->P.npy, [&](auto fy) {
         constexpr int FY = decltype(fy)::value;
         if constexpr (FY != 0) {
@@ -590,6 +724,20 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
     auto* st = static_cast<const cplx<T>*>(state);
     auto* i1 = static_cast<cplx<T>*>(e->i1);
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
+    if constexpr (std::is_same<T, float>::value) {
+        if (e->pair_path) {
+            with_pair_size(P.npy, [&](auto fy) {
+                constexpr int FY = decltype(fy)::value;
+                if constexpr (FY != 0) {
+                    dim3 pg(P.ntiles / (kPairMaxN / FY), P.n_in, P.batch);
+                    pcol_inverse<FY><<<pg, kThreads, e->smem_col_inv, e->stream>>>(P, e->members_dev, st, reinterpret_cast<ulonglong2*>(i1),
+                                                                                 static_cast<const float4*>(e->tw_y));
+                }
+            });
+            check_cuda(cudaGetLastError(), "col_inverse launch");
+            return;
+        }
+    }
     with_size(P.npy, [&](auto fy) {
         constexpr int FY = decltype(fy)::value;
         if constexpr (FY != 0) {
@@ -609,6 +757,21 @@ void launch_row(shhd_engine* e) {
     if (P.n_out == 0) return;
     dim3 grid((P.npy + 1) / 2, P.batch);
     LaunchScope scope(e, 1, static_cast<double>(sizeof(cplx<T>)) * P.batch * (P.n_in + P.n_out) * static_cast<double>(P.hx) * P.npy);
+    if constexpr (std::is_same<T, float>::value) {
+        if (e->pair_path) {
+            with_pair_size(P.npx, [&](auto fx) {
+                constexpr int FX = decltype(fx)::value;
+                if constexpr (FX != 0) {
+                    dim3 pg(P.npy / 2 / (kPairMaxN / FX), P.batch);
+                    prow_pass<FX><<<pg, kThreads, e->smem_row, e->stream>>>(P, e->members_dev, static_cast<const ulonglong2*>(e->i1),
+                                                                           static_cast<ulonglong2*>(e->i2), static_cast<const float4*>(e->tw_x),
+                                                                           e->rho0_dev, e->err_dev);
+                }
+            });
+            check_cuda(cudaGetLastError(), "row_pass launch");
+            return;
+        }
+    }
     with_size(P.npx, [&](auto fx) {
         constexpr int FX = decltype(fx)::value;
         if constexpr (FX != 0) {
@@ -638,6 +801,19 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
                                  e->n_evolved * static_cast<double>(P.hx) * P.kyn * (A.det_mode ? 1.0 : (2.0 + (A.wb != 0.0 ? 1.0 : 0.0))) +
                                  (A.fused_inverse ? P.n_in * static_cast<double>(P.hx) * P.npy : 0.0)));
     auto* tw = static_cast<const cplx<T>*>(e->tw_y);
+    if constexpr (std::is_same<T, float>::value) {
+        if (e->pair_path) {
+            with_pair_size(P.npy, [&](auto fy) {
+                constexpr int FY = decltype(fy)::value;
+                if constexpr (FY != 0) {
+                    dim3 pg(P.ntiles / (kPairMaxN / FY), P.n_groups, P.batch);
+                    pcol_forward<FY><<<pg, kThreads, e->smem_col, e->stream>>>(P, A, static_cast<const float4*>(e->tw_y));
+                }
+            });
+            check_cuda(cudaGetLastError(), "col_forward launch");
+            return;
+        }
+    }
     with_size(P.npy, [&](auto fy) {
         constexpr int FY = decltype(fy)::value;
         if constexpr (FY != 0) {
@@ -827,6 +1003,30 @@ void run_rhs(shhd_engine* e, int member, double* out) {
     download_ref<T>(e, e->det, member, out);
 }
 
+// host twiddle tables of the engine's transforms (bytes), in the format its kernels read
+template <typename T>
+std::vector<unsigned char> host_twiddles(const shhd_engine* e, int n, bool fixed) {
+    std::vector<unsigned char> out;
+    if (e->pair_path) {
+        with_pair_size(n, [&](auto fn) {
+            constexpr int FN = decltype(fn)::value;
+            if constexpr (FN != 0) {
+                const int cnt = std::max(PairPlan<FN>::c.twsz, 1);
+                std::vector<float> t(4 * static_cast<size_t>(cnt), 0.f);
+                pair_twiddles_host<FN>(t.data());
+                out.resize(t.size() * sizeof(float));
+                std::memcpy(out.data(), t.data(), out.size());
+            }
+        });
+        if (out.empty()) throw Failure(SHHD_EUNSUPPORTED, "no pair-path twiddles for size " + std::to_string(n));
+        return out;
+    }
+    const auto t = fixed ? stage_table<T>(n) : twiddle_table<T>(n);
+    out.resize(t.size() * sizeof(cplx<T>));
+    std::memcpy(out.data(), t.data(), out.size());
+    return out;
+}
+
 template <typename T>
 void init_device(shhd_engine* e) {
     const size_t cs = sizeof(cplx<T>);
@@ -845,12 +1045,12 @@ void init_device(shhd_engine* e) {
         check_cuda(cudaMemsetAsync(e->ext_a, 0, e->state_elems * B * cs, e->stream), "memset");
         check_cuda(cudaMemsetAsync(e->ext_b, 0, e->state_elems * B * cs, e->stream), "memset");
     }
-    const auto twx = e->row_fixed ? stage_table<T>(e->cfg.nx) : twiddle_table<T>(e->cfg.nx);
-    const auto twy = e->col_fixed ? stage_table<T>(e->cfg.ny) : twiddle_table<T>(e->cfg.ny);
-    e->tw_x = dalloc(e, twx.size() * cs);
-    e->tw_y = dalloc(e, twy.size() * cs);
-    check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
-    check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    const auto twx = host_twiddles<T>(e, e->cfg.nx, e->row_fixed);
+    const auto twy = host_twiddles<T>(e, e->cfg.ny, e->col_fixed);
+    e->tw_x = dalloc(e, twx.size());
+    e->tw_y = dalloc(e, twy.size());
+    check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
     e->rho0_dev = static_cast<double*>(dalloc(e, sizeof(double) * B));
     check_cuda(cudaMemsetAsync(e->rho0_dev, 0, sizeof(double) * B, e->stream), "memset");
     e->err_dev = static_cast<int*>(dalloc(e, sizeof(int)));
@@ -1148,15 +1348,15 @@ template <typename T>
 void rhs_noalloc(shhd_engine* e, const double* state_dev, double* rhs_dev, unsigned char* base) {
     const StepPlan& P = e->P;
     const size_t cs = sizeof(cplx<T>);
-    const auto twx = e->row_fixed ? stage_table<T>(e->cfg.nx) : twiddle_table<T>(e->cfg.nx);
-    const auto twy = e->col_fixed ? stage_table<T>(e->cfg.ny) : twiddle_table<T>(e->cfg.ny);
+    const auto twx = host_twiddles<T>(e, e->cfg.nx, e->row_fixed);
+    const auto twy = host_twiddles<T>(e, e->cfg.ny, e->col_fixed);
     ScratchCarver sc{base};
     void* act_in = sc.take(e->state_elems * cs);
     void* act_out = sc.take(e->state_elems * cs);
     e->i1 = sc.take(e->i1_elems * cs);
     e->i2 = sc.take(e->i2_elems * cs);
-    e->tw_x = sc.take(twx.size() * cs);
-    e->tw_y = sc.take(twy.size() * cs);
+    e->tw_x = sc.take(twx.size());
+    e->tw_y = sc.take(twy.size());
     e->rho0_dev = static_cast<double*>(sc.take(sizeof(double)));
     e->err_dev = static_cast<int*>(sc.take(sizeof(int)));
     e->flag_dev = static_cast<int*>(sc.take(sizeof(int)));
@@ -1172,8 +1372,8 @@ void rhs_noalloc(shhd_engine* e, const double* state_dev, double* rhs_dev, unsig
     mi.step0 = 0;
     mi.noise_scale = 1.0;
     // the array keeps the previous call's contents: rewrite or clear everything read before written
-    check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, s), "twiddle upload");
-    check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size() * cs, cudaMemcpyHostToDevice, s), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size(), cudaMemcpyHostToDevice, s), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size(), cudaMemcpyHostToDevice, s), "twiddle upload");
     check_cuda(cudaMemcpyAsync(e->members_dev, &mi, sizeof(mi), cudaMemcpyHostToDevice, s), "member upload");
     check_cuda(cudaMemsetAsync(e->err_dev, 0, sizeof(int), s), "error word clear");
     check_cuda(cudaMemsetAsync(e->flag_dev, 0, sizeof(int), s), "flag clear");

@@ -91,6 +91,17 @@ struct StepPlan {
     int row_lb;                    // max lines per row transform call
     int row_nb;                    // work lines for outputs
     int npos;                      // position slots per thread in col_forward
+    // pair-line row pass: outputs transformed two at a time, each product a
+    // combination of the terms psi^3, psi vx, psi vy, vx, vy, jx vx, jx vy, jy vy
+    // with per-output coefficients; inputs read from canonical (line, half) roles
+    int rp_n;                      // output pairs
+    int rp_a[kMaxOut], rp_b[kMaxOut];          // output indices (rp_b = -1: single)
+    float rp_coef[kMaxOut][8][2];  // [pair][term][A, B]
+    int rp_canon;                  // 1: roles below are valid (else the generic product path)
+    int rp_prep;                   // 1: rewrite (rho, jx), (jy, -) into (jx, jy), (vx, vy)
+    int rp_jline, rp_vline;        // line of (jx, jy) and of (vx, vy) (-1: v = j / rho0)
+    int rp_mode[kMaxOut];          // 0 coefficient form; 1 (vx, vy); 2 (jx vx, jy vy);
+                                   // 3 c0 psi^3, 4 c1 psi vx, 5 c2 psi vy with psi = (psi_a, psi_b) one line
 };
 
 // per-member controls of a batched engine (serving): noise key, step origin
