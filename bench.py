@@ -2,7 +2,9 @@
 """Benchmark of the step engine on the headline workload.
 
 Workload (the reference's Hohenberg-Halperin compressible configuration):
-1024x1024 active grid (3/2 rule -> 1536^2 compute grid), Lx = Ly = 1024,
+1024x1024 active grid (3/2 rule -> 1536^2 compute grid), Lx = Ly = 2048 (grid
+spacing 2, which keeps -M k^2 (a + b k^2) dt of every active mode inside the
+SRK3 stability interval at dt = 0.01; at spacing 1 the highest modes grow),
 N = 2 order parameters with phi4 free energy (mu_a = -psi_a + psi_a^3 -
 lap psi_a), M_a = 1, rho0 = 1, eta = zeta = 1, linear EOS cT = 1, advection of
 psi and j, conservative noise kBT = 1e-3, psi initial state equilibrium
@@ -43,7 +45,7 @@ L2_BYTES = 126 * 1024 * 1024
 WORKLOAD = """dimension 2
 boundary p p
 grid 1024 1024
-length 1024 1024
+length 2048 2048
 dealias 3/2
 order_parameters 2
 timestep 0.01
@@ -54,14 +56,15 @@ model transport constant eta 1 zeta 1 M[0,0] 1 M[1,1] 1
 fix 1 all nonlinear on
 fix 2 all noise on seed 7 kBT 1e-3
 set density uniform value 1.0
-set order_parameter all equilibrium/gaussian seed 7 kBT 0.010019559897527924 k0 1 k2 0
+set order_parameter all equilibrium/gaussian seed 7 kBT 0.0400782395901117 k0 1 k2 0
 run 10000
 """
 
-# ensemble configuration: 256 members, 256^2 (3/2 -> 384^2), quiescent phi4 quench
+# ensemble configuration: 256 members, 256^2 (3/2 -> 384^2), quiescent phi4 quench; grid spacing 2
+# (length 512) keeps -M k^2 (a + b k^2) dt inside the SRK3 stability interval at dt = 0.02
 ENSEMBLE = """dimension 2
 grid 256 256
-length 256 256
+length 512 512
 dealias 3/2
 order_parameters 1
 timestep 0.02
@@ -70,13 +73,14 @@ model free_energy phi4 a[0] -1 b[0] 1 u[0] 1
 model transport constant eta 0 zeta 0 M[0,0] 1
 fix 1 order_parameter noise on seed 0 kBT 0.05
 set density uniform value 1.0
-set order_parameter all equilibrium/gaussian seed 0 kBT 0.010078585159554018 k0 1 k2 0
+set order_parameter all equilibrium/gaussian seed 0 kBT 0.040314340638216074 k0 1 k2 0
 run 5000
 """
 
 CONFIG = {
     "workload": "HH compressible 1024^2 (3/2 -> 1536^2), N=2 phi4, advection + noise, SRK3 dt=0.01",
     "grid": [1024, 1024],
+    "length": [2048, 2048],
     "compute_grid": [1536, 1536],
     "order_parameters": 2,
     "mode": "srk3/compressible",
@@ -444,6 +448,8 @@ def run_extras(args, world, rank, local, sb, initial_state, torch):
                       "ensemble_steps_per_s": world * nb / (ms / 1e3) / world, "workload": "256 x 256^2 (3/2), quiescent N=1 phi4, SRK3, FP32"}
     eng.close()
 
+    out["served"] = run_served(sb, initial_state, torch)
+
     # cuFFT beside it: the same transforms per stage (5 C2R + 11 R2C at 1536^2, FP32)
     x = torch.randn(11, 1536, 1536, device="cuda", dtype=torch.float32)
     X = torch.fft.rfft2(x[:5])
@@ -461,6 +467,81 @@ def run_extras(args, world, rank, local, sb, initial_state, torch):
     out["cufft_reference"] = {"ms_per_stage": ms_stage, "steps_per_s_transforms_only": 1e3 / (3 * ms_stage),
                               "what": "torch.fft (cuFFT) 5 irfft2 + 11 rfft2 at 1536^2 FP32 per stage, unfused, no products or RHS"}
     return out
+
+
+# ---------------------------------------------------------------------------
+# served stream: Poisson arrivals of mixed trajectory jobs
+# ---------------------------------------------------------------------------
+SERVED = {"jobs": 32, "rate_per_s": 20.0, "grids": (128, 256, 512), "steps": (200, 800), "seed": 5,
+          "what": "Poisson arrivals (20 jobs/s, seed 5) of trajectory jobs drawn uniformly from grids {128,256,512}^2 (3/2 rule, spacing 2), "
+                  "N in {0..3}, mode in {compressible, incompressible, quiescent}, kBT in [1e-4, 1e-2], 200-800 SRK3 steps; "
+                  "bounded sample of the served configuration (grids up to 2048^2 and 10^3-2x10^4 steps scaled down to finish "
+                  "in seconds; no Green-Kubo measure)"}
+
+
+def served_job_scripts():
+    """(arrival time, script, steps) of the seeded served-stream sample."""
+    import numpy as np
+    rng = np.random.default_rng(SERVED["seed"])
+    t = 0.0
+    out = []
+    for _ in range(SERVED["jobs"]):
+        t += rng.exponential(1.0 / SERVED["rate_per_s"])
+        na = int(rng.choice(SERVED["grids"]))
+        mode = str(rng.choice(["compressible", "incompressible", "quiescent"]))
+        nop = int(rng.integers(0, 4))
+        if mode == "quiescent" and nop == 0:
+            nop = 1
+        kbt = float(rng.uniform(1e-4, 1e-2))
+        nsteps = int(rng.integers(SERVED["steps"][0], SERVED["steps"][1] + 1))
+        lines = ["dimension 2", f"grid {na} {na}", f"length {2 * na} {2 * na}", "dealias 3/2", f"order_parameters {nop}", "timestep 0.01",
+                 f"time_evolution srk3/{mode}"]
+        if mode == "compressible":
+            lines.append("model thermo linear_eos cT 1")
+        if nop:
+            lines.append("model free_energy phi4 " + " ".join(f"a[{a}] -1 b[{a}] 1 u[{a}] 1" for a in range(nop)))
+        eta = {"compressible": 1.0, "incompressible": 0.1, "quiescent": 0.0}[mode]
+        zeta = 1.0 if mode == "compressible" else 0.0
+        lines.append(f"model transport constant eta {eta} zeta {zeta} " + " ".join(f"M[{a},{a}] 1" for a in range(nop)))
+        if mode != "quiescent":
+            lines.append("fix 1 all nonlinear on")
+        lines.append(f"fix 2 all noise on seed 1 kBT {kbt}")
+        lines.append("set density uniform value 1.0")
+        if nop:
+            lines.append("set order_parameter all equilibrium/gaussian seed 3 kBT 0.0001 k0 1 k2 0")
+        lines.append(f"run {nsteps}")
+        out.append((t, "\n".join(lines) + "\n", nsteps))
+    return out
+
+
+def run_served(sb, initial_state, torch):
+    from shhd_b200 import serve
+    specs = served_job_scripts()
+    jobs = []
+    for k, (t, text, n) in enumerate(specs):
+        cfg = sb.config_from_script(text)
+        jobs.append(serve.Job(key=100 + k, config=cfg, state=initial_state(cfg, text), nsteps=n, arrival=t))
+    total_steps = sum(j.nsteps for j in jobs)
+    srv = serve.Server(precision=sb.FP32, seed=77, max_slots=8, chunk=25)
+    stats = srv.run(jobs)
+    srv.close()
+    # the same jobs one at a time through the plain FP64 path (engine creation not timed)
+    t_serial = 0.0
+    for j in jobs:
+        c = j.config.copy()
+        c.precision = sb.FP64
+        with sb.Engine(c) as eng:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.set_state(j.state)
+            eng.step(j.nsteps)
+            eng.get_state()
+            t_serial += time.perf_counter() - t0
+    serial = total_steps / t_serial
+    return {"value": stats["steps_per_s"], "unit": "steps/s (aggregate over jobs)", "p50_s": stats["p50_s"], "p99_s": stats["p99_s"],
+            "makespan_s": stats["makespan_s"], "jobs": stats["jobs"], "buckets": stats["buckets"], "total_steps": total_steps,
+            "precision": "f32", "plain_fp64_serial_steps_per_s": serial, "served_over_plain_fp64": stats["steps_per_s"] / serial,
+            "what": SERVED["what"]}
 
 
 def main():

@@ -178,6 +178,16 @@ int shhd_engine_rhs(shhd_engine* engine, int member, double* det, size_t n_doubl
  * member's cached reference density (a new trajectory). */
 int shhd_engine_set_member(shhd_engine* engine, int member, uint32_t key, int64_t step_origin, double noise_scale, int active);
 
+/* Replay of captured CUDA graphs (no reference counterpart).  With chunk > 0,
+ * a step call of n >= chunk steps runs floor(n / chunk) replays of one
+ * captured graph holding a call of `chunk` steps (its launches and the advance
+ * of the device-side step counter that keys the noise), then the remainder as
+ * ordinary launches; the result equals floor(n / chunk) calls of `chunk` steps
+ * plus one call of the rest.  Euler chunks are rounded up to an even count.
+ * 0 (the default) launches every kernel directly.  Per-kernel profiling uses
+ * direct launches. */
+int shhd_engine_set_graph_chunk(shhd_engine* engine, int chunk);
+
 /* Step counter and time (project.h:136-137). */
 int shhd_engine_set_time(shhd_engine* engine, int64_t step_index, double time);
 

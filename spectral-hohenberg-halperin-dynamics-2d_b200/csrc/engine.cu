@@ -214,6 +214,13 @@ struct shhd_engine {
 
     void* ref_stage = nullptr;       // one member's reference-layout state (FP64) on the device
     int* flag_dev = nullptr;
+    unsigned long long* step_dev = nullptr;  // step index at the start of the current call
+
+    // captured step graph: one call of `graph_chunk` steps, replayed
+    int graph_chunk = 0;
+    cudaGraphExec_t graph_exec = nullptr;
+    int64_t graph_launches[4] = {0, 0, 0, 0};
+    double graph_bytes[4] = {0, 0, 0, 0};
 
     // per-kernel statistics: 0 col_inverse, 1 row_pass, 2 col_forward, 3 other
     bool profiling = false;
@@ -245,6 +252,8 @@ void free_engine(shhd_engine* e) {
                     static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev)})
         if (p) cudaFree(p);
+    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    if (e->step_dev) cudaFree(e->step_dev);
     for (auto& pe : e->pending) { e->event_pool.push_back(pe.a); e->event_pool.push_back(pe.b); }
     for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -887,16 +896,17 @@ StageArgs<T> stage_args(shhd_engine* e, const void* cur, const void* base, void*
     A.wb = wb; A.wc = wc; A.beta = beta;
     A.dt = e->cfg.dt;
     A.sdt = std::sqrt(e->cfg.dt);
-    A.step = static_cast<uint64_t>(e->step_index);
+    A.step_base = e->step_dev;
+    A.step_off = 0;
     A.srk3 = srk3;
     A.fused_inverse = fused;
     A.det_mode = 0;
     return A;
 }
 
+// the launches of one call of nsteps steps (step indices relative to *step_dev)
 template <typename T>
-void enqueue_steps(shhd_engine* e, int nsteps) {
-    ensure_rho0(e);
+void record_steps(shhd_engine* e, int nsteps) {
     prepare_static<T>(e);
     launch_col_inverse<T>(e, e->u);
     const bool srk3 = e->cfg.integrator == SHHD_SRK3;
@@ -908,15 +918,75 @@ void enqueue_steps(shhd_engine* e, int nsteps) {
             for (int k = 0; k < 3; ++k) {
                 launch_row<T>(e);
                 const int fused = !(last_step && k == 2);
-                launch_col_forward<T>(e, stage_args<T>(e, cur[k], e->u, nxt[k], kWb[k], kWc[k], kBeta[k], 1, fused));
+                StageArgs<T> A = stage_args<T>(e, cur[k], e->u, nxt[k], kWb[k], kWc[k], kBeta[k], 1, fused);
+                A.step_off = s;
+                launch_col_forward<T>(e, A);
             }
         } else {
             launch_row<T>(e);
-            launch_col_forward<T>(e, stage_args<T>(e, e->u, e->u, e->s1, 0.0, 1.0, 0.0, 0, last_step ? 0 : 1));
+            StageArgs<T> A = stage_args<T>(e, e->u, e->u, e->s1, 0.0, 1.0, 0.0, 0, last_step ? 0 : 1);
+            A.step_off = s;
+            launch_col_forward<T>(e, A);
             std::swap(e->u, e->s1);
         }
-        e->step_index += 1;
-        e->time += e->cfg.dt;
+    }
+}
+
+void set_step_dev(shhd_engine* e) {
+    set_step_kernel<<<1, 1, 0, e->stream>>>(e->step_dev, static_cast<unsigned long long>(e->step_index));
+    check_cuda(cudaGetLastError(), "set_step launch");
+}
+
+// capture one call of graph_chunk steps (plus the advance of the step counter) as a graph
+template <typename T>
+void capture_graph(shhd_engine* e) {
+    const int K = e->graph_chunk;
+    int64_t l0[4];
+    double b0[4];
+    for (int k = 0; k < 4; ++k) { l0[k] = e->kernel_launches[k]; b0[k] = e->kernel_bytes[k]; }
+    check_cuda(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    cudaGraph_t g = nullptr;
+    try {
+        record_steps<T>(e, K);
+        advance_step_kernel<<<1, 1, 0, e->stream>>>(e->step_dev, static_cast<unsigned long long>(K));
+        check_cuda(cudaGetLastError(), "advance_step launch");
+    } catch (...) {
+        cudaStreamEndCapture(e->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    check_cuda(cudaStreamEndCapture(e->stream, &g), "cudaStreamEndCapture");
+    const cudaError_t rc = cudaGraphInstantiate(&e->graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    check_cuda(rc, "cudaGraphInstantiate");
+    for (int k = 0; k < 4; ++k) {
+        e->graph_launches[k] = e->kernel_launches[k] - l0[k];
+        e->graph_bytes[k] = e->kernel_bytes[k] - b0[k];
+        e->kernel_launches[k] = l0[k];
+        e->kernel_bytes[k] = b0[k];
+    }
+}
+
+template <typename T>
+void enqueue_steps(shhd_engine* e, int nsteps) {
+    ensure_rho0(e);
+    set_step_dev(e);
+    int done = 0;
+    const int K = e->graph_chunk;
+    if (K > 0 && !e->profiling && nsteps >= K) {
+        if (!e->graph_exec) capture_graph<T>(e);
+        for (; done + K <= nsteps; done += K) {
+            check_cuda(cudaGraphLaunch(e->graph_exec, e->stream), "cudaGraphLaunch");
+            for (int k = 0; k < 4; ++k) { e->kernel_launches[k] += e->graph_launches[k]; e->kernel_bytes[k] += e->graph_bytes[k]; }
+        }
+        e->step_index += done;
+        e->time += done * e->cfg.dt;
+        if (done < nsteps) set_step_dev(e);
+    }
+    if (done < nsteps) {
+        record_steps<T>(e, nsteps - done);
+        e->step_index += nsteps - done;
+        e->time += (nsteps - done) * e->cfg.dt;
     }
 }
 
@@ -1054,6 +1124,7 @@ void init_device(shhd_engine* e) {
     e->rho0_dev = static_cast<double*>(dalloc(e, sizeof(double) * B));
     check_cuda(cudaMemsetAsync(e->rho0_dev, 0, sizeof(double) * B, e->stream), "memset");
     e->err_dev = static_cast<int*>(dalloc(e, sizeof(int)));
+    e->step_dev = static_cast<unsigned long long*>(dalloc(e, sizeof(unsigned long long)));
     e->members_dev = static_cast<MemberInfo*>(dalloc(e, sizeof(MemberInfo) * B));
     e->members.resize(B);
     for (size_t m = 0; m < B; ++m) {
@@ -1238,6 +1309,22 @@ int shhd_engine_set_member(shhd_engine* e, int member, uint32_t key, int64_t ste
         mi.active = active ? 1 : 0;
         e->rho0_cached[member] = 0;  // a new trajectory: rho0 is taken again at its first use
         e->members_dirty = true;
+    });
+}
+
+int shhd_engine_set_graph_chunk(shhd_engine* e, int chunk) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (chunk < 0) throw Failure(SHHD_EINVAL, "graph chunk must be nonnegative");
+        // Euler swaps its two state buffers every step: a replayed chunk must hold an even number of steps
+        if (chunk > 0 && e->cfg.integrator == SHHD_EULER && chunk % 2) ++chunk;
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+        if (e->graph_exec) {
+            check_cuda(cudaGraphExecDestroy(e->graph_exec), "cudaGraphExecDestroy");
+            e->graph_exec = nullptr;
+        }
+        e->graph_chunk = chunk;
     });
 }
 

@@ -126,7 +126,8 @@ struct StageArgs {
     const double* rho0;            // per member
     int* err;
     double wb, wc, dt, sdt, beta;
-    uint64_t step;
+    const unsigned long long* step_base;  // step index at the start of the call (device; graph replays advance it)
+    int step_off;                  // step of this stage within the call
     int srk3;                      // draw b exists
     int fused_inverse;
     int det_mode;                  // write det instead of the stage update
@@ -464,7 +465,8 @@ __device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageAr
         if (A.srk3) sto = cadd(sto, cscale(L.eb, beta));
     } else if (P.noise_psi[alpha] && m.k_nonzero) {
         const T sigma = sqrt(static_cast<T>(P.psi_sig2[alpha]) * k2) * static_cast<T>(mi.noise_scale);
-        sto = psi_noise<T>(P, alpha, A.step - static_cast<uint64_t>(mi.step0), mi.key, m.mode_id, m.conj_line, sigma, A.srk3 != 0, beta);
+        const uint64_t step = *A.step_base + static_cast<uint64_t>(A.step_off);
+        sto = psi_noise<T>(P, alpha, step - static_cast<uint64_t>(mi.step0), mi.key, m.mode_id, m.conj_line, sigma, A.srk3 != 0, beta);
     }
     const C inner = cadd(cadd(cur, cscale(det, static_cast<T>(A.dt))), cscale(sto, static_cast<T>(A.sdt)));
     return cadd(cscale(L.base, static_cast<T>(A.wb)), cscale(inner, static_cast<T>(A.wc)));
@@ -539,7 +541,8 @@ __device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const Stage
             sy = cadd(sy, cscale(L.eby, beta));
         }
     } else if (P.noise_j && m.k_nonzero) {
-        j_noise<T>(P, A.step - static_cast<uint64_t>(mi.step0), mi.key, m.mode_id, m.conj_line, kx, kyv, A.srk3 != 0, beta,
+        const uint64_t step = *A.step_base + static_cast<uint64_t>(A.step_off);
+        j_noise<T>(P, step - static_cast<uint64_t>(mi.step0), mi.key, m.mode_id, m.conj_line, kx, kyv, A.srk3 != 0, beta,
                    static_cast<T>(mi.noise_scale), sx, sy);
     }
     const T dt = static_cast<T>(A.dt), sdt = static_cast<T>(A.sdt), wb = static_cast<T>(A.wb), wc = static_cast<T>(A.wc);
@@ -711,6 +714,11 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
         __syncthreads();
     }
 }
+
+// step counter of the call: set from the host at the start of a call, advanced
+// by the last node of a captured step graph
+__global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }
+__global__ void advance_step_kernel(unsigned long long* step, unsigned long long by) { *step += by; }
 
 // ---------------------------------------------------------------------------
 // fields the integrator only copies: symmetrise the kx = 0 line once and

@@ -100,7 +100,7 @@ EXPORTED = (
     "shhd_engine_info", "shhd_engine_set_state", "shhd_engine_get_state", "shhd_engine_step", "shhd_engine_step_async",
     "shhd_engine_synchronize", "shhd_engine_set_external_noise", "shhd_engine_rhs", "shhd_engine_set_time",
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
-    "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc",
+    "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -135,6 +135,7 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_reset_stats.argtypes = [vp]
     lib.shhd_engine_set_member.argtypes = [vp, i, ctypes.c_uint32, ctypes.c_int64, ctypes.c_double, i]
     lib.shhd_rhs_noalloc.argtypes = [ctypes.POINTER(Config), vp, vp, sz, vp]
+    lib.shhd_engine_set_graph_chunk.argtypes = [vp, i]
     return lib
 
 
@@ -240,6 +241,10 @@ class Engine:
     def set_member(self, member: int, key: int, step_origin: int = 0, noise_scale: float = 1.0, active: bool = True) -> None:
         """Per-member noise key, step origin, amplitude factor and active flag (serving)."""
         _check(lib.shhd_engine_set_member(self._h, member, int(key) & 0xFFFFFFFF, int(step_origin), float(noise_scale), 1 if active else 0))
+
+    def set_graph_chunk(self, chunk: int) -> None:
+        """Replay captured CUDA graphs of `chunk` steps (0: direct launches)."""
+        _check(lib.shhd_engine_set_graph_chunk(self._h, int(chunk)))
 
     def set_profiling(self, on: bool) -> None:
         _check(lib.shhd_engine_set_profiling(self._h, 1 if on else 0))

@@ -59,7 +59,7 @@ def _noisy(cfg: Config) -> bool:
 
 
 class _Bucket:
-    def __init__(self, cfg: Config, slots: int, precision: int, seed: int):
+    def __init__(self, cfg: Config, slots: int, precision: int, seed: int, graph_chunk: int = 0):
         c = cfg.copy()
         c.batch = slots
         c.precision = precision
@@ -68,6 +68,8 @@ class _Bucket:
         if _noisy(cfg):
             c.kBT = 1.0  # members carry sqrt(kBT_job) as their amplitude factor
         self.engine = Engine(c)
+        if graph_chunk > 0:
+            self.engine.set_graph_chunk(graph_chunk)
         self.slots: List[Optional[Job]] = [None] * slots
         self.remaining = [0] * slots
         self.step_index = 0
@@ -95,8 +97,9 @@ class _Bucket:
 
 class Server:
     def __init__(self, precision: int = FP32, seed: int = 20240601, max_slots: int = 32, chunk: int = 25,
-                 hbm_budget: Optional[int] = None):
+                 hbm_budget: Optional[int] = None, graphs: bool = True):
         import torch
+        self.graphs = graphs
         self.precision = precision
         self.seed = seed
         self.max_slots = max_slots
@@ -126,7 +129,7 @@ class Server:
         slots = min(self.max_slots, (self.budget - self.used) // per)
         if slots < 1:
             return None
-        b = _Bucket(job.config, int(slots), self.precision, self.seed)
+        b = _Bucket(job.config, int(slots), self.precision, self.seed, self.chunk if self.graphs else 0)
         self.used += int(b.engine.get_info().device_bytes)
         self.buckets.setdefault(key, []).append(b)
         return b, 0

@@ -183,7 +183,7 @@ def test_conservation_and_symmetry_full_size(sb):
     """1024^2, N = 2 compressible (the headline workload) in FP32: mass and
     momentum (k = 0 modes) are conserved, the kx = 0 line stays Hermitian, and
     FP32 stays within tolerance of FP64 over a few steps."""
-    text = script(grid=(1024, 1024), length=(1024.0, 1024.0), nop=2, dt=0.01, noise="kBT 0.001 seed 7")
+    text = script(grid=(1024, 1024), length=(2048.0, 2048.0), nop=2, dt=0.01, noise="kBT 0.001 seed 7")
     cfg = so.parse_script(text)
     u0 = random_state(cfg, seed=9, amp=0.05)
     with make_engine(sb, text, 1) as e32, make_engine(sb, text, 0) as e64:
