@@ -188,6 +188,19 @@ int shhd_engine_set_member(shhd_engine* engine, int member, uint32_t key, int64_
  * direct launches. */
 int shhd_engine_set_graph_chunk(shhd_engine* engine, int chunk);
 
+/* Structure factor of one field (no reference counterpart; the reference's
+ * closest data are `snapshot space spectral` dumps, measure_snapshot.cc).
+ * shhd_engine_sk_accumulate enqueues, on the engine stream, the addition of
+ * S(k) = V |u_k|^2 / Np^4 averaged over the active members to an FP64
+ * accumulator on the device (one sample; u_k the unnormalised padded-grid
+ * coefficient, so S(k) -> kBT / (k0 + k2 k^2) for a quadratic free energy in
+ * equilibrium).  shhd_engine_sk_read copies the sum of the samples in the
+ * engine's mode order [gx < active_nx/2][j < active_ny - 1] (j = ky for
+ * ky >= 0, else ky + active_ny - 1), sets *count to the number of samples and,
+ * with reset != 0, clears the accumulator.  One field at a time. */
+int shhd_engine_sk_accumulate(shhd_engine* engine, int field);
+int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_t* count, int reset);
+
 /* Step counter and time (project.h:136-137). */
 int shhd_engine_set_time(shhd_engine* engine, int64_t step_index, double time);
 

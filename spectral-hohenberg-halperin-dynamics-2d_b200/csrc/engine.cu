@@ -187,6 +187,9 @@ struct shhd_engine {
     void* tw_x = nullptr;
     void* tw_y = nullptr;
     double* rho0_dev = nullptr;
+    double* sk_dev = nullptr;        // FP64 structure-factor accumulator [Hx * Ky] (allocated on first use)
+    int64_t sk_count = 0;
+    int sk_field = -1;
     int* err_dev = nullptr;
     MemberInfo* members_dev = nullptr;
     std::vector<MemberInfo> members;
@@ -253,6 +256,7 @@ void free_engine(shhd_engine* e) {
                     static_cast<void*>(e->flag_dev)})
         if (p) cudaFree(p);
     if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    if (e->sk_dev) cudaFree(e->sk_dev);
     if (e->step_dev) cudaFree(e->step_dev);
     for (auto& pe : e->pending) { e->event_pool.push_back(pe.a); e->event_pool.push_back(pe.b); }
     for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
@@ -1309,6 +1313,53 @@ int shhd_engine_set_member(shhd_engine* e, int member, uint32_t key, int64_t ste
         mi.active = active ? 1 : 0;
         e->rho0_cached[member] = 0;  // a new trajectory: rho0 is taken again at its first use
         e->members_dirty = true;
+    });
+}
+
+int shhd_engine_sk_accumulate(shhd_engine* e, int field) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (field < 0 || field >= e->P.nfields) throw Failure(SHHD_EINVAL, "field index out of range");
+        if (e->sk_count > 0 && field != e->sk_field) throw Failure(SHHD_EINVAL, "the accumulator holds another field: read it with reset first");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        const StepPlan& P = e->P;
+        const size_t modes = static_cast<size_t>(P.hx) * P.kyn;
+        if (!e->sk_dev) {
+            e->sk_dev = static_cast<double*>(dalloc(e, modes * sizeof(double)));
+            check_cuda(cudaMemsetAsync(e->sk_dev, 0, modes * sizeof(double), e->stream), "memset");
+        }
+        int active = 0;
+        for (const MemberInfo& m : e->members) active += m.active ? 1 : 0;
+        if (active == 0) throw Failure(SHHD_EINVAL, "no active member");
+        upload_members(e);
+        const double np2 = static_cast<double>(e->cfg.nx) * e->cfg.ny;
+        const double scale = e->cfg.lx * e->cfg.ly / (np2 * np2) / active;
+        const dim3 g(static_cast<unsigned>((modes + kThreads - 1) / kThreads));
+        if (e->fp32)
+            structure_factor_kernel<float><<<g, kThreads, 0, e->stream>>>(P, e->members_dev, static_cast<const float2*>(e->u), field, scale, e->sk_dev);
+        else
+            structure_factor_kernel<double><<<g, kThreads, 0, e->stream>>>(P, e->members_dev, static_cast<const double2*>(e->u), field, scale, e->sk_dev);
+        check_cuda(cudaGetLastError(), "structure_factor launch");
+        e->sk_field = field;
+        e->sk_count += 1;
+    });
+}
+
+int shhd_engine_sk_read(shhd_engine* e, double* out, size_t n_modes, int64_t* count, int reset) {
+    return guarded([&] {
+        if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");
+        const size_t modes = static_cast<size_t>(e->P.hx) * e->P.kyn;
+        if (n_modes != modes) throw Failure(SHHD_EINVAL, "mode count mismatch: expected " + std::to_string(modes));
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (count) *count = e->sk_count;
+        if (!e->sk_dev || e->sk_count == 0) {
+            std::memset(out, 0, modes * sizeof(double));
+            return;
+        }
+        check_cuda(cudaMemcpyAsync(out, e->sk_dev, modes * sizeof(double), cudaMemcpyDeviceToHost, e->stream), "sk download");
+        if (reset) check_cuda(cudaMemsetAsync(e->sk_dev, 0, modes * sizeof(double), e->stream), "sk reset");
+        check_cuda(cudaStreamSynchronize(e->stream), "sk sync");
+        if (reset) { e->sk_count = 0; e->sk_field = -1; }
     });
 }
 

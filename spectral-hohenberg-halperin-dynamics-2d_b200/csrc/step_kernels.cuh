@@ -715,6 +715,27 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
     }
 }
 
+// ---------------------------------------------------------------------------
+// structure factor S(k) = V <|u_k|^2> / Np^4 of one field, mean over the
+// active members, added in FP64 to acc[mode] (engine mode order); grid:
+// ceil(Hx * Ky / 256).  `scale` = V / Np^4 / (active members).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kThreads) structure_factor_kernel(const StepPlan P, const MemberInfo* __restrict__ members,
+                                                                    const cplx<T>* __restrict__ state, int field, double scale,
+                                                                    double* __restrict__ acc) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
+    if (e >= static_cast<int>(fstride)) return;
+    double s = 0.0;
+    for (int b = 0; b < P.batch; ++b) {
+        if (!members[b].active) continue;
+        const cplx<T> v = state[(static_cast<size_t>(b) * P.nfields + field) * fstride + e];
+        s += static_cast<double>(v.x) * static_cast<double>(v.x) + static_cast<double>(v.y) * static_cast<double>(v.y);
+    }
+    acc[e] += s * scale;
+}
+
 // step counter of the call: set from the host at the start of a call, advanced
 // by the last node of a captured step graph
 __global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }

@@ -101,6 +101,7 @@ EXPORTED = (
     "shhd_engine_synchronize", "shhd_engine_set_external_noise", "shhd_engine_rhs", "shhd_engine_set_time",
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
     "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
+    "shhd_engine_sk_accumulate", "shhd_engine_sk_read",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -136,6 +137,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_set_member.argtypes = [vp, i, ctypes.c_uint32, ctypes.c_int64, ctypes.c_double, i]
     lib.shhd_rhs_noalloc.argtypes = [ctypes.POINTER(Config), vp, vp, sz, vp]
     lib.shhd_engine_set_graph_chunk.argtypes = [vp, i]
+    lib.shhd_engine_sk_accumulate.argtypes = [vp, i]
+    lib.shhd_engine_sk_read.argtypes = [vp, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
     return lib
 
 
@@ -245,6 +248,18 @@ class Engine:
     def set_graph_chunk(self, chunk: int) -> None:
         """Replay captured CUDA graphs of `chunk` steps (0: direct launches)."""
         _check(lib.shhd_engine_set_graph_chunk(self._h, int(chunk)))
+
+    def sk_accumulate(self, field: int) -> None:
+        """Add one FP64 sample of S(k) = V <|u_k|^2> / Np^4 (mean over active members) on the device."""
+        _check(lib.shhd_engine_sk_accumulate(self._h, int(field)))
+
+    def sk_read(self, reset: bool = True):
+        """(sum of the S(k) samples as [gx, j] in the engine's mode order, number of samples)."""
+        n = self.info.active_modes
+        out = np.zeros(n, dtype=np.float64)
+        cnt = ctypes.c_int64()
+        _check(lib.shhd_engine_sk_read(self._h, _dptr(out), n, ctypes.byref(cnt), 1 if reset else 0))
+        return out.reshape(self.cfg.active_nx // 2, self.cfg.active_ny - 1), int(cnt.value)
 
     def set_profiling(self, on: bool) -> None:
         _check(lib.shhd_engine_set_profiling(self._h, 1 if on else 0))

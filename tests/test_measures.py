@@ -1,0 +1,93 @@
+"""Device measures with FP64 accumulation: the structure factor S(k) (GPU).
+
+S(k) = V <|u_k|^2> / Np^4 over the active members, summed over samples in
+FP64 on the device.  Checked exactly against the states read back, and
+physically against equipartition, S(k) = kBT / (k0 + k2 k^2), for a Gaussian
+(phi4 with u = 0) order parameter started in and kept at equilibrium by the
+conservative noise.
+"""
+import numpy as np
+import pytest
+
+import shhd_oracle as so
+from helpers import random_state, script
+
+pytestmark = pytest.mark.gpu
+
+
+def _modes_from_ref(state_field, cfg):
+    """[gx, j] active modes (engine order) of one field given in the reference layout [gy, gx]."""
+    hx, kyn = cfg.active_nx // 2, cfg.active_ny - 1
+    out = np.zeros((hx, kyn), dtype=np.complex128)
+    for j in range(kyn):
+        ky = j if j < cfg.active_ny // 2 else j - kyn
+        gy = ky if ky >= 0 else ky + cfg.ny
+        out[:, j] = state_field[gy, :hx]
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_structure_factor_matches_states(precision):
+    import shhd_b200 as sb
+    text = script(grid=(32, 48), length=(64.0, 96.0), nop=2, dt=0.01)
+    cfg = sb.config_from_script(text)
+    cfg.precision = precision
+    cfg.batch = 3
+    ocfg = so.parse_script(text)
+    with sb.Engine(cfg) as eng:
+        for m in range(3):
+            eng.set_state(random_state(ocfg, seed=40 + m), member=m)
+        eng.set_member(1, key=7, active=False)   # inactive members are left out of the mean
+        field = 2                                # psi_1
+        eng.sk_accumulate(field)
+        eng.step(2)
+        eng.sk_accumulate(field)
+        got, n = eng.sk_read()
+        assert n == 2
+        want = np.zeros_like(got)
+        for m in (0, 2):
+            want += np.abs(_modes_from_ref(eng.get_state(m)[field], cfg)) ** 2
+        # the first sample was taken before the two steps: add it from the initial states
+        for m in (0, 2):
+            want += np.abs(_modes_from_ref(random_state(ocfg, seed=40 + m)[field], cfg)) ** 2
+        want *= cfg.lx * cfg.ly / float(cfg.nx * cfg.ny) ** 2 / 2
+        tol = 1e-12 if precision == 0 else 1e-5
+        assert np.abs(got - want).max() <= tol * np.abs(want).max()
+        again, n2 = eng.sk_read()
+        assert n2 == 0 and not again.any()       # read with reset cleared it
+
+
+def test_structure_factor_equipartition():
+    import shhd_b200 as sb
+    from shhd_b200.initial import initial_state
+    na, L, kbt, a, b = 32, 64.0, 0.05, 1.0, 1.0
+    base = "\n".join([
+        "dimension 2", f"grid {na} {na}", f"length {L} {L}", "dealias 3/2", "order_parameters 1", "timestep 0.01",
+        "time_evolution srk3/quiescent", f"model free_energy phi4 a[0] {a} b[0] {b} u[0] 0",
+        "model transport constant eta 0 zeta 0 M[0,0] 1", f"fix 1 order_parameter noise on seed 4 kBT {kbt}",
+        "set density uniform value 1.0",
+        f"set order_parameter all equilibrium/gaussian seed SEED kBT {kbt} k0 {a} k2 {b}", "run 1", ""])
+    members = 64
+    cfg = sb.config_from_script(base.replace("SEED", "0"))
+    cfg.precision = sb.FP32
+    cfg.batch = members
+    with sb.Engine(cfg) as eng:
+        for m in range(members):
+            eng.set_state(initial_state(cfg, base.replace("SEED", str(m + 1))), member=m)
+        for _ in range(20):
+            eng.step(10)
+            eng.sk_accumulate(1)
+        sk, n = eng.sk_read()
+    assert n == 20
+    sk /= n
+    hx, kyn = na // 2, na - 1
+    gx = np.arange(hx)[:, None]
+    ky = np.array([j if j < na // 2 else j - kyn for j in range(kyn)])[None, :]
+    k2 = (2 * np.pi / L) ** 2 * (gx ** 2 + ky ** 2)
+    theory = kbt / (a + b * k2)
+    # shells of |k| below 1 (SRK3 keeps the stationary law there to well under a percent)
+    kk = np.sqrt(k2)
+    for lo in np.arange(0.1, 1.0, 0.2):
+        sel = (kk >= lo) & (kk < lo + 0.2)
+        ratio = sk[sel].mean() / theory[sel].mean()
+        assert abs(ratio - 1.0) < 0.05, (lo, ratio)
