@@ -187,6 +187,9 @@ struct shhd_engine {
     void* tw_x = nullptr;
     void* tw_y = nullptr;
     double* rho0_dev = nullptr;
+    double2* k0_u = nullptr;         // FP64 k = 0 modes [member][field] of u, s1, s2 (FP32 engines)
+    double2* k0_s1 = nullptr;
+    double2* k0_s2 = nullptr;
     double* sk_dev = nullptr;        // FP64 structure-factor accumulator [Hx * Ky] (allocated on first use)
     int64_t sk_count = 0;
     int sk_field = -1;
@@ -250,6 +253,8 @@ void* dalloc(shhd_engine* e, size_t bytes) {
 }
 
 void free_engine(shhd_engine* e) {
+    for (void* p : {static_cast<void*>(e->k0_u), static_cast<void*>(e->k0_s1), static_cast<void*>(e->k0_s2)})
+        if (p) cudaFree(p);
     for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->ref_stage,
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
                     static_cast<void*>(e->members_dev),
@@ -897,6 +902,17 @@ StageArgs<T> stage_args(shhd_engine* e, const void* cur, const void* base, void*
     A.ext_b = static_cast<const cplx<T>*>(e->ext_b);
     A.rho0 = e->rho0_dev;
     A.err = e->err_dev;
+    auto k0_of = [&](const void* st) -> double2* {
+        if (!e->k0_u) return nullptr;
+        if (st == e->u) return e->k0_u;
+        if (st == e->s1) return e->k0_s1;
+        if (st == e->s2) return e->k0_s2;
+        return nullptr;
+    };
+    A.k0_cur = k0_of(cur);
+    A.k0_base = k0_of(base);
+    A.k0_next = k0_of(next);
+    if (!A.k0_cur || !A.k0_base || !A.k0_next) A.k0_cur = A.k0_base = A.k0_next = nullptr;
     A.wb = wb; A.wc = wc; A.beta = beta;
     A.dt = e->cfg.dt;
     A.sdt = std::sqrt(e->cfg.dt);
@@ -932,6 +948,7 @@ void record_steps(shhd_engine* e, int nsteps) {
             A.step_off = s;
             launch_col_forward<T>(e, A);
             std::swap(e->u, e->s1);
+            std::swap(e->k0_u, e->k0_s1);
         }
     }
 }
@@ -1129,6 +1146,13 @@ void init_device(shhd_engine* e) {
     check_cuda(cudaMemsetAsync(e->rho0_dev, 0, sizeof(double) * B, e->stream), "memset");
     e->err_dev = static_cast<int*>(dalloc(e, sizeof(int)));
     e->step_dev = static_cast<unsigned long long*>(dalloc(e, sizeof(unsigned long long)));
+    if (e->fp32) {
+        const size_t k0b = sizeof(double2) * B * e->P.nfields;
+        e->k0_u = static_cast<double2*>(dalloc(e, k0b));
+        e->k0_s1 = static_cast<double2*>(dalloc(e, k0b));
+        e->k0_s2 = static_cast<double2*>(dalloc(e, k0b));
+        for (double2* p : {e->k0_u, e->k0_s1, e->k0_s2}) check_cuda(cudaMemsetAsync(p, 0, k0b, e->stream), "memset");
+    }
     e->members_dev = static_cast<MemberInfo*>(dalloc(e, sizeof(MemberInfo) * B));
     e->members.resize(B);
     for (size_t m = 0; m < B; ++m) {
@@ -1235,6 +1259,15 @@ int shhd_engine_set_state(shhd_engine* e, int member, const double* state, size_
         if (e->fp32) upload_ref<float>(e, state, e->u, member, true);
         else upload_ref<double>(e, state, e->u, member, true);
         e->rho0_candidate[member] = state[0] / (static_cast<double>(e->cfg.nx) * e->cfg.ny);
+        if (e->k0_u) {  // FP64 copies of the k = 0 modes
+            const size_t block = static_cast<size_t>(e->cfg.nx / 2 + 1) * e->cfg.ny * 2;  // doubles per field
+            std::vector<double2> k0(e->P.nfields);
+            for (int f = 0; f < e->P.nfields; ++f) k0[f] = make_double2(state[f * block], state[f * block + 1]);
+            check_cuda(cudaMemcpyAsync(e->k0_u + static_cast<size_t>(member) * e->P.nfields, k0.data(), sizeof(double2) * k0.size(),
+                                       cudaMemcpyHostToDevice, e->stream),
+                       "k0 upload");
+            check_cuda(cudaStreamSynchronize(e->stream), "k0 upload sync");
+        }
     });
 }
 
@@ -1246,6 +1279,22 @@ int shhd_engine_get_state(shhd_engine* e, int member, double* state, size_t n) {
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         if (e->fp32) download_ref<float>(e, e->u, member, state);
         else download_ref<double>(e, e->u, member, state);
+        if (e->k0_u) {  // the evolved fields' k = 0 modes from their FP64 copies
+            std::vector<double2> k0(e->P.nfields);
+            check_cuda(cudaMemcpyAsync(k0.data(), e->k0_u + static_cast<size_t>(member) * e->P.nfields, sizeof(double2) * k0.size(),
+                                       cudaMemcpyDeviceToHost, e->stream),
+                       "k0 download");
+            check_cuda(cudaStreamSynchronize(e->stream), "k0 download sync");
+            const size_t block = static_cast<size_t>(e->cfg.nx / 2 + 1) * e->cfg.ny * 2;
+            const int nop = e->cfg.num_order_parameters;
+            for (int f = 0; f < e->P.nfields; ++f) {
+                const bool evolved = e->cfg.mode == SHHD_COMPRESSIBLE || (f >= 1 && f <= nop) ||
+                                     (e->cfg.mode == SHHD_INCOMPRESSIBLE && f > nop);
+                if (!evolved) continue;
+                state[f * block] = k0[f].x;
+                state[f * block + 1] = k0[f].y;
+            }
+        }
     });
 }
 

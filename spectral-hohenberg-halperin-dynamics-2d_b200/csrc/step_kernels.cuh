@@ -124,6 +124,11 @@ struct StageArgs {
     const cplx<T>* ext_a;
     const cplx<T>* ext_b;
     const double* rho0;            // per member
+    // FP64 copies of the k = 0 mode of every field ([member][field]) for the
+    // current, base and next state (FP32 engines; null otherwise)
+    const double2* k0_cur;
+    const double2* k0_base;
+    double2* k0_next;
     int* err;
     double wb, wc, dt, sdt, beta;
     const unsigned long long* step_base;  // step index at the start of the call (device; graph replays advance it)
@@ -432,6 +437,20 @@ __device__ __forceinline__ PsiLoads<T> psi_loads(const StepPlan& P, const StageA
     return L;
 }
 
+// Stage update of the k = 0 mode in FP64 from the FP64 copies (FP32 engines):
+// the RHS there is zero unless a force acts on it, so the FP32 update would only
+// add rounding to the conserved mass, momentum and order-parameter means.  The
+// mode is self-conjugate, so its imaginary part is zero (time_integrator.h:70-109).
+template <typename T>
+__device__ __forceinline__ cplx<T> k0_update(const StepPlan& P, const StageArgs<T>& A, int b, int f, cplx<T> det, cplx<T> sto) {
+    const int i = b * P.nfields + f;
+    const double cur = A.k0_cur[i].x;
+    const double base = A.wb != 0.0 ? A.k0_base[i].x : 0.0;
+    const double v = A.wb * base + A.wc * (cur + A.dt * static_cast<double>(det.x) + A.sdt * static_cast<double>(sto.x));
+    A.k0_next[i] = make_double2(v, 0.0);
+    return mk(static_cast<T>(v), T(0));
+}
+
 // psi_alpha: det from the accumulated products plus the spectral terms, then
 // (unless det_mode) the stage update with noise; returns next (or det)
 template <typename T>
@@ -468,6 +487,7 @@ __device__ __forceinline__ cplx<T> psi_epilogue(const StepPlan& P, const StageAr
         const uint64_t step = *A.step_base + static_cast<uint64_t>(A.step_off);
         sto = psi_noise<T>(P, alpha, step - static_cast<uint64_t>(mi.step0), mi.key, m.mode_id, m.conj_line, sigma, A.srk3 != 0, beta);
     }
+    if (A.k0_cur && !m.k_nonzero) return k0_update<T>(P, A, b, f, det, sto);
     const C inner = cadd(cadd(cur, cscale(det, static_cast<T>(A.dt))), cscale(sto, static_cast<T>(A.sdt)));
     return cadd(cscale(L.base, static_cast<T>(A.wb)), cscale(inner, static_cast<T>(A.wc)));
 }
@@ -553,6 +573,11 @@ __device__ __forceinline__ void momentum_epilogue(const StepPlan& P, const Stage
         incx = cscale(cscale(tr, -kyv), T(1) / k2);
         incy = cscale(cscale(tr, kx), T(1) / k2);
     }
+    if (A.k0_cur && !m.k_nonzero) {
+        a0 = k0_update<T>(P, A, b, f_jx, djx, sx);
+        a1 = k0_update<T>(P, A, b, f_jy, djy, sy);
+        return;
+    }
     a0 = cadd(cscale(L.bjx, wb), cscale(cadd(cjx, incx), wc));
     a1 = cadd(cscale(L.bjy, wb), cscale(cadd(cjy, incy), wc));
 }
@@ -563,6 +588,8 @@ __device__ __forceinline__ cplx<T> rho_epilogue(const StepPlan& P, const StageAr
     using C = cplx<T>;
     const C drho = cmulmi(cadd(cscale(A.cur[pos + (P.nop + 1) * fstride], kx), cscale(A.cur[pos + (P.nop + 2) * fstride], kyv)));
     if (A.det_mode) return drho;
+    if (A.k0_cur && kx == T(0) && kyv == T(0))
+        return k0_update<T>(P, A, static_cast<int>(pos / (static_cast<size_t>(P.nfields) * fstride)), 0, drho, czero<C>());
     const C base = (A.wb != 0.0) ? A.base[pos] : czero<C>();
     return cadd(cscale(base, static_cast<T>(A.wb)), cscale(cadd(A.cur[pos], cscale(drho, static_cast<T>(A.dt))), static_cast<T>(A.wc)));
 }

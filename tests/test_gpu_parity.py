@@ -238,3 +238,23 @@ def test_set_state_rejects_inactive_modes(sb):
         with pytest.raises(sb.ShhdError) as ei:
             eng.set_state(bad)
         assert ei.value.code == sb.SHHD_EINVAL
+
+
+def test_fp32_keeps_k0_modes_in_fp64(sb):
+    """FP32 engines carry the k = 0 modes (mass, momentum, order-parameter means) in FP64:
+    their RHS is zero, so over many steps they keep their initial values to FP64 rounding."""
+    text = script(grid=(64, 64), length=(128.0, 128.0), nop=2, dt=0.01, noise="kBT 0.001 seed 3")
+    cfg = so.parse_script(text)
+    u0 = random_state(cfg, seed=8)
+    g = so.Geometry(cfg)
+    means = [1.0, 0.3, -0.2, 0.05, -0.07]          # rho, psi_0, psi_1, jx, jy (real-space means)
+    for f, mval in enumerate(means):
+        u0[f, 0, 0] = mval * g.grid_size
+    with make_engine(sb, text, 1) as e:
+        e.set_state(u0)
+        for _ in range(3):
+            e.step(100)
+        u = e.get_state()
+    assert np.all(np.isfinite(u))
+    for f in range(len(means)):
+        assert abs(u[f, 0, 0] - u0[f, 0, 0]) <= 1e-13 * abs(u0[f, 0, 0]), (f, u[f, 0, 0], u0[f, 0, 0])
