@@ -446,6 +446,15 @@ def run_extras(args, world, rank, local, sb, initial_state, torch):
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     out["batched"] = {"value": world * nb * cfg.batch / (ms / 1e3), "unit": "member-steps/s", "members": cfg.batch * world,
                       "ensemble_steps_per_s": world * nb / (ms / 1e3) / world, "workload": "256 x 256^2 (3/2), quiescent N=1 phi4, SRK3, FP32"}
+    # structure factor of psi over the members (FP64 on the device), summed over ranks by one all-reduce
+    from shhd_b200.ensemble import reduce_structure_factor
+    for _ in range(4):
+        eng.step(5)
+        eng.sk_accumulate(1)
+    sk_sum, nsamp = eng.sk_read()
+    sk_mean, total_members = reduce_structure_factor(sk_sum, nsamp, cfg.batch, device="cuda" if world > 1 else None)
+    out["batched"]["structure_factor"] = {"members": total_members, "samples": nsamp, "mean_over_modes": float(sk_mean.mean()),
+                                          "what": "S(k) = V <|psi_k|^2> / Np^4, FP64 member mean per rank, FP64 all-reduce over ranks"}
     eng.close()
 
     out["served"] = run_served(sb, initial_state, torch)
