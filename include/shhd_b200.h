@@ -201,6 +201,17 @@ int shhd_engine_set_graph_chunk(shhd_engine* engine, int chunk);
 int shhd_engine_sk_accumulate(shhd_engine* engine, int field);
 int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_t* count, int reset);
 
+/* Autotuner (no reference counterpart).  Times trial_steps steps of every
+ * kernel family valid for the configuration (FP32 compute sizes 96-1536: the
+ * pair-line kernels and the single-line kernels; otherwise the one family)
+ * with direct launches and as one replayed graph, on the engine's current
+ * state, then restores the state, step counter and time and keeps the fastest
+ * combination.  *family: 1 pair-line, 0 other; *graph_chunk: the chosen
+ * chunk (0 = direct launches); ms_per_step (optional): the measured ms per
+ * step of each candidate in order (family 0 direct, family 0 graph, family 1
+ * direct, family 1 graph).  Allocates a temporary copy of the state. */
+int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
+
 /* Step counter and time (project.h:136-137). */
 int shhd_engine_set_time(shhd_engine* engine, int64_t step_index, double time);
 

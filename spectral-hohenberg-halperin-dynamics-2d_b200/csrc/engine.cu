@@ -206,6 +206,8 @@ struct shhd_engine {
     bool col_fixed = false;       // compile-time column kernels (group per column)
     bool row_fixed = false;       // compile-time row kernel (group per line)
     bool pair_path = false;       // FP32 pair-line kernels (compile-time sizes up to 1536)
+    int family_override = -1;     // -1 choose, 0 never the pair-line kernels, 1 pair-line where valid
+    size_t tw_bytes = 0;
     size_t smem_col_inv = 0;
     size_t smem_col = 0, smem_row = 0;
     int n_evolved = 0;
@@ -645,7 +647,7 @@ void build_plan(shhd_engine* e) {
 
     // FP32 pair-line kernels: both compute sizes in 96 ... 1536, column pairs
     // that tile the active kx range, row pairs that tile the compute rows
-    if (e->fp32 && is_pair_size(c.nx) && is_pair_size(c.ny) && P.hx % 2 == 0) {
+    if (e->family_override != 0 && e->fp32 && is_pair_size(c.nx) && is_pair_size(c.ny) && P.hx % 2 == 0) {
         const int cp = kPairMaxN / c.ny, rp = kPairMaxN / c.nx;
         const int nip = (P.n_in + 1) / 2;
         const size_t row_b = static_cast<size_t>(rp) * (nip + 1) * c.nx * 16;
@@ -1140,6 +1142,7 @@ void init_device(shhd_engine* e) {
     const auto twy = host_twiddles<T>(e, e->cfg.ny, e->col_fixed);
     e->tw_x = dalloc(e, twx.size());
     e->tw_y = dalloc(e, twy.size());
+    e->tw_bytes = twx.size() + twy.size();
     check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
     check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
     e->rho0_dev = static_cast<double*>(dalloc(e, sizeof(double) * B));
@@ -1409,6 +1412,137 @@ int shhd_engine_sk_read(shhd_engine* e, double* out, size_t n_modes, int64_t* co
         if (reset) check_cuda(cudaMemsetAsync(e->sk_dev, 0, modes * sizeof(double), e->stream), "sk reset");
         check_cuda(cudaStreamSynchronize(e->stream), "sk sync");
         if (reset) { e->sk_count = 0; e->sk_field = -1; }
+    });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// autotuner: kernel family x graph chunk, timed on the engine's own state
+// ---------------------------------------------------------------------------
+namespace {
+
+// switch kernel family: new plan, twiddle tables and shared-memory limits (buffer sizes are
+// the same for every family); any captured graph is dropped
+template <typename T>
+void apply_family(shhd_engine* e, int family) {
+    check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+    if (e->graph_exec) {
+        check_cuda(cudaGraphExecDestroy(e->graph_exec), "cudaGraphExecDestroy");
+        e->graph_exec = nullptr;
+    }
+    e->family_override = family;
+    e->pair_path = e->col_fixed = e->row_fixed = false;
+    build_plan(e);
+    for (void* p : {e->tw_x, e->tw_y})
+        if (p) cudaFree(p);
+    e->device_bytes -= e->tw_bytes;
+    const auto twx = host_twiddles<T>(e, e->cfg.nx, e->row_fixed);
+    const auto twy = host_twiddles<T>(e, e->cfg.ny, e->col_fixed);
+    e->tw_x = dalloc(e, twx.size());
+    e->tw_y = dalloc(e, twy.size());
+    e->tw_bytes = twx.size() + twy.size();
+    check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    set_smem_attrs<T>(e);
+    check_cuda(cudaStreamSynchronize(e->stream), "family sync");
+}
+
+template <typename T>
+void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, double* ms_out) {
+    if (trial_steps < 1) throw Failure(SHHD_EINVAL, "trial_steps must be positive");
+    if (e->cfg.noise_source == SHHD_NOISE_EXTERNAL) throw Failure(SHHD_EINVAL, "autotune needs Philox noise (external noise steps one at a time)");
+    check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+    const size_t bytes = e->state_elems * e->cfg.batch * sizeof(cplx<T>);
+    const size_t k0b = e->k0_u ? sizeof(double2) * e->cfg.batch * e->P.nfields : 0;
+    void* save = nullptr;
+    void* save_k0 = nullptr;
+    check_cuda(cudaMalloc(&save, bytes), "autotune save buffer");
+    if (k0b) check_cuda(cudaMalloc(&save_k0, k0b), "autotune save buffer");
+    cudaEvent_t a = nullptr, b = nullptr;
+    const int64_t step0 = e->step_index;
+    const double time0 = e->time;
+    const int64_t l0[4] = {e->kernel_launches[0], e->kernel_launches[1], e->kernel_launches[2], e->kernel_launches[3]};
+    const double b0[4] = {e->kernel_bytes[0], e->kernel_bytes[1], e->kernel_bytes[2], e->kernel_bytes[3]};
+    const bool prof = e->profiling;
+    e->profiling = false;
+    auto restore = [&] {
+        check_cuda(cudaMemcpyAsync(e->u, save, bytes, cudaMemcpyDeviceToDevice, e->stream), "autotune restore");
+        if (k0b) check_cuda(cudaMemcpyAsync(e->k0_u, save_k0, k0b, cudaMemcpyDeviceToDevice, e->stream), "autotune restore");
+        e->step_index = step0;
+        e->time = time0;
+    };
+    try {
+        check_cuda(cudaMemcpyAsync(save, e->u, bytes, cudaMemcpyDeviceToDevice, e->stream), "autotune save");
+        if (k0b) check_cuda(cudaMemcpyAsync(save_k0, e->k0_u, k0b, cudaMemcpyDeviceToDevice, e->stream), "autotune save");
+        check_cuda(cudaEventCreate(&a), "cudaEventCreate");
+        check_cuda(cudaEventCreate(&b), "cudaEventCreate");
+        // candidates: kernel families valid for this configuration x {direct launches, one graph of trial_steps}
+        std::vector<int> families = {0};
+        {
+            shhd_engine probe = *e;  // host copy for planning only: is the pair-line family valid here?
+            probe.family_override = 1;
+            probe.pair_path = probe.col_fixed = probe.row_fixed = false;
+            build_plan(&probe);
+            if (probe.pair_path) families.push_back(1);
+        }
+        int chunk_trial = trial_steps;
+        if (e->cfg.integrator == SHHD_EULER && chunk_trial % 2) ++chunk_trial;
+        double best = 1e300;
+        int best_family = 0, best_chunk = 0, idx = 0;
+        for (int fam : families) {
+            apply_family<T>(e, fam);
+            for (int chunk : {0, chunk_trial}) {
+                e->graph_chunk = chunk;
+                if (e->graph_exec) { cudaGraphExecDestroy(e->graph_exec); e->graph_exec = nullptr; }
+                enqueue(e, chunk_trial);  // warm-up (and capture)
+                check_cuda(cudaEventRecord(a, e->stream), "cudaEventRecord");
+                enqueue(e, chunk_trial);
+                check_cuda(cudaEventRecord(b, e->stream), "cudaEventRecord");
+                sync_and_check(e);
+                float ms = 0.f;
+                check_cuda(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+                const double per = ms / chunk_trial;
+                if (ms_out) ms_out[idx] = per;
+                ++idx;
+                if (per < best) { best = per; best_family = fam; best_chunk = chunk; }
+                restore();
+            }
+        }
+        if (e->graph_exec) { cudaGraphExecDestroy(e->graph_exec); e->graph_exec = nullptr; }
+        apply_family<T>(e, best_family);
+        e->graph_chunk = best_chunk;
+        if (family_out) *family_out = best_family;
+        if (chunk_out) *chunk_out = best_chunk;
+    } catch (...) {
+        e->profiling = prof;
+        cudaStreamSynchronize(e->stream);
+        cudaFree(save);
+        if (save_k0) cudaFree(save_k0);
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+        throw;
+    }
+    restore();
+    check_cuda(cudaStreamSynchronize(e->stream), "autotune sync");
+    for (int k = 0; k < 4; ++k) { e->kernel_launches[k] = l0[k]; e->kernel_bytes[k] = b0[k]; }
+    e->profiling = prof;
+    cudaFree(save);
+    if (save_k0) cudaFree(save_k0);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int shhd_engine_autotune(shhd_engine* e, int trial_steps, int* family, int* graph_chunk, double* ms_per_step) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) autotune<float>(e, trial_steps, family, graph_chunk, ms_per_step);
+        else autotune<double>(e, trial_steps, family, graph_chunk, ms_per_step);
     });
 }
 

@@ -101,7 +101,7 @@ EXPORTED = (
     "shhd_engine_synchronize", "shhd_engine_set_external_noise", "shhd_engine_rhs", "shhd_engine_set_time",
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
     "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
-    "shhd_engine_sk_accumulate", "shhd_engine_sk_read",
+    "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -139,6 +139,7 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_set_graph_chunk.argtypes = [vp, i]
     lib.shhd_engine_sk_accumulate.argtypes = [vp, i]
     lib.shhd_engine_sk_read.argtypes = [vp, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
+    lib.shhd_engine_autotune.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), dp]
     return lib
 
 
@@ -260,6 +261,14 @@ class Engine:
         cnt = ctypes.c_int64()
         _check(lib.shhd_engine_sk_read(self._h, _dptr(out), n, ctypes.byref(cnt), 1 if reset else 0))
         return out.reshape(self.cfg.active_nx // 2, self.cfg.active_ny - 1), int(cnt.value)
+
+    def autotune(self, trial_steps: int = 3) -> dict:
+        """Time the valid kernel families x {direct, graph} on the current state; keep the fastest."""
+        fam, chunk = ctypes.c_int(), ctypes.c_int()
+        ms = np.full(4, np.nan)
+        _check(lib.shhd_engine_autotune(self._h, int(trial_steps), ctypes.byref(fam), ctypes.byref(chunk), _dptr(ms)))
+        return {"family": "pair-line" if fam.value == 1 else "single-line", "graph_chunk": chunk.value,
+                "ms_per_step": [None if np.isnan(x) else float(x) for x in ms]}
 
     def set_profiling(self, on: bool) -> None:
         _check(lib.shhd_engine_set_profiling(self._h, 1 if on else 0))

@@ -81,3 +81,25 @@ def test_euler_chunks_round_to_even():
         got = g.get_state()
         assert np.all(np.isfinite(got))
         assert np.array_equal(got, d.get_state())
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autotune_restores_state_and_keeps_results(precision):
+    import shhd_b200 as sb
+    cfg = so.parse_script(SRK3)
+    u0 = random_state(cfg, seed=21)
+    ref = u0
+    o = so.Oracle(cfg)
+    for _ in range(4):
+        ref = o.step(ref, "philox")
+    with _engine(sb, SRK3, precision) as e:
+        e.set_state(u0)
+        before = e.get_state()
+        choice = e.autotune(2)
+        assert choice["family"] in ("pair-line", "single-line")
+        timed = [x for x in choice["ms_per_step"] if x is not None]
+        assert len(timed) == (4 if precision == 1 else 2) and all(x > 0 for x in timed)
+        assert e.get_info().step_index == 0
+        assert np.array_equal(e.get_state(), before)
+        e.step(4)
+        assert so.rel_l2(e.get_state(), ref) < (1e-12 if precision == 0 else 1e-5)
