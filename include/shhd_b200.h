@@ -212,6 +212,21 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * direct, family 1 graph).  Allocates a temporary copy of the state. */
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
+/* Yokota-Green-Kubo stress measure (measure_yokota_green_kubo.cc:16-225),
+ * accumulated on the device in FP64.  shhd_engine_gk_enable selects the wave
+ * vectors as the reference does (selection 0 "diagonal": (n, n), 1 "all"),
+ * and from then on every step adds, per member and mode, the step's momentum
+ * flux pi_xy (stage-weighted deterministic flux plus the first noise draw's
+ * flux / sqrt(dt)) to the block integral I and, every `nevery` steps of a
+ * block of `nblock`, |I|^2 / (2 tau kBT V) to the sum for that tau.  A
+ * member's blocks count from its own first step (serving: step_origin).
+ * shhd_engine_gk_read copies one member's sums in [tau][mode] order
+ * (ntau = nblock / nevery; the reference's S_mean = sum / *nsample) and the
+ * number of completed blocks since the last reset.  Needs kBT > 0, momentum
+ * dynamics and the engine's own (Philox) noise. */
+int shhd_engine_gk_enable(shhd_engine* engine, int nevery, int nblock, int selection);
+int shhd_engine_gk_read(shhd_engine* engine, int member, double* sums, size_t n, int64_t* nsample, int reset);
+
 /* Step counter and time (project.h:136-137). */
 int shhd_engine_set_time(shhd_engine* engine, int64_t step_index, double time);
 

@@ -674,6 +674,133 @@ class Oracle:
         return out
 
 
+    # --- momentum flux pi_xy and the Yokota-Green-Kubo accumulation --------
+    def momentum_flux_xy(self, state: np.ndarray) -> np.ndarray:
+        """Deterministic pi_xy of one RHS evaluation, as j_det records it in the flux
+        buffer: viscous (fcalculator.cc:302-341 incompressible, 343-398 compressible)
+        plus advection (fcalculator.cc:400-494); the pressure enters pi_xx, pi_yy only."""
+        cfg, g = self.cfg, self.geo
+        n = cfg.num_order_parameters
+        act = g.active
+        kx, ky = g.kx, g.ky
+        out = np.zeros((g.ny, g.hx), dtype=np.complex128)
+        if cfg.mode == "quiescent":
+            return out
+        eta, zeta = cfg.eta, cfg.zeta
+        has_visc = eta != 0.0 or zeta != 0.0
+        if not (cfg.cT * cfg.cT != 0.0 or has_visc or cfg.momentum_advection):
+            return out
+        p = None
+        if has_visc and cfg.mode == "incompressible" and eta != 0.0:
+            rho0 = self.reference_density(state)
+            out += np.where(act, -1j * eta * (ky * state[n + 1] / rho0 + kx * state[n + 2] / rho0), 0.0)
+        if has_visc and cfg.mode == "compressible":
+            p = self.physical_fields(state)
+            vx, vy = g.forward(p["vx"]), g.forward(p["vy"])
+            out += np.where(act, -1j * eta * (ky * vx + kx * vy), 0.0)
+        if cfg.momentum_advection:
+            p = p or self.physical_fields(state)
+            out += np.where(act, g.forward(p["jx"] * p["vy"]), 0.0)
+        return out
+
+    def noise_flux_xy(self, xi3: np.ndarray) -> np.ndarray:
+        """pi_xy of one j_sto draw (fcalculator.cc:587-700): -s sqrt(eta) xi3 on the
+        active k != 0 modes with gx > 0, and on the kx = 0 line the drawn half with
+        its conjugate partner."""
+        cfg, g = self.cfg, self.geo
+        out = np.zeros((g.ny, g.hx), dtype=np.complex128)
+        if not (cfg.noise_momentum and cfg.mode != "quiescent" and cfg.kBT != 0.0 and (cfg.eta != 0.0 or cfg.zeta != 0.0)):
+            return out
+        use = g.active & (g.k2 != 0.0)
+        line = use & (g.gx == 0) & (g.gy < (g.ny - g.gy) % g.ny)
+        bulk = use & (g.gx != 0)
+        s = math.sqrt(0.5 * 2.0 * cfg.kBT * g.grid_size * g.grid_size / g.volume)
+        pxy = -s * math.sqrt(cfg.eta) * xi3
+        out = np.where(bulk, pxy, 0.0)
+        lv = np.where(line, pxy, 0.0)[:, 0]
+        conj_rows = (g.ny - np.arange(g.ny)) % g.ny
+        out[:, 0] += lv
+        out[conj_rows, 0] += np.conj(lv)
+        return out
+
+    def step_with_flux(self, u: np.ndarray, noise=None):
+        """(next state, step flux pi_xy): the SRK3 stage-weighted deterministic flux
+        (1/6, 1/6, 2/3; Euler 1) plus the first draw's stochastic flux / sqrt(dt)
+        (time_integrator_srk3_compressible.h:99-146, buffer_flux.cc:170-195)."""
+        cfg = self.cfg
+        step = self.step_index
+        flux = np.zeros((self.geo.ny, self.geo.hx), dtype=np.complex128)
+        if cfg.integrator == "euler":
+            flux += self.momentum_flux_xy(u)
+            out = self.step(u, noise)
+        else:
+            noisy = cfg.noise_order_parameter or (cfg.noise_momentum and cfg.mode != "quiescent")
+            if noise == "philox" and noisy:
+                sa, sb = self.philox_noise(step)
+            elif noise is None or not noisy:
+                sa = sb = np.zeros(self.shape, dtype=np.complex128)
+            else:
+                sa, sb = noise
+            u1 = self._stage(u, u, sa + BETA[0] * sb, *STAGE_WEIGHTS[0])
+            u2 = self._stage(u1, u, sa + BETA[1] * sb, *STAGE_WEIGHTS[1])
+            out = self._stage(u2, u, sa + BETA[2] * sb, *STAGE_WEIGHTS[2])
+            for w, cur in zip((1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0), (u, u1, u2)):
+                flux += w * self.momentum_flux_xy(cur)
+            self.step_index += 1
+            self.time += cfg.dt
+        if noise == "philox":
+            xa = philox_normals(cfg.noise_seed, self.member, step, j_stream(2), self.mode_ids())[0]
+            flux += self.noise_flux_xy(xa) / math.sqrt(cfg.dt)
+        return out, flux
+
+
+def green_kubo_modes(cfg: Config, selection: str = "diagonal") -> List[Tuple[int, int]]:
+    """Wave numbers (nx, ny) of measure_yokota_green_kubo.cc:42-96."""
+    max_nx = max(0, cfg.active[0] // 2 - 1)
+    max_ny = max(0, cfg.active[1] // 2 - 1)
+    if selection == "diagonal":
+        return [(n, n) for n in range(1, min(max_nx, max_ny) + 1)]
+    out = [(0, n) for n in range(1, max_ny + 1)]
+    for nx in range(1, max_nx + 1):
+        for ny in range(-max_ny, max_ny + 1):
+            out.append((nx, ny))
+    return out
+
+
+class GreenKubo:
+    """YokotaGreenKuboMeasure::observe (measure_yokota_green_kubo.cc:128-190) over
+    a step flux pi_xy given per step; S sums per (tau, mode) and completed blocks."""
+
+    def __init__(self, cfg: Config, nevery: int, nblock: int, selection: str = "diagonal", kBT: Optional[float] = None):
+        self.cfg = cfg
+        self.geo = Geometry(cfg)
+        self.nevery, self.nblock = nevery, nblock
+        self.ntau = nblock // nevery
+        self.kBT = cfg.kBT if kBT is None else kBT
+        self.modes = green_kubo_modes(cfg, selection)
+        g = self.geo
+        self.index = [(ny % g.ny, nx) for nx, ny in self.modes]
+        self.integrals = np.zeros(len(self.modes), dtype=np.complex128)
+        self.sums = np.zeros((self.ntau, len(self.modes)))
+        self.block_step = 0
+        self.nsample = 0
+
+    def observe(self, flux: np.ndarray) -> None:
+        self.block_step += 1
+        area = self.geo.volume
+        cell_area = area / self.geo.grid_size
+        wdt = 0.5 * self.cfg.dt if self.block_step == 1 else self.cfg.dt
+        self.integrals += wdt * cell_area * np.array([flux[gy, gx] for gy, gx in self.index])
+        if self.block_step % self.nevery == 0:
+            ti = self.block_step // self.nevery - 1
+            tau = self.block_step * self.cfg.dt
+            self.sums[ti] += np.abs(self.integrals) ** 2 / (2.0 * tau * self.kBT * area)
+        if self.block_step == self.nblock:
+            self.nsample += 1
+            self.block_step = 0
+            self.integrals[:] = 0.0
+
+
 # --------------------------------------------------------------------------
 # layout helpers shared by the tests
 # --------------------------------------------------------------------------

@@ -191,6 +191,11 @@ struct shhd_engine {
     double2* k0_s1 = nullptr;
     double2* k0_s2 = nullptr;
     double* sk_dev = nullptr;        // FP64 structure-factor accumulator [Hx * Ky] (allocated on first use)
+    // Yokota-Green-Kubo taps (FP64): selected modes, step flux, block integrals, sums [member][tau][mode]
+    bool gk_on = false;
+    GkArgs gk{};
+    std::vector<int2> gk_modes;
+    std::vector<int64_t> gk_sample_base;
     int64_t sk_count = 0;
     int sk_field = -1;
     int* err_dev = nullptr;
@@ -264,6 +269,9 @@ void free_engine(shhd_engine* e) {
         if (p) cudaFree(p);
     if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
     if (e->sk_dev) cudaFree(e->sk_dev);
+    for (const void* p : {static_cast<const void*>(e->gk.modes), static_cast<const void*>(e->gk.flux_step), static_cast<const void*>(e->gk.integral),
+                          static_cast<const void*>(e->gk.sums), static_cast<const void*>(e->gk.wtab)})
+        if (p) cudaFree(const_cast<void*>(p));
     if (e->step_dev) cudaFree(e->step_dev);
     for (auto& pe : e->pending) { e->event_pool.push_back(pe.a); e->event_pool.push_back(pe.b); }
     for (cudaEvent_t ev : e->event_pool) cudaEventDestroy(ev);
@@ -926,6 +934,16 @@ StageArgs<T> stage_args(shhd_engine* e, const void* cur, const void* base, void*
     return A;
 }
 
+template <typename T>
+void launch_gk_tap(shhd_engine* e, const void* cur, int step_off, double weight, int first, int last) {
+    if (!e->gk_on) return;
+    const int warps = e->P.batch * e->gk.nmodes;
+    const dim3 g(static_cast<unsigned>((static_cast<long long>(warps) * 32 + kThreads - 1) / kThreads));
+    gk_tap_kernel<T><<<g, kThreads, 0, e->stream>>>(e->P, e->gk, e->members_dev, static_cast<const T*>(e->i2), static_cast<const cplx<T>*>(cur),
+                                                    e->rho0_dev, e->step_dev, step_off, weight, first, last, e->cfg.dt);
+    check_cuda(cudaGetLastError(), "gk_tap launch");
+}
+
 // the launches of one call of nsteps steps (step indices relative to *step_dev)
 template <typename T>
 void record_steps(shhd_engine* e, int nsteps) {
@@ -943,12 +961,15 @@ void record_steps(shhd_engine* e, int nsteps) {
                 StageArgs<T> A = stage_args<T>(e, cur[k], e->u, nxt[k], kWb[k], kWc[k], kBeta[k], 1, fused);
                 A.step_off = s;
                 launch_col_forward<T>(e, A);
+                // stage flux weights 1/6, 1/6, 2/3 (time_integrator_srk3_compressible.h:15-21)
+                launch_gk_tap<T>(e, cur[k], s, k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0, k == 2);
             }
         } else {
             launch_row<T>(e);
             StageArgs<T> A = stage_args<T>(e, e->u, e->u, e->s1, 0.0, 1.0, 0.0, 0, last_step ? 0 : 1);
             A.step_off = s;
             launch_col_forward<T>(e, A);
+            launch_gk_tap<T>(e, e->u, s, 1.0, 1, 1);
             std::swap(e->u, e->s1);
             std::swap(e->k0_u, e->k0_s1);
         }
@@ -1543,6 +1564,94 @@ int shhd_engine_autotune(shhd_engine* e, int trial_steps, int* family, int* grap
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         if (e->fp32) autotune<float>(e, trial_steps, family, graph_chunk, ms_per_step);
         else autotune<double>(e, trial_steps, family, graph_chunk, ms_per_step);
+    });
+}
+
+int shhd_engine_gk_enable(shhd_engine* e, int nevery, int nblock, int selection) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (e->gk_on) throw Failure(SHHD_EINVAL, "the Green-Kubo measure is already enabled");
+        if (nevery <= 0 || nblock <= 0) throw Failure(SHHD_EINVAL, "nevery and nblock must be positive");
+        if (nblock % nevery != 0) throw Failure(SHHD_EINVAL, "nblock must be a multiple of nevery");
+        if (!(e->cfg.kBT > 0.0)) throw Failure(SHHD_EINVAL, "YokotaGreenKuboMeasure requires positive kBT from fix noise.");
+        if (e->cfg.mode == SHHD_QUIESCENT) throw Failure(SHHD_EUNSUPPORTED, "the Green-Kubo stress measure needs momentum dynamics (not quiescent)");
+        if (e->cfg.noise_source == SHHD_NOISE_EXTERNAL) throw Failure(SHHD_EUNSUPPORTED, "the Green-Kubo measure needs the engine's own noise draws");
+        if (selection != 0 && selection != 1) throw Failure(SHHD_EINVAL, "YokotaGreenKuboMeasure: mode must be diagonal|all.");
+        const StepPlan& P = e->P;
+        // wave numbers of measure_yokota_green_kubo.cc:42-96
+        const int max_nx = std::max(0, e->cfg.active_nx / 2 - 1), max_ny = std::max(0, e->cfg.active_ny / 2 - 1);
+        std::vector<int2> modes;
+        if (selection == 0) {
+            for (int n = 1; n <= std::min(max_nx, max_ny); ++n) modes.push_back(make_int2(n, n));
+        } else {
+            for (int n = 1; n <= max_ny; ++n) modes.push_back(make_int2(0, n));
+            for (int nx = 1; nx <= max_nx; ++nx)
+                for (int ny = -max_ny; ny <= max_ny; ++ny) modes.push_back(make_int2(nx, ny));
+        }
+        if (modes.empty()) throw Failure(SHHD_EINVAL, "YokotaGreenKuboMeasure: no active wave vector is selected.");
+        if (static_cast<double>(modes.size()) * P.npy > 64.0 * 1024 * 1024)
+            throw Failure(SHHD_EUNSUPPORTED, "too many Green-Kubo modes for the direct column transforms at this grid (use diagonal)");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        GkArgs& G = e->gk;
+        G.nmodes = static_cast<int>(modes.size());
+        G.nevery = nevery;
+        G.nblock = nblock;
+        G.ntau = nblock / nevery;
+        G.kbt = e->cfg.kBT;
+        G.area = e->cfg.lx * e->cfg.ly;
+        G.cell_area = G.area / (static_cast<double>(e->cfg.nx) * e->cfg.ny);
+        G.o_pxy = G.o_vx = G.o_vy = -1;
+        for (int o = 0; o < P.n_out; ++o) {
+            if (P.out_kind[o] == OUT_PXY) G.o_pxy = o;
+            if (P.out_kind[o] == OUT_VX) G.o_vx = o;
+            if (P.out_kind[o] == OUT_VY) G.o_vy = o;
+        }
+        G.pair_layout = e->pair_path ? 1 : 0;
+        G.incomp_visc = P.incomp_visc;
+        const size_t B = e->cfg.batch, nm = modes.size();
+        std::vector<double2> wt(P.npy);
+        for (int n = 0; n < P.npy; ++n) {
+            const double a = -2.0 * M_PI * n / P.npy;
+            wt[n] = make_double2(std::cos(a), std::sin(a));
+        }
+        G.modes = static_cast<const int2*>(dalloc(e, sizeof(int2) * nm));
+        G.flux_step = static_cast<double2*>(dalloc(e, sizeof(double2) * B * nm));
+        G.integral = static_cast<double2*>(dalloc(e, sizeof(double2) * B * nm));
+        G.sums = static_cast<double*>(dalloc(e, sizeof(double) * B * G.ntau * nm));
+        G.wtab = static_cast<const double2*>(dalloc(e, sizeof(double2) * P.npy));
+        check_cuda(cudaMemcpyAsync(const_cast<int2*>(G.modes), modes.data(), sizeof(int2) * nm, cudaMemcpyHostToDevice, e->stream), "gk upload");
+        check_cuda(cudaMemcpyAsync(const_cast<double2*>(G.wtab), wt.data(), sizeof(double2) * P.npy, cudaMemcpyHostToDevice, e->stream), "gk upload");
+        check_cuda(cudaMemsetAsync(G.flux_step, 0, sizeof(double2) * B * nm, e->stream), "memset");
+        check_cuda(cudaMemsetAsync(G.integral, 0, sizeof(double2) * B * nm, e->stream), "memset");
+        check_cuda(cudaMemsetAsync(G.sums, 0, sizeof(double) * B * G.ntau * nm, e->stream), "memset");
+        check_cuda(cudaStreamSynchronize(e->stream), "gk sync");
+        e->gk_modes = modes;
+        e->gk_sample_base.assign(B, 0);
+        for (size_t m = 0; m < B; ++m) e->gk_sample_base[m] = (e->step_index - e->members[m].step0) / nblock;
+        e->gk_on = true;
+        if (e->graph_exec) {  // captured graphs do not hold the taps yet
+            check_cuda(cudaGraphExecDestroy(e->graph_exec), "cudaGraphExecDestroy");
+            e->graph_exec = nullptr;
+        }
+    });
+}
+
+int shhd_engine_gk_read(shhd_engine* e, int member, double* sums, size_t n, int64_t* nsample, int reset) {
+    return guarded([&] {
+        if (!e || !sums) throw Failure(SHHD_EINVAL, "null argument");
+        if (!e->gk_on) throw Failure(SHHD_EINVAL, "the Green-Kubo measure is not enabled");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        const GkArgs& G = e->gk;
+        const size_t per = static_cast<size_t>(G.ntau) * G.nmodes;
+        if (n != per) throw Failure(SHHD_EINVAL, "size mismatch: expected ntau * nmodes = " + std::to_string(per));
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        double* src = G.sums + static_cast<size_t>(member) * per;
+        check_cuda(cudaMemcpyAsync(sums, src, per * sizeof(double), cudaMemcpyDeviceToHost, e->stream), "gk download");
+        if (reset) check_cuda(cudaMemsetAsync(src, 0, per * sizeof(double), e->stream), "gk reset");
+        check_cuda(cudaStreamSynchronize(e->stream), "gk sync");
+        const int64_t done = (e->step_index - e->members[member].step0) / G.nblock;
+        if (nsample) *nsample = done - e->gk_sample_base[member];
+        if (reset) e->gk_sample_base[member] = done;
     });
 }
 

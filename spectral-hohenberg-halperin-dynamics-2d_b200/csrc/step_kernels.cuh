@@ -763,6 +763,128 @@ __global__ void __launch_bounds__(kThreads) structure_factor_kernel(const StepPl
     acc[e] += s * scale;
 }
 
+// ---------------------------------------------------------------------------
+// Yokota-Green-Kubo tap (measure_yokota_green_kubo.cc:128-190): the momentum
+// flux pi_xy of each RHS evaluation at the selected modes, weighted by the
+// stage's flux weight into the step flux; after the last stage the first
+// draw's stochastic flux / sqrt(dt) is added and the block integral and its
+// normalised square are accumulated, all in FP64.  One warp per (member, mode);
+// the y-transform of the x-transformed product planes at the mode is a direct
+// DFT over the column (table w^n = e^{-2 pi i n / Np_y}).
+// ---------------------------------------------------------------------------
+struct GkArgs {
+    const int2* modes;          // (gx, ky) per selected mode
+    int nmodes, ntau, nevery, nblock;
+    double2* flux_step;         // [member][mode]
+    double2* integral;          // [member][mode]
+    double* sums;               // [member][tau][mode]
+    const double2* wtab;        // [Np_y]
+    int o_pxy, o_vx, o_vy;      // product planes in I2 (-1: absent)
+    int pair_layout;            // I2 element (re_2t, re_2t+1, im_2t, im_2t+1) with W = 2
+    int incomp_visc;            // pi_xy from j / rho0 of the stage state
+    double kbt, area, cell_area;
+};
+
+template <typename T>
+__device__ __forceinline__ double2 gk_column_dft(const StepPlan& P, const GkArgs& G, const T* plane, int gx, int ky) {
+    const int npy = P.npy;
+    const int t = gx / P.W, w = gx - t * P.W;
+    const long long kk = ((ky % npy) + npy) % npy;
+    double re = 0.0, im = 0.0;
+    for (int y = threadIdx.x & 31; y < npy; y += 32) {
+        T xr, xi;
+        if (G.pair_layout) {
+            const T* e = plane + 4 * (static_cast<size_t>(t) * npy + y);
+            xr = e[w];
+            xi = e[2 + w];
+        } else {
+            const T* e = plane + 2 * ((static_cast<size_t>(t) * npy + y) * P.W + w);
+            xr = e[0];
+            xi = e[1];
+        }
+        const double2 tw = G.wtab[(kk * y) % npy];
+        re += static_cast<double>(xr) * tw.x - static_cast<double>(xi) * tw.y;
+        im += static_cast<double>(xr) * tw.y + static_cast<double>(xi) * tw.x;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    return make_double2(re, im);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) gk_tap_kernel(const StepPlan P, const GkArgs G, const MemberInfo* __restrict__ members,
+                                                          const T* __restrict__ i2, const cplx<T>* __restrict__ cur, const double* __restrict__ rho0,
+                                                          const unsigned long long* __restrict__ step_base, int step_off, double weight,
+                                                          int first_stage, int last_stage, double dt) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= P.batch * G.nmodes) return;
+    const int b = warp / G.nmodes, i = warp - b * G.nmodes;
+    const MemberInfo mi = members[b];
+    if (!mi.active) return;
+    const int gx = G.modes[i].x, ky = G.modes[i].y;
+    const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky;
+    const size_t plane = static_cast<size_t>(P.hx) * P.npy * 2;  // scalars of one I2 plane
+    const T* base = i2 + static_cast<size_t>(b) * P.n_out * plane;
+    double2 pxy = make_double2(0.0, 0.0);
+    if (G.o_pxy >= 0) pxy = gk_column_dft<T>(P, G, base + G.o_pxy * plane, gx, ky);
+    if (G.o_vx >= 0) {  // compressible viscous: -i eta (ky vx + kx vy) with v transformed from physical space
+        const double2 vx = gk_column_dft<T>(P, G, base + G.o_vx * plane, gx, ky);
+        const double2 vy = gk_column_dft<T>(P, G, base + G.o_vy * plane, gx, ky);
+        const double sr = kyv * vx.x + kx * vy.x, si = kyv * vx.y + kx * vy.y;
+        pxy.x += P.eta * si;
+        pxy.y -= P.eta * sr;
+    }
+    if (lane != 0) return;
+    if (G.incomp_visc) {  // incompressible viscous: v = j / rho0 of the stage state
+        const int j = ky >= 0 ? ky : ky + P.kyn;
+        const size_t fst = static_cast<size_t>(P.hx) * P.kyn;
+        const size_t pos = static_cast<size_t>(b) * P.nfields * fst + static_cast<size_t>(gx) * P.kyn + j;
+        const double r0 = 1.0 / rho0[b];
+        const cplx<T> jx = cur[pos + (P.nop + 1) * fst], jy = cur[pos + (P.nop + 2) * fst];
+        const double sr = (kyv * jx.x + kx * jy.x) * r0, si = (kyv * jx.y + kx * jy.y) * r0;
+        pxy.x += P.eta * si;
+        pxy.y -= P.eta * sr;
+    }
+    double2* fs = G.flux_step + static_cast<size_t>(b) * G.nmodes + i;
+    double2 f = first_stage ? make_double2(0.0, 0.0) : *fs;
+    f.x += weight * pxy.x;
+    f.y += weight * pxy.y;
+    if (!last_stage) {
+        *fs = f;
+        return;
+    }
+    const uint64_t step = *step_base + static_cast<uint64_t>(step_off);
+    if (P.noise_j && !(gx == 0 && ky == 0)) {  // first draw of j_sto (fcalculator.cc:587-700), / sqrt(dt)
+        const bool conj_line = (gx == 0 && ky < 0);
+        const int aky = conj_line ? -ky : ky;
+        const uint32_t mode_id = static_cast<uint32_t>(gx) * static_cast<uint32_t>(P.nay) + static_cast<uint32_t>((aky % P.nay + P.nay) % P.nay);
+        cplx<T> xa, xb;  // the engine's own draw (its precision's normals)
+        complex_normals<T>(P.seed, mi.key, step - static_cast<uint64_t>(mi.step0), j_stream(2), mode_id, false, xa, xb);
+        const double xr = static_cast<double>(xa.x), xi = conj_line ? -static_cast<double>(xa.y) : static_cast<double>(xa.y);
+        const double s = -P.j_s * mi.noise_scale * P.sqrt_eta / sqrt(dt);
+        f.x += s * xr;
+        f.y += s * xi;
+    }
+    // block accounting with the member's own step count
+    const long long msteps = static_cast<long long>(step - static_cast<uint64_t>(mi.step0)) + 1;
+    const int bs = static_cast<int>((msteps - 1) % G.nblock) + 1;
+    double2* in = G.integral + static_cast<size_t>(b) * G.nmodes + i;
+    double2 I = bs == 1 ? make_double2(0.0, 0.0) : *in;
+    const double wdt = (bs == 1 ? 0.5 * dt : dt) * G.cell_area;
+    I.x += wdt * f.x;
+    I.y += wdt * f.y;
+    if (bs % G.nevery == 0) {
+        const int ti = bs / G.nevery - 1;
+        const double tau = bs * dt;
+        const double kbt = G.kbt * mi.noise_scale * mi.noise_scale;
+        G.sums[(static_cast<size_t>(b) * G.ntau + ti) * G.nmodes + i] += (I.x * I.x + I.y * I.y) / (2.0 * tau * kbt * G.area);
+    }
+    *in = I;
+}
+
 // step counter of the call: set from the host at the start of a call, advanced
 // by the last node of a captured step graph
 __global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }

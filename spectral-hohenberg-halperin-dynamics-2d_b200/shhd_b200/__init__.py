@@ -102,6 +102,7 @@ EXPORTED = (
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
     "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
     "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
+    "shhd_engine_gk_enable", "shhd_engine_gk_read",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -140,6 +141,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_sk_accumulate.argtypes = [vp, i]
     lib.shhd_engine_sk_read.argtypes = [vp, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
     lib.shhd_engine_autotune.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), dp]
+    lib.shhd_engine_gk_enable.argtypes = [vp, i, i, i]
+    lib.shhd_engine_gk_read.argtypes = [vp, i, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
     return lib
 
 
@@ -269,6 +272,24 @@ class Engine:
         _check(lib.shhd_engine_autotune(self._h, int(trial_steps), ctypes.byref(fam), ctypes.byref(chunk), _dptr(ms)))
         return {"family": "pair-line" if fam.value == 1 else "single-line", "graph_chunk": chunk.value,
                 "ms_per_step": [None if np.isnan(x) else float(x) for x in ms]}
+
+    def gk_enable(self, nevery: int, nblock: int, selection: str = "diagonal") -> None:
+        """Start the Yokota-Green-Kubo stress measure (FP64, on the device)."""
+        sel = {"diagonal": 0, "all": 1}[selection]
+        _check(lib.shhd_engine_gk_enable(self._h, int(nevery), int(nblock), sel))
+        mx, my = max(0, self.cfg.active_nx // 2 - 1), max(0, self.cfg.active_ny // 2 - 1)
+        if sel == 0:
+            self.gk_modes = [(n, n) for n in range(1, min(mx, my) + 1)]
+        else:
+            self.gk_modes = [(0, n) for n in range(1, my + 1)] + [(nx, ny) for nx in range(1, mx + 1) for ny in range(-my, my + 1)]
+        self.gk_ntau = nblock // nevery
+
+    def gk_read(self, member: int = 0, reset: bool = False):
+        """(sums [tau, mode] of |I|^2 / (2 tau kBT V), completed blocks); S_mean = sums / blocks."""
+        out = np.zeros((self.gk_ntau, len(self.gk_modes)), dtype=np.float64)
+        cnt = ctypes.c_int64()
+        _check(lib.shhd_engine_gk_read(self._h, int(member), _dptr(out), out.size, ctypes.byref(cnt), 1 if reset else 0))
+        return out, int(cnt.value)
 
     def set_profiling(self, on: bool) -> None:
         _check(lib.shhd_engine_set_profiling(self._h, 1 if on else 0))
