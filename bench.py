@@ -484,11 +484,12 @@ def run_extras(args, world, rank, local, sb, initial_state, torch):
 # ---------------------------------------------------------------------------
 # served stream: Poisson arrivals of mixed trajectory jobs
 # ---------------------------------------------------------------------------
-SERVED = {"jobs": 32, "rate_per_s": 20.0, "grids": (128, 256, 512), "steps": (200, 800), "seed": 5,
+SERVED = {"jobs": 32, "rate_per_s": 20.0, "grids": (128, 256, 512), "steps": (200, 800), "seed": 5, "green_kubo": (10, 100),
           "what": "Poisson arrivals (20 jobs/s, seed 5) of trajectory jobs drawn uniformly from grids {128,256,512}^2 (3/2 rule, spacing 2), "
                   "N in {0..3}, mode in {compressible, incompressible, quiescent}, kBT in [1e-4, 1e-2], 200-800 SRK3 steps; "
                   "bounded sample of the served configuration (grids up to 2048^2 and 10^3-2x10^4 steps scaled down to finish "
-                  "in seconds; no Green-Kubo measure)"}
+                  "in seconds); every non-quiescent job accumulates the Yokota-Green-Kubo stress measure (diagonal modes, "
+                  "every 10 steps, blocks of 100) in FP64, in the server and in the serial FP64 baseline alike"}
 
 
 def served_job_scripts():
@@ -522,7 +523,7 @@ def served_job_scripts():
         if nop:
             lines.append("set order_parameter all equilibrium/gaussian seed 3 kBT 0.0001 k0 1 k2 0")
         lines.append(f"run {nsteps}")
-        out.append((t, "\n".join(lines) + "\n", nsteps))
+        out.append((t, "\n".join(lines) + "\n", nsteps, mode != "quiescent"))
     return out
 
 
@@ -530,17 +531,24 @@ def run_served(sb, initial_state, torch):
     from shhd_b200 import serve
     specs = served_job_scripts()
     jobs = []
-    for k, (t, text, n) in enumerate(specs):
+    for k, (t, text, n, gk) in enumerate(specs):
         cfg = sb.config_from_script(text)
-        jobs.append(serve.Job(key=100 + k, config=cfg, state=initial_state(cfg, text), nsteps=n, arrival=t))
+        jobs.append(serve.Job(key=100 + k, config=cfg, state=initial_state(cfg, text), nsteps=n, arrival=t,
+                              green_kubo=SERVED["green_kubo"] if gk else None))
     total_steps = sum(j.nsteps for j in jobs)
+    # untimed warm-up: every job configuration once, 50 steps (first launches, graph captures)
+    warm = [serve.Job(key=j.key, config=j.config, state=j.state, nsteps=50, arrival=0.0, green_kubo=j.green_kubo) for j in jobs]
     srv = serve.Server(precision=sb.FP32, seed=77, max_slots=8, chunk=25)
-    stats = srv.run(jobs)
+    srv.run(warm)
     srv.close()
-    # capacity: the same jobs all present at t = 0 (the Poisson run is arrival-bound)
-    sat_jobs = [serve.Job(key=j.key, config=j.config, state=j.state, nsteps=j.nsteps, arrival=0.0) for j in jobs]
+    # capacity: the jobs all present at t = 0
+    sat_jobs = [serve.Job(key=j.key, config=j.config, state=j.state, nsteps=j.nsteps, arrival=0.0, green_kubo=j.green_kubo) for j in jobs]
     srv = serve.Server(precision=sb.FP32, seed=77, max_slots=8, chunk=25)
     sat = srv.run(sat_jobs)
+    srv.close()
+    # latency under Poisson arrivals (its throughput is bounded by the arrivals)
+    srv = serve.Server(precision=sb.FP32, seed=77, max_slots=8, chunk=25)
+    stats = srv.run(jobs)
     srv.close()
     # the same jobs one at a time through the plain FP64 path (engine creation not timed)
     t_serial = 0.0
@@ -548,11 +556,15 @@ def run_served(sb, initial_state, torch):
         c = j.config.copy()
         c.precision = sb.FP64
         with sb.Engine(c) as eng:
+            if j.green_kubo is not None:
+                eng.gk_enable(*j.green_kubo)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             eng.set_state(j.state)
             eng.step(j.nsteps)
             eng.get_state()
+            if j.green_kubo is not None:
+                eng.gk_read()
             t_serial += time.perf_counter() - t0
     serial = total_steps / t_serial
     return {"value": stats["steps_per_s"], "unit": "steps/s (aggregate over jobs)", "p50_s": stats["p50_s"], "p99_s": stats["p99_s"],

@@ -33,8 +33,11 @@ class Job:
     state: np.ndarray             # initial State (reference layout, complex128)
     nsteps: int
     arrival: float = 0.0          # seconds after the server starts
+    green_kubo: Optional[Tuple[int, int]] = None   # (nevery, nblock): Yokota-Green-Kubo stress measure
     # filled by the server
     result: Optional[np.ndarray] = None
+    gk_sums: Optional[np.ndarray] = None          # [tau, mode] sums; S_mean = gk_sums / gk_blocks
+    gk_blocks: int = 0
     admitted: Optional[float] = None
     finished: Optional[float] = None
 
@@ -43,15 +46,16 @@ class Job:
         return self.finished - self.arrival
 
 
-def bucket_key(cfg: Config) -> bytes:
-    """Configuration bytes with the per-job fields (temperature, seed, batch) cleared."""
+def bucket_key(cfg: Config, green_kubo: Optional[Tuple[int, int]] = None) -> bytes:
+    """Configuration bytes with the per-job fields (temperature, seed, batch) cleared,
+    plus the Green-Kubo request (one measure setting per bucket engine)."""
     c = cfg.copy()
     c.kBT = 0.0
     c.noise_seed = 0
     c.batch = 1
     c.member_offset = 0
     c.precision = 0
-    return bytes(memoryview(c).cast("B"))
+    return bytes(memoryview(c).cast("B")) + repr(green_kubo).encode()
 
 
 def _noisy(cfg: Config) -> bool:
@@ -59,7 +63,8 @@ def _noisy(cfg: Config) -> bool:
 
 
 class _Bucket:
-    def __init__(self, cfg: Config, slots: int, precision: int, seed: int, graph_chunk: int = 0):
+    def __init__(self, cfg: Config, slots: int, precision: int, seed: int, graph_chunk: int = 0,
+                 green_kubo: Optional[Tuple[int, int]] = None):
         c = cfg.copy()
         c.batch = slots
         c.precision = precision
@@ -70,6 +75,9 @@ class _Bucket:
         self.engine = Engine(c)
         if graph_chunk > 0:
             self.engine.set_graph_chunk(graph_chunk)
+        self.green_kubo = green_kubo
+        if green_kubo is not None:
+            self.engine.gk_enable(*green_kubo)
         self.slots: List[Optional[Job]] = [None] * slots
         self.remaining = [0] * slots
         self.step_index = 0
@@ -87,6 +95,8 @@ class _Bucket:
         self.engine.set_state(job.state, member=m)
         scale = math.sqrt(job.config.kBT) if self.noisy else 0.0
         self.engine.set_member(m, key=job.key, step_origin=self.step_index, noise_scale=scale, active=True)
+        if self.green_kubo is not None:
+            self.engine.gk_read(m, reset=True)  # the slot's previous job's sums
         self.slots[m] = job
         self.remaining[m] = job.nsteps
         job.admitted = now
@@ -120,7 +130,7 @@ class Server:
         return self._member_bytes[key]
 
     def _slot_for(self, job: Job) -> Optional[Tuple[_Bucket, int]]:
-        key = bucket_key(job.config)
+        key = bucket_key(job.config, job.green_kubo)
         for b in self.buckets.get(key, []):
             m = b.free_slot()
             if m is not None:
@@ -129,7 +139,7 @@ class Server:
         slots = min(self.max_slots, (self.budget - self.used) // per)
         if slots < 1:
             return None
-        b = _Bucket(job.config, int(slots), self.precision, self.seed, self.chunk if self.graphs else 0)
+        b = _Bucket(job.config, int(slots), self.precision, self.seed, self.chunk if self.graphs else 0, job.green_kubo)
         self.used += int(b.engine.get_info().device_bytes)
         self.buckets.setdefault(key, []).append(b)
         return b, 0
@@ -174,6 +184,8 @@ class Server:
                     b.remaining[m] -= n
                     if b.remaining[m] == 0:
                         job.result = b.engine.get_state(m)
+                        if b.green_kubo is not None:
+                            job.gk_sums, job.gk_blocks = b.engine.gk_read(m, reset=True)
                         job.finished = now
                         b.engine.set_member(m, key=0, active=False)
                         b.slots[m] = None
@@ -197,10 +209,13 @@ class Server:
 
 
 def run_alone(job: Job, precision: int, seed: int) -> np.ndarray:
-    """The job on its own (batch of one) with the same noise key and scale as in the server."""
-    b = _Bucket(job.config, 1, precision, seed)
+    """The job on its own (batch of one) with the same noise key and scale as in the server.
+    Fills job.gk_sums / gk_blocks when the job asks for the Green-Kubo measure."""
+    b = _Bucket(job.config, 1, precision, seed, 0, job.green_kubo)
     b.admit(0, job, 0.0)
     b.engine.step(job.nsteps)
     out = b.engine.get_state(0)
+    if b.green_kubo is not None:
+        job.gk_sums, job.gk_blocks = b.engine.gk_read(0)
     b.engine.close()
     return out

@@ -81,3 +81,22 @@ def test_engines_sharing_a_kernel_size_coexist():
         for _ in range(2):
             u = ref.step(u, "philox")
         assert so.rel_l2(eb.get_state(), u) < 1e-12
+
+
+def test_served_green_kubo_equals_alone():
+    """Green-Kubo sums of a served job (slots reused, other jobs running) equal the job run alone."""
+    import shhd_b200 as sb
+    from shhd_b200 import serve
+    text = script(grid=(32, 32), length=(64.0, 64.0), nop=1, dt=0.01, eta=0.5, zeta=0.5, noise="kBT 0.002 seed 1")
+    ocfg = so.parse_script(text)
+    jobs = [serve.Job(key=500 + k, config=sb.config_from_script(text), state=random_state(ocfg, seed=60 + k), nsteps=n,
+                      arrival=0.002 * k, green_kubo=(2, 8)) for k, n in enumerate((24, 40, 16, 32))]
+    srv = serve.Server(precision=0, seed=5, max_slots=2, chunk=8)
+    srv.run(jobs)
+    srv.close()
+    for job in jobs:
+        sums, blocks = job.gk_sums, job.gk_blocks
+        alone = serve.Job(key=job.key, config=job.config, state=job.state, nsteps=job.nsteps, green_kubo=(2, 8))
+        serve.run_alone(alone, 0, seed=5)
+        assert blocks == alone.gk_blocks == job.nsteps // 8
+        assert np.abs(sums - alone.gk_sums).max() <= 1e-12 * np.abs(alone.gk_sums).max()
