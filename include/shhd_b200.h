@@ -179,11 +179,14 @@ int shhd_engine_rhs(shhd_engine* engine, int member, double* det, size_t n_doubl
 int shhd_engine_set_member(shhd_engine* engine, int member, uint32_t key, int64_t step_origin, double noise_scale, int active);
 
 /* Replay of captured CUDA graphs (no reference counterpart).  With chunk > 0,
- * a step call of n >= chunk steps runs floor(n / chunk) replays of one
- * captured graph holding a call of `chunk` steps (its launches and the advance
- * of the device-side step counter that keys the noise), then the remainder as
- * ordinary launches; the result equals floor(n / chunk) calls of `chunk` steps
- * plus one call of the rest.  Euler chunks are rounded up to an even count.
+ * a step call is split into replays of captured graphs, each holding one call
+ * of a fixed number of steps (its launches and the advance of the device-side
+ * step counter that keys the noise): as many of `chunk` as fit, then of each
+ * power of two below `chunk`, largest first, so any call costs at most about
+ * log2(chunk) + n / chunk graph launches; the result equals the same sequence
+ * of calls made directly.  Graphs are captured on first use of each size.
+ * Euler uses even sizes only (its two state buffers swap every step; the
+ * chunk is rounded up to even) and steps a leftover single step directly.
  * 0 (the default) launches every kernel directly.  Per-kernel profiling uses
  * direct launches. */
 int shhd_engine_set_graph_chunk(shhd_engine* engine, int chunk);

@@ -229,11 +229,15 @@ struct shhd_engine {
     int* flag_dev = nullptr;
     unsigned long long* step_dev = nullptr;  // step index at the start of the current call
 
-    // captured step graph: one call of `graph_chunk` steps, replayed
+    // captured step graphs: one call of `size` steps each, for the chunk and every power of two
+    // below it (a call is replayed as a sum of those), captured on first use
+    struct CachedGraph {
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches[4] = {0, 0, 0, 0};
+        double bytes[4] = {0, 0, 0, 0};
+    };
     int graph_chunk = 0;
-    cudaGraphExec_t graph_exec = nullptr;
-    int64_t graph_launches[4] = {0, 0, 0, 0};
-    double graph_bytes[4] = {0, 0, 0, 0};
+    std::map<int, CachedGraph> graphs;
 
     // per-kernel statistics: 0 col_inverse, 1 row_pass, 2 col_forward, 3 other
     bool profiling = false;
@@ -267,7 +271,8 @@ void free_engine(shhd_engine* e) {
                     static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev)})
         if (p) cudaFree(p);
-    if (e->graph_exec) cudaGraphExecDestroy(e->graph_exec);
+    for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
+    e->graphs.clear();
     if (e->sk_dev) cudaFree(e->sk_dev);
     for (const void* p : {static_cast<const void*>(e->gk.modes), static_cast<const void*>(e->gk.flux_step), static_cast<const void*>(e->gk.integral),
                           static_cast<const void*>(e->gk.sums), static_cast<const void*>(e->gk.wtab)})
@@ -981,10 +986,23 @@ void set_step_dev(shhd_engine* e) {
     check_cuda(cudaGetLastError(), "set_step launch");
 }
 
-// capture one call of graph_chunk steps (plus the advance of the step counter) as a graph
+void drop_graphs(shhd_engine* e) {
+    for (auto& kv : e->graphs) check_cuda(cudaGraphExecDestroy(kv.second.exec), "cudaGraphExecDestroy");
+    e->graphs.clear();
+}
+
+// graph sizes a call is split into: the chunk, then every power of two below it
+// (even sizes only for Euler, whose two state buffers swap every step)
+std::vector<int> graph_sizes(const shhd_engine* e) {
+    std::vector<int> s{e->graph_chunk};
+    for (int p = 1 << 30; p >= 1; p >>= 1)
+        if (p < e->graph_chunk && (e->cfg.integrator != SHHD_EULER || p % 2 == 0)) s.push_back(p);
+    return s;
+}
+
+// capture one call of K steps (plus the advance of the step counter) as a graph
 template <typename T>
-void capture_graph(shhd_engine* e) {
-    const int K = e->graph_chunk;
+shhd_engine::CachedGraph& capture_graph(shhd_engine* e, int K) {
     int64_t l0[4];
     double b0[4];
     for (int k = 0; k < 4; ++k) { l0[k] = e->kernel_launches[k]; b0[k] = e->kernel_bytes[k]; }
@@ -1000,15 +1018,17 @@ void capture_graph(shhd_engine* e) {
         throw;
     }
     check_cuda(cudaStreamEndCapture(e->stream, &g), "cudaStreamEndCapture");
-    const cudaError_t rc = cudaGraphInstantiate(&e->graph_exec, g, 0);
+    shhd_engine::CachedGraph cg;
+    const cudaError_t rc = cudaGraphInstantiate(&cg.exec, g, 0);
     cudaGraphDestroy(g);
     check_cuda(rc, "cudaGraphInstantiate");
     for (int k = 0; k < 4; ++k) {
-        e->graph_launches[k] = e->kernel_launches[k] - l0[k];
-        e->graph_bytes[k] = e->kernel_bytes[k] - b0[k];
+        cg.launches[k] = e->kernel_launches[k] - l0[k];
+        cg.bytes[k] = e->kernel_bytes[k] - b0[k];
         e->kernel_launches[k] = l0[k];
         e->kernel_bytes[k] = b0[k];
     }
+    return e->graphs[K] = cg;
 }
 
 template <typename T>
@@ -1016,12 +1036,15 @@ void enqueue_steps(shhd_engine* e, int nsteps) {
     ensure_rho0(e);
     set_step_dev(e);
     int done = 0;
-    const int K = e->graph_chunk;
-    if (K > 0 && !e->profiling && nsteps >= K) {
-        if (!e->graph_exec) capture_graph<T>(e);
-        for (; done + K <= nsteps; done += K) {
-            check_cuda(cudaGraphLaunch(e->graph_exec, e->stream), "cudaGraphLaunch");
-            for (int k = 0; k < 4; ++k) { e->kernel_launches[k] += e->graph_launches[k]; e->kernel_bytes[k] += e->graph_bytes[k]; }
+    if (e->graph_chunk > 0 && !e->profiling) {
+        for (const int size : graph_sizes(e)) {
+            while (nsteps - done >= size) {
+                auto it = e->graphs.find(size);
+                shhd_engine::CachedGraph& cg = it != e->graphs.end() ? it->second : capture_graph<T>(e, size);
+                check_cuda(cudaGraphLaunch(cg.exec, e->stream), "cudaGraphLaunch");
+                for (int k = 0; k < 4; ++k) { e->kernel_launches[k] += cg.launches[k]; e->kernel_bytes[k] += cg.bytes[k]; }
+                done += size;
+            }
         }
         e->step_index += done;
         e->time += done * e->cfg.dt;
@@ -1448,10 +1471,7 @@ namespace {
 template <typename T>
 void apply_family(shhd_engine* e, int family) {
     check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
-    if (e->graph_exec) {
-        check_cuda(cudaGraphExecDestroy(e->graph_exec), "cudaGraphExecDestroy");
-        e->graph_exec = nullptr;
-    }
+    drop_graphs(e);
     e->family_override = family;
     e->pair_path = e->col_fixed = e->row_fixed = false;
     build_plan(e);
@@ -1515,7 +1535,7 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
             apply_family<T>(e, fam);
             for (int chunk : {0, chunk_trial}) {
                 e->graph_chunk = chunk;
-                if (e->graph_exec) { cudaGraphExecDestroy(e->graph_exec); e->graph_exec = nullptr; }
+                drop_graphs(e);
                 enqueue(e, chunk_trial);  // warm-up (and capture)
                 check_cuda(cudaEventRecord(a, e->stream), "cudaEventRecord");
                 enqueue(e, chunk_trial);
@@ -1530,7 +1550,7 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
                 restore();
             }
         }
-        if (e->graph_exec) { cudaGraphExecDestroy(e->graph_exec); e->graph_exec = nullptr; }
+        drop_graphs(e);
         apply_family<T>(e, best_family);
         e->graph_chunk = best_chunk;
         if (family_out) *family_out = best_family;
@@ -1629,10 +1649,7 @@ int shhd_engine_gk_enable(shhd_engine* e, int nevery, int nblock, int selection)
         e->gk_sample_base.assign(B, 0);
         for (size_t m = 0; m < B; ++m) e->gk_sample_base[m] = (e->step_index - e->members[m].step0) / nblock;
         e->gk_on = true;
-        if (e->graph_exec) {  // captured graphs do not hold the taps yet
-            check_cuda(cudaGraphExecDestroy(e->graph_exec), "cudaGraphExecDestroy");
-            e->graph_exec = nullptr;
-        }
+        drop_graphs(e);  // captured graphs do not hold the taps yet
     });
 }
 
@@ -1663,10 +1680,7 @@ int shhd_engine_set_graph_chunk(shhd_engine* e, int chunk) {
         if (chunk > 0 && e->cfg.integrator == SHHD_EULER && chunk % 2) ++chunk;
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
-        if (e->graph_exec) {
-            check_cuda(cudaGraphExecDestroy(e->graph_exec), "cudaGraphExecDestroy");
-            e->graph_exec = nullptr;
-        }
+        drop_graphs(e);
         e->graph_chunk = chunk;
     });
 }
