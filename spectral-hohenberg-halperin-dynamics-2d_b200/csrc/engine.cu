@@ -764,7 +764,7 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
                 if constexpr (FY != 0) {
                     dim3 pg(P.ntiles / (kPairMaxN / FY), P.n_in, P.batch);
                     pcol_inverse<FY><<<pg, kThreads, e->smem_col_inv, e->stream>>>(P, e->members_dev, st, reinterpret_cast<ulonglong2*>(i1),
-                                                                                 static_cast<const float4*>(e->tw_y));
+                                                                                 static_cast<const float2*>(e->tw_y));
                 }
             });
             check_cuda(cudaGetLastError(), "col_inverse launch");
@@ -797,7 +797,7 @@ void launch_row(shhd_engine* e) {
                 if constexpr (FX != 0) {
                     dim3 pg(P.npy / 2 / (kPairMaxN / FX), P.batch);
                     prow_pass<FX><<<pg, kThreads, e->smem_row, e->stream>>>(P, e->members_dev, static_cast<const ulonglong2*>(e->i1),
-                                                                           static_cast<ulonglong2*>(e->i2), static_cast<const float4*>(e->tw_x),
+                                                                           static_cast<ulonglong2*>(e->i2), static_cast<const float2*>(e->tw_x),
                                                                            e->rho0_dev, e->err_dev);
                 }
             });
@@ -840,7 +840,7 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
                 constexpr int FY = decltype(fy)::value;
                 if constexpr (FY != 0) {
                     dim3 pg(P.ntiles / (kPairMaxN / FY), P.n_groups, P.batch);
-                    pcol_forward<FY><<<pg, kThreads, e->smem_col, e->stream>>>(P, A, static_cast<const float4*>(e->tw_y));
+                    pcol_forward<FY><<<pg, kThreads, e->smem_col, e->stream>>>(P, A, static_cast<const float2*>(e->tw_y));
                 }
             });
             check_cuda(cudaGetLastError(), "col_forward launch");
@@ -1149,7 +1149,7 @@ std::vector<unsigned char> host_twiddles(const shhd_engine* e, int n, bool fixed
             constexpr int FN = decltype(fn)::value;
             if constexpr (FN != 0) {
                 const int cnt = std::max(PairPlan<FN>::c.twsz, 1);
-                std::vector<float> t(4 * static_cast<size_t>(cnt), 0.f);
+                std::vector<float> t(2 * static_cast<size_t>(cnt), 0.f);
                 pair_twiddles_host<FN>(t.data());
                 out.resize(t.size() * sizeof(float));
                 std::memcpy(out.data(), t.data(), out.size());

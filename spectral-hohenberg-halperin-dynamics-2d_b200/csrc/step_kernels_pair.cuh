@@ -44,10 +44,10 @@ __device__ __forceinline__ float f2_lo(u64 r) { float v; asm("{.reg .f32 t; mov.
 __device__ __forceinline__ float f2_hi(u64 r) { float v; asm("{.reg .f32 t; mov.b64 {t, %0}, %1;}" : "=f"(v) : "l"(r)); return v; }
 __device__ __forceinline__ u64 f2_splat(float a) { return f2_pack(a, a); }
 
-// twiddle rows: read-only and shared by every CTA, so kept in L1 (evict last)
-__device__ __forceinline__ float4 ld_tw(const float4* p) {
-    float4 v;
-    asm("ld.global.nc.L1::evict_last.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+// twiddles: read-only and shared by every CTA, so kept in L1 (evict last)
+__device__ __forceinline__ float2 ld_tw2(const float2* p) {
+    float2 v;
+    asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
     return v;
 }
 // transform planes: read once per kernel, so not allocated in L1
@@ -82,6 +82,25 @@ __device__ __forceinline__ float2 pc_col(PC v, int half) {  // one line's comple
     return half ? make_float2(f2_hi(v.re), f2_hi(v.im)) : make_float2(f2_lo(v.re), f2_lo(v.im));
 }
 __device__ __forceinline__ PC pc_make(float2 a, float2 b) { return PC{f2_pack(a.x, b.x), f2_pack(a.y, b.y)}; }
+
+// x_q *= w^q (q = 1..R-1, DIR < 0) or conj: from one table twiddle w, powers by a product tree
+// at most three roundings deep
+template <int R, int DIR>
+__device__ __forceinline__ void ptwiddle_pow(PC* v, float2 w1) {
+    float2 w[8];
+    w[1] = w1;
+    auto cm = [](float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+    if constexpr (R > 2) w[2] = cm(w1, w1);
+    if constexpr (R > 3) w[3] = cm(w[2], w1);
+    if constexpr (R > 4) {
+        w[4] = cm(w[2], w[2]);
+        w[5] = cm(w[4], w1);
+        w[6] = cm(w[4], w[2]);
+        w[7] = cm(w[4], w[3]);
+    }
+#pragma unroll
+    for (int q = 1; q < R; ++q) v[q] = pcmul<DIR>(v[q], f2_splat(w[q].x), f2_splat(w[q].y));
+}
 
 // ---------------------------------------------------------------------------
 // butterflies: y_q = sum_p x_p e^{DIR 2 pi i p q / R}
@@ -152,7 +171,7 @@ struct PPlan {
     int s[kPairMaxStages];      // stride of stage s (sub-transform length / radix)
     int lg[kPairMaxStages];     // log2 of the stride
     int lr[kPairMaxStages];     // log2 of the radix (stages >= 1)
-    int twoff[kPairMaxStages];  // offset of the stage's twiddle rows [j][q - 1] (float4 entries)
+    int twoff[kPairMaxStages];  // offset of the stage's twiddles w_L^j, j < stride (float2 entries)
     int twsz;
 };
 
@@ -175,7 +194,7 @@ __host__ __device__ constexpr PPlan make_pplan(int n) {
         p.lg[i] = ilog2c(p.s[i]);
         p.lr[i] = ilog2c(p.r[i]);
         p.twoff[i] = off;
-        if (L > p.r[i]) off += p.s[i] * (p.r[i] - 1);
+        if (L > p.r[i]) off += p.s[i];
         L /= p.r[i];
     }
     p.twsz = off;
@@ -223,7 +242,7 @@ template <int N> __device__ __forceinline__ int ppinv(int p) {
 // the butterfly, DIT before; the stage-s twiddle of butterfly j is w_L^(j q).
 // ---------------------------------------------------------------------------
 template <int N, int S, int DIR, bool DIT, typename Load, typename Store>
-__device__ __forceinline__ void pstage_io(int nl, const float4* __restrict__ tw, Load&& load, Store&& store) {
+__device__ __forceinline__ void pstage_io(int nl, const float2* __restrict__ tw, Load&& load, Store&& store) {
     constexpr PPlan pp = PairPlan<N>::c;
     constexpr int R = pp.r[S], ST = pp.s[S], L = R * ST, NB = N / R;
     const int tot = nl * NB;
@@ -236,25 +255,11 @@ __device__ __forceinline__ void pstage_io(int nl, const float4* __restrict__ tw,
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = load(l, base + q * ST);
         if constexpr (L > R) {
-            if constexpr (DIT) {
-                const float4* t = tw + pp.twoff[S] + j * (R - 1);
-#pragma unroll
-                for (int q = 1; q < R; ++q) {
-                    const float4 w = ld_tw(t + q - 1);
-                    v[q] = pcmul<DIR>(v[q], f2_pack(w.x, w.y), f2_pack(w.z, w.w));
-                }
-            }
+            if constexpr (DIT) ptwiddle_pow<R, DIR>(v, ld_tw2(tw + pp.twoff[S] + j));
         }
         pbfly<R, DIR>(v);
         if constexpr (L > R) {
-            if constexpr (!DIT) {
-                const float4* t = tw + pp.twoff[S] + j * (R - 1);
-#pragma unroll
-                for (int q = 1; q < R; ++q) {
-                    const float4 w = ld_tw(t + q - 1);
-                    v[q] = pcmul<DIR>(v[q], f2_pack(w.x, w.y), f2_pack(w.z, w.w));
-                }
-            }
+            if constexpr (!DIT) ptwiddle_pow<R, DIR>(v, ld_tw2(tw + pp.twoff[S] + j));
         }
 #pragma unroll
         for (int q = 0; q < R; ++q) store(l, base + q * ST, v[q]);
@@ -271,7 +276,7 @@ struct SmemIO {
 
 // stages [S, E) in shared memory (DIF ascending, DIT descending), a barrier after each
 template <int N, int S, int E, int DIR>
-__device__ __forceinline__ void pdif_range(ulonglong2* lines, int nl, const float4* tw) {
+__device__ __forceinline__ void pdif_range(ulonglong2* lines, int nl, const float2* tw) {
     if constexpr (S < E) {
         const SmemIO io{lines, N};
         pstage_io<N, S, DIR, false>(nl, tw, io, io);
@@ -280,7 +285,7 @@ __device__ __forceinline__ void pdif_range(ulonglong2* lines, int nl, const floa
     }
 }
 template <int N, int S, int E, int DIR>
-__device__ __forceinline__ void pdit_range(ulonglong2* lines, int nl, const float4* tw) {
+__device__ __forceinline__ void pdit_range(ulonglong2* lines, int nl, const float2* tw) {
     if constexpr (S > E) {
         const SmemIO io{lines, N};
         pstage_io<N, S - 1, DIR, true>(nl, tw, io, io);
@@ -289,21 +294,19 @@ __device__ __forceinline__ void pdit_range(ulonglong2* lines, int nl, const floa
     }
 }
 
-// host: per-stage twiddle rows (wx, wx, wy, wy) of w_L^(j q), forward sign
+// host: per-stage twiddles w_L^j (forward sign) as float2; the kernels form w^(j q) from them
 template <int N>
-void pair_twiddles_host(float* out /* 4 * twsz floats */) {
+void pair_twiddles_host(float* out /* 2 * twsz floats */) {
     constexpr PPlan pp = PairPlan<N>::c;
     int L = N;
     for (int s = 0; s < pp.m; ++s) {
         const int R = pp.r[s], ST = pp.s[s];
         if (L > R) {
-            for (int j = 0; j < ST; ++j)
-                for (int q = 1; q < R; ++q) {
-                    const double a = -2.0 * M_PI * static_cast<double>(j) * q / L;
-                    float* e = out + 4 * (pp.twoff[s] + j * (R - 1) + (q - 1));
-                    e[0] = e[1] = static_cast<float>(cos(a));
-                    e[2] = e[3] = static_cast<float>(sin(a));
-                }
+            for (int j = 0; j < ST; ++j) {
+                const double a = -2.0 * M_PI * static_cast<double>(j) / L;
+                out[2 * (pp.twoff[s] + j)] = static_cast<float>(cos(a));
+                out[2 * (pp.twoff[s] + j) + 1] = static_cast<float>(sin(a));
+            }
         }
         L /= R;
     }
@@ -325,7 +328,7 @@ __device__ __forceinline__ int pky_of_y(int y, int n) { return y < n / 2 ? y : y
 template <int NY>
 __global__ void __launch_bounds__(kThreads) pcol_inverse(const StepPlan P, const MemberInfo* __restrict__ members,
                                                          const float2* __restrict__ state, ulonglong2* __restrict__ i1,
-                                                         const float4* __restrict__ tw) {
+                                                         const float2* __restrict__ tw) {
     if (!members[blockIdx.z].active) return;
     constexpr int CP = kPairMaxN / NY;
     constexpr PPlan pp = PairPlan<NY>::c;
@@ -370,7 +373,7 @@ __device__ __forceinline__ float2 pin(const ulonglong2* in, int nx, int s, int s
 template <int NX>
 __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const MemberInfo* __restrict__ members,
                                                       const ulonglong2* __restrict__ i1, ulonglong2* __restrict__ i2,
-                                                      const float4* __restrict__ tw, const double* __restrict__ rho0_member,
+                                                      const float2* __restrict__ tw, const double* __restrict__ rho0_member,
                                                       int* __restrict__ err) {
     if (!members[blockIdx.y].active) return;
     constexpr int RP = kPairMaxN / NX;
@@ -606,7 +609,7 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
 // (accumulators / new values: psi or jx, jy, rho), two columns per element.
 // ---------------------------------------------------------------------------
 template <int NY>
-__global__ void __launch_bounds__(kThreads, 2) pcol_forward(const StepPlan P, const StageArgs<float> A, const float4* __restrict__ tw) {
+__global__ void __launch_bounds__(kThreads, 2) pcol_forward(const StepPlan P, const StageArgs<float> A, const float2* __restrict__ tw) {
     constexpr int CP = kPairMaxN / NY;
     constexpr PPlan pp = PairPlan<NY>::c;
     extern __shared__ __align__(16) unsigned char smem_raw[];
