@@ -461,6 +461,7 @@ def run_extras(args, world, rank, local, sb, initial_state, torch):
     eng.close()
 
     out["served"] = run_served(sb, initial_state, torch)
+    out["other_configs"] = run_other_configs(sb, initial_state, torch, world)
 
     # cuFFT beside it: the same transforms per stage (5 C2R + 11 R2C at 1536^2, FP32)
     x = torch.randn(11, 1536, 1536, device="cuda", dtype=torch.float32)
@@ -478,6 +479,67 @@ def run_extras(args, world, rank, local, sb, initial_state, torch):
     ms_stage = e0.elapsed_time(e1) / 10
     out["cufft_reference"] = {"ms_per_stage": ms_stage, "steps_per_s_transforms_only": 1e3 / (3 * ms_stage),
                               "what": "torch.fft (cuFFT) 5 irfft2 + 11 rfft2 at 1536^2 FP32 per stage, unfused, no products or RHS"}
+    return out
+
+
+# ---------------------------------------------------------------------------
+# the other single-trajectory configurations, timed as reference points
+# ---------------------------------------------------------------------------
+PLAIN_128 = """dimension 2
+grid 128 128
+length 128 128
+dealias 3/2
+order_parameters 0
+timestep 0.05
+time_evolution srk3/compressible
+model thermo linear_eos cT 1
+model transport constant eta 1 zeta 1
+fix 1 all nonlinear on
+fix 2 all noise on seed 1 kBT 1e-4
+set density equilibrium/gaussian kBT 1e-4 rho0 1 cT 1 seed 1
+set momentum all equilibrium/gaussian/compressible kBT 1e-4 seed 1
+run 2000
+"""
+
+TURB_4096 = """dimension 2
+grid 4096 4096
+length 4096 4096
+dealias 3/2
+order_parameters 0
+timestep 0.001
+time_evolution srk3/incompressible
+model transport constant eta 1e-4 zeta 0
+fix 1 momentum nonlinear on
+fix 2 all noise on seed 11 kBT 1e-6
+set density uniform value 1.0
+run 2000
+"""
+
+
+def run_other_configs(sb, initial_state, torch, world):
+    out = {}
+    for name, text, prec, nsteps, what in (
+            ("plain_128_fp64", PLAIN_128, sb.FP64, 200,
+             "128^2 (3/2 -> 192^2), N=0 compressible, linear EOS, eta = zeta = 1, kBT 1e-4, equilibrium ICs seed 1, SRK3 dt 0.05, FP64"),
+            ("turbulence_4096_fp32", TURB_4096, sb.FP32, 5,
+             "4096^2 (3/2 -> 6144^2), N=0 incompressible, eta 1e-4, advection, kBT 1e-6, SRK3 dt 1e-3, FP32; zero initial "
+             "momentum (the random-vorticity initial condition is not restated on the host; the step cost does not depend on it)")):
+        cfg = sb.config_from_script(text)
+        cfg.precision = prec
+        eng = sb.Engine(cfg)
+        eng.set_state(initial_state(cfg, text))
+        tuning = eng.autotune(3) if nsteps > 50 else None
+        eng.step(3)
+        stream = torch.cuda.ExternalStream(eng.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.step_async(nsteps)
+        e1.record(stream)
+        eng.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        out[name] = {"value": world * nsteps / (ms / 1e3), "unit": "steps/s", "steps": nsteps, "what": what,
+                     "autotune": tuning}
+        eng.close()
     return out
 
 

@@ -215,6 +215,14 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * direct, family 1 graph).  Allocates a temporary copy of the state. */
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
+/* Spectral L2 columns of the time-series measure (measure_time_series.cc:
+ * |rho|^2, |d_rho|^2, |j|^2, |d_j|^2, |psi[a]|^2, |d_psi[a]|^2) for one member
+ * of the current state, in FP64 on the device: out[2 f] = (V / Np^2) / Np^2
+ * * sum w |u_f|^2 and out[2 f + 1] the same with a factor k^2, over the active
+ * modes but (0, 0), w = 2 off the kx = 0 line (n = 2 * nfields).  The
+ * momentum columns are the sums of the jx and jy entries. */
+int shhd_engine_l2_sums(shhd_engine* engine, int member, double* out, size_t n);
+
 /* Yokota-Green-Kubo stress measure (measure_yokota_green_kubo.cc:16-225),
  * accumulated on the device in FP64.  shhd_engine_gk_enable selects the wave
  * vectors as the reference does (selection 0 "diagonal": (n, n), 1 "all"),

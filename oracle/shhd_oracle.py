@@ -754,6 +754,26 @@ class Oracle:
         return out, flux
 
 
+def time_series_l2(cfg: Config, state: np.ndarray) -> Dict[str, float]:
+    """Spectral L2 columns of TimeSeriesMeasure (measure_time_series.cc:233-275):
+    cell_area / grid_size * sum over active modes but (0, 0) of w (k^2) |u|^2, w = 2 off kx = 0."""
+    g = Geometry(cfg)
+    use = g.active & ~((g.gx == 0) & (g.sgy == 0))
+    w = np.where(g.gx == 0, 1.0, 2.0)
+    pref = (g.volume / g.grid_size) / g.grid_size
+
+    def s(f, k2=False):
+        return float(pref * np.sum(np.where(use, w * (g.k2 if k2 else 1.0) * np.abs(f) ** 2, 0.0)))
+
+    n = cfg.num_order_parameters
+    out = {"|rho|^2": s(state[0]), "|d_rho|^2": s(state[0], True),
+           "|j|^2": s(state[n + 1]) + s(state[n + 2]), "|d_j|^2": s(state[n + 1], True) + s(state[n + 2], True)}
+    for a in range(n):
+        out[f"|psi[{a}]|^2"] = s(state[1 + a])
+        out[f"|d_psi[{a}]|^2"] = s(state[1 + a], True)
+    return out
+
+
 def green_kubo_modes(cfg: Config, selection: str = "diagonal") -> List[Tuple[int, int]]:
     """Wave numbers (nx, ny) of measure_yokota_green_kubo.cc:42-96."""
     max_nx = max(0, cfg.active[0] // 2 - 1)

@@ -191,6 +191,7 @@ struct shhd_engine {
     double2* k0_s1 = nullptr;
     double2* k0_s2 = nullptr;
     double* sk_dev = nullptr;        // FP64 structure-factor accumulator [Hx * Ky] (allocated on first use)
+    double* l2_dev = nullptr;        // FP64 spectral L2 sums [field][2] (allocated on first use)
     // Yokota-Green-Kubo taps (FP64): selected modes, step flux, block integrals, sums [member][tau][mode]
     bool gk_on = false;
     GkArgs gk{};
@@ -274,6 +275,7 @@ void free_engine(shhd_engine* e) {
     for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
     e->graphs.clear();
     if (e->sk_dev) cudaFree(e->sk_dev);
+    if (e->l2_dev) cudaFree(e->l2_dev);
     for (const void* p : {static_cast<const void*>(e->gk.modes), static_cast<const void*>(e->gk.flux_step), static_cast<const void*>(e->gk.integral),
                           static_cast<const void*>(e->gk.sums), static_cast<const void*>(e->gk.wtab)})
         if (p) cudaFree(const_cast<void*>(p));
@@ -1584,6 +1586,29 @@ int shhd_engine_autotune(shhd_engine* e, int trial_steps, int* family, int* grap
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         if (e->fp32) autotune<float>(e, trial_steps, family, graph_chunk, ms_per_step);
         else autotune<double>(e, trial_steps, family, graph_chunk, ms_per_step);
+    });
+}
+
+int shhd_engine_l2_sums(shhd_engine* e, int member, double* out, size_t n) {
+    return guarded([&] {
+        if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        const int nf = e->P.nfields;
+        if (n != static_cast<size_t>(2 * nf)) throw Failure(SHHD_EINVAL, "size mismatch: expected 2 * nfields = " + std::to_string(2 * nf));
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (!e->l2_dev) e->l2_dev = static_cast<double*>(dalloc(e, sizeof(double) * 2 * kMaxFields));
+        check_cuda(cudaMemsetAsync(e->l2_dev, 0, sizeof(double) * 2 * nf, e->stream), "memset");
+        const size_t modes = static_cast<size_t>(e->P.hx) * e->P.kyn;
+        const dim3 g(static_cast<unsigned>((modes + kThreads - 1) / kThreads));
+        if (e->fp32) l2_sums_kernel<float><<<g, kThreads, 0, e->stream>>>(e->P, static_cast<const float2*>(e->u), member, e->l2_dev);
+        else l2_sums_kernel<double><<<g, kThreads, 0, e->stream>>>(e->P, static_cast<const double2*>(e->u), member, e->l2_dev);
+        check_cuda(cudaGetLastError(), "l2_sums launch");
+        check_cuda(cudaMemcpyAsync(out, e->l2_dev, sizeof(double) * 2 * nf, cudaMemcpyDeviceToHost, e->stream), "l2 download");
+        check_cuda(cudaStreamSynchronize(e->stream), "l2 sync");
+        // prefactor cell_area / grid_size (measure_time_series.cc:295-298, 262-275)
+        const double np2 = static_cast<double>(e->cfg.nx) * e->cfg.ny;
+        const double pref = e->cfg.lx * e->cfg.ly / np2 / np2;
+        for (int q = 0; q < 2 * nf; ++q) out[q] *= pref;
     });
 }
 

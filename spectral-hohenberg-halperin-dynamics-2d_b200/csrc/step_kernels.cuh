@@ -885,6 +885,48 @@ __global__ void __launch_bounds__(kThreads) gk_tap_kernel(const StepPlan P, cons
     *in = I;
 }
 
+// ---------------------------------------------------------------------------
+// spectral L2 sums of the time-series measure (measure_time_series.cc, the
+// |rho|^2 ... |d_psi[a]|^2 columns): per field, sum over the active modes but
+// (0, 0) of w |u|^2 and w k^2 |u|^2, w = 2 off the kx = 0 line; FP64, one
+// member; grid: ceil(Hx * Ky / 256); out[field][2] accumulated with atomics
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(kThreads) l2_sums_kernel(const StepPlan P, const cplx<T>* __restrict__ state, int b, double* __restrict__ out) {
+    __shared__ double red[kThreads / 32][2 * kMaxFields];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
+    double acc[2 * kMaxFields];
+    for (int q = 0; q < 2 * kMaxFields; ++q) acc[q] = 0.0;
+    if (e < static_cast<int>(fstride)) {
+        const int gx = e / P.kyn, j = e - gx * P.kyn;
+        const int ky = ky_of_j(j, P.nay);
+        if (gx != 0 || ky != 0) {
+            const double w = gx == 0 ? 1.0 : 2.0;
+            const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky;
+            const double k2 = kx * kx + kyv * kyv;
+            for (int f = 0; f < P.nfields; ++f) {
+                const cplx<T> v = state[(static_cast<size_t>(b) * P.nfields + f) * fstride + e];
+                const double n2 = static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y;
+                acc[2 * f] = w * n2;
+                acc[2 * f + 1] = w * k2 * n2;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = 0; q < 2 * P.nfields; ++q) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * P.nfields) {
+        double v = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) v += red[w][threadIdx.x];
+        atomicAdd(out + threadIdx.x, v);
+    }
+}
+
 // step counter of the call: set from the host at the start of a call, advanced
 // by the last node of a captured step graph
 __global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }

@@ -102,7 +102,7 @@ EXPORTED = (
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
     "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
     "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
-    "shhd_engine_gk_enable", "shhd_engine_gk_read",
+    "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -143,6 +143,7 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_autotune.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), dp]
     lib.shhd_engine_gk_enable.argtypes = [vp, i, i, i]
     lib.shhd_engine_gk_read.argtypes = [vp, i, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
+    lib.shhd_engine_l2_sums.argtypes = [vp, i, dp, sz]
     return lib
 
 
@@ -272,6 +273,19 @@ class Engine:
         _check(lib.shhd_engine_autotune(self._h, int(trial_steps), ctypes.byref(fam), ctypes.byref(chunk), _dptr(ms)))
         return {"family": "pair-line" if fam.value == 1 else "single-line", "graph_chunk": chunk.value,
                 "ms_per_step": [None if np.isnan(x) else float(x) for x in ms]}
+
+    def time_series_l2(self, member: int = 0) -> dict:
+        """The reference time-series measure's spectral L2 columns of the current state (FP64)."""
+        nf = self.info.nfields
+        raw = np.zeros(2 * nf, dtype=np.float64)
+        _check(lib.shhd_engine_l2_sums(self._h, int(member), _dptr(raw), raw.size))
+        n = nf - 3
+        out = {"|rho|^2": raw[0], "|d_rho|^2": raw[1], "|j|^2": raw[2 * (n + 1)] + raw[2 * (n + 2)],
+               "|d_j|^2": raw[2 * (n + 1) + 1] + raw[2 * (n + 2) + 1]}
+        for a in range(n):
+            out[f"|psi[{a}]|^2"] = raw[2 * (1 + a)]
+            out[f"|d_psi[{a}]|^2"] = raw[2 * (1 + a) + 1]
+        return {k: float(v) for k, v in out.items()}
 
     def gk_enable(self, nevery: int, nblock: int, selection: str = "diagonal") -> None:
         """Start the Yokota-Green-Kubo stress measure (FP64, on the device)."""

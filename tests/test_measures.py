@@ -91,3 +91,26 @@ def test_structure_factor_equipartition():
         sel = (kk >= lo) & (kk < lo + 0.2)
         ratio = sk[sel].mean() / theory[sel].mean()
         assert abs(ratio - 1.0) < 0.05, (lo, ratio)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_time_series_l2_columns_match_restatement(precision):
+    import shhd_b200 as sb
+    for text in (script(grid=(32, 48), length=(64.0, 96.0), nop=2, dt=0.01),
+                 script(grid=(48, 32), length=(96.0, 64.0), nop=1, dt=0.01, te="srk3/incompressible", cT=None, eta=0.2,
+                        zeta=0.0, nonlinear="momentum")):
+        ocfg = so.parse_script(text)
+        cfg = sb.config_from_script(text)
+        cfg.precision = precision
+        cfg.batch = 2
+        u = [random_state(ocfg, seed=70 + m, transverse=(ocfg.mode == "incompressible")) for m in range(2)]
+        with sb.Engine(cfg) as eng:
+            for m in range(2):
+                eng.set_state(u[m], member=m)
+            for m in range(2):
+                got = eng.time_series_l2(m)
+                want = so.time_series_l2(ocfg, u[m])
+                assert set(got) == set(want)
+                tol = 1e-12 if precision == 0 else 1e-6
+                for k in want:
+                    assert abs(got[k] - want[k]) <= tol * max(abs(want[k]), 1e-300), (k, got[k], want[k])
