@@ -215,6 +215,18 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * direct, family 1 graph).  Allocates a temporary copy of the state. */
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
+/* Equilibrium Gaussian initial conditions generated on the device (the
+ * `set density equilibrium/gaussian`, `set momentum ... equilibrium/gaussian/
+ * compressible` and `set order_parameter ... equilibrium/gaussian` styles,
+ * initial_condition_equilibrium_gaussian_*.cc:16-108, and `uniform` with
+ * s0 = 0): writes one field of one member, every active mode k != 0 as
+ * sigma(k) xi_k with sigma(k)^2 = s0 / (c0 + c2 k^2 + c4 k^4) and xi_k the
+ * style's counter-based complex Gaussian for (seed, channel, mode), mode
+ * (0, 0) as `mean` (an unnormalised coefficient: value * nx * ny).  The same
+ * draws as the host restatement, without moving a State across PCIe. */
+int shhd_engine_set_gaussian_field(shhd_engine* engine, int member, int field, uint64_t seed, int channel, double mean, double s0,
+                                   double c0, double c2, double c4);
+
 /* Spectral L2 columns of the time-series measure (measure_time_series.cc:
  * |rho|^2, |d_rho|^2, |j|^2, |d_j|^2, |psi[a]|^2, |d_psi[a]|^2) for one member
  * of the current state, in FP64 on the device: out[2 f] = (V / Np^2) / Np^2

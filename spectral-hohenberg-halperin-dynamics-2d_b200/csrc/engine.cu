@@ -1589,6 +1589,44 @@ int shhd_engine_autotune(shhd_engine* e, int trial_steps, int* family, int* grap
     });
 }
 
+int shhd_engine_set_gaussian_field(shhd_engine* e, int member, int field, uint64_t seed, int channel, double mean, double s0, double c0,
+                                   double c2, double c4) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (field < 0 || field >= e->P.nfields) throw Failure(SHHD_EINVAL, "field index out of range");
+        if (s0 < 0.0) throw Failure(SHHD_EINVAL, "the variance scale must be nonnegative");
+        const StepPlan& P = e->P;
+        if (s0 != 0.0) {  // initial_condition_equilibrium_gaussian_order_parameter.cc: positive coefficient on every active k != 0
+            for (int gx = 0; gx < P.hx; ++gx)
+                for (int j = 0; j < P.kyn; ++j) {
+                    const int ky = j < P.nay / 2 ? j : j - P.kyn;
+                    if (gx == 0 && ky == 0) continue;
+                    const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky, k2 = kx * kx + kyv * kyv;
+                    if (!(c0 + c2 * k2 + c4 * k2 * k2 > 0.0))
+                        throw Failure(SHHD_EINVAL, "set order_parameter equilibrium/gaussian requires positive linear chemical-potential "
+                                                   "coefficient for every active nonzero mode.");
+                }
+        }
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        const size_t modes = static_cast<size_t>(P.hx) * P.kyn;
+        const dim3 g(static_cast<unsigned>((modes + kThreads - 1) / kThreads));
+        if (e->fp32)
+            gaussian_field_kernel<float><<<g, kThreads, 0, e->stream>>>(P, static_cast<float2*>(e->u), member, field, seed, channel, mean, s0, c0, c2, c4);
+        else
+            gaussian_field_kernel<double><<<g, kThreads, 0, e->stream>>>(P, static_cast<double2*>(e->u), member, field, seed, channel, mean, s0, c0, c2, c4);
+        check_cuda(cudaGetLastError(), "gaussian_field launch");
+        if (e->k0_u) {
+            const double2 k0 = make_double2(mean, 0.0);
+            check_cuda(cudaMemcpyAsync(e->k0_u + static_cast<size_t>(member) * P.nfields + field, &k0, sizeof(double2), cudaMemcpyHostToDevice,
+                                       e->stream),
+                       "k0 upload");
+        }
+        check_cuda(cudaStreamSynchronize(e->stream), "gaussian_field sync");
+        if (field == 0) e->rho0_candidate[member] = mean / (static_cast<double>(e->cfg.nx) * e->cfg.ny);
+    });
+}
+
 int shhd_engine_l2_sums(shhd_engine* e, int member, double* out, size_t n) {
     return guarded([&] {
         if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");

@@ -927,6 +927,55 @@ __global__ void __launch_bounds__(kThreads) l2_sums_kernel(const StepPlan P, con
     }
 }
 
+// ---------------------------------------------------------------------------
+// equilibrium Gaussian initial conditions written on the device
+// (initial_condition_equilibrium_gaussian_*.cc:16-108): every active mode k != 0
+// gets sigma(k) xi_k, sigma(k)^2 = s0 / (c0 + c2 k^2 + c4 k^4), xi_k a complex
+// unit Gaussian from the counter-based key (seed, channel, gx, ky', draw)
+// through splitmix64 and Box-Muller, ky' = |ky| on the kx = 0 line (ky < 0
+// takes the conjugate); mode (0, 0) gets `mean`.  grid: ceil(Hx * Ky / 256).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long ic_splitmix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+__device__ __forceinline__ double ic_uniform(unsigned long long seed, int channel, int gx, int ky, int draw) {
+    unsigned long long k = (seed & 0xFFFFFFFFull) ^ (static_cast<unsigned long long>(static_cast<unsigned>(channel)) << 48);
+    k ^= (static_cast<unsigned long long>(static_cast<unsigned>(gx)) & 0xFFFFFFFFull) << 32;
+    k ^= (static_cast<unsigned long long>(static_cast<long long>(ky)) & 0xFFFFFFFFull) << 8;
+    k ^= static_cast<unsigned long long>(static_cast<unsigned>(draw));
+    return static_cast<double>(ic_splitmix64(k) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) gaussian_field_kernel(const StepPlan P, cplx<T>* __restrict__ state, int b, int field,
+                                                                  unsigned long long seed, int channel, double mean, double s0, double c0,
+                                                                  double c2, double c4) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
+    if (e >= static_cast<int>(fstride)) return;
+    const int gx = e / P.kyn, j = e - gx * P.kyn;
+    const int ky = ky_of_j(j, P.nay);
+    double re = 0.0, im = 0.0;
+    if (gx == 0 && ky == 0) {
+        re = mean;
+    } else if (s0 != 0.0) {
+        const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky;
+        const double k2 = kx * kx + kyv * kyv;
+        const double sigma = sqrt(s0 / (c0 + c2 * k2 + c4 * k2 * k2));
+        const int pky = gx == 0 ? (ky < 0 ? -ky : ky) : ky;
+        const double u1 = fmax(ic_uniform(seed, channel, gx, pky, 0), 1.0e-300);
+        const double u2 = ic_uniform(seed, channel, gx, pky, 1);
+        const double r = sqrt(-2.0 * log(u1)), th = 2.0 * 3.14159265358979323846 * u2;
+        re = sigma * (r * cos(th));
+        im = sigma * (r * sin(th));
+        if (gx == 0 && ky < 0) im = -im;
+    }
+    state[(static_cast<size_t>(b) * P.nfields + field) * fstride + e] = mk(static_cast<T>(re), static_cast<T>(im));
+}
+
 // step counter of the call: set from the host at the start of a call, advanced
 // by the last node of a captured step graph
 __global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }

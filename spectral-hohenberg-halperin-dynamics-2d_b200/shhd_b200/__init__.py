@@ -102,7 +102,7 @@ EXPORTED = (
     "shhd_engine_stream", "shhd_engine_state_device", "shhd_engine_set_profiling", "shhd_engine_kernel_stats",
     "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
     "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
-    "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums",
+    "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums", "shhd_engine_set_gaussian_field",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -144,6 +144,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_gk_enable.argtypes = [vp, i, i, i]
     lib.shhd_engine_gk_read.argtypes = [vp, i, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
     lib.shhd_engine_l2_sums.argtypes = [vp, i, dp, sz]
+    d = ctypes.c_double
+    lib.shhd_engine_set_gaussian_field.argtypes = [vp, i, i, ctypes.c_uint64, i, d, d, d, d, d]
     return lib
 
 
@@ -273,6 +275,12 @@ class Engine:
         _check(lib.shhd_engine_autotune(self._h, int(trial_steps), ctypes.byref(fam), ctypes.byref(chunk), _dptr(ms)))
         return {"family": "pair-line" if fam.value == 1 else "single-line", "graph_chunk": chunk.value,
                 "ms_per_step": [None if np.isnan(x) else float(x) for x in ms]}
+
+    def set_gaussian_field(self, member: int, field: int, seed: int, channel: int, mean: float, s0: float,
+                           c0: float = 1.0, c2: float = 0.0, c4: float = 0.0) -> None:
+        """Write one field on the device: sigma(k) xi_k per active mode, `mean` at k = 0."""
+        _check(lib.shhd_engine_set_gaussian_field(self._h, int(member), int(field), int(seed) & 0xFFFFFFFFFFFFFFFF, int(channel),
+                                                  float(mean), float(s0), float(c0), float(c2), float(c4)))
 
     def time_series_l2(self, member: int = 0) -> dict:
         """The reference time-series measure's spectral L2 columns of the current state (FP64)."""

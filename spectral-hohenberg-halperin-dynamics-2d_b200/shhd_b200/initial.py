@@ -81,11 +81,9 @@ def _kv(tokens: List[str]) -> Dict[str, str]:
     return dict(zip(tokens[0::2], tokens[1::2]))
 
 
-def initial_state(cfg, script_text: str) -> np.ndarray:
-    """State from the `set` lines of a script; cfg is a shhd_b200.Config (grid, length, N)."""
-    g = _Grid((cfg.active_nx, cfg.active_ny), (cfg.nx, cfg.ny), (cfg.lx, cfg.ly))
+def _set_commands(cfg, script_text: str):
+    """The `set` lines of a script grouped as (density, momentum, order parameter) commands."""
     n = cfg.num_order_parameters
-    u = np.zeros((n + 3, g.ny, g.hx), dtype=np.complex128)
     dens, mom, psi = [], [], []
     for raw in script_text.splitlines():
         t = raw.split("#", 1)[0].split()
@@ -101,6 +99,15 @@ def initial_state(cfg, script_text: str) -> np.ndarray:
             targets = list(range(n)) if t[2] == "all" else [int(t[2])]
             for a in targets:
                 psi.append((a, t[3], _kv(t[4:])))
+    return dens, mom, psi
+
+
+def initial_state(cfg, script_text: str) -> np.ndarray:
+    """State from the `set` lines of a script; cfg is a shhd_b200.Config (grid, length, N)."""
+    g = _Grid((cfg.active_nx, cfg.active_ny), (cfg.nx, cfg.ny), (cfg.lx, cfg.ly))
+    n = cfg.num_order_parameters
+    u = np.zeros((n + 3, g.ny, g.hx), dtype=np.complex128)
+    dens, mom, psi = _set_commands(cfg, script_text)
     act = g.active
     for style, kv in dens:
         rho = np.zeros((g.ny, g.hx), dtype=np.complex128)
@@ -157,3 +164,62 @@ def initial_state(cfg, script_text: str) -> np.ndarray:
             raise NotImplementedError(f"set order_parameter {style}")
         u[f] = p
     return u
+
+
+def field_generators(cfg, script_text: str) -> List[Tuple[int, int, int, float, float, float, float, float]]:
+    """One (field, seed, channel, mean, s0, c0, c2, c4) per field: the state `initial_state` builds,
+    as sigma(k)^2 = s0 / (c0 + c2 k^2 + c4 k^4) per active mode k != 0 and `mean` at k = 0.
+
+    Every `set` command rewrites its whole field, so the last command on a field decides it; the
+    momentum styles read the reference density the density commands left (src/project.h:92-116).
+    """
+    n = cfg.num_order_parameters
+    ng = float(cfg.nx) * float(cfg.ny)
+    cell = cfg.lx * cfg.ly / ng
+    gens = {f: (f, 0, 0, 0.0, 0.0, 1.0, 0.0, 0.0) for f in range(n + 3)}
+    dens, mom, psi = _set_commands(cfg, script_text)
+    for style, kv in dens:
+        if style == "uniform":
+            gens[0] = (0, 0, 0, float(kv["value"]) * ng, 0.0, 1.0, 0.0, 0.0)
+        elif style == "equilibrium/gaussian":
+            kbt, rho0, cT, seed = float(kv["kBT"]), float(kv.get("rho0", 1.0)), float(kv["cT"]), int(kv.get("seed", 0))
+            s0 = kbt * ng * rho0 / (2.0 * (cT * cT) * cell) if kbt != 0.0 else 0.0
+            gens[0] = (0, seed, 0, rho0 * ng, s0, 1.0, 0.0, 0.0)
+        else:
+            raise NotImplementedError(f"set density {style}")
+    rho0 = gens[0][3] / ng
+    for d, style, kv in mom:
+        f = n + 1 + d
+        if style == "uniform":
+            gens[f] = (f, 0, d, float(kv["value"]) * ng, 0.0, 1.0, 0.0, 0.0)
+        elif style == "equilibrium/gaussian/compressible":
+            kbt, seed = float(kv["kBT"]), int(kv.get("seed", 0))
+            s0 = 0.0
+            if kbt != 0.0:
+                if rho0 <= 0.0:
+                    raise ValueError("set momentum equilibrium/gaussian/compressible requires positive reference density.")
+                s0 = kbt * ng * rho0 / (2.0 * cell)
+            gens[f] = (f, seed, d, 0.0, s0, 1.0, 0.0, 0.0)
+        else:
+            raise NotImplementedError(f"set momentum {style}")
+    for a, style, kv in psi:
+        f = 1 + a
+        if style == "uniform":
+            gens[f] = (f, 0, a, float(kv["value"]) * ng, 0.0, 1.0, 0.0, 0.0)
+        elif style == "equilibrium/gaussian":
+            kbt, seed, psi0 = float(kv["kBT"]), int(kv.get("seed", 0)), float(kv.get("psi0", 0.0))
+            k0, k2c, k4 = float(kv.get("k0", 0.0)), float(kv.get("k2", 0.0)), float(kv.get("k4", 0.0))
+            s0 = kbt * ng / (2.0 * cell) if kbt != 0.0 else 0.0
+            gens[f] = (f, seed, a, psi0 * ng, s0, k0, k2c, k4)
+        else:
+            raise NotImplementedError(f"set order_parameter {style}")
+    return [gens[f] for f in range(n + 3)]
+
+
+def initial_state_device(engine, script_text: str, member: int = 0) -> None:
+    """Write the state of a script's `set` lines into one member of `engine`, generated on the device.
+
+    The draws are those of `initial_state`; no state crosses PCIe (one kernel per field).
+    """
+    for f, seed, channel, mean, s0, c0, c2, c4 in field_generators(engine.cfg, script_text):
+        engine.set_gaussian_field(member, f, seed, channel, mean, s0, c0, c2, c4)

@@ -24,15 +24,17 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 
 from . import FP32, Config, Engine
+from .initial import initial_state_device
 
 
 @dataclasses.dataclass
 class Job:
     key: int                      # unique id; keys the job's noise stream
     config: Config                # solver configuration (precision ignored; the server sets it)
-    state: np.ndarray             # initial State (reference layout, complex128)
+    state: Optional[np.ndarray]   # initial State (reference layout, complex128), or None with `initial`
     nsteps: int
     arrival: float = 0.0          # seconds after the server starts
+    initial: Optional[str] = None  # `set` lines generating the initial state on the device (when state is None)
     green_kubo: Optional[Tuple[int, int]] = None   # (nevery, nblock): Yokota-Green-Kubo stress measure
     # filled by the server
     result: Optional[np.ndarray] = None
@@ -92,7 +94,12 @@ class _Bucket:
         return None
 
     def admit(self, m: int, job: Job, now: float) -> None:
-        self.engine.set_state(job.state, member=m)
+        if job.state is not None:
+            self.engine.set_state(job.state, member=m)
+        elif job.initial is not None:
+            initial_state_device(self.engine, job.initial, member=m)
+        else:
+            raise ValueError(f"job {job.key}: neither an initial state nor `set` lines")
         scale = math.sqrt(job.config.kBT) if self.noisy else 0.0
         self.engine.set_member(m, key=job.key, step_origin=self.step_index, noise_scale=scale, active=True)
         if self.green_kubo is not None:

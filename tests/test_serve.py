@@ -100,3 +100,30 @@ def test_served_green_kubo_equals_alone():
         serve.run_alone(alone, 0, seed=5)
         assert blocks == alone.gk_blocks == job.nsteps // 8
         assert np.abs(sums - alone.gk_sums).max() <= 1e-12 * np.abs(alone.gk_sums).max()
+
+
+def test_jobs_from_set_lines_equal_jobs_with_host_states():
+    """A job may carry its `set` lines instead of a state: admission generates it on the device."""
+    import shhd_b200 as sb
+    from shhd_b200 import serve
+    from shhd_b200.initial import initial_state
+    base = script(grid=(64, 64), length=(128.0, 128.0), nop=2, dt=0.01, noise="kBT 0.002 seed 1")
+    jobs_dev, jobs_host = [], []
+    for k in range(3):
+        text = base + "\n".join([
+            "",
+            f"set density equilibrium/gaussian kBT 1e-3 rho0 1 cT 1 seed {10 + k}",
+            f"set momentum all equilibrium/gaussian/compressible kBT 1e-3 seed {20 + k}",
+            f"set order_parameter all equilibrium/gaussian seed {30 + k} kBT 0.002 k0 2 k2 1",
+        ])
+        cfg = sb.config_from_script(text)
+        jobs_dev.append(serve.Job(key=500 + k, config=cfg, state=None, initial=text, nsteps=20 + 5 * k, arrival=0.002 * k))
+        jobs_host.append(serve.Job(key=500 + k, config=cfg, state=initial_state(cfg, text), nsteps=20 + 5 * k,
+                                   arrival=0.002 * k))
+    for jobs in (jobs_dev, jobs_host):
+        srv = serve.Server(precision=0, seed=5, max_slots=2, chunk=5)
+        srv.run(jobs)
+        srv.close()
+    for a, b in zip(jobs_dev, jobs_host):
+        assert np.all(np.isfinite(a.result))
+        assert so.rel_l2(a.result, b.result) < 1e-12, a.key
