@@ -215,15 +215,62 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * direct, family 1 graph).  Allocates a temporary copy of the state. */
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
-/* Equilibrium Gaussian initial conditions generated on the device (the
- * `set density equilibrium/gaussian`, `set momentum ... equilibrium/gaussian/
- * compressible` and `set order_parameter ... equilibrium/gaussian` styles,
- * initial_condition_equilibrium_gaussian_*.cc:16-108, and `uniform` with
- * s0 = 0): writes one field of one member, every active mode k != 0 as
- * sigma(k) xi_k with sigma(k)^2 = s0 / (c0 + c2 k^2 + c4 k^4) and xi_k the
- * style's counter-based complex Gaussian for (seed, channel, mode), mode
- * (0, 0) as `mean` (an unnormalised coefficient: value * nx * ny).  The same
- * draws as the host restatement, without moving a State across PCIe. */
+/* Initial conditions generated on the device: the reference's `set` styles
+ * (initial_condition_*.cc), one field of one member per call, every active
+ * mode evaluated in FP64 (FP32 engines round once and keep the (0, 0) value
+ * in their FP64 copy).  Wave numbers are 2 pi g / L; Ng = nx * ny (padded).
+ *
+ *   GAUSSIAN_MODES      sigma(k) xi_k at k != 0, sigma(k)^2 = s0 / (c0 + c2 k^2
+ *                       + c4 k^4), xi_k the equilibrium styles' complex unit
+ *                       Gaussian for (seed, channel, kx, ky); `mean` at (0, 0).
+ *                       uniform (s0 = 0), equilibrium/gaussian density and
+ *                       order parameter, equilibrium/gaussian/compressible
+ *                       momentum (channel = direction).
+ *   TRANSVERSE_GAUSSIAN equilibrium/gaussian/incompressible momentum, direction
+ *                       `channel`: (-ky/k or kx/k) sqrt(s0) xi_k (key channel 0).
+ *   RANDOM_VORTICITY    random_vorticity, direction `channel`: the shell
+ *                       exp(-((|n| - n0)/sigma)^2 / 2) with one random phase per
+ *                       mode (seed, gx, ky), as velocity, normalised so the rms
+ *                       velocity is `amplitude` (urms), times `rho0`.
+ *   BUMP                gaussian: amplitude Ng 2 pi sx sy / (Lx Ly)
+ *                       exp(-(sx^2 kx^2 + sy^2 ky^2)/2) e^{-i(kx x0 + ky y0)},
+ *                       plus `mean` (base * Ng) at (0, 0).
+ *   SINE                sine: -i amplitude Ng / 2 at (nkx, nky) (and its
+ *                       conjugate on the kx = 0 line), `mean` at (0, 0).
+ *
+ * Errors are the reference's (e.g. a nonpositive chemical-potential
+ * coefficient, a zero random-vorticity norm or reference density). */
+enum shhd_ic_style {
+    SHHD_IC_GAUSSIAN_MODES = 0,
+    SHHD_IC_TRANSVERSE_GAUSSIAN = 1,
+    SHHD_IC_RANDOM_VORTICITY = 2,
+    SHHD_IC_BUMP = 3,
+    SHHD_IC_SINE = 4
+};
+
+typedef struct shhd_initial_field {
+    int style;                 /* enum shhd_ic_style */
+    int channel;               /* key channel (GAUSSIAN_MODES) or direction 0 = x, 1 = y */
+    uint64_t seed;             /* counter-based key (low 32 bits used) */
+    double mean;               /* (0, 0) coefficient */
+    double s0, c0, c2, c4;     /* variance law of GAUSSIAN_MODES / TRANSVERSE_GAUSSIAN (c0 = 1 for density, momentum) */
+    double amplitude;          /* BUMP, SINE: amplitude; RANDOM_VORTICITY: urms */
+    double rho0;               /* RANDOM_VORTICITY: reference density */
+    double n0, sigma;          /* RANDOM_VORTICITY: shell radius and width in mode numbers */
+    double x0, y0;             /* BUMP: centre */
+    double sigma_x, sigma_y;   /* BUMP: widths */
+    int nkx, nky;              /* SINE: mode numbers */
+} shhd_initial_field;
+
+int shhd_engine_set_initial_field(shhd_engine* engine, int member, int field, const shhd_initial_field* spec);
+
+/* The incompressible check on the initial momentum (initial_condition.cc:7-40),
+ * evaluated in FP64 on the two momentum specs: SHHD_EINVAL with the
+ * reference's message when |k . j| > 1e-10 + 1e-10 |k| |j| at an active
+ * k != 0. */
+int shhd_engine_check_transverse(shhd_engine* engine, const shhd_initial_field* jx, const shhd_initial_field* jy);
+
+/* GAUSSIAN_MODES with the given arguments (shorthand of shhd_engine_set_initial_field). */
 int shhd_engine_set_gaussian_field(shhd_engine* engine, int member, int field, uint64_t seed, int channel, double mean, double s0,
                                    double c0, double c2, double c4);
 

@@ -228,6 +228,8 @@ struct shhd_engine {
 
     void* ref_stage = nullptr;       // one member's reference-layout state (FP64) on the device
     int* flag_dev = nullptr;
+    double* ic_scratch = nullptr;    // random-vorticity norm [0] and block partial sums [1..]
+    size_t ic_scratch_bytes = 0;
     unsigned long long* step_dev = nullptr;  // step index at the start of the current call
 
     // captured step graphs: one call of `size` steps each, for the chunk and every power of two
@@ -270,7 +272,7 @@ void free_engine(shhd_engine* e) {
     for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->ref_stage,
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
                     static_cast<void*>(e->members_dev),
-                    static_cast<void*>(e->flag_dev)})
+                    static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch)})
         if (p) cudaFree(p);
     for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
     e->graphs.clear();
@@ -1589,42 +1591,151 @@ int shhd_engine_autotune(shhd_engine* e, int trial_steps, int* family, int* grap
     });
 }
 
-int shhd_engine_set_gaussian_field(shhd_engine* e, int member, int field, uint64_t seed, int channel, double mean, double s0, double c0,
-                                   double c2, double c4) {
-    return guarded([&] {
-        if (!e) throw Failure(SHHD_EINVAL, "null engine");
-        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
-        if (field < 0 || field >= e->P.nfields) throw Failure(SHHD_EINVAL, "field index out of range");
-        if (s0 < 0.0) throw Failure(SHHD_EINVAL, "the variance scale must be nonnegative");
-        const StepPlan& P = e->P;
-        if (s0 != 0.0) {  // initial_condition_equilibrium_gaussian_order_parameter.cc: positive coefficient on every active k != 0
-            for (int gx = 0; gx < P.hx; ++gx)
-                for (int j = 0; j < P.kyn; ++j) {
-                    const int ky = j < P.nay / 2 ? j : j - P.kyn;
-                    if (gx == 0 && ky == 0) continue;
-                    const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky, k2 = kx * kx + kyv * kyv;
-                    if (!(c0 + c2 * k2 + c4 * k2 * k2 > 0.0))
+}  // extern "C"
+
+namespace {
+
+// device spec of a C-ABI initial-field description, with its style's checks (the reference's
+// parse-time and apply-time errors, in its words)
+IcSpec resolve_initial_field(shhd_engine* e, const shhd_initial_field& in) {
+    const StepPlan& P = e->P;
+    const double ng = static_cast<double>(e->cfg.nx) * e->cfg.ny;
+    constexpr double PI = 3.14159265358979323846;
+    IcSpec s{};
+    s.style = in.style;
+    s.channel = in.channel;
+    s.seed = in.seed;
+    s.mean = in.mean;
+    s.s0 = in.s0; s.c0 = in.c0; s.c2 = in.c2; s.c4 = in.c4;
+    s.n0 = in.n0; s.sigma = in.sigma;
+    s.x0 = in.x0; s.y0 = in.y0; s.sx = in.sigma_x; s.sy = in.sigma_y;
+    s.nkx = in.nkx; s.nky = in.nky;
+    s.lx = e->cfg.lx; s.ly = e->cfg.ly;
+    auto each_active_k2 = [&](auto&& f) {
+        for (int gx = 0; gx < P.hx; ++gx)
+            for (int j = 0; j < P.kyn; ++j) {
+                const int ky = j < P.nay / 2 ? j : j - P.kyn;
+                if (gx == 0 && ky == 0) continue;
+                const double kx = 2.0 * PI * gx / s.lx, kyv = 2.0 * PI * ky / s.ly;
+                f(kx * kx + kyv * kyv);
+            }
+    };
+    switch (in.style) {
+        case SHHD_IC_GAUSSIAN_MODES:
+            if (in.s0 < 0.0) throw Failure(SHHD_EINVAL, "the variance scale must be nonnegative");
+            if (in.s0 != 0.0)  // initial_condition_equilibrium_gaussian_order_parameter.cc: positive coefficient on every active k != 0
+                each_active_k2([&](double k2) {
+                    if (!(in.c0 + in.c2 * k2 + in.c4 * k2 * k2 > 0.0))
                         throw Failure(SHHD_EINVAL, "set order_parameter equilibrium/gaussian requires positive linear chemical-potential "
                                                    "coefficient for every active nonzero mode.");
-                }
+                });
+            break;
+        case SHHD_IC_TRANSVERSE_GAUSSIAN:
+            if (in.s0 < 0.0) throw Failure(SHHD_EINVAL, "the variance scale must be nonnegative");
+            if (in.channel != 0 && in.channel != 1) throw Failure(SHHD_EINVAL, "direction must be 0 or 1");
+            break;
+        case SHHD_IC_RANDOM_VORTICITY:
+            if (in.channel != 0 && in.channel != 1) throw Failure(SHHD_EINVAL, "direction must be 0 or 1");
+            if (!(in.n0 > 0.0)) throw Failure(SHHD_EINVAL, "set momentum random_vorticity requires positive n0.");
+            if (!(in.sigma > 0.0)) throw Failure(SHHD_EINVAL, "set momentum random_vorticity requires positive sigma.");
+            if (!(in.amplitude > 0.0)) throw Failure(SHHD_EINVAL, "set momentum random_vorticity requires positive urms.");
+            break;  // factor: from the device norm
+        case SHHD_IC_BUMP:
+            if (!(in.sigma_x > 0.0) || !(in.sigma_y > 0.0)) throw Failure(SHHD_EINVAL, "gaussian requires positive sigma values");
+            s.factor = in.amplitude * ng * 2.0 * PI * in.sigma_x * in.sigma_y / (s.lx * s.ly);
+            break;
+        case SHHD_IC_SINE:
+            if (in.nkx < 0 || in.nkx >= P.hx) throw Failure(SHHD_EINVAL, "sine requires 0 <= nkx < Nx/2; Nyquist line is fixed to zero");
+            if (in.nky <= -(P.nay / 2) || in.nky >= P.nay / 2)
+                throw Failure(SHHD_EINVAL, "sine requires -Ny/2 < nky < Ny/2; Nyquist line is fixed to zero");
+            if (in.nkx == 0 && in.nky == 0) throw Failure(SHHD_EINVAL, "sine requires a nonzero wave number");
+            s.factor = -0.5 * in.amplitude * ng;
+            break;
+        default: throw Failure(SHHD_EINVAL, "unknown initial-field style " + std::to_string(in.style));
+    }
+    if (in.style == SHHD_IC_RANDOM_VORTICITY) {
+        // initial_condition_random_vorticity_momentum.cc:108-131: the norm of the unnormalised shell over both
+        // components, summed on the device in a fixed order
+        const int nblk = static_cast<int>((static_cast<size_t>(P.hx) * P.kyn + kThreads - 1) / kThreads);
+        const size_t need = sizeof(double) * (static_cast<size_t>(nblk) + 1);
+        if (e->ic_scratch_bytes < need) {
+            if (e->ic_scratch) { check_cuda(cudaFree(e->ic_scratch), "cudaFree"); e->device_bytes -= e->ic_scratch_bytes; e->ic_scratch = nullptr; }
+            e->ic_scratch = static_cast<double*>(dalloc(e, need));
+            e->ic_scratch_bytes = need;
         }
+        vorticity_norm_kernel<<<nblk, kThreads, 0, e->stream>>>(P, s, e->ic_scratch + 1);
+        check_cuda(cudaGetLastError(), "vorticity_norm launch");
+        sum_partials_kernel<<<1, kThreads, 0, e->stream>>>(e->ic_scratch + 1, nblk, e->ic_scratch);
+        check_cuda(cudaGetLastError(), "sum_partials launch");
+        double norm = 0.0;
+        check_cuda(cudaMemcpyAsync(&norm, e->ic_scratch, sizeof(double), cudaMemcpyDeviceToHost, e->stream), "norm read");
+        check_cuda(cudaStreamSynchronize(e->stream), "norm sync");
+        if (norm == 0.0) throw Failure(SHHD_EINVAL, "set momentum random_vorticity generated zero velocity field.");
+        if (in.rho0 == 0.0) throw Failure(SHHD_EINVAL, "set momentum random_vorticity requires nonzero reference density.");
+        const double scale = in.amplitude * ng / std::sqrt(norm);
+        s.factor = in.rho0 * scale;
+    }
+    return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int shhd_engine_set_initial_field(shhd_engine* e, int member, int field, const shhd_initial_field* spec) {
+    return guarded([&] {
+        if (!e || !spec) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (field < 0 || field >= e->P.nfields) throw Failure(SHHD_EINVAL, "field index out of range");
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        const IcSpec s = resolve_initial_field(e, *spec);
+        const StepPlan& P = e->P;
         const size_t modes = static_cast<size_t>(P.hx) * P.kyn;
         const dim3 g(static_cast<unsigned>((modes + kThreads - 1) / kThreads));
+        double2* k0 = e->k0_u ? e->k0_u + static_cast<size_t>(member) * P.nfields + field : nullptr;
         if (e->fp32)
-            gaussian_field_kernel<float><<<g, kThreads, 0, e->stream>>>(P, static_cast<float2*>(e->u), member, field, seed, channel, mean, s0, c0, c2, c4);
+            initial_field_kernel<float><<<g, kThreads, 0, e->stream>>>(P, static_cast<float2*>(e->u), member, field, s, k0);
         else
-            gaussian_field_kernel<double><<<g, kThreads, 0, e->stream>>>(P, static_cast<double2*>(e->u), member, field, seed, channel, mean, s0, c0, c2, c4);
-        check_cuda(cudaGetLastError(), "gaussian_field launch");
-        if (e->k0_u) {
-            const double2 k0 = make_double2(mean, 0.0);
-            check_cuda(cudaMemcpyAsync(e->k0_u + static_cast<size_t>(member) * P.nfields + field, &k0, sizeof(double2), cudaMemcpyHostToDevice,
-                                       e->stream),
-                       "k0 upload");
-        }
-        check_cuda(cudaStreamSynchronize(e->stream), "gaussian_field sync");
-        if (field == 0) e->rho0_candidate[member] = mean / (static_cast<double>(e->cfg.nx) * e->cfg.ny);
+            initial_field_kernel<double><<<g, kThreads, 0, e->stream>>>(P, static_cast<double2*>(e->u), member, field, s, k0);
+        check_cuda(cudaGetLastError(), "initial_field launch");
+        double2 v00{};  // the (0, 0) coefficient in FP64: the FP32 engines' copy, else the state itself
+        const void* src = k0 ? static_cast<const void*>(k0)
+                             : static_cast<const void*>(static_cast<const double2*>(e->u) + (static_cast<size_t>(member) * P.nfields + field) * modes);
+        check_cuda(cudaMemcpyAsync(&v00, src, sizeof(double2), cudaMemcpyDeviceToHost, e->stream), "k = 0 read");
+        check_cuda(cudaStreamSynchronize(e->stream), "initial_field sync");
+        if (field == 0) e->rho0_candidate[member] = v00.x / (static_cast<double>(e->cfg.nx) * e->cfg.ny);  // as set_state takes it
     });
+}
+
+int shhd_engine_check_transverse(shhd_engine* e, const shhd_initial_field* jx, const shhd_initial_field* jy) {
+    return guarded([&] {
+        if (!e || !jx || !jy) throw Failure(SHHD_EINVAL, "null argument");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        const IcSpec sx = resolve_initial_field(e, *jx), sy = resolve_initial_field(e, *jy);
+        if (!e->flag_dev) e->flag_dev = static_cast<int*>(dalloc(e, sizeof(int)));
+        check_cuda(cudaMemsetAsync(e->flag_dev, 0, sizeof(int), e->stream), "flag clear");
+        const StepPlan& P = e->P;
+        const size_t modes = static_cast<size_t>(P.hx) * P.kyn;
+        transverse_check_kernel<<<static_cast<unsigned>((modes + kThreads - 1) / kThreads), kThreads, 0, e->stream>>>(P, sx, sy, e->flag_dev);
+        check_cuda(cudaGetLastError(), "transverse_check launch");
+        int bad = 0;
+        check_cuda(cudaMemcpyAsync(&bad, e->flag_dev, sizeof(int), cudaMemcpyDeviceToHost, e->stream), "flag read");
+        check_cuda(cudaStreamSynchronize(e->stream), "transverse_check sync");
+        if (bad)
+            throw Failure(SHHD_EINVAL, "incompressible initial momentum must be transverse: k dot j must be zero for every nonzero active "
+                                       "spectral mode.");
+    });
+}
+
+int shhd_engine_set_gaussian_field(shhd_engine* e, int member, int field, uint64_t seed, int channel, double mean, double s0, double c0,
+                                   double c2, double c4) {
+    shhd_initial_field spec{};
+    spec.style = SHHD_IC_GAUSSIAN_MODES;
+    spec.channel = channel;
+    spec.seed = seed;
+    spec.mean = mean;
+    spec.s0 = s0; spec.c0 = c0; spec.c2 = c2; spec.c4 = c4;
+    return shhd_engine_set_initial_field(e, member, field, &spec);
 }
 
 int shhd_engine_l2_sums(shhd_engine* e, int member, double* out, size_t n) {

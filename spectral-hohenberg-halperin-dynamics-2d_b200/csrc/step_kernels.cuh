@@ -928,52 +928,180 @@ __global__ void __launch_bounds__(kThreads) l2_sums_kernel(const StepPlan P, con
 }
 
 // ---------------------------------------------------------------------------
-// equilibrium Gaussian initial conditions written on the device
-// (initial_condition_equilibrium_gaussian_*.cc:16-108): every active mode k != 0
-// gets sigma(k) xi_k, sigma(k)^2 = s0 / (c0 + c2 k^2 + c4 k^4), xi_k a complex
-// unit Gaussian from the counter-based key (seed, channel, gx, ky', draw)
-// through splitmix64 and Box-Muller, ky' = |ky| on the kx = 0 line (ky < 0
-// takes the conjugate); mode (0, 0) gets `mean`.  grid: ceil(Hx * Ky / 256).
+// initial conditions written on the device (initial_condition_*.cc): one spec
+// per field, evaluated per active mode in FP64 by ic_value, which the writer,
+// the random-vorticity norm and the transversality check share.  Wave numbers
+// are formed as the reference's Domain2D::kx/ky do (2 pi g / L).
 // ---------------------------------------------------------------------------
+enum IcStyle { IC_GAUSSIAN_MODES = 0, IC_TRANSVERSE_GAUSSIAN = 1, IC_RANDOM_VORTICITY = 2, IC_BUMP = 3, IC_SINE = 4 };
+
+struct IcSpec {
+    int style, channel;
+    unsigned long long seed;
+    double mean;              // (0, 0) coefficient (GAUSSIAN_MODES, SINE; added to the bump's own)
+    double s0, c0, c2, c4;    // sigma(k)^2 = s0 / (c0 + c2 k^2 + c4 k^4)
+    double factor;            // RANDOM_VORTICITY: rho0 * urms Ng / sqrt(norm); BUMP: A Ng 2 pi sx sy / (Lx Ly); SINE: -A Ng / 2
+    double n0, sigma;         // RANDOM_VORTICITY shell in mode numbers
+    double x0, y0, sx, sy;    // BUMP
+    int nkx, nky;             // SINE
+    double lx, ly;            // box lengths
+};
+
 __device__ __forceinline__ unsigned long long ic_splitmix64(unsigned long long x) {
     x += 0x9E3779B97F4A7C15ull;
     x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
     x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
     return x ^ (x >> 31);
 }
+__device__ __forceinline__ unsigned long long ic_u32(long long v) { return static_cast<unsigned long long>(v) & 0xFFFFFFFFull; }
+__device__ __forceinline__ double ic_unit(unsigned long long key) {
+    return static_cast<double>(ic_splitmix64(key) >> 11) * (1.0 / 9007199254740992.0);
+}
+// key of the equilibrium styles: seed ^ channel << 48 ^ gx << 32 ^ ky << 8 ^ draw
 __device__ __forceinline__ double ic_uniform(unsigned long long seed, int channel, int gx, int ky, int draw) {
-    unsigned long long k = (seed & 0xFFFFFFFFull) ^ (static_cast<unsigned long long>(static_cast<unsigned>(channel)) << 48);
-    k ^= (static_cast<unsigned long long>(static_cast<unsigned>(gx)) & 0xFFFFFFFFull) << 32;
-    k ^= (static_cast<unsigned long long>(static_cast<long long>(ky)) & 0xFFFFFFFFull) << 8;
-    k ^= static_cast<unsigned long long>(static_cast<unsigned>(draw));
-    return static_cast<double>(ic_splitmix64(k) >> 11) * (1.0 / 9007199254740992.0);
+    return ic_unit(ic_u32(static_cast<long long>(seed)) ^ (ic_u32(channel) << 48) ^ (ic_u32(gx) << 32) ^ (ic_u32(ky) << 8) ^
+                   ic_u32(draw));
+}
+// complex unit Gaussian of the equilibrium styles at (gx, ky), kx = 0 line conjugated for ky < 0
+__device__ __forceinline__ double2 ic_gaussian(unsigned long long seed, int channel, int gx, int ky) {
+    const int pky = gx == 0 ? (ky < 0 ? -ky : ky) : ky;
+    const double u1 = fmax(ic_uniform(seed, channel, gx, pky, 0), 1.0e-300);
+    const double u2 = ic_uniform(seed, channel, gx, pky, 1);
+    const double r = sqrt(-2.0 * log(u1)), th = 2.0 * 3.14159265358979323846 * u2;
+    double2 v = make_double2(r * cos(th), r * sin(th));
+    if (gx == 0 && ky < 0) v.y = -v.y;
+    return v;
+}
+// random-vorticity velocity (u_x, u_y) before normalisation; zero at k = 0
+__device__ __forceinline__ void ic_vorticity(const IcSpec& s, int gx, int ky, double kx, double kyv, double k2, double2& ux,
+                                             double2& uy) {
+    ux = uy = make_double2(0.0, 0.0);
+    if (k2 == 0.0) return;
+    const int pky = gx == 0 ? (ky < 0 ? -ky : ky) : ky;
+    const double n = sqrt(static_cast<double>(gx) * gx + static_cast<double>(ky) * ky);
+    const double d = (n - s.n0) / s.sigma;
+    const double env = exp(-0.5 * d * d);
+    const double th = 2.0 * 3.14159265358979323846 *
+                      ic_unit(ic_u32(static_cast<long long>(s.seed)) ^ (ic_u32(gx) << 32) ^ ic_u32(pky));
+    double2 om = make_double2(env * cos(th), env * sin(th));
+    if (gx == 0 && ky < 0) om.y = -om.y;
+    const double ax = kyv / k2, ay = kx / k2;
+    ux = make_double2(-ax * om.y, ax * om.x);   // (i ky / k^2) omega
+    uy = make_double2(ay * om.y, -ay * om.x);   // -(i kx / k^2) omega
 }
 
+__device__ double2 ic_value(const IcSpec& s, int gx, int ky) {
+    const double kx = 2.0 * 3.14159265358979323846 * gx / s.lx, kyv = 2.0 * 3.14159265358979323846 * ky / s.ly;
+    const double k2 = kx * kx + kyv * kyv;
+    const bool zero = gx == 0 && ky == 0;
+    switch (s.style) {
+        case IC_GAUSSIAN_MODES: {
+            if (zero) return make_double2(s.mean, 0.0);
+            if (s.s0 == 0.0) return make_double2(0.0, 0.0);
+            const double sigma = sqrt(s.s0 / (s.c0 + s.c2 * k2 + s.c4 * k2 * k2));
+            const double2 g = ic_gaussian(s.seed, s.channel, gx, ky);
+            return make_double2(sigma * g.x, sigma * g.y);
+        }
+        case IC_TRANSVERSE_GAUSSIAN: {
+            if (zero || s.s0 == 0.0) return make_double2(0.0, 0.0);
+            const double k = sqrt(k2);
+            const double comp = s.channel == 0 ? (-kyv / k) : (kx / k);
+            const double sigma = sqrt(s.s0);
+            const double2 g = ic_gaussian(s.seed, 0, gx, ky);
+            return make_double2(comp * (sigma * g.x), comp * (sigma * g.y));
+        }
+        case IC_RANDOM_VORTICITY: {
+            double2 ux, uy;
+            ic_vorticity(s, gx, ky, kx, kyv, k2, ux, uy);
+            const double2 u = s.channel == 0 ? ux : uy;
+            return make_double2(s.factor * u.x, s.factor * u.y);
+        }
+        case IC_BUMP: {
+            const double env = exp(-0.5 * (s.sx * s.sx * kx * kx + s.sy * s.sy * kyv * kyv));
+            const double ph = -(kx * s.x0 + kyv * s.y0);
+            const double a = s.factor * env;
+            double2 v = make_double2(a * cos(ph), a * sin(ph));
+            if (zero) v.x += s.mean;
+            return v;
+        }
+        case IC_SINE: {
+            if (zero) return make_double2(s.mean, 0.0);
+            if (gx == s.nkx && ky == s.nky) return make_double2(0.0, s.factor);
+            if (s.nkx == 0 && s.nky != 0 && gx == 0 && ky == -s.nky) return make_double2(0.0, -s.factor);
+            return make_double2(0.0, 0.0);
+        }
+        default: return make_double2(0.0, 0.0);
+    }
+}
+
+// writes every active mode of one field of member b; the (0, 0) value also to k0 (FP64 copy) when given.
+// grid: ceil(Hx * Ky / 256)
 template <typename T>
-__global__ void __launch_bounds__(kThreads) gaussian_field_kernel(const StepPlan P, cplx<T>* __restrict__ state, int b, int field,
-                                                                  unsigned long long seed, int channel, double mean, double s0, double c0,
-                                                                  double c2, double c4) {
+__global__ void __launch_bounds__(kThreads) initial_field_kernel(const StepPlan P, cplx<T>* __restrict__ state, int b, int field,
+                                                                 const IcSpec s, double2* __restrict__ k0) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
     if (e >= static_cast<int>(fstride)) return;
     const int gx = e / P.kyn, j = e - gx * P.kyn;
     const int ky = ky_of_j(j, P.nay);
-    double re = 0.0, im = 0.0;
-    if (gx == 0 && ky == 0) {
-        re = mean;
-    } else if (s0 != 0.0) {
-        const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky;
-        const double k2 = kx * kx + kyv * kyv;
-        const double sigma = sqrt(s0 / (c0 + c2 * k2 + c4 * k2 * k2));
-        const int pky = gx == 0 ? (ky < 0 ? -ky : ky) : ky;
-        const double u1 = fmax(ic_uniform(seed, channel, gx, pky, 0), 1.0e-300);
-        const double u2 = ic_uniform(seed, channel, gx, pky, 1);
-        const double r = sqrt(-2.0 * log(u1)), th = 2.0 * 3.14159265358979323846 * u2;
-        re = sigma * (r * cos(th));
-        im = sigma * (r * sin(th));
-        if (gx == 0 && ky < 0) im = -im;
+    const double2 v = ic_value(s, gx, ky);
+    state[(static_cast<size_t>(b) * P.nfields + field) * fstride + e] = mk(static_cast<T>(v.x), static_cast<T>(v.y));
+    if (k0 && e == 0) *k0 = v;
+}
+
+// block sums of w (|u_x|^2 + |u_y|^2) of the random-vorticity shell over the active modes, w = 2 off the
+// kx = 0 line; partial[blockIdx.x].  grid: ceil(Hx * Ky / 256)
+__global__ void __launch_bounds__(kThreads) vorticity_norm_kernel(const StepPlan P, const IcSpec s, double* __restrict__ partial) {
+    __shared__ double red[kThreads / 32];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (e < P.hx * P.kyn) {
+        const int gx = e / P.kyn, j = e - gx * P.kyn;
+        const int ky = ky_of_j(j, P.nay);
+        const double kx = 2.0 * 3.14159265358979323846 * gx / s.lx, kyv = 2.0 * 3.14159265358979323846 * ky / s.ly;
+        double2 ux, uy;
+        ic_vorticity(s, gx, ky, kx, kyv, kx * kx + kyv * kyv, ux, uy);
+        v = (gx == 0 ? 1.0 : 2.0) * ((ux.x * ux.x + ux.y * ux.y) + (uy.x * uy.x + uy.y * uy.y));
     }
-    state[(static_cast<size_t>(b) * P.nfields + field) * fstride + e] = mk(static_cast<T>(re), static_cast<T>(im));
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) t += red[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// out[0] = sum of n partial sums in a fixed order (deterministic); one block of kThreads
+__global__ void __launch_bounds__(kThreads) sum_partials_kernel(const double* __restrict__ partial, int n, double* __restrict__ out) {
+    __shared__ double red[kThreads];
+    double t = 0.0;
+    for (int i = threadIdx.x; i < n; i += kThreads) t += partial[i];
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = red[0];
+}
+
+// the incompressible check on two momentum specs, in FP64 (initial_condition.cc:7-40): sets *bad when
+// |k . j| > 1e-10 + 1e-10 |k| |j| at an active mode k != 0.  grid: ceil(Hx * Ky / 256)
+__global__ void __launch_bounds__(kThreads) transverse_check_kernel(const StepPlan P, const IcSpec sx, const IcSpec sy, int* __restrict__ bad) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= P.hx * P.kyn) return;
+    const int gx = e / P.kyn, j = e - gx * P.kyn;
+    const int ky = ky_of_j(j, P.nay);
+    const double kx = 2.0 * 3.14159265358979323846 * gx / sx.lx, kyv = 2.0 * 3.14159265358979323846 * ky / sx.ly;
+    const double k2 = kx * kx + kyv * kyv;
+    if (k2 == 0.0) return;
+    const double2 jx = ic_value(sx, gx, ky), jy = ic_value(sy, gx, ky);
+    const double re = kx * jx.x + kyv * jy.x, im = kx * jx.y + kyv * jy.y;
+    const double viol = sqrt(re * re + im * im);
+    const double scale = sqrt(k2) * sqrt((jx.x * jx.x + jx.y * jx.y) + (jy.x * jy.x + jy.y * jy.y));
+    if (viol > 1.0e-10 + 1.0e-10 * scale) atomicOr(bad, 1);
 }
 
 // step counter of the call: set from the host at the start of a call, advanced

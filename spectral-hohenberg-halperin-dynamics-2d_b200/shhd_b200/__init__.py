@@ -88,6 +88,27 @@ class Info(ctypes.Structure):
     ]
 
 
+class InitialField(ctypes.Structure):
+    """Mirror of shhd_initial_field (one device-generated initial field)."""
+    _fields_ = [
+        ("style", ctypes.c_int), ("channel", ctypes.c_int), ("seed", ctypes.c_uint64),
+        ("mean", ctypes.c_double), ("s0", ctypes.c_double), ("c0", ctypes.c_double), ("c2", ctypes.c_double),
+        ("c4", ctypes.c_double), ("amplitude", ctypes.c_double), ("rho0", ctypes.c_double),
+        ("n0", ctypes.c_double), ("sigma", ctypes.c_double), ("x0", ctypes.c_double), ("y0", ctypes.c_double),
+        ("sigma_x", ctypes.c_double), ("sigma_y", ctypes.c_double), ("nkx", ctypes.c_int), ("nky", ctypes.c_int),
+    ]
+
+    @classmethod
+    def of(cls, spec) -> "InitialField":
+        if isinstance(spec, cls):
+            return spec
+        f = cls()
+        for name, _t in cls._fields_:
+            v = spec[name]
+            setattr(f, name, int(v) & 0xFFFFFFFFFFFFFFFF if name == "seed" else v)
+        return f
+
+
 class ShhdError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(message)
@@ -103,6 +124,7 @@ EXPORTED = (
     "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
     "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
     "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums", "shhd_engine_set_gaussian_field",
+    "shhd_engine_set_initial_field", "shhd_engine_check_transverse",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -146,6 +168,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_l2_sums.argtypes = [vp, i, dp, sz]
     d = ctypes.c_double
     lib.shhd_engine_set_gaussian_field.argtypes = [vp, i, i, ctypes.c_uint64, i, d, d, d, d, d]
+    lib.shhd_engine_set_initial_field.argtypes = [vp, i, i, ctypes.POINTER(InitialField)]
+    lib.shhd_engine_check_transverse.argtypes = [vp, ctypes.POINTER(InitialField), ctypes.POINTER(InitialField)]
     return lib
 
 
@@ -281,6 +305,16 @@ class Engine:
         """Write one field on the device: sigma(k) xi_k per active mode, `mean` at k = 0."""
         _check(lib.shhd_engine_set_gaussian_field(self._h, int(member), int(field), int(seed) & 0xFFFFFFFFFFFFFFFF, int(channel),
                                                   float(mean), float(s0), float(c0), float(c2), float(c4)))
+
+    def set_initial_field(self, member: int, field: int, spec) -> None:
+        """Generate one field on the device from an InitialField (or a dict of its fields)."""
+        f = InitialField.of(spec)
+        _check(lib.shhd_engine_set_initial_field(self._h, int(member), int(field), ctypes.byref(f)))
+
+    def check_transverse(self, jx, jy) -> None:
+        """Raise ShhdError unless the two momentum specs are transverse at every active k != 0 (FP64)."""
+        a, b = InitialField.of(jx), InitialField.of(jy)
+        _check(lib.shhd_engine_check_transverse(self._h, ctypes.byref(a), ctypes.byref(b)))
 
     def time_series_l2(self, member: int = 0) -> dict:
         """The reference time-series measure's spectral L2 columns of the current state (FP64)."""

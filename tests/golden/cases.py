@@ -154,3 +154,64 @@ set order_parameter all equilibrium/gaussian seed 5 kBT 1 k0 4 k2 0
 run 2
 """,
 }
+
+
+# Initial-condition-only cases: the state (or the error) the reference's `set`
+# styles produce, recorded without stepping.  They reach every built-in style,
+# the default seed, the `all` targets, last-command-wins and the parse / apply
+# errors.
+def _ic(grid, length, dealias, nop, te, sets, thermo=True):
+    lines = [f"grid {grid[0]} {grid[1]}", f"length {length[0]} {length[1]}", f"dealias {dealias}",
+             f"order_parameters {nop}", "timestep 0.01", f"time_evolution {te}"]
+    if thermo:
+        lines.append("model thermo linear_eos cT 1")
+    if nop:
+        lines.append("model free_energy phi4 " + " ".join(f"a[{i}] -1 b[{i}] 1 u[{i}] 1" for i in range(nop)))
+    lines.append("model transport constant eta 1 zeta 1" + "".join(f" M[{i},{i}] 1" for i in range(nop)))
+    return _HEAD + "\n".join(lines + sets) + "\nrun 1\n"
+
+
+IC_CASES = {
+    "bump_and_sine": _ic((16, 16), (16.0, 12.0), "3/2", 2, "srk3/compressible", [
+        "set density gaussian base 1 amplitude 0.3 x0 3 y0 5 sigma 1.5",
+        "set momentum x sine base 0.02 amplitude 0.1 nkx 2 nky -3",
+        "set momentum y sine base 0 amplitude 0.05 nkx 0 nky -2",
+        "set order_parameter 0 gaussian base 0.1 amplitude -0.2 x0 8 y0 2 sigma_x 2 sigma_y 1",
+        "set order_parameter 1 sine amplitude 0.4 nkx 0 nky 3",
+    ]),
+    "default_seeds_rect": _ic((20, 12), (20.0, 9.0), "two", 1, "euler/compressible", [
+        "set density sine base 1 amplitude 0.5 nkx 3",
+        "set density equilibrium/gaussian kBT 2e-3 rho0 1.2 cT 0.9",
+        "set momentum all equilibrium/gaussian/compressible kBT 1e-3",
+        "set order_parameter all equilibrium/gaussian kBT 0.5 k0 1 k2 1 k4 0.25 psi0 -0.1",
+    ]),
+    "vorticity_on_bump_density": _ic((16, 16), (10.0, 10.0), "3/2", 1, "srk3/incompressible", [
+        "set density gaussian base 1.1 amplitude 0.2 x0 5 y0 5 sigma 2",
+        "set momentum all random_vorticity n0 2.5 sigma 1.2 urms 0.3",
+        "set order_parameter 0 equilibrium/gaussian seed 9 kBT 1 k0 4 k2 0",
+        "set order_parameter 0 uniform value 0.25",
+    ], thermo=False),
+    "incompressible_gaussian_default_seed": _ic((12, 16), (9.0, 12.0), "3/2", 0, "euler/incompressible", [
+        "set density uniform value 0.8",
+        "set momentum all equilibrium/gaussian/incompressible kBT 2e-3",
+    ], thermo=False),
+    "error_sine_density_base": _ic((16, 16), (16.0, 16.0), "3/2", 0, "srk3/compressible", [
+        "set density sine base 0.1 amplitude 0.5 nkx 1",
+    ]),
+    "error_not_transverse": _ic((16, 16), (16.0, 16.0), "3/2", 0, "srk3/incompressible", [
+        "set density uniform value 1",
+        "set momentum all equilibrium/gaussian/compressible kBT 1e-3 seed 2",
+    ], thermo=False),
+    "error_x_replaced_not_transverse": _ic((16, 16), (16.0, 16.0), "3/2", 0, "srk3/incompressible", [
+        "set density uniform value 1",
+        "set momentum all equilibrium/gaussian/incompressible kBT 1e-3 seed 4",
+        "set momentum x uniform value 0.01",
+    ], thermo=False),
+    "error_vorticity_zero_density": _ic((16, 16), (16.0, 16.0), "3/2", 0, "srk3/compressible", [
+        "set momentum x random_vorticity n0 2 sigma 1 urms 0.1 seed 3",
+    ]),
+    "error_order_parameter_coefficient": _ic((16, 16), (16.0, 16.0), "3/2", 1, "srk3/compressible", [
+        "set density uniform value 1",
+        "set order_parameter 0 equilibrium/gaussian seed 1 kBT 1 k0 -1 k2 0",
+    ]),
+}

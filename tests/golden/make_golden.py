@@ -7,7 +7,11 @@ the input script, the initial state the reference's initial-condition styles
 produce, the deterministic RHS at that state, and two steps of the reference
 integrator with the stochastic right-hand sides it drew.
 
-    python tests/golden/make_golden.py      # writes tests/golden/ref_cases.npz
+    python tests/golden/make_golden.py            # writes tests/golden/ref_cases.npz
+    python tests/golden/make_golden.py --initial  # writes tests/golden/ref_initial.npz
+
+The second form records, per initial-condition case, the reference's initial
+state or, where the reference refuses the script, its error message.
 """
 import ctypes
 import os
@@ -18,7 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-from cases import CASES  # noqa: E402
+from cases import CASES, IC_CASES  # noqa: E402
 
 NSTEPS = 2
 
@@ -58,5 +62,30 @@ def main() -> None:
     np.savez_compressed(os.path.join(HERE, "ref_cases.npz"), **out)
 
 
+def main_initial() -> None:
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libshhd_ref.so"))
+    lib.shref_create.restype = ctypes.c_void_p
+    lib.shref_last_error.restype = ctypes.c_char_p
+    out = {}
+    for name, script in IC_CASES.items():
+        h = ctypes.c_void_p(lib.shref_create(script.encode()))
+        if not h.value:
+            out[f"{name}/error"] = np.array(lib.shref_last_error().decode())
+            print(f"{name}: error {out[name + '/error']}")
+            continue
+        info = (ctypes.c_long * 10)()
+        dinfo = (ctypes.c_double * 4)()
+        lib.shref_info(h, info, dinfo)
+        u0 = np.zeros((info[4], info[1], info[0] // 2 + 1), complex)
+        lib.shref_get_state(h, u0.ctypes.data_as(ctypes.c_void_p))
+        lib.shref_destroy(h)
+        out[f"{name}/u0"] = u0
+        print(f"{name}: shape {u0.shape}, |u0| {np.abs(u0).max():.3g}")
+    np.savez_compressed(os.path.join(HERE, "ref_initial.npz"), **out)
+
+
 if __name__ == "__main__":
-    main()
+    if "--initial" in sys.argv[1:]:
+        main_initial()
+    else:
+        main()

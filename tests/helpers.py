@@ -18,6 +18,21 @@ def load_golden():
     return out
 
 
+GOLDEN_INITIAL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_initial.npz")
+
+
+def load_initial_golden():
+    """Initial-condition cases: script, and the reference's initial state or its error message."""
+    from golden.cases import IC_CASES
+    data = np.load(GOLDEN_INITIAL)
+    out = {}
+    for name, script in IC_CASES.items():
+        err = f"{name}/error"
+        out[name] = dict(script=script, u0=None if err in data else data[f"{name}/u0"],
+                         error=str(data[err]) if err in data else None)
+    return out
+
+
 def random_state(cfg: so.Config, seed: int, amp: float = 0.05, rho0: float = 1.0, transverse: bool = False) -> np.ndarray:
     """A valid spectral state: active modes only, Hermitian kx = 0 line, smooth spectrum.
 
