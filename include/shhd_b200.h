@@ -274,6 +274,17 @@ int shhd_engine_check_transverse(shhd_engine* engine, const shhd_initial_field* 
 int shhd_engine_set_gaussian_field(shhd_engine* engine, int member, int field, uint64_t seed, int channel, double mean, double s0,
                                    double c0, double c2, double c4);
 
+/* Energy columns of the time-series measure (measure_time_series.cc:152-188,
+ * 305-470) for one member, FP64 sums: out[0..3] = E_T, E_K, E_psi, E_C.
+ * E_K: compressible, the sum over the padded grid of (jx^2 + jy^2) / (2 rho) dA
+ * from the inverse-transformed fields; incompressible, cell / (2 Ng rho0) times
+ * the weighted spectral sum of |j|^2; quiescent, 0.  E_C: compressible,
+ * cT^2 cell / (2 Ng rho0) times the weighted sum of |rho|^2 over k != 0.  E_psi:
+ * the quadratic chemical-potential terms spectrally, plus u psi^4 / 4 dA over
+ * the padded grid for phi4.  The physical-space sums use their own transforms
+ * (allocated on first use). */
+int shhd_engine_energies(shhd_engine* engine, int member, double* out, size_t n);
+
 /* Spectral L2 columns of the time-series measure (measure_time_series.cc:
  * |rho|^2, |d_rho|^2, |j|^2, |d_j|^2, |psi[a]|^2, |d_psi[a]|^2) for one member
  * of the current state, in FP64 on the device: out[2 f] = (V / Np^2) / Np^2

@@ -13,12 +13,18 @@
  * FCalculator + TimeIntegrator pair FluidSolver wires (fluid_solver.h:37-99).
  * The one addition is that the RHSOperators it binds copy each psi_sto /
  * j_sto output aside, so the noise the reference drew can be replayed.
+ * The script's `measure` commands run through the reference's own
+ * MeasurementManager after every step of shref_step, with the integrator's
+ * flux buffer, as Project::run_steps does (project.h:127-143);
+ * shref_finalize closes their files.
  */
 #include "domain.h"
 #include "fcalculator.h"
 #include "fcalculator_dynamics_mode.h"
 #include "initial_condition.h"
+#include "fourier_transform.h"
 #include "initial_condition_registry_builtin.h"
+#include "measure_manager.h"
 #include "measure_registry_builtin.h"
 #include "model_free_energy_null.h"
 #include "model_free_energy_registry_builtin.h"
@@ -62,6 +68,10 @@ struct RefRun {
     std::unique_ptr<FCalculator> fcalc;
     std::unique_ptr<TimeIntegrator> integrator;
     RHSOperators rhs;
+    // measures of the script (absent when it has none)
+    std::unique_ptr<MeasureRegistry> measure_registry;
+    std::unique_ptr<FourierTransform2D> fft;
+    std::unique_ptr<MeasurementManager> measures;
     bool srk3 = true;
     double time = 0.0;
     long step = 0;
@@ -145,6 +155,18 @@ void build(RefRun& r) {
 
     r.fcalc = std::make_unique<FCalculator>(r.params, *r.domain, *r.mask, *r.thermo, *r.free_energy, *r.transport);
     r.integrator = make_integrator(r.params, *r.domain, *r.mask, r.srk3);
+
+    bool any_measure = false;
+    for (const auto& c : r.params.commands) any_measure |= c.type == Command::Type::Measure;
+    if (any_measure) {
+        r.measure_registry = std::make_unique<MeasureRegistry>(build_measure_registry());
+        r.fft = std::make_unique<FourierTransform2D>(*r.domain);
+        r.measures = std::make_unique<MeasurementManager>(r.params, *r.domain, *r.measure_registry, *r.thermo, *r.free_energy,
+                                                          *r.transport);
+        for (const auto& c : r.params.commands)
+            if (c.type == Command::Type::Measure) r.measures->apply_measure_command(c.measure);
+        r.integrator->set_flux_request(r.measures->flux_request());
+    }
 
     const std::size_t nspec = r.domain->spectral_size();
     const int nfields = r.params.physics.num_order_parameters + 3;
@@ -264,8 +286,18 @@ int shref_step(void* h, int nsteps, double* noise_out) {
             r->integrator->step(*r->state, r->time, r->rhs);
             ++r->step;
             r->time += r->params.runtime.dt;
+            if (r->measures)
+                r->measures->observe(*r->state, *r->fft, r->integrator->flux_buffer(), static_cast<int>(r->step), r->time);
             if (noise_out) std::memcpy(noise_out + 2 * per_step * s, r->noise.data(), per_step * sizeof(Complex));
         }
+    });
+}
+
+/* Close the files of the script's measures (MeasurementManager::finalize). */
+int shref_finalize(void* h) {
+    RefRun* r = static_cast<RefRun*>(h);
+    return guarded([&] {
+        if (r->measures) r->measures->finalize();
     });
 }
 

@@ -774,6 +774,55 @@ def time_series_l2(cfg: Config, state: np.ndarray) -> Dict[str, float]:
     return out
 
 
+def time_series_energies(cfg: Config, state: np.ndarray) -> Dict[str, float]:
+    """Energy columns of TimeSeriesMeasure (measure_time_series.cc:152-188, 305-470):
+
+    E_K   compressible: sum over the padded grid of (jx^2 + jy^2) / (2 rho) dA (physical fields);
+          incompressible: cell / (2 Ng rho0) sum over active modes of w (|jx|^2 + |jy|^2); quiescent: 0
+    E_C   compressible with cT^2 != 0: cT^2 cell / (2 Ng rho0) sum over active modes but (0, 0) of w |rho|^2
+    E_psi per order parameter cell / (2 Ng) sum over active modes of w (k0 + k2 k^2 + k4 k^4) |psi|^2,
+          plus, for phi4 with some u != 0, sum over the padded grid of u psi^4 / 4 dA
+    E_T   E_K + E_psi + E_C
+    with w = 2 off the kx = 0 line, rho0 = Re rho(0) / Ng, dA = cell = V / Ng.
+    """
+    g = Geometry(cfg)
+    n = cfg.num_order_parameters
+    w = np.where(g.gx == 0, 1.0, 2.0)
+    act = g.active
+    cell = g.volume / g.grid_size
+    rho0 = state[0, 0, 0].real / g.grid_size
+    mode = cfg.mode
+    kin = 0.0
+    if mode == "compressible":
+        rho, jx, jy = g.backward(state[0]), g.backward(state[n + 1]), g.backward(state[n + 2])
+        kin = float(np.sum(0.5 * (jx * jx + jy * jy) / rho * cell))
+    elif mode == "incompressible":
+        kin = 0.5 * cell / (g.grid_size * rho0) * float(np.sum(np.where(act, w * (np.abs(state[n + 1]) ** 2 + np.abs(state[n + 2]) ** 2), 0.0)))
+    comp = 0.0
+    if mode == "compressible" and cfg.cT * cfg.cT != 0.0:
+        use = act & ~((g.gx == 0) & (g.sgy == 0))
+        comp = 0.5 * cfg.cT * cfg.cT * cell / (g.grid_size * rho0) * float(np.sum(np.where(use, w * np.abs(state[0]) ** 2, 0.0)))
+    free = 0.0
+    for a in range(n):
+        if cfg.free_energy == "phi4":
+            k0, k2c, k4 = cfg.phi4_a[a], cfg.phi4_b[a], 0.0
+        elif cfg.free_energy == "quadratic":
+            k0, k2c, k4 = cfg.quad_a[a], 0.0, 0.0
+        else:
+            k0 = k2c = k4 = 0.0
+        if k0 == 0.0 and k2c == 0.0 and k4 == 0.0:
+            continue
+        coef = k0 + k2c * g.k2 + k4 * g.k2 * g.k2
+        free += 0.5 * cell / g.grid_size * float(np.sum(np.where(act, w * coef * np.abs(state[1 + a]) ** 2, 0.0)))
+    if cfg.free_energy == "phi4" and any(u != 0.0 for u in cfg.phi4_u):
+        dens = np.zeros((g.ny, g.nx))
+        for a in range(n):
+            p = g.backward(state[1 + a])
+            dens += 0.25 * cfg.phi4_u[a] * p ** 4
+        free += float(np.sum(dens * cell))
+    return {"E_T": kin + free + comp, "E_K": kin, "E_psi": free, "E_C": comp}
+
+
 def green_kubo_modes(cfg: Config, selection: str = "diagonal") -> List[Tuple[int, int]]:
     """Wave numbers (nx, ny) of measure_yokota_green_kubo.cc:42-96."""
     max_nx = max(0, cfg.active[0] // 2 - 1)

@@ -168,6 +168,20 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 // ---------------------------------------------------------------------------
 // engine
 // ---------------------------------------------------------------------------
+// Transforms of the physical-space measures: runtime-plan column and row transforms of one member,
+// independent of the step's kernel family, with their own twiddle tables and scratch (built on first use).
+struct MeasurePlan {
+    bool ready = false;
+    StepPlan P{};                 // geometry, physics and transforms; inputs are set per term
+    void* tw_x = nullptr;
+    void* tw_y = nullptr;
+    void* i1 = nullptr;           // up to 3 x-spectral planes of one member
+    void* member = nullptr;       // one always-active MemberInfo
+    double* scratch = nullptr;    // partial sums, then the summed values
+    size_t scratch_doubles = 0;
+    size_t smem_col = 0, smem_row = 0;
+};
+
 struct shhd_engine {
     shhd_config cfg{};
     StepPlan P{};
@@ -228,6 +242,7 @@ struct shhd_engine {
 
     void* ref_stage = nullptr;       // one member's reference-layout state (FP64) on the device
     int* flag_dev = nullptr;
+    MeasurePlan meas;
     double* ic_scratch = nullptr;    // random-vorticity norm [0] and block partial sums [1..]
     size_t ic_scratch_bytes = 0;
     unsigned long long* step_dev = nullptr;  // step index at the start of the current call
@@ -272,7 +287,8 @@ void free_engine(shhd_engine* e) {
     for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->ref_stage,
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
                     static_cast<void*>(e->members_dev),
-                    static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch)})
+                    static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch), e->meas.tw_x, e->meas.tw_y, e->meas.i1,
+                    e->meas.member, static_cast<void*>(e->meas.scratch)})
         if (p) cudaFree(p);
     for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
     e->graphs.clear();
@@ -866,6 +882,12 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
     check_cuda(cudaGetLastError(), "col_forward launch");
 }
 
+// the run's time, advanced one dt per step as the reference's driver does (project.h:134-136),
+// so that printed times match its measures digit for digit
+void advance_time(shhd_engine* e, int64_t steps) {
+    for (int64_t s = 0; s < steps; ++s) e->time += e->cfg.dt;
+}
+
 void upload_members(shhd_engine* e) {
     if (!e->members_dirty) return;
     check_cuda(cudaMemcpyAsync(e->members_dev, e->members.data(), sizeof(MemberInfo) * e->members.size(), cudaMemcpyHostToDevice, e->stream),
@@ -1051,13 +1073,13 @@ void enqueue_steps(shhd_engine* e, int nsteps) {
             }
         }
         e->step_index += done;
-        e->time += done * e->cfg.dt;
+        advance_time(e, done);
         if (done < nsteps) set_step_dev(e);
     }
     if (done < nsteps) {
         record_steps<T>(e, nsteps - done);
         e->step_index += nsteps - done;
-        e->time += (nsteps - done) * e->cfg.dt;
+        advance_time(e, nsteps - done);
     }
 }
 
@@ -1665,7 +1687,7 @@ IcSpec resolve_initial_field(shhd_engine* e, const shhd_initial_field& in) {
         }
         vorticity_norm_kernel<<<nblk, kThreads, 0, e->stream>>>(P, s, e->ic_scratch + 1);
         check_cuda(cudaGetLastError(), "vorticity_norm launch");
-        sum_partials_kernel<<<1, kThreads, 0, e->stream>>>(e->ic_scratch + 1, nblk, e->ic_scratch);
+        sum_partials_kernel<<<1, kThreads, 0, e->stream>>>(e->ic_scratch + 1, nblk, 1, e->ic_scratch);
         check_cuda(cudaGetLastError(), "sum_partials launch");
         double norm = 0.0;
         check_cuda(cudaMemcpyAsync(&norm, e->ic_scratch, sizeof(double), cudaMemcpyDeviceToHost, e->stream), "norm read");
@@ -1736,6 +1758,162 @@ int shhd_engine_set_gaussian_field(shhd_engine* e, int member, int field, uint64
     spec.mean = mean;
     spec.s0 = s0; spec.c0 = c0; spec.c2 = c2; spec.c4 = c4;
     return shhd_engine_set_initial_field(e, member, field, &spec);
+}
+
+}  // extern "C"
+
+namespace {
+
+// the measure plan: the step plan's geometry and physics with runtime-plan transforms
+template <typename T>
+void build_measure_plan(shhd_engine* e) {
+    MeasurePlan& M = e->meas;
+    if (M.ready) return;
+    const shhd_config& c = e->cfg;
+    const size_t cs = sizeof(cplx<T>);
+    const size_t smem_cap = 227 * 1024;
+    StepPlan P = e->P;
+    P.batch = 1;
+    P.n_out = 0;
+    P.n_groups = 0;
+    P.fy = make_fft_plan(c.ny);
+    P.fx = make_fft_plan(c.nx);
+    P.twy_count = kTwLo + P.fy.tw_hi_count;
+    P.twx_count = kTwLo + P.fx.tw_hi_count;
+    auto col_bytes = [&](int w) { return static_cast<size_t>(P.twy_count + 2L * w * c.ny) * cs; };
+    int W = 8;
+    while (W > 1 && (P.hx % W != 0 || col_bytes(W) > 100 * 1024)) W /= 2;
+    if (col_bytes(W) > smem_cap) throw Failure(SHHD_EUNSUPPORTED, "energy measure: compute grid too large for the column transform");
+    P.W = W;
+    P.logw = W == 8 ? 3 : (W == 4 ? 2 : (W == 2 ? 1 : 0));
+    P.ntiles = P.hx / W;
+    P.fy.swz = swizzle_mask(c.ny, e->fp32 ? 16 : 8, W);
+    P.fx.swz = swizzle_mask(c.nx, e->fp32 ? 16 : 8, 1);
+    P.div_w = make_fastdiv(W);
+    P.div_kyn = make_fastdiv(P.kyn);
+    P.div_npy = make_fastdiv(c.ny);
+    P.div_hx = make_fastdiv(P.hx);
+    // row pass: at most 3 input lines and row_lb ping-pong lines
+    const size_t line = static_cast<size_t>(c.nx) * cs;
+    auto row_bytes = [&](int lb) { return static_cast<size_t>(P.twx_count) * cs + (3 + lb) * line; };
+    int lb = 3;
+    while (lb > 1 && row_bytes(lb) > 113 * 1024) --lb;
+    if (row_bytes(lb) > smem_cap) throw Failure(SHHD_EUNSUPPORTED, "energy measure: compute grid too large for the row transform");
+    P.row_lb = lb;
+    P.row_nb = lb;
+    M.P = P;
+    M.smem_col = col_bytes(W);
+    M.smem_row = row_bytes(lb);
+    const auto twx = twiddle_table<T>(c.nx), twy = twiddle_table<T>(c.ny);
+    M.tw_x = dalloc(e, twx.size() * cs);
+    M.tw_y = dalloc(e, twy.size() * cs);
+    check_cuda(cudaMemcpyAsync(M.tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    check_cuda(cudaMemcpyAsync(M.tw_y, twy.data(), twy.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    M.i1 = dalloc(e, 3 * static_cast<size_t>(P.hx) * c.ny * cs);
+    MemberInfo mi{};
+    mi.active = 1;
+    M.member = dalloc(e, sizeof(MemberInfo));
+    check_cuda(cudaMemcpyAsync(M.member, &mi, sizeof(MemberInfo), cudaMemcpyHostToDevice, e->stream), "member upload");
+    const size_t nblk = (static_cast<size_t>(P.hx) * P.kyn + kThreads - 1) / kThreads;
+    M.scratch_doubles = std::max(nblk * (2 + kMaxOp), static_cast<size_t>(c.ny / 2 + 1)) + 8 + kMaxOp;
+    M.scratch = static_cast<double*>(dalloc(e, M.scratch_doubles * sizeof(double)));
+    raise_smem_limit(reinterpret_cast<const void*>(col_inverse_kernel<T, 0>), M.smem_col);
+    raise_smem_limit(reinterpret_cast<const void*>(energy_row_kernel<T>), M.smem_row);
+    check_cuda(cudaStreamSynchronize(e->stream), "measure plan");
+    M.ready = true;
+}
+
+// sum over the padded grid of one physical-space energy density (term 0 kinetic, 1 psi^4 of field f)
+template <typename T>
+double physical_energy_sum(shhd_engine* e, const cplx<T>* st, int term, int field) {
+    MeasurePlan& M = e->meas;
+    StepPlan P = M.P;
+    if (term == 0) {
+        P.n_in = 3;
+        P.in_field[0] = 0;
+        P.in_field[1] = P.nop + 1;
+        P.in_field[2] = P.nop + 2;
+    } else {
+        P.n_in = 1;
+        P.in_field[0] = field;
+    }
+    auto* i1 = static_cast<cplx<T>*>(M.i1);
+    col_inverse_kernel<T, 0><<<dim3(P.ntiles, P.n_in, 1), kThreads, M.smem_col, e->stream>>>(
+        P, static_cast<const MemberInfo*>(M.member), st, i1, static_cast<const cplx<T>*>(M.tw_y));
+    check_cuda(cudaGetLastError(), "measure col_inverse launch");
+    const int pairs = (P.npy + 1) / 2;
+    energy_row_kernel<T><<<pairs, kThreads, M.smem_row, e->stream>>>(P, i1, static_cast<const cplx<T>*>(M.tw_x), term, M.scratch);
+    check_cuda(cudaGetLastError(), "energy_row launch");
+    double* out = M.scratch + M.scratch_doubles - 1;
+    sum_partials_kernel<<<1, kThreads, 0, e->stream>>>(M.scratch, pairs, 1, out);
+    check_cuda(cudaGetLastError(), "sum_partials launch");
+    double v = 0.0;
+    check_cuda(cudaMemcpyAsync(&v, out, sizeof(double), cudaMemcpyDeviceToHost, e->stream), "energy read");
+    check_cuda(cudaStreamSynchronize(e->stream), "energy sync");
+    return v;
+}
+
+// E_T, E_K, E_psi, E_C of one member (measure_time_series.cc:152-188, 305-470)
+template <typename T>
+void energies(shhd_engine* e, int member, double* out) {
+    build_measure_plan<T>(e);
+    MeasurePlan& M = e->meas;
+    const StepPlan& P = e->P;
+    const shhd_config& c = e->cfg;
+    const int nop = P.nop;
+    const double ng = static_cast<double>(c.nx) * c.ny, cell = c.lx * c.ly / ng;
+    const auto* st = static_cast<const cplx<T>*>(e->u) + static_cast<size_t>(member) * e->state_elems;
+    const double2* k0 = e->k0_u ? e->k0_u + static_cast<size_t>(member) * P.nfields : nullptr;
+    // spectral sums
+    const int nv = 2 + nop;
+    const int nblk = static_cast<int>((static_cast<size_t>(P.hx) * P.kyn + kThreads - 1) / kThreads);
+    double* sums = M.scratch + M.scratch_doubles - 1 - nv;
+    energy_spectral_kernel<T><<<nblk, kThreads, 0, e->stream>>>(P, st, k0, M.scratch);
+    check_cuda(cudaGetLastError(), "energy_spectral launch");
+    sum_partials_kernel<<<nv, kThreads, 0, e->stream>>>(M.scratch, nblk, nv, sums);
+    check_cuda(cudaGetLastError(), "sum_partials launch");
+    std::vector<double> v(nv);
+    check_cuda(cudaMemcpyAsync(v.data(), sums, sizeof(double) * nv, cudaMemcpyDeviceToHost, e->stream), "energy read");
+    double2 rho00{};
+    const void* src = k0 ? static_cast<const void*>(k0) : static_cast<const void*>(st);
+    if (k0 || !e->fp32) {
+        check_cuda(cudaMemcpyAsync(&rho00, src, sizeof(double2), cudaMemcpyDeviceToHost, e->stream), "rho(0) read");
+    } else {
+        float2 r{};
+        check_cuda(cudaMemcpyAsync(&r, src, sizeof(float2), cudaMemcpyDeviceToHost, e->stream), "rho(0) read");
+        check_cuda(cudaStreamSynchronize(e->stream), "energy sync");
+        rho00.x = r.x;
+    }
+    check_cuda(cudaStreamSynchronize(e->stream), "energy sync");
+    const double rho0 = rho00.x / ng;
+    const bool comp = c.mode == SHHD_COMPRESSIBLE, incomp = c.mode == SHHD_INCOMPRESSIBLE;
+    double kin = 0.0, free_e = 0.0, compress = 0.0;
+    if (comp) kin = physical_energy_sum<T>(e, st, 0, 0) * cell;
+    else if (incomp) kin = 0.5 * cell / (ng * rho0) * v[0];
+    if (comp && P.cT2 != 0.0) compress = 0.5 * P.cT2 * cell / (ng * rho0) * v[1];
+    for (int a = 0; a < nop; ++a)
+        if (P.mu_k0[a] != 0.0 || P.mu_k2[a] != 0.0 || P.mu_k4[a] != 0.0) free_e += 0.5 * cell / ng * v[2 + a];
+    for (int a = 0; a < nop; ++a)
+        if (P.mu_u3[a] != 0.0) free_e += 0.25 * P.mu_u3[a] * physical_energy_sum<T>(e, st, 1, 1 + a) * cell;
+    out[0] = kin + free_e + compress;
+    out[1] = kin;
+    out[2] = free_e;
+    out[3] = compress;
+}
+
+}  // namespace
+
+extern "C" {
+
+int shhd_engine_energies(shhd_engine* e, int member, double* out, size_t n) {
+    return guarded([&] {
+        if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (n < 4) throw Failure(SHHD_EINVAL, "energies need 4 doubles");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) energies<float>(e, member, out);
+        else energies<double>(e, member, out);
+    });
 }
 
 int shhd_engine_l2_sums(shhd_engine* e, int member, double* out, size_t n) {

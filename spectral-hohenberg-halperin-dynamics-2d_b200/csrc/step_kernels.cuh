@@ -200,6 +200,41 @@ __device__ __forceinline__ T product_value(const StepPlan& P, int kind, int arg,
     }
 }
 
+// row-pass inputs: rows y0, y0 + 1 of the P.n_in x-spectral planes of one member (i1_member),
+// packed as Z[k] = X0[k] + i X1[k] with the Hermitian mirror, zero outside |kx| < Na/2, and
+// inverse transformed in place into `lines` (P.row_lb lines at a time through `scr`); the
+// physical rows come back as (row y0, row y0 + 1) in the real and imaginary parts
+template <typename T, int FX>
+__device__ __forceinline__ void row_inputs_inverse(const StepPlan& P, const cplx<T>* __restrict__ i1_member, int y0, bool has1,
+                                                   cplx<T>* lines, cplx<T>* scr, const cplx<T>* s_tw) {
+    using C = cplx<T>;
+    const int npx = P.npx, npy = P.npy, W = P.W, hx = P.hx;
+    const uint32_t mask = P.fx.swz;
+    for (int s0 = 0; s0 < P.n_in; s0 += P.row_lb) {
+        const int nl = min(P.row_lb, P.n_in - s0);
+        C* in = xform_input<FX>(lines + static_cast<size_t>(s0) * npx, scr, P.fx);
+        for (int l = 0; l < nl; ++l) {
+            C* z = in + static_cast<size_t>(l) * npx;
+            const C* src = i1_member + static_cast<size_t>(s0 + l) * P.ntiles * npy * W;
+            for (int k = threadIdx.x; k < npx; k += blockDim.x) {
+                if (k < hx) {
+                    const int t = fdiv(k, P.div_w), w = k - t * W;
+                    const C* p0 = src + (static_cast<size_t>(t) * npy + y0) * W + w;
+                    C a = p0[0];
+                    C c = has1 ? p0[W] : czero<C>();
+                    if (k == 0) { a.y = 0; c.y = 0; }  // C2R uses the real part of the kx = 0 entry
+                    z[sw(k, mask)] = mk(a.x - c.y, a.y + c.x);
+                    if (k > 0) z[sw(npx - k, mask)] = mk(a.x + c.y, c.x - a.y);
+                } else if (k <= npx - hx) {
+                    z[sw(k, mask)] = czero<C>();
+                }
+            }
+        }
+        __syncthreads();
+        xform<FX, +1, false>(lines + static_cast<size_t>(s0) * npx, scr, P.fx, nl, P.div_w, npx, 1, 0, s_tw);
+    }
+}
+
 template <typename T, int FX>
 __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, const MemberInfo* __restrict__ members,
                                                             const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
@@ -221,32 +256,8 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
     load_table(s_tw, tw, P.twx_count);
     __syncthreads();
 
-    // 1. inputs, lb lines at a time: Z[k] = X0[k] + i X1[k] with the Hermitian
-    //    mirror (rows y0, y0+1), zero outside |kx| < Na/2; inverse transform
-    const size_t i1_member = static_cast<size_t>(b) * P.n_in * P.ntiles * npy * W;
-    for (int s0 = 0; s0 < P.n_in; s0 += P.row_lb) {
-        const int nl = min(P.row_lb, P.n_in - s0);
-        C* in = xform_input<FX>(lines + static_cast<size_t>(s0) * npx, scr, P.fx);
-        for (int l = 0; l < nl; ++l) {
-            C* z = in + static_cast<size_t>(l) * npx;
-            const C* src = i1 + i1_member + static_cast<size_t>(s0 + l) * P.ntiles * npy * W;
-            for (int k = threadIdx.x; k < npx; k += blockDim.x) {
-                if (k < hx) {
-                    const int t = fdiv(k, P.div_w), w = k - t * W;
-                    const C* p0 = src + (static_cast<size_t>(t) * npy + y0) * W + w;
-                    C a = p0[0];
-                    C c = has1 ? p0[W] : czero<C>();
-                    if (k == 0) { a.y = 0; c.y = 0; }  // C2R uses the real part of the kx = 0 entry
-                    z[sw(k, mask)] = mk(a.x - c.y, a.y + c.x);
-                    if (k > 0) z[sw(npx - k, mask)] = mk(a.x + c.y, c.x - a.y);
-                } else if (k <= npx - hx) {
-                    z[sw(k, mask)] = czero<C>();
-                }
-            }
-        }
-        __syncthreads();
-        xform<FX, +1, false>(lines + static_cast<size_t>(s0) * npx, scr, P.fx, nl, P.div_w, npx, 1, 0, s_tw);
-    }
+    // 1. inputs: rows y0, y0 + 1 of every input, inverse transformed
+    row_inputs_inverse<T, FX>(P, i1 + static_cast<size_t>(b) * P.n_in * P.ntiles * npy * W, y0, has1, lines, scr, s_tw);
 
     // 2. velocity: v = j / rho (compressible) or j / rho0 (fcalculator_workspace.cc:115-142),
     //    formed where a product needs it; the zero-density check runs once per row pair.
@@ -1073,18 +1084,19 @@ __global__ void __launch_bounds__(kThreads) vorticity_norm_kernel(const StepPlan
     }
 }
 
-// out[0] = sum of n partial sums in a fixed order (deterministic); one block of kThreads
-__global__ void __launch_bounds__(kThreads) sum_partials_kernel(const double* __restrict__ partial, int n, double* __restrict__ out) {
+// out[v] = sum over i < n of partial[i * nv + v] in a fixed order (deterministic); grid: nv blocks of kThreads
+__global__ void __launch_bounds__(kThreads) sum_partials_kernel(const double* __restrict__ partial, int n, int nv, double* __restrict__ out) {
     __shared__ double red[kThreads];
+    const int v = blockIdx.x;
     double t = 0.0;
-    for (int i = threadIdx.x; i < n; i += kThreads) t += partial[i];
+    for (int i = threadIdx.x; i < n; i += kThreads) t += partial[static_cast<size_t>(i) * nv + v];
     red[threadIdx.x] = t;
     __syncthreads();
     for (int w = kThreads / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[0] = red[0];
+    if (threadIdx.x == 0) out[v] = red[0];
 }
 
 // the incompressible check on two momentum specs, in FP64 (initial_condition.cc:7-40): sets *bad when
@@ -1102,6 +1114,94 @@ __global__ void __launch_bounds__(kThreads) transverse_check_kernel(const StepPl
     const double viol = sqrt(re * re + im * im);
     const double scale = sqrt(k2) * sqrt((jx.x * jx.x + jx.y * jx.y) + (jy.x * jy.x + jy.y * jy.y));
     if (viol > 1.0e-10 + 1.0e-10 * scale) atomicOr(bad, 1);
+}
+
+// ---------------------------------------------------------------------------
+// time-series energies (measure_time_series.cc:152-188, 305-470), FP64 sums
+// ---------------------------------------------------------------------------
+// spectral terms of one member, per block: [0] w (|jx|^2 + |jy|^2) over every active mode,
+// [1] w |rho|^2 over the active modes but (0, 0), [2 + a] w (k0 + k2 k^2 + k4 k^4) |psi_a|^2 over
+// every active mode; w = 2 off the kx = 0 line.  The (0, 0) values come from k0 (FP64) when given.
+// partial[block][2 + nop]; grid: ceil(Hx * Ky / 256)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) energy_spectral_kernel(const StepPlan P, const cplx<T>* __restrict__ state,
+                                                                   const double2* __restrict__ k0, double* __restrict__ partial) {
+    __shared__ double red[kThreads / 32][2 + kMaxOp];
+    const int nv = 2 + P.nop;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
+    double acc[2 + kMaxOp];
+    for (int q = 0; q < 2 + kMaxOp; ++q) acc[q] = 0.0;
+    if (e < static_cast<int>(fstride)) {
+        const int gx = e / P.kyn, j = e - gx * P.kyn;
+        const int ky = ky_of_j(j, P.nay);
+        const bool zero = gx == 0 && ky == 0;
+        const double w = gx == 0 ? 1.0 : 2.0;
+        const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky;
+        const double k2 = kx * kx + kyv * kyv;
+        auto norm2 = [&](int f) {
+            if (zero && k0) return k0[f].x * k0[f].x + k0[f].y * k0[f].y;
+            const cplx<T> v = state[static_cast<size_t>(f) * fstride + e];
+            return static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y;
+        };
+        acc[0] = w * (norm2(P.nop + 1) + norm2(P.nop + 2));
+        if (!zero) acc[1] = w * norm2(0);
+        for (int a = 0; a < P.nop; ++a) acc[2 + a] = w * (P.mu_k0[a] + P.mu_k2[a] * k2 + P.mu_k4[a] * k2 * k2) * norm2(1 + a);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int q = 0; q < nv; ++q) {
+        double v = acc[q];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double v = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) v += red[w][threadIdx.x];
+        partial[static_cast<size_t>(blockIdx.x) * nv + threadIdx.x] = v;
+    }
+}
+
+// physical-space terms over one row pair of a single-member plan's inputs (runtime-plan transforms):
+// term 0: (jx^2 + jy^2) / (2 rho) with inputs rho, jx, jy; term 1: psi^4 with input psi (the host
+// scales by u / 4).  partial[pair]; grid: ceil(npy / 2)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) energy_row_kernel(const StepPlan P, const cplx<T>* __restrict__ i1, const cplx<T>* __restrict__ tw,
+                                                              int term, double* __restrict__ partial) {
+    using C = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[kThreads / 32];
+    C* s_tw = reinterpret_cast<C*>(smem_raw);
+    const int npx = P.npx;
+    C* lines = s_tw + P.twx_count;
+    C* scr = lines + static_cast<size_t>(P.n_in) * npx;
+    const int y0 = 2 * blockIdx.x;
+    const bool has1 = (y0 + 1) < P.npy;
+    load_table(s_tw, tw, P.twx_count);
+    __syncthreads();
+    row_inputs_inverse<T, 0>(P, i1, y0, has1, lines, scr, s_tw);
+    __syncthreads();
+    double acc = 0.0;
+    for (int x = threadIdx.x; x < npx; x += blockDim.x) {
+        if (term == 0) {
+            const C rho = lines[x], jx = lines[npx + x], jy = lines[2 * npx + x];
+            acc += 0.5 * (static_cast<double>(jx.x) * jx.x + static_cast<double>(jy.x) * jy.x) / static_cast<double>(rho.x);
+            if (has1) acc += 0.5 * (static_cast<double>(jx.y) * jx.y + static_cast<double>(jy.y) * jy.y) / static_cast<double>(rho.y);
+        } else {
+            const C p = lines[x];
+            const double a = static_cast<double>(p.x) * p.x, b = static_cast<double>(p.y) * p.y;
+            acc += a * a;
+            if (has1) acc += b * b;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) t += red[w];
+        partial[blockIdx.x] = t;
+    }
 }
 
 // step counter of the call: set from the host at the start of a call, advanced

@@ -124,7 +124,7 @@ EXPORTED = (
     "shhd_engine_reset_stats", "shhd_engine_set_member", "shhd_rhs_noalloc", "shhd_engine_set_graph_chunk",
     "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
     "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums", "shhd_engine_set_gaussian_field",
-    "shhd_engine_set_initial_field", "shhd_engine_check_transverse",
+    "shhd_engine_set_initial_field", "shhd_engine_check_transverse", "shhd_engine_energies",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -170,6 +170,7 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_set_gaussian_field.argtypes = [vp, i, i, ctypes.c_uint64, i, d, d, d, d, d]
     lib.shhd_engine_set_initial_field.argtypes = [vp, i, i, ctypes.POINTER(InitialField)]
     lib.shhd_engine_check_transverse.argtypes = [vp, ctypes.POINTER(InitialField), ctypes.POINTER(InitialField)]
+    lib.shhd_engine_energies.argtypes = [vp, i, dp, sz]
     return lib
 
 
@@ -315,6 +316,12 @@ class Engine:
         """Raise ShhdError unless the two momentum specs are transverse at every active k != 0 (FP64)."""
         a, b = InitialField.of(jx), InitialField.of(jy)
         _check(lib.shhd_engine_check_transverse(self._h, ctypes.byref(a), ctypes.byref(b)))
+
+    def time_series_energies(self, member: int = 0) -> dict:
+        """The reference time-series measure's energy columns of the current state (FP64 sums)."""
+        raw = np.zeros(4, dtype=np.float64)
+        _check(lib.shhd_engine_energies(self._h, int(member), _dptr(raw), raw.size))
+        return {"E_T": float(raw[0]), "E_K": float(raw[1]), "E_psi": float(raw[2]), "E_C": float(raw[3])}
 
     def time_series_l2(self, member: int = 0) -> dict:
         """The reference time-series measure's spectral L2 columns of the current state (FP64)."""

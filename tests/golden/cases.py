@@ -215,3 +215,30 @@ IC_CASES = {
         "set order_parameter 0 equilibrium/gaussian seed 1 kBT 1 k0 -1 k2 0",
     ]),
 }
+
+
+# Measure cases: a step case with the reference's own measures appended; the
+# fixtures hold the state after every step and the text of every file the
+# measures wrote (@DIR@ is replaced by a scratch directory when they are made).
+_TS_ALL = "E_T E_K E_psi E_C pi_xx pi_xy pi_yy |rho|^2 |d_rho|^2 |j|^2 |d_j|^2"
+
+
+def _measured(name, extra_targets, nsteps=3):
+    body = CASES[name].rsplit("run ", 1)[0]
+    return body + "\n".join([
+        f"measure ts time_series on nevery 1 file @DIR@/ts.dat target {_TS_ALL} {extra_targets}".rstrip(),
+        "measure sp snapshot on nevery 3 file @DIR@/phys space physical",
+        "measure ss snapshot on nevery 3 file @DIR@/spec space spectral",
+        f"run {nsteps}",
+    ]) + "\n"
+
+
+MEASURE_CASES = {
+    "srk3_compressible_n2": _measured("srk3_compressible_n2",
+                                      "|psi[0]|^2 |d_psi[0]|^2 |psi[1]|^2 |d_psi[1]|^2 Jpsi[0]_x Jpsi[0]_y Jpsi[1]_x Jpsi[1]_y"),
+    "euler_compressible_n2": _measured("euler_compressible_n2", "|psi[1]|^2 Jpsi[1]_y"),
+    "srk3_incompressible_n1_forces": _measured("srk3_incompressible_n1_forces", "|psi[0]|^2 |d_psi[0]|^2 Jpsi[0]_x"),
+    "euler_quiescent_n2_quadratic": _measured("euler_quiescent_n2_quadratic", "|psi[0]|^2 |d_psi[1]|^2 Jpsi[0]_y"),
+    "srk3_compressible_n0_rect_nodealias": _measured("srk3_compressible_n0_rect_nodealias", ""),
+    "srk3_compressible_two_dealias": _measured("srk3_compressible_two_dealias", "Jpsi[0]_x"),
+}

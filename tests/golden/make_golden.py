@@ -9,9 +9,13 @@ integrator with the stochastic right-hand sides it drew.
 
     python tests/golden/make_golden.py            # writes tests/golden/ref_cases.npz
     python tests/golden/make_golden.py --initial  # writes tests/golden/ref_initial.npz
+    python tests/golden/make_golden.py --measures # writes tests/golden/ref_measures.npz
 
 The second form records, per initial-condition case, the reference's initial
-state or, where the reference refuses the script, its error message.
+state or, where the reference refuses the script, its error message.  The
+third runs measure cases through the reference's own MeasurementManager and
+records the state after every step, the noise each step drew and the text of
+every file the measures wrote.
 """
 import ctypes
 import os
@@ -22,7 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-from cases import CASES, IC_CASES  # noqa: E402
+from cases import CASES, IC_CASES, MEASURE_CASES  # noqa: E402
 
 NSTEPS = 2
 
@@ -84,8 +88,47 @@ def main_initial() -> None:
     np.savez_compressed(os.path.join(HERE, "ref_initial.npz"), **out)
 
 
+def main_measures() -> None:
+    import tempfile
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libshhd_ref.so"))
+    lib.shref_create.restype = ctypes.c_void_p
+    lib.shref_last_error.restype = ctypes.c_char_p
+    out = {}
+    for name, template in MEASURE_CASES.items():
+        with tempfile.TemporaryDirectory() as tmp:
+            script = template.replace("@DIR@", tmp)
+            nsteps = int(script.rsplit("run ", 1)[1].split()[0])
+            h = ctypes.c_void_p(lib.shref_create(script.encode()))
+            if not h.value:
+                raise RuntimeError(f"{name}: {lib.shref_last_error().decode()}")
+            info = (ctypes.c_long * 10)()
+            dinfo = (ctypes.c_double * 4)()
+            lib.shref_info(h, info, dinfo)
+            shape = (info[4], info[1], info[0] // 2 + 1)
+            u0 = np.zeros(shape, complex)
+            lib.shref_get_state(h, u0.ctypes.data_as(ctypes.c_void_p))
+            states = np.zeros((nsteps,) + shape, complex)
+            noise = np.zeros((nsteps, 2) + shape, complex)
+            for s in range(nsteps):
+                if lib.shref_step(h, 1, noise[s].ctypes.data_as(ctypes.c_void_p)) != 0:
+                    raise RuntimeError(f"{name}: {lib.shref_last_error().decode()}")
+                lib.shref_get_state(h, states[s].ctypes.data_as(ctypes.c_void_p))
+            lib.shref_finalize(h)
+            lib.shref_destroy(h)
+            out[f"{name}/u0"] = u0
+            out[f"{name}/states"] = states
+            out[f"{name}/noise"] = noise
+            for fn in sorted(os.listdir(tmp)):
+                with open(os.path.join(tmp, fn)) as f:
+                    out[f"{name}/file/{fn}"] = np.array(f.read())
+            print(f"{name}: {nsteps} steps, files {sorted(os.listdir(tmp))}")
+    np.savez_compressed(os.path.join(HERE, "ref_measures.npz"), **out)
+
+
 if __name__ == "__main__":
     if "--initial" in sys.argv[1:]:
         main_initial()
+    elif "--measures" in sys.argv[1:]:
+        main_measures()
     else:
         main()

@@ -1,0 +1,179 @@
+"""Time-series energy / L2 columns and snapshot files against the reference's own measure output.
+
+The fixtures (tests/golden/ref_measures.npz, made by make_golden.py --measures)
+hold, per case, the state after every step, the noise each step drew and the
+files the reference's MeasurementManager wrote along that trajectory.
+
+CPU: the oracle's restatement of the energy and L2 columns reproduces the
+reference's time-series values (1e-12 relative); the snapshot writer
+reproduces the reference's snapshot files (the spectral file byte for byte,
+the physical one to 1e-12 of the field's scale: the host inverse transform is
+not the reference's); snapshot file names and the column checks.
+
+GPU: the engine's FP64 device sums reproduce the reference's values on the
+reference's states (FP64 1e-12, FP32 1e-5 relative); replaying the
+reference's noise, the measures written along the engine's own trajectory
+reproduce the reference's files.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import shhd_oracle as so
+from golden.cases import MEASURE_CASES
+
+DATA = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_measures.npz"))
+ENERGY = ("E_T", "E_K", "E_psi", "E_C")
+
+
+def _ts(name):
+    """(columns, rows) of the reference's ts.dat: rows are (step, time, {column: value})."""
+    lines = str(DATA[f"{name}/file/ts.dat"]).splitlines()
+    cols = lines[1].split()[3:]
+    rows = []
+    for ln in lines[2:]:
+        t = ln.split()
+        rows.append((int(t[0]), float(t[1]), dict(zip(cols, map(float, t[2:])))))
+    return cols, rows
+
+
+def _close(got, want, rtol, scale=None):
+    s = scale if scale is not None else max(abs(want), 1e-300)
+    return abs(got - want) <= rtol * s
+
+
+def _script(name, tmp):
+    return MEASURE_CASES[name].replace("@DIR@", str(tmp))
+
+
+@pytest.mark.parametrize("name", sorted(MEASURE_CASES))
+def test_oracle_columns_match_reference_measure(name, tmp_path):
+    cfg = so.parse_script(_script(name, tmp_path))
+    cols, rows = _ts(name)
+    states = DATA[f"{name}/states"]
+    for s, (step, _time, want) in enumerate(rows):
+        got = {**so.time_series_energies(cfg, states[s]), **so.time_series_l2(cfg, states[s])}
+        for c in cols:
+            if c in got:
+                # E_T sums terms of either sign: compare on the scale of its largest term
+                scale = max(abs(want["E_K"]), abs(want["E_psi"]), abs(want["E_C"])) if c == "E_T" else None
+                assert _close(got[c], want[c], 1e-12, scale), (name, step, c, got[c], want[c])
+
+
+def _compare_snapshot(text, want_text, exact):
+    got, want = text.splitlines(), want_text.splitlines()
+    assert len(got) == len(want)
+    assert got[:4] == want[:4]                       # the four header lines
+    if exact:
+        assert text == want_text
+        return
+    g = np.array([[float(x) for x in ln.split()] for ln in got[4:]])
+    w = np.array([[float(x) for x in ln.split()] for ln in want[4:]])
+    assert np.array_equal(g[:, :2], w[:, :2])        # grid indices
+    scale = np.max(np.abs(w[:, 2:]), axis=0)
+    assert np.all(np.abs(g[:, 2:] - w[:, 2:]) <= 1e-12 * scale)
+
+
+@pytest.mark.parametrize("name", sorted(MEASURE_CASES))
+def test_snapshot_writer_matches_reference_files(name, tmp_path):
+    import shhd_b200 as sb
+    from shhd_b200.measures import snapshot_filename, write_snapshot
+    text = _script(name, tmp_path)
+    cfg = sb.config_from_script(text)
+    nsteps = DATA[f"{name}/states"].shape[0]
+    state = DATA[f"{name}/states"][nsteps - 1]
+    _cols, rows = _ts(name)
+    step, time = rows[-1][0], rows[-1][1]
+    for space, prefix in (("physical", "phys"), ("spectral", "spec")):
+        path = snapshot_filename(str(tmp_path / prefix), step, nsteps)
+        write_snapshot(path, cfg, state, step, time, space)
+        fn = os.path.basename(path)
+        assert f"{name}/file/{fn}" in DATA.files, fn
+        with open(path) as f:
+            _compare_snapshot(f.read(), str(DATA[f"{name}/file/{fn}"]), exact=(space == "spectral"))
+
+
+def test_snapshot_filename_width():
+    from shhd_b200.measures import snapshot_filename
+    assert snapshot_filename("a", 3, 3) == "a_step03.snapshot"
+    assert snapshot_filename("a", 50, 1000) == "a_step00050.snapshot"
+    assert snapshot_filename("a", 0, 0) == "a_step00.snapshot"
+
+
+def test_time_series_rejects_unknown_and_flux_columns():
+    from shhd_b200.measures import TimeSeries
+
+    class _Eng:
+        class cfg:
+            num_order_parameters = 1
+
+    with pytest.raises(NotImplementedError):
+        TimeSeries(_Eng(), "x", 1, ["E_K", "pi_xy"])
+    with pytest.raises(ValueError):
+        TimeSeries(_Eng(), "x", 1, ["|psi[1]|^2"])
+    with pytest.raises(ValueError):
+        TimeSeries(_Eng(), "x", 1, ["E_Q"])
+    with pytest.raises(ValueError):
+        TimeSeries(_Eng(), "x", 0, ["E_K"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", sorted(MEASURE_CASES))
+def test_device_columns_match_reference_measure(name, precision, tmp_path):
+    import shhd_b200 as sb
+    cfg = sb.config_from_script(_script(name, tmp_path))
+    cfg.precision = precision
+    rtol = 1e-12 if precision == 0 else 1e-5
+    cols, rows = _ts(name)
+    states = DATA[f"{name}/states"]
+    with sb.Engine(cfg) as eng:
+        for s, (step, _time, want) in enumerate(rows):
+            eng.set_state(states[s])
+            got = {**eng.time_series_energies(), **eng.time_series_l2()}
+            for c in cols:
+                if c in got:
+                    scale = max(abs(want["E_K"]), abs(want["E_psi"]), abs(want["E_C"])) if c == "E_T" else None
+                    assert _close(got[c], want[c], rtol, scale), (name, precision, step, c, got[c], want[c])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["srk3_compressible_n2", "srk3_incompressible_n1_forces", "euler_quiescent_n2_quadratic"])
+def test_measure_files_along_the_reference_trajectory(name, tmp_path):
+    """Replaying the reference's noise, the engine's measures write the reference's files."""
+    import shhd_b200 as sb
+    from shhd_b200.measures import Snapshot, TimeSeries
+    text = _script(name, tmp_path)
+    cfg = sb.config_from_script(text)
+    cfg.noise_source = 1
+    cols, rows = _ts(name)
+    energy_l2 = [c for c in cols if not (c.startswith("pi_") or c.startswith("Jpsi"))]
+    nsteps = DATA[f"{name}/states"].shape[0]
+    noise = DATA[f"{name}/noise"]
+    with sb.Engine(cfg) as eng:
+        eng.set_state(DATA[f"{name}/u0"])
+        ts = TimeSeries(eng, str(tmp_path / "ts_dev.dat"), 1, energy_l2)
+        snaps = [Snapshot(eng, str(tmp_path / "phys"), 3, "physical", nsteps), Snapshot(eng, str(tmp_path / "spec"), 3, "spectral", nsteps)]
+        for s in range(nsteps):
+            eng.set_external_noise(noise[s, 0], noise[s, 1])
+            eng.step(1)
+            info = eng.get_info()
+            for m in [ts] + snaps:
+                m.observe(int(info.step_index), float(info.time))
+        ts.close()
+    with open(tmp_path / "ts_dev.dat") as f:
+        lines = f.read().splitlines()
+    assert lines[0] == "# measure time_series"
+    assert lines[1] == "# step time " + " ".join(energy_l2)
+    for ln, (step, time, want) in zip(lines[2:], rows):
+        t = ln.split()
+        assert int(t[0]) == step and t[1] == f"{time:.16e}"
+        for c, v in zip(energy_l2, map(float, t[2:])):
+            scale = max(abs(want["E_K"]), abs(want["E_psi"]), abs(want["E_C"])) if c == "E_T" else None
+            assert _close(v, want[c], 1e-11, scale), (name, step, c, v, want[c])
+    for prefix in ("phys", "spec"):
+        fn = f"{prefix}_step03.snapshot"
+        with open(tmp_path / fn) as f:
+            # the engine's trajectory differs from the reference's in the last digits
+            _compare_snapshot(f.read(), str(DATA[f"{name}/file/{fn}"]), exact=False)
