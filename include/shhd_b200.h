@@ -285,6 +285,16 @@ int shhd_engine_set_gaussian_field(shhd_engine* engine, int member, int field, u
  * (allocated on first use). */
 int shhd_engine_energies(shhd_engine* engine, int member, double* out, size_t n);
 
+/* k = 0 flux columns of the time-series measure (measure_time_series.cc:190-229):
+ * after enabling, every step records, per member, the stage-weighted (0, 0)
+ * coefficients of the momentum and order-parameter fluxes (pressure and
+ * advective terms; gradient terms and noise vanish at k = 0).  read gives the
+ * last step's values divided by nx * ny: out[0..2] = pi_xx, pi_xy, pi_yy, then
+ * Jpsi[a]_x, Jpsi[a]_y per order parameter (n >= 3 + 2 * num_order_parameters).
+ * Enabling drops captured graphs. */
+int shhd_engine_flux0_enable(shhd_engine* engine);
+int shhd_engine_flux0_read(shhd_engine* engine, int member, double* out, size_t n);
+
 /* Spectral L2 columns of the time-series measure (measure_time_series.cc:
  * |rho|^2, |d_rho|^2, |j|^2, |d_j|^2, |psi[a]|^2, |d_psi[a]|^2) for one member
  * of the current state, in FP64 on the device: out[2 f] = (V / Np^2) / Np^2

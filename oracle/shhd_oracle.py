@@ -703,6 +703,55 @@ class Oracle:
             out += np.where(act, g.forward(p["jx"] * p["vy"]), 0.0)
         return out
 
+    def k0_flux(self, state: np.ndarray) -> Dict[str, float]:
+        """Real part of the (0, 0) coefficient of the fluxes one RHS evaluation records
+        (unnormalised): the gradient terms (viscous, chemical potential, projection) vanish at
+        k = 0 and no noise is drawn there, so pi_xx = pi_yy = cT^2 rho(0) + sum jx vx | jy vy,
+        pi_xy = sum jx vy (fcalculator.cc:110-150, 276-300, 400-494) and Jpsi[a] = sum psi_a v
+        (fcalculator.cc:86-108, 189-274), each term where the reference evaluates it."""
+        cfg, g = self.cfg, self.geo
+        n = cfg.num_order_parameters
+        out = {"pi_xx": 0.0, "pi_xy": 0.0, "pi_yy": 0.0}
+        for a in range(n):
+            out[f"Jpsi[{a}]_x"] = out[f"Jpsi[{a}]_y"] = 0.0
+        p = self.physical_fields(state)
+        if cfg.mode != "quiescent":
+            if cfg.cT * cfg.cT != 0.0:
+                out["pi_xx"] += cfg.cT * cfg.cT * state[0, 0, 0].real
+                out["pi_yy"] += cfg.cT * cfg.cT * state[0, 0, 0].real
+            if cfg.momentum_advection:
+                out["pi_xx"] += float(np.sum(p["jx"] * p["vx"]))
+                out["pi_xy"] += float(np.sum(p["jx"] * p["vy"]))
+                out["pi_yy"] += float(np.sum(p["jy"] * p["vy"]))
+        if cfg.order_parameter_advection:
+            psi = p["psi"]
+            for a in range(n):
+                out[f"Jpsi[{a}]_x"] += float(np.sum(psi[a] * p["vx"]))
+                out[f"Jpsi[{a}]_y"] += float(np.sum(psi[a] * p["vy"]))
+        return out
+
+    def step_with_k0_flux(self, u: np.ndarray, noise=None):
+        """(next state, the step's k = 0 flux columns of the time-series measure): the stage
+        fluxes weighted 1/6, 1/6, 2/3 (SRK3) or 1 (Euler), divided by the grid size
+        (time_integrator_srk3_compressible.h:99-146, measure_time_series.cc:190-229)."""
+        cfg = self.cfg
+        if cfg.integrator == "euler":
+            stages, weights = [u], [1.0]
+            out = self.step(u, noise)
+        else:
+            sa, sb = noise if noise is not None else (np.zeros(self.shape, complex),) * 2
+            u1 = self._stage(u, u, sa + BETA[0] * sb, *STAGE_WEIGHTS[0])
+            u2 = self._stage(u1, u, sa + BETA[1] * sb, *STAGE_WEIGHTS[1])
+            out = self._stage(u2, u, sa + BETA[2] * sb, *STAGE_WEIGHTS[2])
+            self.step_index += 1
+            self.time += cfg.dt
+            stages, weights = [u, u1, u2], [1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0]
+        acc: Dict[str, float] = {}
+        for w, st in zip(weights, stages):
+            for k, v in self.k0_flux(st).items():
+                acc[k] = acc.get(k, 0.0) + w * v
+        return out, {k: v / self.geo.grid_size for k, v in acc.items()}
+
     def noise_flux_xy(self, xi3: np.ndarray) -> np.ndarray:
         """pi_xy of one j_sto draw (fcalculator.cc:587-700): -s sqrt(eta) xi3 on the
         active k != 0 modes with gx > 0, and on the kx = 0 line the drawn half with

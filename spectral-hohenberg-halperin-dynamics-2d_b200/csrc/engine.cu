@@ -207,6 +207,8 @@ struct shhd_engine {
     double* sk_dev = nullptr;        // FP64 structure-factor accumulator [Hx * Ky] (allocated on first use)
     double* l2_dev = nullptr;        // FP64 spectral L2 sums [field][2] (allocated on first use)
     // Yokota-Green-Kubo taps (FP64): selected modes, step flux, block integrals, sums [member][tau][mode]
+    bool flux0_on = false;
+    Flux0Args flux0{};               // k = 0 fluxes of the last step [member][3 + 2 nop] (allocated on enable)
     bool gk_on = false;
     GkArgs gk{};
     std::vector<int2> gk_modes;
@@ -288,7 +290,7 @@ void free_engine(shhd_engine* e) {
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
                     static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch), e->meas.tw_x, e->meas.tw_y, e->meas.i1,
-                    e->meas.member, static_cast<void*>(e->meas.scratch)})
+                    e->meas.member, static_cast<void*>(e->meas.scratch), static_cast<void*>(e->flux0.acc)})
         if (p) cudaFree(p);
     for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
     e->graphs.clear();
@@ -975,6 +977,18 @@ void launch_gk_tap(shhd_engine* e, const void* cur, int step_off, double weight,
     check_cuda(cudaGetLastError(), "gk_tap launch");
 }
 
+template <typename T>
+void launch_flux0_tap(shhd_engine* e, const void* cur, double weight, int first) {
+    if (!e->flux0_on) return;
+    const double2* k0 = nullptr;
+    if (e->k0_u) k0 = cur == e->u ? e->k0_u : (cur == e->s1 ? e->k0_s1 : (cur == e->s2 ? e->k0_s2 : nullptr));
+    const long long threads = static_cast<long long>(e->P.batch) * e->flux0.ncol * 32;
+    const dim3 g(static_cast<unsigned>((threads + kThreads - 1) / kThreads));
+    flux0_tap_kernel<T><<<g, kThreads, 0, e->stream>>>(e->P, e->flux0, e->members_dev, static_cast<const T*>(e->i2),
+                                                       static_cast<const cplx<T>*>(cur), k0, weight, first);
+    check_cuda(cudaGetLastError(), "flux0_tap launch");
+}
+
 // the launches of one call of nsteps steps (step indices relative to *step_dev)
 template <typename T>
 void record_steps(shhd_engine* e, int nsteps) {
@@ -994,6 +1008,7 @@ void record_steps(shhd_engine* e, int nsteps) {
                 launch_col_forward<T>(e, A);
                 // stage flux weights 1/6, 1/6, 2/3 (time_integrator_srk3_compressible.h:15-21)
                 launch_gk_tap<T>(e, cur[k], s, k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0, k == 2);
+                launch_flux0_tap<T>(e, cur[k], k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0);
             }
         } else {
             launch_row<T>(e);
@@ -1001,6 +1016,7 @@ void record_steps(shhd_engine* e, int nsteps) {
             A.step_off = s;
             launch_col_forward<T>(e, A);
             launch_gk_tap<T>(e, e->u, s, 1.0, 1, 1);
+            launch_flux0_tap<T>(e, e->u, 1.0, 1);
             std::swap(e->u, e->s1);
             std::swap(e->k0_u, e->k0_s1);
         }
@@ -1936,6 +1952,53 @@ int shhd_engine_l2_sums(shhd_engine* e, int member, double* out, size_t n) {
         const double np2 = static_cast<double>(e->cfg.nx) * e->cfg.ny;
         const double pref = e->cfg.lx * e->cfg.ly / np2 / np2;
         for (int q = 0; q < 2 * nf; ++q) out[q] *= pref;
+    });
+}
+
+int shhd_engine_flux0_enable(shhd_engine* e) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (e->flux0_on) return;
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        const StepPlan& P = e->P;
+        Flux0Args F{};
+        F.ncol = 3 + 2 * P.nop;
+        for (int c = 0; c < F.ncol; ++c) F.o[c] = -1;
+        for (int o = 0; o < P.n_out; ++o) {
+            const int k = P.out_kind[o], a = P.out_arg[o];
+            if (k == OUT_PXX) F.o[0] = o;
+            if (k == OUT_PXY) F.o[1] = o;
+            if (k == OUT_PYY) F.o[2] = o;
+            if (k == OUT_PSIVX) F.o[3 + 2 * a] = o;
+            if (k == OUT_PSIVY) F.o[4 + 2 * a] = o;
+        }
+        // j_det records the linear pressure flux whenever it runs with cT^2 != 0 (fcalculator.cc:110-136)
+        F.pressure = e->cfg.mode != SHHD_QUIESCENT && P.cT2 != 0.0;
+        F.pair_layout = e->pair_path ? 1 : 0;
+        const size_t bytes = sizeof(double) * e->cfg.batch * F.ncol;
+        F.acc = static_cast<double*>(dalloc(e, bytes));
+        check_cuda(cudaMemsetAsync(F.acc, 0, bytes, e->stream), "memset");
+        check_cuda(cudaStreamSynchronize(e->stream), "flux0 sync");
+        e->flux0 = F;
+        e->flux0_on = true;
+        drop_graphs(e);  // captured graphs do not hold the tap yet
+    });
+}
+
+int shhd_engine_flux0_read(shhd_engine* e, int member, double* out, size_t n) {
+    return guarded([&] {
+        if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");
+        if (!e->flux0_on) throw Failure(SHHD_EINVAL, "the k = 0 flux tap is not enabled");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        const int ncol = e->flux0.ncol;
+        if (n < static_cast<size_t>(ncol)) throw Failure(SHHD_EINVAL, "flux0 read needs 3 + 2 * num_order_parameters doubles");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        check_cuda(cudaMemcpyAsync(out, e->flux0.acc + static_cast<size_t>(member) * ncol, sizeof(double) * ncol, cudaMemcpyDeviceToHost,
+                                   e->stream),
+                   "flux0 read");
+        check_cuda(cudaStreamSynchronize(e->stream), "flux0 sync");
+        const double ng = static_cast<double>(e->cfg.nx) * e->cfg.ny;
+        for (int c = 0; c < ncol; ++c) out[c] /= ng;
     });
 }
 

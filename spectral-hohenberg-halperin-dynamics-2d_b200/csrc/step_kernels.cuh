@@ -897,6 +897,52 @@ __global__ void __launch_bounds__(kThreads) gk_tap_kernel(const StepPlan P, cons
 }
 
 // ---------------------------------------------------------------------------
+// k = 0 fluxes of the time-series measure (measure_time_series.cc:190-229): per
+// stage, the stage's flux weight times the (0, 0) coefficient of pi_xx, pi_xy,
+// pi_yy and of psi_a v_x, psi_a v_y, i.e. the sums over y of the kx = 0 column
+// of the stage's x-transformed product planes, plus the linear pressure
+// cT^2 rho(0) on the diagonal; the gradient terms and the noise vanish at
+// k = 0.  The first stage of a step overwrites, so acc holds the last step's.
+// acc[member][3 + 2 nop]; one warp per (member, column)
+// ---------------------------------------------------------------------------
+struct Flux0Args {
+    double* acc;
+    int ncol;                     // 3 + 2 nop: pi_xx, pi_xy, pi_yy, then (Jpsi[a]_x, Jpsi[a]_y) per a
+    int o[3 + 2 * kMaxOp];        // product plane of each column in I2 (-1: no advective term)
+    int pressure;                 // cT^2 rho(0) on pi_xx and pi_yy
+    int pair_layout;              // I2 element (re_2t, re_2t+1, im_2t, im_2t+1) with W = 2
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) flux0_tap_kernel(const StepPlan P, const Flux0Args F, const MemberInfo* __restrict__ members,
+                                                             const T* __restrict__ i2, const cplx<T>* __restrict__ cur,
+                                                             const double2* __restrict__ k0cur, double weight, int first) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= P.batch * F.ncol) return;
+    const int b = warp / F.ncol, c = warp - b * F.ncol;
+    if (!members[b].active) return;
+    double v = 0.0;
+    const int o = F.o[c];
+    if (o >= 0) {
+        const size_t plane = static_cast<size_t>(P.hx) * P.npy * 2;  // scalars of one I2 plane
+        const T* base = i2 + (static_cast<size_t>(b) * P.n_out + o) * plane;
+        for (int y = lane; y < P.npy; y += 32)  // kx = 0: tile 0, slot 0, real part
+            v += static_cast<double>(F.pair_layout ? base[4 * static_cast<size_t>(y)] : base[2 * static_cast<size_t>(y) * P.W]);
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    }
+    if (lane != 0) return;
+    if (F.pressure && (c == 0 || c == 2)) {
+        const size_t fst = static_cast<size_t>(P.hx) * P.kyn;
+        const double r00 = k0cur ? k0cur[static_cast<size_t>(b) * P.nfields].x
+                                 : static_cast<double>(cur[static_cast<size_t>(b) * P.nfields * fst].x);
+        v += P.cT2 * r00;
+    }
+    double* a = F.acc + static_cast<size_t>(b) * F.ncol + c;
+    *a = first ? weight * v : *a + weight * v;
+}
+
+// ---------------------------------------------------------------------------
 // spectral L2 sums of the time-series measure (measure_time_series.cc, the
 // |rho|^2 ... |d_psi[a]|^2 columns): per field, sum over the active modes but
 // (0, 0) of w |u|^2 and w k^2 |u|^2, w = 2 off the kx = 0 line; FP64, one

@@ -125,6 +125,7 @@ EXPORTED = (
     "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
     "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums", "shhd_engine_set_gaussian_field",
     "shhd_engine_set_initial_field", "shhd_engine_check_transverse", "shhd_engine_energies",
+    "shhd_engine_flux0_enable", "shhd_engine_flux0_read",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -171,6 +172,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_set_initial_field.argtypes = [vp, i, i, ctypes.POINTER(InitialField)]
     lib.shhd_engine_check_transverse.argtypes = [vp, ctypes.POINTER(InitialField), ctypes.POINTER(InitialField)]
     lib.shhd_engine_energies.argtypes = [vp, i, dp, sz]
+    lib.shhd_engine_flux0_enable.argtypes = [vp]
+    lib.shhd_engine_flux0_read.argtypes = [vp, i, dp, sz]
     return lib
 
 
@@ -322,6 +325,21 @@ class Engine:
         raw = np.zeros(4, dtype=np.float64)
         _check(lib.shhd_engine_energies(self._h, int(member), _dptr(raw), raw.size))
         return {"E_T": float(raw[0]), "E_K": float(raw[1]), "E_psi": float(raw[2]), "E_C": float(raw[3])}
+
+    def flux0_enable(self) -> None:
+        """Record the k = 0 flux columns of every step from now on (drops captured graphs)."""
+        _check(lib.shhd_engine_flux0_enable(self._h))
+
+    def flux0_read(self, member: int = 0) -> dict:
+        """The last step's k = 0 flux columns: pi_xx, pi_xy, pi_yy, Jpsi[a]_x, Jpsi[a]_y."""
+        n = self.cfg.num_order_parameters
+        raw = np.zeros(3 + 2 * n, dtype=np.float64)
+        _check(lib.shhd_engine_flux0_read(self._h, int(member), _dptr(raw), raw.size))
+        out = {"pi_xx": raw[0], "pi_xy": raw[1], "pi_yy": raw[2]}
+        for a in range(n):
+            out[f"Jpsi[{a}]_x"] = raw[3 + 2 * a]
+            out[f"Jpsi[{a}]_y"] = raw[4 + 2 * a]
+        return {k: float(v) for k, v in out.items()}
 
     def time_series_l2(self, member: int = 0) -> dict:
         """The reference time-series measure's spectral L2 columns of the current state (FP64)."""

@@ -4,8 +4,9 @@
       (shhd_engine_energies) and the spectral L2 columns |rho|^2 ... |d_psi[a]|^2
       (shhd_engine_l2_sums), FP64 sums on the device; one line per observed step,
       `step time v...` in scientific notation with 16 digits.  The k = 0 flux
-      columns (pi_*, Jpsi[a]_*) read the reference's flux buffer, which the
-      engine does not keep; asking for them raises NotImplementedError.
+      columns pi_xx pi_xy pi_yy Jpsi[a]_x Jpsi[a]_y come from the engine's flux
+      tap (shhd_engine_flux0_*), enabled when a column asks for it: the last
+      step's stage-weighted (0, 0) fluxes, as the reference's flux buffer holds.
   snapshot (measure_snapshot.cc:43-138): `<file>_step<step>.snapshot`, the step
       zero-padded to the digits of the script's total run steps; space physical
       (every field inverse-transformed on the padded grid, rows gy-major) or
@@ -23,7 +24,8 @@ import numpy as np
 
 _ENERGY = ("E_T", "E_K", "E_psi", "E_C")
 _L2 = ("|rho|^2", "|d_rho|^2", "|j|^2", "|d_j|^2")
-_FLUX = re.compile(r"^(pi_xx|pi_xy|pi_yy|Jpsi\[\d+\]_[xy])$")
+_PI = ("pi_xx", "pi_xy", "pi_yy")
+_JPSI = re.compile(r"^Jpsi\[(\d+)\]_[xy]$")
 _PSI_L2 = re.compile(r"^\|(d_)?psi\[(\d+)\]\|\^2$")
 
 
@@ -39,13 +41,16 @@ class TimeSeries:
             raise ValueError("time_series measure: nevery must be positive.")
         nop = engine.cfg.num_order_parameters
         for t in targets:
-            if _FLUX.match(t):
-                raise NotImplementedError(f"time_series column {t}: the k = 0 fluxes are not produced by the device measures")
             m = _PSI_L2.match(t)
-            if m and not 0 <= int(m.group(2)) < nop:
+            j = _JPSI.match(t)
+            a = int(m.group(2)) if m else (int(j.group(1)) if j else None)
+            if a is not None and not 0 <= a < nop:
                 raise ValueError(f"time_series target order-parameter index out of range: {t}")
-            if not (t in _ENERGY or t in _L2 or m):
+            if not (t in _ENERGY or t in _L2 or t in _PI or a is not None):
                 raise ValueError(f"unknown time_series target: {t}")
+        self._flux = any(t in _PI or _JPSI.match(t) for t in targets)
+        if self._flux:
+            engine.flux0_enable()
         self.engine, self.file, self.nevery, self.targets, self.member = engine, file, int(nevery), list(targets), member
         self._out: Optional[TextIO] = None
 
@@ -63,6 +68,8 @@ class TimeSeries:
             vals.update(self.engine.time_series_energies(self.member))
         if any(t in _L2 or _PSI_L2.match(t) for t in self.targets):
             vals.update(self.engine.time_series_l2(self.member))
+        if self._flux:
+            vals.update(self.engine.flux0_read(self.member))
         return {t: vals[t] for t in self.targets}
 
     def observe(self, step: int, time: float) -> None:

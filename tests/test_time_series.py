@@ -4,16 +4,18 @@ The fixtures (tests/golden/ref_measures.npz, made by make_golden.py --measures)
 hold, per case, the state after every step, the noise each step drew and the
 files the reference's MeasurementManager wrote along that trajectory.
 
-CPU: the oracle's restatement of the energy and L2 columns reproduces the
-reference's time-series values (1e-12 relative); the snapshot writer
+CPU: the oracle's restatement of the energy, L2 and k = 0 flux columns
+reproduces the reference's time-series values (1e-12 relative; the flux
+columns on the scale of their terms, which can cancel); the snapshot writer
 reproduces the reference's snapshot files (the spectral file byte for byte,
 the physical one to 1e-12 of the field's scale: the host inverse transform is
 not the reference's); snapshot file names and the column checks.
 
 GPU: the engine's FP64 device sums reproduce the reference's values on the
 reference's states (FP64 1e-12, FP32 1e-5 relative); replaying the
-reference's noise, the measures written along the engine's own trajectory
-reproduce the reference's files.
+reference's noise, the flux tap reproduces the reference's k = 0 flux
+columns step by step, and the measures written along the engine's own
+trajectory reproduce the reference's files (every column).
 """
 import os
 
@@ -101,15 +103,37 @@ def test_snapshot_filename_width():
     assert snapshot_filename("a", 0, 0) == "a_step00.snapshot"
 
 
-def test_time_series_rejects_unknown_and_flux_columns():
+def _flux_scale(want, c):
+    """Scale of a k = 0 flux column: its terms (pressure, advection) can cancel."""
+    if c.startswith("pi_"):
+        return max(abs(want["pi_xx"]), abs(want["pi_yy"]), abs(want[c]), 1e-300)
+    return max(max(abs(v) for k, v in want.items() if k.startswith("Jpsi")), 1e-300)
+
+
+@pytest.mark.parametrize("name", sorted(MEASURE_CASES))
+def test_oracle_k0_flux_matches_reference_measure(name, tmp_path):
+    cfg = so.parse_script(_script(name, tmp_path))
+    cols, rows = _ts(name)
+    o = so.Oracle(cfg)
+    u = DATA[f"{name}/u0"]
+    for s, (step, _time, want) in enumerate(rows):
+        nz = DATA[f"{name}/noise"][s]
+        _u, got = o.step_with_k0_flux(u, (nz[0], nz[1]) if cfg.integrator == "srk3" else (nz[0],))
+        for c in cols:
+            if c in got:
+                assert _close(got[c], want[c], 1e-12, _flux_scale(want, c)), (name, step, c, got[c], want[c])
+        u = DATA[f"{name}/states"][s]
+
+
+def test_time_series_rejects_unknown_columns():
     from shhd_b200.measures import TimeSeries
 
     class _Eng:
         class cfg:
             num_order_parameters = 1
 
-    with pytest.raises(NotImplementedError):
-        TimeSeries(_Eng(), "x", 1, ["E_K", "pi_xy"])
+    with pytest.raises(ValueError):
+        TimeSeries(_Eng(), "x", 1, ["Jpsi[1]_x"])
     with pytest.raises(ValueError):
         TimeSeries(_Eng(), "x", 1, ["|psi[1]|^2"])
     with pytest.raises(ValueError):
@@ -139,6 +163,47 @@ def test_device_columns_match_reference_measure(name, precision, tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name", sorted(MEASURE_CASES))
+def test_device_k0_flux_matches_reference_measure(name, precision, tmp_path):
+    """Replaying the reference's noise, the flux tap reads the reference's pi_* / Jpsi columns."""
+    import shhd_b200 as sb
+    cfg = sb.config_from_script(_script(name, tmp_path))
+    cfg.precision = precision
+    cfg.noise_source = 1
+    rtol = 1e-11 if precision == 0 else 2e-5
+    cols, rows = _ts(name)
+    noise = DATA[f"{name}/noise"]
+    with sb.Engine(cfg) as eng:
+        eng.set_state(DATA[f"{name}/u0"])
+        eng.flux0_enable()
+        for s, (step, _time, want) in enumerate(rows):
+            eng.set_external_noise(noise[s, 0], noise[s, 1])
+            eng.step(1)
+            got = eng.flux0_read()
+            for c in cols:
+                if c in got:
+                    assert _close(got[c], want[c], rtol, _flux_scale(want, c)), (name, precision, step, c, got[c], want[c])
+
+
+@pytest.mark.gpu
+def test_k0_flux_survives_graph_replay(tmp_path):
+    """The tap is part of captured steps: graph replays record the same last-step flux."""
+    import shhd_b200 as sb
+    name = "srk3_compressible_n2"
+    cfg = sb.config_from_script(_script(name, tmp_path))
+    with sb.Engine(cfg) as g, sb.Engine(cfg) as d:
+        for e in (g, d):
+            e.set_state(DATA[f"{name}/u0"])
+            e.flux0_enable()
+        g.set_graph_chunk(4)
+        g.step(8)
+        d.step(4)
+        d.step(4)
+        assert g.flux0_read() == d.flux0_read()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", ["srk3_compressible_n2", "srk3_incompressible_n1_forces", "euler_quiescent_n2_quadratic"])
 def test_measure_files_along_the_reference_trajectory(name, tmp_path):
     """Replaying the reference's noise, the engine's measures write the reference's files."""
@@ -148,12 +213,11 @@ def test_measure_files_along_the_reference_trajectory(name, tmp_path):
     cfg = sb.config_from_script(text)
     cfg.noise_source = 1
     cols, rows = _ts(name)
-    energy_l2 = [c for c in cols if not (c.startswith("pi_") or c.startswith("Jpsi"))]
     nsteps = DATA[f"{name}/states"].shape[0]
     noise = DATA[f"{name}/noise"]
     with sb.Engine(cfg) as eng:
         eng.set_state(DATA[f"{name}/u0"])
-        ts = TimeSeries(eng, str(tmp_path / "ts_dev.dat"), 1, energy_l2)
+        ts = TimeSeries(eng, str(tmp_path / "ts_dev.dat"), 1, cols)
         snaps = [Snapshot(eng, str(tmp_path / "phys"), 3, "physical", nsteps), Snapshot(eng, str(tmp_path / "spec"), 3, "spectral", nsteps)]
         for s in range(nsteps):
             eng.set_external_noise(noise[s, 0], noise[s, 1])
@@ -165,12 +229,15 @@ def test_measure_files_along_the_reference_trajectory(name, tmp_path):
     with open(tmp_path / "ts_dev.dat") as f:
         lines = f.read().splitlines()
     assert lines[0] == "# measure time_series"
-    assert lines[1] == "# step time " + " ".join(energy_l2)
+    assert lines[1] == str(DATA[f"{name}/file/ts.dat"]).splitlines()[1]
     for ln, (step, time, want) in zip(lines[2:], rows):
         t = ln.split()
         assert int(t[0]) == step and t[1] == f"{time:.16e}"
-        for c, v in zip(energy_l2, map(float, t[2:])):
-            scale = max(abs(want["E_K"]), abs(want["E_psi"]), abs(want["E_C"])) if c == "E_T" else None
+        for c, v in zip(cols, map(float, t[2:])):
+            if c.startswith("pi_") or c.startswith("Jpsi"):
+                scale = _flux_scale(want, c)
+            else:
+                scale = max(abs(want["E_K"]), abs(want["E_psi"]), abs(want["E_C"])) if c == "E_T" else None
             assert _close(v, want[c], 1e-11, scale), (name, step, c, v, want[c])
     for prefix in ("phys", "spec"):
         fn = f"{prefix}_step03.snapshot"
