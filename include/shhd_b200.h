@@ -295,6 +295,19 @@ int shhd_engine_energies(shhd_engine* engine, int member, double* out, size_t n)
 int shhd_engine_flux0_enable(shhd_engine* engine);
 int shhd_engine_flux0_read(shhd_engine* engine, int member, double* out, size_t n);
 
+/* One sample of the ave/profile measure (measure_ave_profile.cc:180-374) for
+ * one member.  axis 0 bins over x (averaging over y), axis 1 bins over y.
+ * profile_line: the spectral line of `field` the profile needs, FP64 complex
+ * as interleaved doubles: axis 0 the ky = 0 row over the active kx
+ * (active_nx / 2 entries), axis 1 the kx = 0 column in the engine's ky order (ky = 0 .. Na/2 - 1, then
+ * -(Na/2 - 1) .. -1).  The transverse sum of the field is the 1-D inverse
+ * transform of that line.  profile_velocity: the compressible velocity
+ * component j_c / rho summed over the transverse axis on the padded grid
+ * (nx or ny doubles), FP64 sums on the device; SHHD_EINVAL with the
+ * reference's message on a zero density. */
+int shhd_engine_profile_line(shhd_engine* engine, int member, int field, int axis, double* out, size_t n);
+int shhd_engine_profile_velocity(shhd_engine* engine, int member, int component, int axis, double* out, size_t n);
+
 /* Spectral L2 columns of the time-series measure (measure_time_series.cc:
  * |rho|^2, |d_rho|^2, |j|^2, |d_j|^2, |psi[a]|^2, |d_psi[a]|^2) for one member
  * of the current state, in FP64 on the device: out[2 f] = (V / Np^2) / Np^2

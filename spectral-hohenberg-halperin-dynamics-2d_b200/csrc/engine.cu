@@ -179,6 +179,9 @@ struct MeasurePlan {
     void* member = nullptr;       // one always-active MemberInfo
     double* scratch = nullptr;    // partial sums, then the summed values
     size_t scratch_doubles = 0;
+    double* profile = nullptr;    // profile partial rows [pairs][npx] and the result (allocated on first use)
+    int* flag = nullptr;
+    double2* line = nullptr;      // one spectral line of a profile sample
     size_t smem_col = 0, smem_row = 0;
 };
 
@@ -290,7 +293,8 @@ void free_engine(shhd_engine* e) {
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
                     static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch), e->meas.tw_x, e->meas.tw_y, e->meas.i1,
-                    e->meas.member, static_cast<void*>(e->meas.scratch), static_cast<void*>(e->flux0.acc)})
+                    e->meas.member, static_cast<void*>(e->meas.scratch), static_cast<void*>(e->flux0.acc), static_cast<void*>(e->meas.profile),
+                    static_cast<void*>(e->meas.flag), static_cast<void*>(e->meas.line)})
         if (p) cudaFree(p);
     for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
     e->graphs.clear();
@@ -921,7 +925,7 @@ void prepare_static(shhd_engine* e) {
     dim3 grid(e->n_static, e->P.batch);
     LaunchScope scope(e, 3, static_cast<double>(sizeof(cplx<T>)) * e->P.batch * e->n_static * 3.0 * e->P.hx * e->P.kyn);
     prepare_static_kernel<T><<<grid, kThreads, 0, e->stream>>>(e->P, e->static_dev, static_cast<cplx<T>*>(e->u), static_cast<cplx<T>*>(e->s1),
-                                                             static_cast<cplx<T>*>(e->s2));
+                                                             static_cast<cplx<T>*>(e->s2), e->k0_u, e->k0_s1, e->k0_s2);
     check_cuda(cudaGetLastError(), "prepare_static launch");
 }
 
@@ -1835,6 +1839,7 @@ void build_measure_plan(shhd_engine* e) {
     M.scratch = static_cast<double*>(dalloc(e, M.scratch_doubles * sizeof(double)));
     raise_smem_limit(reinterpret_cast<const void*>(col_inverse_kernel<T, 0>), M.smem_col);
     raise_smem_limit(reinterpret_cast<const void*>(energy_row_kernel<T>), M.smem_row);
+    raise_smem_limit(reinterpret_cast<const void*>(profile_velocity_row_kernel<T>), M.smem_row);
     check_cuda(cudaStreamSynchronize(e->stream), "measure plan");
     M.ready = true;
 }
@@ -1867,6 +1872,59 @@ double physical_energy_sum(shhd_engine* e, const cplx<T>* st, int term, int fiel
     check_cuda(cudaMemcpyAsync(&v, out, sizeof(double), cudaMemcpyDeviceToHost, e->stream), "energy read");
     check_cuda(cudaStreamSynchronize(e->stream), "energy sync");
     return v;
+}
+
+// the spectral line of one field that a profile along `axis` needs (FP64)
+template <typename T>
+void profile_line(shhd_engine* e, int member, int field, int axis, double* out) {
+    const StepPlan& P = e->P;
+    const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
+    const auto* f = static_cast<const cplx<T>*>(e->u) + static_cast<size_t>(member) * e->state_elems + field * fstride;
+    const double2* k0 = e->k0_u ? e->k0_u + static_cast<size_t>(member) * P.nfields + field : nullptr;
+    const int n = axis == 0 ? P.hx : P.kyn;
+    MeasurePlan& M = e->meas;
+    if (!M.line) M.line = static_cast<double2*>(dalloc(e, sizeof(double2) * std::max(P.hx, P.kyn)));
+    profile_line_kernel<T><<<(n + kThreads - 1) / kThreads, kThreads, 0, e->stream>>>(P, f, k0, axis, M.line);
+    check_cuda(cudaGetLastError(), "profile_line launch");
+    check_cuda(cudaMemcpyAsync(out, M.line, sizeof(double2) * n, cudaMemcpyDeviceToHost, e->stream), "profile line read");
+    check_cuda(cudaStreamSynchronize(e->stream), "profile sync");
+}
+
+// compressible velocity component of one member summed over the transverse axis
+template <typename T>
+void profile_velocity(shhd_engine* e, int member, int component, int axis, double* out) {
+    build_measure_plan<T>(e);
+    MeasurePlan& M = e->meas;
+    StepPlan P = M.P;
+    P.n_in = 3;
+    P.in_field[0] = 0;
+    P.in_field[1] = P.nop + 1;
+    P.in_field[2] = P.nop + 2;
+    const int pairs = (P.npy + 1) / 2;
+    if (!M.profile) {
+        M.profile = static_cast<double*>(dalloc(e, sizeof(double) * (static_cast<size_t>(pairs) * P.npx + std::max(P.npx, P.npy))));
+        M.flag = static_cast<int*>(dalloc(e, sizeof(int)));
+    }
+    const auto* st = static_cast<const cplx<T>*>(e->u) + static_cast<size_t>(member) * e->state_elems;
+    auto* i1 = static_cast<cplx<T>*>(M.i1);
+    check_cuda(cudaMemsetAsync(M.flag, 0, sizeof(int), e->stream), "flag clear");
+    col_inverse_kernel<T, 0><<<dim3(P.ntiles, P.n_in, 1), kThreads, M.smem_col, e->stream>>>(
+        P, static_cast<const MemberInfo*>(M.member), st, i1, static_cast<const cplx<T>*>(M.tw_y));
+    check_cuda(cudaGetLastError(), "measure col_inverse launch");
+    double* res = M.profile + static_cast<size_t>(pairs) * P.npx;
+    profile_velocity_row_kernel<T><<<pairs, kThreads, M.smem_row, e->stream>>>(P, i1, static_cast<const cplx<T>*>(M.tw_x), axis, component,
+                                                                               axis == 0 ? M.profile : res, M.flag);
+    check_cuda(cudaGetLastError(), "profile_velocity launch");
+    if (axis == 0) {
+        column_sums_kernel<<<(P.npx + kThreads - 1) / kThreads, kThreads, 0, e->stream>>>(M.profile, pairs, P.npx, res);
+        check_cuda(cudaGetLastError(), "column_sums launch");
+    }
+    int bad = 0;
+    const int n = axis == 0 ? P.npx : P.npy;
+    check_cuda(cudaMemcpyAsync(out, res, sizeof(double) * n, cudaMemcpyDeviceToHost, e->stream), "profile read");
+    check_cuda(cudaMemcpyAsync(&bad, M.flag, sizeof(int), cudaMemcpyDeviceToHost, e->stream), "flag read");
+    check_cuda(cudaStreamSynchronize(e->stream), "profile sync");
+    if (bad) throw Failure(SHHD_EINVAL, "AveProfileMeasure compressible velocity encountered zero density.");
 }
 
 // E_T, E_K, E_psi, E_C of one member (measure_time_series.cc:152-188, 305-470)
@@ -1929,6 +1987,35 @@ int shhd_engine_energies(shhd_engine* e, int member, double* out, size_t n) {
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         if (e->fp32) energies<float>(e, member, out);
         else energies<double>(e, member, out);
+    });
+}
+
+int shhd_engine_profile_line(shhd_engine* e, int member, int field, int axis, double* out, size_t n) {
+    return guarded([&] {
+        if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (field < 0 || field >= e->P.nfields) throw Failure(SHHD_EINVAL, "field index out of range");
+        if (axis != 0 && axis != 1) throw Failure(SHHD_EINVAL, "ave/profile measure: axis must be x|y|0|1.");
+        const size_t need = 2 * static_cast<size_t>(axis == 0 ? e->P.hx : e->P.kyn);
+        if (n < need) throw Failure(SHHD_EINVAL, "profile line needs " + std::to_string(need) + " doubles");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) profile_line<float>(e, member, field, axis, out);
+        else profile_line<double>(e, member, field, axis, out);
+    });
+}
+
+int shhd_engine_profile_velocity(shhd_engine* e, int member, int component, int axis, double* out, size_t n) {
+    return guarded([&] {
+        if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        if (component != 0 && component != 1) throw Failure(SHHD_EINVAL, "component must be 0 (x) or 1 (y)");
+        if (axis != 0 && axis != 1) throw Failure(SHHD_EINVAL, "ave/profile measure: axis must be x|y|0|1.");
+        if (e->cfg.mode != SHHD_COMPRESSIBLE) throw Failure(SHHD_EINVAL, "the physical-space velocity profile is the compressible one");
+        const size_t need = static_cast<size_t>(axis == 0 ? e->cfg.nx : e->cfg.ny);
+        if (n < need) throw Failure(SHHD_EINVAL, "profile needs " + std::to_string(need) + " doubles");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) profile_velocity<float>(e, member, component, axis, out);
+        else profile_velocity<double>(e, member, component, axis, out);
     });
 }
 

@@ -1250,6 +1250,97 @@ __global__ void __launch_bounds__(kThreads) energy_row_kernel(const StepPlan P, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// ave/profile (measure_ave_profile.cc:180-374): one sample of a profile
+// ---------------------------------------------------------------------------
+// the spectral line a profile needs, FP64: axis 0 (bins over x) the ky = 0 row, out[gx] for gx < hx;
+// axis 1 (bins over y) the kx = 0 column, out[j] in the engine's ky order (j < kyn).  (0, 0) from
+// k0 (FP64) when given.  grid: ceil(max(hx, kyn) / 256)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) profile_line_kernel(const StepPlan P, const cplx<T>* __restrict__ field_modes,
+                                                                const double2* __restrict__ k0, int axis, double2* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = axis == 0 ? P.hx : P.kyn;
+    if (i >= n) return;
+    const size_t e = axis == 0 ? static_cast<size_t>(i) * P.kyn : static_cast<size_t>(i);
+    double2 v;
+    if (i == 0 && k0) {
+        v = *k0;
+    } else {
+        const cplx<T> a = field_modes[e];
+        v = make_double2(static_cast<double>(a.x), static_cast<double>(a.y));
+    }
+    out[i] = v;
+}
+
+// compressible velocity j_c / rho of one sample summed over the transverse axis (single-member plan
+// inputs rho, jx, jy): axis 1 writes out[y] = sum over x for the block's rows; axis 0 writes the block's
+// two rows summed, partial[pair][x] (physical x at shared slot sw(x)).  Sets *bad on a zero density.
+// grid: ceil(npy / 2)
+template <typename T>
+__global__ void __launch_bounds__(kThreads) profile_velocity_row_kernel(const StepPlan P, const cplx<T>* __restrict__ i1,
+                                                                        const cplx<T>* __restrict__ tw, int axis, int component,
+                                                                        double* __restrict__ out, int* __restrict__ bad) {
+    using C = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[2][kThreads / 32];
+    C* s_tw = reinterpret_cast<C*>(smem_raw);
+    const int npx = P.npx;
+    C* lines = s_tw + P.twx_count;
+    C* scr = lines + static_cast<size_t>(P.n_in) * npx;
+    const int y0 = 2 * blockIdx.x;
+    const bool has1 = (y0 + 1) < P.npy;
+    load_table(s_tw, tw, P.twx_count);
+    __syncthreads();
+    row_inputs_inverse<T, 0>(P, i1, y0, has1, lines, scr, s_tw);
+    __syncthreads();
+    const C* j = lines + static_cast<size_t>(1 + component) * npx;
+    double a0 = 0.0, a1 = 0.0;
+    int zero = 0;
+    for (int x = threadIdx.x; x < npx; x += blockDim.x) {
+        const uint32_t q = axis == 0 ? sw(static_cast<uint32_t>(x), P.fx.swz) : static_cast<uint32_t>(x);
+        const C rho = lines[q], jc = j[q];
+        if (rho.x == T(0) || (has1 && rho.y == T(0))) zero = 1;
+        const double v0 = static_cast<double>(jc.x) / static_cast<double>(rho.x);
+        const double v1 = has1 ? static_cast<double>(jc.y) / static_cast<double>(rho.y) : 0.0;
+        if (axis == 0) {
+            out[static_cast<size_t>(blockIdx.x) * npx + x] = v0 + v1;
+        } else {
+            a0 += v0;
+            a1 += v1;
+        }
+    }
+    if (zero) atomicOr(bad, 1);
+    if (axis == 0) return;
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = a0;
+        red[1][threadIdx.x >> 5] = a1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) {
+            t0 += red[0][w];
+            t1 += red[1][w];
+        }
+        out[y0] = t0;
+        if (has1) out[y0 + 1] = t1;
+    }
+}
+
+// out[x] = sum over the row pairs of partial[pair][x] in a fixed order; grid: ceil(npx / 256)
+__global__ void __launch_bounds__(kThreads) column_sums_kernel(const double* __restrict__ partial, int npairs, int npx, double* __restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= npx) return;
+    double t = 0.0;
+    for (int p = 0; p < npairs; ++p) t += partial[static_cast<size_t>(p) * npx + x];
+    out[x] = t;
+}
+
 // step counter of the call: set from the host at the start of a call, advanced
 // by the last node of a captured step graph
 __global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }
@@ -1261,13 +1352,22 @@ __global__ void advance_step_kernel(unsigned long long* step, unsigned long long
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads) prepare_static_kernel(const StepPlan P, const int* __restrict__ fields, cplx<T>* u, cplx<T>* s1,
-                                                                 cplx<T>* s2) {
+                                                                 cplx<T>* s2, double2* k0u, double2* k0s1, double2* k0s2) {
     using C = cplx<T>;
     const int f = fields[blockIdx.x], b = blockIdx.y;
     const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
     C* uf = u + (static_cast<size_t>(b) * P.nfields + f) * fstride;
     const int half = P.nay / 2;
-    if (threadIdx.x == 0) uf[0].y = T(0);
+    if (threadIdx.x == 0) {
+        uf[0].y = T(0);
+        if (k0u) {  // FP32 engines: the FP64 k = 0 copy of the static field follows it into every buffer
+            const size_t q = static_cast<size_t>(b) * P.nfields + f;
+            const double2 v = make_double2(k0u[q].x, 0.0);
+            k0u[q] = v;
+            k0s1[q] = v;
+            k0s2[q] = v;
+        }
+    }
     for (int ky = 1 + threadIdx.x; ky < half; ky += blockDim.x) {
         const int jn = P.kyn - ky;  // j of -ky
         const C a = uf[ky];

@@ -125,7 +125,7 @@ EXPORTED = (
     "shhd_engine_sk_accumulate", "shhd_engine_sk_read", "shhd_engine_autotune",
     "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums", "shhd_engine_set_gaussian_field",
     "shhd_engine_set_initial_field", "shhd_engine_check_transverse", "shhd_engine_energies",
-    "shhd_engine_flux0_enable", "shhd_engine_flux0_read",
+    "shhd_engine_flux0_enable", "shhd_engine_flux0_read", "shhd_engine_profile_line", "shhd_engine_profile_velocity",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -174,6 +174,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_energies.argtypes = [vp, i, dp, sz]
     lib.shhd_engine_flux0_enable.argtypes = [vp]
     lib.shhd_engine_flux0_read.argtypes = [vp, i, dp, sz]
+    lib.shhd_engine_profile_line.argtypes = [vp, i, i, i, dp, sz]
+    lib.shhd_engine_profile_velocity.argtypes = [vp, i, i, i, dp, sz]
     return lib
 
 
@@ -340,6 +342,21 @@ class Engine:
             out[f"Jpsi[{a}]_x"] = raw[3 + 2 * a]
             out[f"Jpsi[{a}]_y"] = raw[4 + 2 * a]
         return {k: float(v) for k, v in out.items()}
+
+    def profile_line(self, field: int, axis: int, member: int = 0) -> np.ndarray:
+        """The spectral line of `field` an ave/profile along `axis` needs (complex128): axis 0 the
+        ky = 0 row over the active kx, axis 1 the kx = 0 column in the engine's ky order."""
+        n = self.cfg.active_nx // 2 if axis == 0 else self.cfg.active_ny - 1
+        raw = np.zeros(2 * n, dtype=np.float64)
+        _check(lib.shhd_engine_profile_line(self._h, int(member), int(field), int(axis), _dptr(raw), raw.size))
+        return raw.view(np.complex128)
+
+    def profile_velocity(self, component: int, axis: int, member: int = 0) -> np.ndarray:
+        """The compressible velocity component j_c / rho summed over the transverse axis (FP64)."""
+        n = self.cfg.nx if axis == 0 else self.cfg.ny
+        raw = np.zeros(n, dtype=np.float64)
+        _check(lib.shhd_engine_profile_velocity(self._h, int(member), int(component), int(axis), _dptr(raw), raw.size))
+        return raw
 
     def time_series_l2(self, member: int = 0) -> dict:
         """The reference time-series measure's spectral L2 columns of the current state (FP64)."""

@@ -7,6 +7,8 @@
       columns pi_xx pi_xy pi_yy Jpsi[a]_x Jpsi[a]_y come from the engine's flux
       tap (shhd_engine_flux0_*), enabled when a column asks for it: the last
       step's stage-weighted (0, 0) fluxes, as the reference's flux buffer holds.
+  ave/profile (measure_ave_profile.cc:180-453): block or running averages of
+      field profiles over one axis (class AveProfile).
   snapshot (measure_snapshot.cc:43-138): `<file>_step<step>.snapshot`, the step
       zero-padded to the digits of the script's total run steps; space physical
       (every field inverse-transformed on the padded grid, rows gy-major) or
@@ -151,7 +153,7 @@ class Snapshot:
 
 
 def parse_measures(engine, script_text: str, member: int = 0) -> List[object]:
-    """The script's `measure` commands (time_series, snapshot) over one engine member."""
+    """The script's `measure` commands (time_series, snapshot, ave/profile) over one engine member."""
     total = sum(int(t[1]) for t in (ln.split("#", 1)[0].split() for ln in script_text.splitlines()) if len(t) >= 2 and t[0] == "run")
     out = []
     for raw in script_text.splitlines():
@@ -168,6 +170,8 @@ def parse_measures(engine, script_text: str, member: int = 0) -> List[object]:
             i += 2
         if kind == "time_series":
             out.append(TimeSeries(engine, kv["file"], int(kv["nevery"]), targets, member))
+        elif kind == "ave/profile":
+            out.append(AveProfile(engine, kv["file"], kv["axis"], int(kv["nevery"]), int(kv["nblock"]), kv["average"], targets, member))
         elif kind == "snapshot":
             out.append(Snapshot(engine, kv["file"], int(kv["nevery"]), kv["space"], total, member))
         else:
@@ -183,7 +187,8 @@ def run_script_measures(engine, script_text: str, member: int = 0) -> List[objec
     measures = parse_measures(engine, script_text, member)
     runs = [int(t[1]) for t in (ln.split("#", 1)[0].split() for ln in script_text.splitlines()) if len(t) >= 2 and t[0] == "run"]
     step = int(engine.get_info().step_index)
-    periods = [m.nevery for m in measures if m.nevery > 0]
+    # ave/profile counts every step it observes: step one at a time while one is present
+    periods = [1] if any(isinstance(m, AveProfile) for m in measures) else [m.nevery for m in measures if m.nevery > 0]
     for n in runs:
         end = step + n
         while step < end:
@@ -198,3 +203,154 @@ def run_script_measures(engine, script_text: str, member: int = 0) -> List[objec
     for m in measures:
         m.close()
     return measures
+
+
+_PROFILE_FIELDS = {"rho": "rho", "jx": "jx", "jy": "jy", "vx": "vx", "vy": "vy"}
+_PROFILE_FLUX = {"pi_xx": "pi_xx", "pixx": "pi_xx", "pi_xy": "pi_xy", "pixy": "pi_xy", "pi_yy": "pi_yy", "piyy": "pi_yy"}
+_PROFILE_PSI = re.compile(r"^psi\[(\d+)\]$")
+_PROFILE_JPSI = re.compile(r"^Jpsi\[(\d+)\]_[xy]$")
+
+
+class AveProfile:
+    """`measure <id> ave/profile on axis x|y nevery N nblock B file F average block|running target ...`
+    over one engine member (measure_ave_profile.cc:180-453).
+
+    Every nevery-th observed step adds a sample; every nblock-th step closes a block and writes
+    the profiles averaged over the block (block) or over every block so far (running): the field
+    averaged over the transverse axis on the padded grid, one bin per grid line.  Spectral
+    targets (rho, psi[a], jx, jy; vx, vy = j / rho0 outside compressible dynamics) accumulate
+    the one spectral line the transverse average needs, read from the device in FP64; the
+    compressible vx, vy are summed over the transverse axis on the device per sample.  The flux
+    targets (pi_*, Jpsi[a]_*) need the full flux buffer and are not produced.
+    """
+
+    def __init__(self, engine, file: str, axis: str, nevery: int, nblock: int, average: str, targets: List[str], member: int = 0):
+        cfg = engine.cfg
+        if axis not in ("x", "y", "0", "1"):
+            raise ValueError("ave/profile measure: axis must be x|y|0|1.")
+        if average not in ("block", "running"):
+            raise ValueError("ave/profile measure: average must be block|running.")
+        if nevery <= 0:
+            raise ValueError("ave/profile measure: nevery must be positive.")
+        if nblock <= 0:
+            raise ValueError("ave/profile measure: nblock must be positive.")
+        self.axis = 0 if axis in ("x", "0") else 1
+        self.engine, self.file, self.nevery, self.nblock, self.average, self.member = (
+            engine, file, int(nevery), int(nblock), average, member)
+        nop = cfg.num_order_parameters
+        self.targets = []   # (name, kind, field index / component)
+        for t in targets:
+            if t in _PROFILE_FLUX or _PROFILE_JPSI.match(t):
+                j = _PROFILE_JPSI.match(t)
+                if j and not 0 <= int(j.group(1)) < nop:
+                    raise ValueError(f"ave/profile target order-parameter index out of range: {t}")
+                raise NotImplementedError(f"ave/profile target {t}: the flux buffer is not kept by the engine")
+            m = _PROFILE_PSI.match(t)
+            if m:
+                a = int(m.group(1))
+                if not 0 <= a < nop:
+                    raise ValueError(f"ave/profile target order-parameter index out of range: {t}")
+                self.targets.append((t, "spectral", 1 + a, 1.0))
+            elif t in ("rho", "jx", "jy"):
+                self.targets.append((t, "spectral", {"rho": 0, "jx": nop + 1, "jy": nop + 2}[t], 1.0))
+            elif t in ("vx", "vy"):
+                if cfg.mode == 2:
+                    raise ValueError("AveProfileMeasure vx/vy is not available in quiescent dynamics.")
+                comp = 0 if t == "vx" else 1
+                if cfg.mode == 0:
+                    self.targets.append((t, "velocity", comp, 1.0))
+                else:
+                    self.targets.append((t, "spectral_v", nop + 1 + comp, None))
+            else:
+                raise ValueError(f"unknown ave/profile target: {t}")
+        self.nx, self.ny = cfg.nx, cfg.ny
+        self.profile_size = self.nx if self.axis == 0 else self.ny
+        self.spacing = (cfg.lx / cfg.nx) if self.axis == 0 else (cfg.ly / cfg.ny)
+        self._rho0 = None
+        self.block_step = 0
+        self.samples_in_block = 0
+        self.completed_blocks = 0
+        self.running_samples = 0
+        self._block = [None] * len(self.targets)
+        self._running = [None] * len(self.targets)
+        self._out: Optional[TextIO] = None
+
+    def _reference_density(self) -> float:
+        """Re rho(0) / Ng of the first sample that needs it (measure_ave_profile.cc:123-149)."""
+        if self._rho0 is None:
+            line = self.engine.profile_line(0, 0, self.member)
+            rho0 = line[0].real / (float(self.nx) * float(self.ny))
+            if rho0 == 0.0:
+                raise ValueError("AveProfileMeasure encountered zero reference density.")
+            self._rho0 = rho0
+        return self._rho0
+
+    def _sample(self) -> None:
+        for i, (_name, kind, idx, _scale) in enumerate(self.targets):
+            if kind == "velocity":
+                v = self.engine.profile_velocity(idx, self.axis, self.member)
+            else:
+                v = self.engine.profile_line(idx, self.axis, self.member)
+                if kind == "spectral_v":
+                    v = v * (1.0 / self._reference_density())
+            self._block[i] = v.copy() if self._block[i] is None else self._block[i] + v
+        self.samples_in_block += 1
+
+    def _transverse_sum(self, kind: str, acc: np.ndarray) -> np.ndarray:
+        """The field summed over the transverse axis from its accumulated line."""
+        if kind == "velocity":
+            return acc
+        if self.axis == 0:
+            row = np.zeros(self.nx // 2 + 1, dtype=np.complex128)
+            row[:acc.size] = acc
+            return np.fft.irfft(row, n=self.nx)
+        col = np.zeros(self.ny, dtype=np.complex128)
+        half = (acc.size + 1) // 2
+        col[:half] = acc[:half]
+        col[self.ny - (acc.size - half):] = acc[half:]
+        return np.fft.ifft(col).real
+
+    def _finish(self, step: int, time: float) -> None:
+        if self.samples_in_block <= 0:
+            raise RuntimeError("AveProfileMeasure tried to finish an empty block.")
+        for i in range(len(self.targets)):
+            self._running[i] = self._block[i].copy() if self._running[i] is None else self._running[i] + self._block[i]
+        self.completed_blocks += 1
+        self.running_samples += self.samples_in_block
+        block = self.average == "block"
+        src = self._block if block else self._running
+        samples = self.samples_in_block if block else self.running_samples
+        transverse = float(self.ny) if self.axis == 0 else float(self.nx)
+        norm = float(samples) * transverse
+        profiles = [self._transverse_sum(kind, acc) / norm for (_n, kind, _i, _s), acc in zip(self.targets, src)]
+        lines = [f"# block {self.completed_blocks} step {step} time {_sci(time)} samples {samples}",
+                 "# columns coord" + "".join(" " + n for n, _k, _i, _s in self.targets)]
+        for b in range(self.profile_size):
+            lines.append(_sci(self.spacing * float(b)) + "".join(" " + _sci(p[b]) for p in profiles))
+        text = "\n".join(lines) + "\n\n"
+        header = (f"# measure ave/profile\n# axis {'x' if self.axis == 0 else 'y'} nevery {self.nevery} nblock {self.nblock} "
+                  f"average {self.average}\n")
+        if block:
+            if self._out is None:
+                self._out = open(self.file, "w")
+                self._out.write(header)
+            self._out.write(text)
+            self._out.flush()
+        else:
+            with open(self.file, "w") as f:
+                f.write(header + text)
+        self._block = [None] * len(self.targets)
+        self.samples_in_block = 0
+
+    def observe(self, step: int, time: float) -> None:
+        self.block_step += 1
+        if self.block_step % self.nevery == 0:
+            self._sample()
+        if self.block_step == self.nblock:
+            self._finish(step, time)
+            self.block_step = 0
+
+    def close(self) -> None:
+        if self._out is not None:
+            self._out.close()
+            self._out = None

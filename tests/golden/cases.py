@@ -242,3 +242,28 @@ MEASURE_CASES = {
     "srk3_compressible_n0_rect_nodealias": _measured("srk3_compressible_n0_rect_nodealias", ""),
     "srk3_compressible_two_dealias": _measured("srk3_compressible_two_dealias", "Jpsi[0]_x"),
 }
+
+
+# ave/profile cases: both axes, block and running averages, nevery > 1, spectral
+# targets and the compressible (physical-space) velocity; 6 steps each.
+def _profiled(name, lines, nsteps=6):
+    body = CASES[name].rsplit("run ", 1)[0]
+    return body + "\n".join(lines + [f"run {nsteps}"]) + "\n"
+
+
+PROFILE_CASES = {
+    "profile_srk3_compressible_n2": _profiled("srk3_compressible_n2", [
+        "measure p1 ave/profile on axis x nevery 1 nblock 3 file @DIR@/px_block.dat average block target rho jx vy psi[1] vx",
+        "measure p2 ave/profile on axis y nevery 2 nblock 4 file @DIR@/py_running.dat average running target vx jy psi[0] rho",
+    ]),
+    "profile_srk3_incompressible_n1_forces": _profiled("srk3_incompressible_n1_forces", [
+        "measure p1 ave/profile on axis y nevery 1 nblock 3 file @DIR@/py_block.dat average block target vx vy psi[0]",
+        "measure p2 ave/profile on axis x nevery 1 nblock 2 file @DIR@/px_running.dat average running target jx rho vy",
+    ]),
+    "profile_euler_quiescent_n2_quadratic": _profiled("euler_quiescent_n2_quadratic", [
+        "measure p1 ave/profile on axis x nevery 1 nblock 3 file @DIR@/px.dat average block target psi[0] psi[1] rho",
+    ]),
+    "profile_srk3_compressible_n0_rect_nodealias": _profiled("srk3_compressible_n0_rect_nodealias", [
+        "measure p1 ave/profile on axis y nevery 1 nblock 2 file @DIR@/py.dat average running target vx vy rho jx",
+    ]),
+}

@@ -244,3 +244,28 @@ def test_measure_files_along_the_reference_trajectory(name, tmp_path):
         with open(tmp_path / fn) as f:
             # the engine's trajectory differs from the reference's in the last digits
             _compare_snapshot(f.read(), str(DATA[f"{name}/file/{fn}"]), exact=False)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("te", ["euler/incompressible", "euler/quiescent"])
+def test_fp32_static_fields_keep_their_k0_values_through_euler_swaps(te):
+    """Euler engines swap their state buffers every step; the FP64 k = 0 copies of the fields a
+    mode does not evolve (density, and momentum in quiescent dynamics) must follow, since the
+    measures read them: density line, reference density and energies after an odd step count."""
+    import shhd_b200 as sb
+    from helpers import random_state, script
+    text = script(grid=(32, 32), length=(64.0, 64.0), nop=1, dt=0.01, te=te, cT=None, eta=0.05 if "incomp" in te else 0.0,
+                  zeta=0.0, nonlinear="momentum" if "incomp" in te else None)
+    ocfg = so.parse_script(text)
+    u0 = random_state(ocfg, seed=4, rho0=1.3, transverse=True)
+    got = {}
+    for precision in (0, 1):
+        cfg = sb.config_from_script(text)
+        cfg.precision = precision
+        with sb.Engine(cfg) as eng:
+            eng.set_state(u0)
+            eng.step(3)
+            got[precision] = (eng.profile_line(0, 0), eng.time_series_energies())
+    assert got[1][0][0] == got[0][0][0] == u0[0, 0, 0]
+    for k in ENERGY:
+        assert _close(got[1][1][k], got[0][1][k], 1e-5, max(abs(v) for v in got[0][1].values())), k
