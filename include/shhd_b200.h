@@ -308,6 +308,18 @@ int shhd_engine_flux0_read(shhd_engine* engine, int member, double* out, size_t 
 int shhd_engine_profile_line(shhd_engine* engine, int member, int field, int axis, double* out, size_t n);
 int shhd_engine_profile_velocity(shhd_engine* engine, int member, int component, int axis, double* out, size_t n);
 
+/* The step's flux buffer along one spectral line, for the ave/profile flux
+ * targets (measure_ave_profile.cc:216-238): after enabling an axis (0: the
+ * ky = 0 row, 1: the kx = 0 column), every step records per member the
+ * stage-weighted fluxes the deterministic RHS records at the line's modes,
+ * the first noise draw's flux / sqrt(dt) and, incompressible, the projection
+ * pressure.  read gives the last step's values as interleaved complex doubles
+ * [comp][line], comp = pi_xx, pi_xy, pi_yy, then Jpsi[a]_x, Jpsi[a]_y; the line
+ * in the order of shhd_engine_profile_line.  Refused with replayed (external)
+ * noise when the noise is on.  Enabling drops captured graphs. */
+int shhd_engine_flux_line_enable(shhd_engine* engine, int axis);
+int shhd_engine_flux_line_read(shhd_engine* engine, int axis, int member, double* out, size_t n);
+
 /* Spectral L2 columns of the time-series measure (measure_time_series.cc:
  * |rho|^2, |d_rho|^2, |j|^2, |d_j|^2, |psi[a]|^2, |d_psi[a]|^2) for one member
  * of the current state, in FP64 on the device: out[2 f] = (V / Np^2) / Np^2

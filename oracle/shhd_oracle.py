@@ -752,6 +752,166 @@ class Oracle:
                 acc[k] = acc.get(k, 0.0) + w * v
         return out, {k: v / self.geo.grid_size for k, v in acc.items()}
 
+    def _mu_coefficients(self, a: int) -> Tuple[float, float, float]:
+        cfg = self.cfg
+        if cfg.free_energy == "phi4":
+            return cfg.phi4_a[a], cfg.phi4_b[a], 0.0
+        if cfg.free_energy == "quadratic":
+            return cfg.quad_a[a], 0.0, 0.0
+        return 0.0, 0.0, 0.0
+
+    def flux_fields(self, state: np.ndarray) -> Dict[str, np.ndarray]:
+        """Every flux one deterministic RHS evaluation records in the flux buffer, per mode:
+        psi_det's -i M k mu (linear and physical chemical potential) and psi v (fcalculator.cc:86-274),
+        j_det's linear pressure, viscous and advective stresses (fcalculator.cc:110-494), each where
+        the reference evaluates it.  Keys pi_xx, pi_xy, pi_yy, Jpsi[a]_x, Jpsi[a]_y."""
+        cfg, g = self.cfg, self.geo
+        n = cfg.num_order_parameters
+        act = g.active
+        kx, ky, k2 = g.kx, g.ky, g.k2
+        zero = lambda: np.zeros((g.ny, g.hx), dtype=np.complex128)  # noqa: E731
+        out = {"pi_xx": zero(), "pi_xy": zero(), "pi_yy": zero()}
+        for a in range(n):
+            out[f"Jpsi[{a}]_x"], out[f"Jpsi[{a}]_y"] = zero(), zero()
+        p = self.physical_fields(state)
+        has_phys = cfg.free_energy == "phi4" and any(u != 0.0 for u in cfg.phi4_u)
+        for a in range(n):
+            M = cfg.mobility[a]
+            adv = cfg.order_parameter_advection
+            if M == 0.0 and not adv:
+                continue
+            fx, fy = out[f"Jpsi[{a}]_x"], out[f"Jpsi[{a}]_y"]
+            c0, c2, c4 = self._mu_coefficients(a)
+            if M != 0.0 and (c0 != 0.0 or c2 != 0.0 or c4 != 0.0):
+                mu = (c0 + c2 * k2 + c4 * k2 * k2) * state[1 + a]
+                fx += np.where(act, -1j * (M * kx) * mu, 0.0)
+                fy += np.where(act, -1j * (M * ky) * mu, 0.0)
+            if adv or has_phys:
+                if M != 0.0 and has_phys:
+                    mu_p = g.forward(cfg.phi4_u[a] * p["psi"][a] ** 3)
+                    fx += np.where(act, -1j * (M * kx) * mu_p, 0.0)
+                    fy += np.where(act, -1j * (M * ky) * mu_p, 0.0)
+                if adv:
+                    fx += np.where(act, g.forward(p["psi"][a] * p["vx"]), 0.0)
+                    fy += np.where(act, g.forward(p["psi"][a] * p["vy"]), 0.0)
+        if cfg.mode != "quiescent":
+            eta, zeta = cfg.eta, cfg.zeta
+            has_lp = cfg.cT * cfg.cT != 0.0
+            has_visc = eta != 0.0 or zeta != 0.0
+            if has_lp or has_visc or cfg.momentum_advection:
+                xx, xy, yy = out["pi_xx"], out["pi_xy"], out["pi_yy"]
+                if has_lp:
+                    pr = cfg.cT * cfg.cT * state[0]
+                    xx += np.where(act, pr, 0.0)
+                    yy += np.where(act, pr, 0.0)
+                if has_visc and cfg.mode == "incompressible" and eta != 0.0:
+                    rho0 = self.reference_density(state)
+                    vx, vy = state[n + 1] / rho0, state[n + 2] / rho0
+                    xx += np.where(act, -1j * eta * (2.0 * kx * vx), 0.0)
+                    xy += np.where(act, -1j * eta * (ky * vx + kx * vy), 0.0)
+                    yy += np.where(act, -1j * eta * (2.0 * ky * vy), 0.0)
+                if has_visc and cfg.mode == "compressible":
+                    vx, vy = g.forward(p["vx"]), g.forward(p["vy"])
+                    kv = kx * vx + ky * vy
+                    xx += np.where(act, -1j * (2.0 * eta * kx * vx - (eta - zeta) * kv), 0.0)
+                    xy += np.where(act, -1j * eta * (ky * vx + kx * vy), 0.0)
+                    yy += np.where(act, -1j * (2.0 * eta * ky * vy - (eta - zeta) * kv), 0.0)
+                if cfg.momentum_advection:
+                    xx += np.where(act, g.forward(p["jx"] * p["vx"]), 0.0)
+                    xy += np.where(act, g.forward(p["jx"] * p["vy"]), 0.0)
+                    yy += np.where(act, g.forward(p["jy"] * p["vy"]), 0.0)
+        return out
+
+    def noise_flux_fields(self, xi_psi: Sequence[np.ndarray], xi_j: Sequence[np.ndarray]) -> Dict[str, np.ndarray]:
+        """Fluxes psi_sto and j_sto record for one draw (fcalculator.cc:496-700): psi i k / k^2 sigma xi
+        (x-component zero on the kx = 0 line), momentum -s (sqrt(zeta) xi1 +- sqrt(eta) xi2) on the
+        diagonal and -s sqrt(eta) xi3 off it; on the kx = 0 line the drawn half and its conjugate."""
+        cfg, g = self.cfg, self.geo
+        n = cfg.num_order_parameters
+        use = g.active & (g.k2 != 0.0)
+        line = use & (g.gx == 0) & (g.gy < (g.ny - g.gy) % g.ny)
+        bulk = use & (g.gx != 0)
+        conj_rows = (g.ny - np.arange(g.ny)) % g.ny
+        kx, ky, k2 = g.kx, g.ky, g.k2
+
+        def place(v):
+            o = np.where(bulk, v, 0.0)
+            lv = np.where(line, v, 0.0)[:, 0]
+            o[:, 0] += lv
+            o[conj_rows, 0] += np.conj(lv)
+            return o
+
+        out: Dict[str, np.ndarray] = {}
+        for a in range(n):
+            out[f"Jpsi[{a}]_x"] = np.zeros((g.ny, g.hx), dtype=np.complex128)
+            out[f"Jpsi[{a}]_y"] = np.zeros((g.ny, g.hx), dtype=np.complex128)
+        for k in ("pi_xx", "pi_xy", "pi_yy"):
+            out[k] = np.zeros((g.ny, g.hx), dtype=np.complex128)
+        kbt = cfg.kBT * cfg.chi
+        if cfg.noise_order_parameter and kbt != 0.0:
+            pref = 2.0 * kbt * g.grid_size * g.grid_size / g.volume
+            for a in range(n):
+                M = cfg.mobility[a]
+                if M == 0.0:
+                    continue
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    sig = np.sqrt(0.5 * pref * M * k2)
+                    fx = np.where(bulk, 1j * (kx / k2) * sig * xi_psi[a], 0.0)
+                    fy = np.where(use, 1j * (ky / k2) * sig * xi_psi[a], 0.0)
+                out[f"Jpsi[{a}]_x"] = fx
+                out[f"Jpsi[{a}]_y"] = place(fy)
+        if cfg.noise_momentum and cfg.mode != "quiescent" and cfg.kBT != 0.0 and (cfg.eta != 0.0 or cfg.zeta != 0.0):
+            s = math.sqrt(0.5 * 2.0 * cfg.kBT * g.grid_size * g.grid_size / g.volume)
+            se, sz = math.sqrt(cfg.eta), math.sqrt(cfg.zeta)
+            x1, x2, x3 = xi_j
+            out["pi_xx"] = place(-s * (sz * x1 + se * x2))
+            out["pi_yy"] = place(-s * (sz * x1 - se * x2))
+            out["pi_xy"] = place(-s * se * x3)
+        return out
+
+    def step_with_flux_fields(self, u: np.ndarray, noise=None):
+        """(next state, the step's flux buffer): stage fluxes weighted 1/6, 1/6, 2/3 (SRK3) or 1
+        (Euler), the first draw's noise flux / sqrt(dt) ("philox" noise only), and in incompressible
+        dynamics the projection pressure on pi_xx, pi_yy at k != 0 (time_integrator_*.h,
+        buffer_flux.cc:170-226)."""
+        cfg, g = self.cfg, self.geo
+        step = self.step_index
+        if cfg.integrator == "euler":
+            stages, weights = [u], [1.0]
+            out = self.step(u, noise)
+        else:
+            if noise == "philox":
+                sa, sb = self.philox_noise(step)
+            elif noise is None:
+                sa = sb = np.zeros(self.shape, dtype=np.complex128)
+            else:
+                sa, sb = noise
+            u1 = self._stage(u, u, sa + BETA[0] * sb, *STAGE_WEIGHTS[0])
+            u2 = self._stage(u1, u, sa + BETA[1] * sb, *STAGE_WEIGHTS[1])
+            out = self._stage(u2, u, sa + BETA[2] * sb, *STAGE_WEIGHTS[2])
+            self.step_index += 1
+            self.time += cfg.dt
+            stages, weights = [u, u1, u2], [1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0]
+        acc: Dict[str, np.ndarray] = {}
+        for w, st in zip(weights, stages):
+            for k, v in self.flux_fields(st).items():
+                acc[k] = acc[k] + w * v if k in acc else w * v
+        if noise == "philox":
+            ids = self.mode_ids()
+            xp = [philox_normals(cfg.noise_seed, self.member, step, psi_stream(a), ids)[0] for a in range(cfg.num_order_parameters)]
+            xj = [philox_normals(cfg.noise_seed, self.member, step, j_stream(m), ids)[0] for m in range(3)]
+            for k, v in self.noise_flux_fields(xp, xj).items():
+                acc[k] = acc[k] + v / math.sqrt(cfg.dt)
+        if cfg.mode == "incompressible":
+            use = g.active & (g.k2 != 0.0)
+            kx, ky, k2 = g.kx, g.ky, np.where(use, g.k2, 1.0)
+            rx = -1j * (kx * acc["pi_xx"] + ky * acc["pi_xy"])
+            ry = -1j * (kx * acc["pi_xy"] + ky * acc["pi_yy"])
+            ph = np.where(use, -1j * (kx * rx + ky * ry) / k2, 0.0)
+            acc["pi_xx"] = acc["pi_xx"] + ph
+            acc["pi_yy"] = acc["pi_yy"] + ph
+        return out, acc
+
     def noise_flux_xy(self, xi3: np.ndarray) -> np.ndarray:
         """pi_xy of one j_sto draw (fcalculator.cc:587-700): -s sqrt(eta) xi3 on the
         active k != 0 modes with gx > 0, and on the kx = 0 line the drawn half with

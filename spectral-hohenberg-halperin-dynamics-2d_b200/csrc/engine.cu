@@ -210,6 +210,8 @@ struct shhd_engine {
     double* sk_dev = nullptr;        // FP64 structure-factor accumulator [Hx * Ky] (allocated on first use)
     double* l2_dev = nullptr;        // FP64 spectral L2 sums [field][2] (allocated on first use)
     // Yokota-Green-Kubo taps (FP64): selected modes, step flux, block integrals, sums [member][tau][mode]
+    bool fline_on[2] = {false, false};
+    FluxLineArgs fline[2]{};         // the step's flux buffer along the ky = 0 row / kx = 0 column (allocated on enable)
     bool flux0_on = false;
     Flux0Args flux0{};               // k = 0 fluxes of the last step [member][3 + 2 nop] (allocated on enable)
     bool gk_on = false;
@@ -294,7 +296,9 @@ void free_engine(shhd_engine* e) {
                     static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch), e->meas.tw_x, e->meas.tw_y, e->meas.i1,
                     e->meas.member, static_cast<void*>(e->meas.scratch), static_cast<void*>(e->flux0.acc), static_cast<void*>(e->meas.profile),
-                    static_cast<void*>(e->meas.flag), static_cast<void*>(e->meas.line)})
+                    static_cast<void*>(e->meas.flag), static_cast<void*>(e->meas.line), static_cast<void*>(e->fline[0].acc),
+                    static_cast<void*>(e->fline[1].acc), static_cast<void*>(const_cast<double2*>(e->fline[0].wtab)),
+                    static_cast<void*>(const_cast<double2*>(e->fline[1].wtab))})
         if (p) cudaFree(p);
     for (auto& kv : e->graphs) cudaGraphExecDestroy(kv.second.exec);
     e->graphs.clear();
@@ -993,6 +997,21 @@ void launch_flux0_tap(shhd_engine* e, const void* cur, double weight, int first)
     check_cuda(cudaGetLastError(), "flux0_tap launch");
 }
 
+template <typename T>
+void launch_flux_line_taps(shhd_engine* e, const void* cur, int step_off, double weight, int first, int last) {
+    for (int ax = 0; ax < 2; ++ax) {
+        if (!e->fline_on[ax]) continue;
+        const FluxLineArgs& L = e->fline[ax];
+        const double2* k0 = nullptr;
+        if (e->k0_u) k0 = cur == e->u ? e->k0_u : (cur == e->s1 ? e->k0_s1 : (cur == e->s2 ? e->k0_s2 : nullptr));
+        const long long threads = static_cast<long long>(e->P.batch) * L.nline * 32;
+        const dim3 g(static_cast<unsigned>((threads + kThreads - 1) / kThreads));
+        flux_line_tap_kernel<T><<<g, kThreads, 0, e->stream>>>(e->P, L, e->members_dev, static_cast<const T*>(e->i2), static_cast<const cplx<T>*>(cur),
+                                                                k0, e->rho0_dev, e->step_dev, step_off, weight, first, last, e->cfg.dt);
+        check_cuda(cudaGetLastError(), "flux_line_tap launch");
+    }
+}
+
 // the launches of one call of nsteps steps (step indices relative to *step_dev)
 template <typename T>
 void record_steps(shhd_engine* e, int nsteps) {
@@ -1013,6 +1032,7 @@ void record_steps(shhd_engine* e, int nsteps) {
                 // stage flux weights 1/6, 1/6, 2/3 (time_integrator_srk3_compressible.h:15-21)
                 launch_gk_tap<T>(e, cur[k], s, k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0, k == 2);
                 launch_flux0_tap<T>(e, cur[k], k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0);
+                launch_flux_line_taps<T>(e, cur[k], s, k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0, k == 2);
             }
         } else {
             launch_row<T>(e);
@@ -1021,6 +1041,7 @@ void record_steps(shhd_engine* e, int nsteps) {
             launch_col_forward<T>(e, A);
             launch_gk_tap<T>(e, e->u, s, 1.0, 1, 1);
             launch_flux0_tap<T>(e, e->u, 1.0, 1);
+            launch_flux_line_taps<T>(e, e->u, s, 1.0, 1, 1);
             std::swap(e->u, e->s1);
             std::swap(e->k0_u, e->k0_s1);
         }
@@ -2069,6 +2090,82 @@ int shhd_engine_flux0_enable(shhd_engine* e) {
         e->flux0 = F;
         e->flux0_on = true;
         drop_graphs(e);  // captured graphs do not hold the tap yet
+    });
+}
+
+int shhd_engine_flux_line_enable(shhd_engine* e, int axis) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (axis != 0 && axis != 1) throw Failure(SHHD_EINVAL, "ave/profile measure: axis must be x|y|0|1.");
+        if (e->fline_on[axis]) return;
+        const StepPlan& P = e->P;
+        const bool noisy = P.noise_j || [&] { for (int a = 0; a < P.nop; ++a) if (P.noise_psi[a]) return true; return false; }();
+        if (noisy && e->cfg.noise_source == SHHD_NOISE_EXTERNAL)
+            throw Failure(SHHD_EUNSUPPORTED, "the flux buffer needs the engine's own noise draws (replayed noise gives only its divergence)");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        FluxLineArgs L{};
+        L.axis = axis;
+        L.nline = axis == 0 ? P.hx : P.kyn;
+        L.ncomp = 3 + 2 * P.nop;
+        L.pair_layout = e->pair_path ? 1 : 0;
+        L.o_vx = L.o_vy = L.o_pxx = L.o_pxy = L.o_pyy = -1;
+        for (int a = 0; a < kMaxOp; ++a) L.o_mu[a] = L.o_px[a] = L.o_py[a] = -1;
+        for (int o = 0; o < P.n_out; ++o) {
+            const int k = P.out_kind[o], a = P.out_arg[o];
+            if (k == OUT_VX) L.o_vx = o;
+            if (k == OUT_VY) L.o_vy = o;
+            if (k == OUT_PXX) L.o_pxx = o;
+            if (k == OUT_PXY) L.o_pxy = o;
+            if (k == OUT_PYY) L.o_pyy = o;
+            if (k == OUT_MU) L.o_mu[a] = o;
+            if (k == OUT_PSIVX) L.o_px[a] = o;
+            if (k == OUT_PSIVY) L.o_py[a] = o;
+        }
+        // the reference's conditions (fcalculator.cc:86-150)
+        const shhd_config& c = e->cfg;
+        const bool has_visc = c.eta != 0.0 || c.zeta != 0.0;
+        L.mom_on = c.mode != SHHD_QUIESCENT && (P.cT2 != 0.0 || has_visc || c.momentum_advection);
+        L.pressure = L.mom_on && P.cT2 != 0.0;
+        L.visc_comp = L.mom_on && has_visc && c.mode == SHHD_COMPRESSIBLE;
+        L.visc_incomp = L.mom_on && c.mode == SHHD_INCOMPRESSIBLE && c.eta != 0.0;
+        if (L.visc_comp && (L.o_vx < 0 || L.o_vy < 0)) throw Failure(SHHD_EUNSUPPORTED, "viscous flux planes missing");
+        for (int a = 0; a < P.nop; ++a) {
+            L.psi_on[a] = c.mobility[a] != 0.0 || c.order_parameter_advection;
+            L.psi_lin[a] = c.mobility[a] != 0.0 && (P.mu_k0[a] != 0.0 || P.mu_k2[a] != 0.0 || P.mu_k4[a] != 0.0);
+            if (c.mobility[a] == 0.0) L.o_mu[a] = -1;
+        }
+        L.noise_j = P.noise_j;
+        L.incompressible = c.mode == SHHD_INCOMPRESSIBLE;
+        std::vector<double2> wt(P.npy);
+        for (int n = 0; n < P.npy; ++n) {
+            const double ang = -2.0 * M_PI * n / P.npy;
+            wt[n] = make_double2(std::cos(ang), std::sin(ang));
+        }
+        L.wtab = static_cast<const double2*>(dalloc(e, sizeof(double2) * P.npy));
+        check_cuda(cudaMemcpyAsync(const_cast<double2*>(L.wtab), wt.data(), sizeof(double2) * P.npy, cudaMemcpyHostToDevice, e->stream), "upload");
+        const size_t bytes = sizeof(double2) * e->cfg.batch * L.ncomp * L.nline;
+        L.acc = static_cast<double2*>(dalloc(e, bytes));
+        check_cuda(cudaMemsetAsync(L.acc, 0, bytes, e->stream), "memset");
+        check_cuda(cudaStreamSynchronize(e->stream), "flux line sync");
+        e->fline[axis] = L;
+        e->fline_on[axis] = true;
+        drop_graphs(e);  // captured graphs do not hold the tap yet
+    });
+}
+
+int shhd_engine_flux_line_read(shhd_engine* e, int axis, int member, double* out, size_t n) {
+    return guarded([&] {
+        if (!e || !out) throw Failure(SHHD_EINVAL, "null argument");
+        if (axis != 0 && axis != 1) throw Failure(SHHD_EINVAL, "ave/profile measure: axis must be x|y|0|1.");
+        if (!e->fline_on[axis]) throw Failure(SHHD_EINVAL, "the flux line tap of this axis is not enabled");
+        if (member < 0 || member >= e->cfg.batch) throw Failure(SHHD_EINVAL, "member index out of range");
+        const FluxLineArgs& L = e->fline[axis];
+        const size_t cnt = static_cast<size_t>(L.ncomp) * L.nline;
+        if (n < 2 * cnt) throw Failure(SHHD_EINVAL, "flux line read needs " + std::to_string(2 * cnt) + " doubles");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        check_cuda(cudaMemcpyAsync(out, L.acc + static_cast<size_t>(member) * cnt, sizeof(double2) * cnt, cudaMemcpyDeviceToHost, e->stream),
+                   "flux line read");
+        check_cuda(cudaStreamSynchronize(e->stream), "flux line sync");
     });
 }
 

@@ -796,15 +796,18 @@ struct GkArgs {
     double kbt, area, cell_area;
 };
 
+// forward y-transform at ky of column gx of one I2 plane (x-transformed, y-physical): the plane's 2-D
+// coefficient at (gx, ky); one warp, FP64 sums; wtab[n] = exp(-2 pi i n / npy)
 template <typename T>
-__device__ __forceinline__ double2 gk_column_dft(const StepPlan& P, const GkArgs& G, const T* plane, int gx, int ky) {
+__device__ __forceinline__ double2 column_dft(const StepPlan& P, const double2* __restrict__ wtab, int pair_layout, const T* plane, int gx,
+                                              int ky) {
     const int npy = P.npy;
     const int t = gx / P.W, w = gx - t * P.W;
     const long long kk = ((ky % npy) + npy) % npy;
     double re = 0.0, im = 0.0;
     for (int y = threadIdx.x & 31; y < npy; y += 32) {
         T xr, xi;
-        if (G.pair_layout) {
+        if (pair_layout) {
             const T* e = plane + 4 * (static_cast<size_t>(t) * npy + y);
             xr = e[w];
             xi = e[2 + w];
@@ -813,7 +816,7 @@ __device__ __forceinline__ double2 gk_column_dft(const StepPlan& P, const GkArgs
             xr = e[0];
             xi = e[1];
         }
-        const double2 tw = G.wtab[(kk * y) % npy];
+        const double2 tw = wtab[(kk * y) % npy];
         re += static_cast<double>(xr) * tw.x - static_cast<double>(xi) * tw.y;
         im += static_cast<double>(xr) * tw.y + static_cast<double>(xi) * tw.x;
     }
@@ -822,6 +825,11 @@ __device__ __forceinline__ double2 gk_column_dft(const StepPlan& P, const GkArgs
         im += __shfl_xor_sync(0xffffffffu, im, o);
     }
     return make_double2(re, im);
+}
+
+template <typename T>
+__device__ __forceinline__ double2 gk_column_dft(const StepPlan& P, const GkArgs& G, const T* plane, int gx, int ky) {
+    return column_dft<T>(P, G.wtab, G.pair_layout, plane, gx, ky);
 }
 
 template <typename T>
@@ -894,6 +902,149 @@ __global__ void __launch_bounds__(kThreads) gk_tap_kernel(const StepPlan P, cons
         G.sums[(static_cast<size_t>(b) * G.ntau + ti) * G.nmodes + i] += (I.x * I.x + I.y * I.y) / (2.0 * tau * kbt * G.area);
     }
     *in = I;
+}
+
+// ---------------------------------------------------------------------------
+// the step's flux buffer along one spectral line, for the ave/profile flux
+// targets (measure_ave_profile.cc:216-238): axis 0 the ky = 0 row (gx < hx),
+// axis 1 the kx = 0 column (engine ky order).  Per stage, the stage's flux
+// weight times every flux the deterministic RHS records at the line's modes
+// (fcalculator.cc:86-494: -i M k mu from the linear and physical chemical
+// potential, psi v, cT^2 rho, the viscous stresses, j v); after the last stage
+// the first noise draw's flux / sqrt(dt) (fcalculator.cc:496-700) and, in
+// incompressible dynamics, the projection pressure (buffer_flux.cc:196-226).
+// acc[member][comp][nline], comp = pi_xx, pi_xy, pi_yy, then Jpsi[a]_x,
+// Jpsi[a]_y; one warp per (member, line mode); the first stage overwrites
+// ---------------------------------------------------------------------------
+struct FluxLineArgs {
+    double2* acc;
+    int axis, nline, ncomp;
+    const double2* wtab;          // exp(-2 pi i n / npy)
+    int pair_layout;
+    int mom_on;                   // j_det records anything
+    int pressure;                 // linear pressure cT^2 rho on the diagonal
+    int visc_comp, visc_incomp;   // compressible viscous stress from the VX, VY planes; incompressible from j / rho0
+    int o_vx, o_vy, o_pxx, o_pxy, o_pyy;
+    int psi_on[kMaxOp];           // psi_det records anything
+    int psi_lin[kMaxOp];          // linear chemical-potential flux
+    int o_mu[kMaxOp], o_px[kMaxOp], o_py[kMaxOp];
+    int noise_j;                  // the momentum noise flux
+    int incompressible;
+};
+
+__device__ __forceinline__ double2 cmi(double2 a) { return make_double2(a.y, -a.x); }  // -i a
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 dscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) flux_line_tap_kernel(const StepPlan P, const FluxLineArgs L, const MemberInfo* __restrict__ members,
+                                                                 const T* __restrict__ i2, const cplx<T>* __restrict__ cur,
+                                                                 const double2* __restrict__ k0cur, const double* __restrict__ rho0,
+                                                                 const unsigned long long* __restrict__ step_base, int step_off, double weight,
+                                                                 int first, int last, double dt) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= P.batch * L.nline) return;
+    const int b = warp / L.nline, i = warp - b * L.nline;
+    const MemberInfo mi = members[b];
+    if (!mi.active) return;
+    const int gx = L.axis == 0 ? i : 0;
+    const int ky = L.axis == 0 ? 0 : ky_of_j(i, P.nay);
+    const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky, k2 = kx * kx + kyv * kyv;
+    const bool zero = gx == 0 && ky == 0;
+    const size_t plane = static_cast<size_t>(P.hx) * P.npy * 2;
+    const T* base = i2 + static_cast<size_t>(b) * P.n_out * plane;
+    const size_t fst = static_cast<size_t>(P.hx) * P.kyn;
+    const size_t pos = static_cast<size_t>(b) * P.nfields * fst + static_cast<size_t>(gx) * P.kyn + (ky >= 0 ? ky : ky + P.kyn);
+    auto sv = [&](int f) {
+        if (zero && k0cur) return k0cur[static_cast<size_t>(b) * P.nfields + f];
+        const cplx<T> v = cur[pos + f * fst];
+        return make_double2(static_cast<double>(v.x), static_cast<double>(v.y));
+    };
+    auto dft = [&](int o) { return column_dft<T>(P, L.wtab, L.pair_layout, base + o * plane, gx, ky); };
+    double2 F[3 + 2 * kMaxOp];
+    for (int c = 0; c < 3 + 2 * kMaxOp; ++c) F[c] = make_double2(0.0, 0.0);
+    if (L.mom_on) {
+        if (L.pressure) {
+            const double2 pr = dscale(sv(0), P.cT2);
+            F[0] = dadd(F[0], pr);
+            F[2] = dadd(F[2], pr);
+        }
+        if (L.visc_incomp) {
+            const double r0 = 1.0 / rho0[b];
+            const double2 vx = dscale(sv(P.nop + 1), r0), vy = dscale(sv(P.nop + 2), r0);
+            F[0] = dadd(F[0], cmi(dscale(vx, P.eta * 2.0 * kx)));
+            F[1] = dadd(F[1], cmi(dscale(dadd(dscale(vx, kyv), dscale(vy, kx)), P.eta)));
+            F[2] = dadd(F[2], cmi(dscale(vy, P.eta * 2.0 * kyv)));
+        }
+        if (L.visc_comp) {
+            const double2 vx = dft(L.o_vx), vy = dft(L.o_vy);
+            const double2 kv = dadd(dscale(vx, kx), dscale(vy, kyv));
+            F[0] = dadd(F[0], cmi(dadd(dscale(vx, 2.0 * P.eta * kx), dscale(kv, -(P.eta - P.zeta)))));
+            F[1] = dadd(F[1], cmi(dscale(dadd(dscale(vx, kyv), dscale(vy, kx)), P.eta)));
+            F[2] = dadd(F[2], cmi(dadd(dscale(vy, 2.0 * P.eta * kyv), dscale(kv, -(P.eta - P.zeta)))));
+        }
+        if (L.o_pxx >= 0) F[0] = dadd(F[0], dft(L.o_pxx));
+        if (L.o_pxy >= 0) F[1] = dadd(F[1], dft(L.o_pxy));
+        if (L.o_pyy >= 0) F[2] = dadd(F[2], dft(L.o_pyy));
+    }
+    for (int a = 0; a < P.nop; ++a) {
+        if (!L.psi_on[a]) continue;
+        const double M = P.mobility[a];
+        if (L.psi_lin[a]) {
+            const double2 mu = dscale(sv(1 + a), P.mu_k0[a] + P.mu_k2[a] * k2 + P.mu_k4[a] * k2 * k2);
+            F[3 + 2 * a] = dadd(F[3 + 2 * a], cmi(dscale(mu, M * kx)));
+            F[4 + 2 * a] = dadd(F[4 + 2 * a], cmi(dscale(mu, M * kyv)));
+        }
+        if (L.o_mu[a] >= 0) {
+            const double2 mu = dft(L.o_mu[a]);
+            F[3 + 2 * a] = dadd(F[3 + 2 * a], cmi(dscale(mu, M * kx)));
+            F[4 + 2 * a] = dadd(F[4 + 2 * a], cmi(dscale(mu, M * kyv)));
+        }
+        if (L.o_px[a] >= 0) F[3 + 2 * a] = dadd(F[3 + 2 * a], dft(L.o_px[a]));
+        if (L.o_py[a] >= 0) F[4 + 2 * a] = dadd(F[4 + 2 * a], dft(L.o_py[a]));
+    }
+    if (lane != 0) return;
+    double2* acc = L.acc + static_cast<size_t>(b) * L.ncomp * L.nline + i;
+    for (int c = 0; c < L.ncomp; ++c) {
+        double2& a = acc[static_cast<size_t>(c) * L.nline];
+        a = first ? dscale(F[c], weight) : dadd(a, dscale(F[c], weight));
+    }
+    if (!last || zero) return;
+    // the first draw of psi_sto / j_sto (the engine's own, as the epilogue drew it), / sqrt(dt)
+    const uint64_t step = *step_base + static_cast<uint64_t>(step_off) - static_cast<uint64_t>(mi.step0);
+    const bool conj_line = gx == 0 && ky < 0;
+    const int aky = conj_line ? -ky : ky;
+    const uint32_t mode_id = static_cast<uint32_t>(gx) * static_cast<uint32_t>(P.nay) + static_cast<uint32_t>((aky % P.nay + P.nay) % P.nay);
+    const double isdt = 1.0 / sqrt(dt);
+    auto draw = [&](uint32_t stream) {
+        cplx<T> xa, xb;
+        complex_normals<T>(P.seed, mi.key, step, stream, mode_id, false, xa, xb);
+        return make_double2(static_cast<double>(xa.x), conj_line ? -static_cast<double>(xa.y) : static_cast<double>(xa.y));
+    };
+    if (L.noise_j) {
+        const double2 x0 = draw(j_stream(0)), x1 = draw(j_stream(1)), x2 = draw(j_stream(2));
+        const double s = -P.j_s * mi.noise_scale * isdt;
+        acc[0] = dadd(acc[0], dscale(dadd(dscale(x0, P.sqrt_zeta), dscale(x1, P.sqrt_eta)), s));
+        acc[2 * static_cast<size_t>(L.nline)] = dadd(acc[2 * static_cast<size_t>(L.nline)], dscale(dadd(dscale(x0, P.sqrt_zeta), dscale(x1, -P.sqrt_eta)), s));
+        acc[static_cast<size_t>(L.nline)] = dadd(acc[static_cast<size_t>(L.nline)], dscale(x2, s * P.sqrt_eta));
+    }
+    for (int a = 0; a < P.nop; ++a) {
+        if (!P.noise_psi[a]) continue;
+        const double2 x = draw(psi_stream(a));
+        const double sig = sqrt(P.psi_sig2[a] * k2) * mi.noise_scale * isdt;
+        // i k / k^2 sigma x; no x-component on the kx = 0 line
+        const double2 ix = make_double2(-x.y, x.x);
+        if (gx != 0) acc[static_cast<size_t>(3 + 2 * a) * L.nline] = dadd(acc[static_cast<size_t>(3 + 2 * a) * L.nline], dscale(ix, sig * kx / k2));
+        acc[static_cast<size_t>(4 + 2 * a) * L.nline] = dadd(acc[static_cast<size_t>(4 + 2 * a) * L.nline], dscale(ix, sig * kyv / k2));
+    }
+    if (L.incompressible) {
+        const double2 xx = acc[0], xy = acc[L.nline], yy = acc[2 * static_cast<size_t>(L.nline)];
+        const double2 rx = cmi(dadd(dscale(xx, kx), dscale(xy, kyv))), ry = cmi(dadd(dscale(xy, kx), dscale(yy, kyv)));
+        const double2 ph = dscale(cmi(dadd(dscale(rx, kx), dscale(ry, kyv))), 1.0 / k2);
+        acc[0] = dadd(xx, ph);
+        acc[2 * static_cast<size_t>(L.nline)] = dadd(yy, ph);
+    }
 }
 
 // ---------------------------------------------------------------------------

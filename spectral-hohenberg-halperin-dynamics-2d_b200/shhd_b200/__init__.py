@@ -126,6 +126,7 @@ EXPORTED = (
     "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums", "shhd_engine_set_gaussian_field",
     "shhd_engine_set_initial_field", "shhd_engine_check_transverse", "shhd_engine_energies",
     "shhd_engine_flux0_enable", "shhd_engine_flux0_read", "shhd_engine_profile_line", "shhd_engine_profile_velocity",
+    "shhd_engine_flux_line_enable", "shhd_engine_flux_line_read",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -176,6 +177,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_flux0_read.argtypes = [vp, i, dp, sz]
     lib.shhd_engine_profile_line.argtypes = [vp, i, i, i, dp, sz]
     lib.shhd_engine_profile_velocity.argtypes = [vp, i, i, i, dp, sz]
+    lib.shhd_engine_flux_line_enable.argtypes = [vp, i]
+    lib.shhd_engine_flux_line_read.argtypes = [vp, i, i, dp, sz]
     return lib
 
 
@@ -357,6 +360,20 @@ class Engine:
         raw = np.zeros(n, dtype=np.float64)
         _check(lib.shhd_engine_profile_velocity(self._h, int(member), int(component), int(axis), _dptr(raw), raw.size))
         return raw
+
+    def flux_line_enable(self, axis: int) -> None:
+        """Record the step's flux buffer along the ky = 0 row (axis 0) or kx = 0 column (axis 1)."""
+        _check(lib.shhd_engine_flux_line_enable(self._h, int(axis)))
+
+    def flux_line(self, axis: int, member: int = 0) -> dict:
+        """The last step's fluxes along the line, {pi_xx, pi_xy, pi_yy, Jpsi[a]_x, Jpsi[a]_y: complex128}."""
+        n = self.cfg.num_order_parameters
+        nline = self.cfg.active_nx // 2 if axis == 0 else self.cfg.active_ny - 1
+        raw = np.zeros(2 * (3 + 2 * n) * nline, dtype=np.float64)
+        _check(lib.shhd_engine_flux_line_read(self._h, int(axis), int(member), _dptr(raw), raw.size))
+        z = raw.view(np.complex128).reshape(3 + 2 * n, nline)
+        names = ["pi_xx", "pi_xy", "pi_yy"] + [f"Jpsi[{a}]_{d}" for a in range(n) for d in "xy"]
+        return {k: z[c].copy() for c, k in enumerate(names)}
 
     def time_series_l2(self, member: int = 0) -> dict:
         """The reference time-series measure's spectral L2 columns of the current state (FP64)."""

@@ -221,7 +221,8 @@ class AveProfile:
     targets (rho, psi[a], jx, jy; vx, vy = j / rho0 outside compressible dynamics) accumulate
     the one spectral line the transverse average needs, read from the device in FP64; the
     compressible vx, vy are summed over the transverse axis on the device per sample.  The flux
-    targets (pi_*, Jpsi[a]_*) need the full flux buffer and are not produced.
+    targets (pi_xx pi_xy pi_yy, with the aliases pixx pixy piyy, and Jpsi[a]_x Jpsi[a]_y) read
+    the last step's flux buffer along the same line from the engine's flux-line tap.
     """
 
     def __init__(self, engine, file: str, axis: str, nevery: int, nblock: int, average: str, targets: List[str], member: int = 0):
@@ -240,11 +241,15 @@ class AveProfile:
         nop = cfg.num_order_parameters
         self.targets = []   # (name, kind, field index / component)
         for t in targets:
-            if t in _PROFILE_FLUX or _PROFILE_JPSI.match(t):
-                j = _PROFILE_JPSI.match(t)
-                if j and not 0 <= int(j.group(1)) < nop:
+            if t in _PROFILE_FLUX:
+                self.targets.append((_PROFILE_FLUX[t], "flux", _PROFILE_FLUX[t], None))
+                continue
+            j = _PROFILE_JPSI.match(t)
+            if j:
+                if not 0 <= int(j.group(1)) < nop:
                     raise ValueError(f"ave/profile target order-parameter index out of range: {t}")
-                raise NotImplementedError(f"ave/profile target {t}: the flux buffer is not kept by the engine")
+                self.targets.append((t, "flux", t, None))
+                continue
             m = _PROFILE_PSI.match(t)
             if m:
                 a = int(m.group(1))
@@ -274,6 +279,8 @@ class AveProfile:
         self._block = [None] * len(self.targets)
         self._running = [None] * len(self.targets)
         self._out: Optional[TextIO] = None
+        if any(kind == "flux" for _n, kind, _i, _s in self.targets):
+            engine.flux_line_enable(self.axis)
 
     def _reference_density(self) -> float:
         """Re rho(0) / Ng of the first sample that needs it (measure_ave_profile.cc:123-149)."""
@@ -286,9 +293,14 @@ class AveProfile:
         return self._rho0
 
     def _sample(self) -> None:
+        flux = None
         for i, (_name, kind, idx, _scale) in enumerate(self.targets):
             if kind == "velocity":
                 v = self.engine.profile_velocity(idx, self.axis, self.member)
+            elif kind == "flux":
+                if flux is None:
+                    flux = self.engine.flux_line(self.axis, self.member)
+                v = flux[idx]
             else:
                 v = self.engine.profile_line(idx, self.axis, self.member)
                 if kind == "spectral_v":

@@ -267,3 +267,33 @@ PROFILE_CASES = {
         "measure p1 ave/profile on axis y nevery 1 nblock 2 file @DIR@/py.dat average running target vx vy rho jx",
     ]),
 }
+
+
+# ave/profile flux targets on noise-free copies of step cases (the reference's
+# flux buffer then holds only the deterministic stage fluxes, which the engine
+# reproduces without replaying the reference's noise); 6 steps each.
+def _noiseless(name):
+    return "\n".join(ln for ln in CASES[name].splitlines() if not (ln.startswith("fix") and " noise " in ln)) + "\n"
+
+
+def _flux_profiled(name, lines, nsteps=6):
+    body = _noiseless(name).rsplit("run ", 1)[0]
+    return body + "\n".join(lines + [f"run {nsteps}"]) + "\n"
+
+
+FLUX_PROFILE_CASES = {
+    "fluxprof_srk3_compressible_n2": _flux_profiled("srk3_compressible_n2", [
+        "measure p1 ave/profile on axis y nevery 1 nblock 3 file @DIR@/py_block.dat average block target pi_xx pi_xy pi_yy Jpsi[0]_x Jpsi[1]_y",
+        "measure p2 ave/profile on axis x nevery 2 nblock 2 file @DIR@/px_running.dat average running target pixy Jpsi[0]_y piyy Jpsi[1]_x rho",
+    ]),
+    "fluxprof_srk3_incompressible_n1_forces": _flux_profiled("srk3_incompressible_n1_forces", [
+        "measure p1 ave/profile on axis y nevery 1 nblock 3 file @DIR@/py_block.dat average block target vx pi_xy pi_xx pi_yy Jpsi[0]_y",
+        "measure p2 ave/profile on axis x nevery 1 nblock 2 file @DIR@/px_running.dat average running target pi_xx Jpsi[0]_x pi_yy",
+    ]),
+    "fluxprof_euler_compressible_n2": _flux_profiled("euler_compressible_n2", [
+        "measure p1 ave/profile on axis x nevery 1 nblock 3 file @DIR@/px_block.dat average block target pi_xx pi_xy pi_yy Jpsi[0]_x Jpsi[0]_y",
+    ]),
+    "fluxprof_euler_quiescent_n2_quadratic": _flux_profiled("euler_quiescent_n2_quadratic", [
+        "measure p1 ave/profile on axis y nevery 1 nblock 2 file @DIR@/py.dat average running target Jpsi[0]_y Jpsi[1]_x psi[1]",
+    ]),
+}
