@@ -409,6 +409,50 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_measures(sb, torch, world):
+    """The device measures on the headline workload (1024^2, N = 2, FP32): wall time of one call
+    (launches, FP64 reduction, read-back), and the step rate with the per-stage flux taps on."""
+    import time as _time
+    from shhd_b200.initial import initial_state_device
+    cfg = sb.config_from_script(WORKLOAD)
+    cfg.precision = sb.FP32
+    eng = sb.Engine(cfg)
+    initial_state_device(eng, WORKLOAD)
+    eng.step(2)
+
+    def wall_ms(fn, reps=5):
+        fn()
+        t0 = _time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (_time.perf_counter() - t0) / reps * 1e3
+
+    def rate(n=30):
+        stream = torch.cuda.ExternalStream(eng.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        eng.step(3)
+        eng.synchronize()
+        e0.record(stream)
+        eng.step_async(n)
+        e1.record(stream)
+        eng.synchronize()
+        return world * n / (max_over_ranks(e0.elapsed_time(e1), world) / 1e3)
+
+    out = {"energies_ms": wall_ms(eng.time_series_energies), "l2_ms": wall_ms(eng.time_series_l2),
+           "profile_line_ms": wall_ms(lambda: eng.profile_line(0, 1)), "profile_velocity_x_ms": wall_ms(lambda: eng.profile_velocity(0, 0)),
+           "steps_per_s_plain": rate()}
+    eng.flux0_enable()
+    out["steps_per_s_with_k0_flux_tap"] = rate()
+    eng.flux_line_enable(1)
+    out["steps_per_s_with_k0_and_flux_line_y_taps"] = rate()
+    out["flux_line_read_ms"] = wall_ms(lambda: eng.flux_line(1))
+    out["what"] = ("1024^2 (3/2 -> 1536^2), N = 2, FP32 engine: wall time per measure call (E_T..E_C with the physical-space "
+                   "transforms; L2 columns; one spectral profile line; the compressible vx profile over x); step rate "
+                   "without taps, with the k = 0 flux tap, and with the kx = 0 flux-line tap added (1535 modes, every flux)")
+    eng.close()
+    return out
+
+
 def run_extras(args, world, rank, local, sb, initial_state, torch):
     out = {}
     # the plain one-job-at-a-time FP64 path on the same workload
@@ -429,16 +473,18 @@ def run_extras(args, world, rank, local, sb, initial_state, torch):
     out["fp64_plain"] = {"value": world * n64 / (ms / 1e3), "unit": UNIT, "steps": n64}
     eng.close()
 
+    out["measures"] = run_measures(sb, torch, world)
+
     # batched ensemble: 256 members advanced together
     cfg = sb.config_from_script(ENSEMBLE)
     cfg.precision = sb.FP32
     cfg.batch = 256
     cfg.member_offset = rank * 256
     eng = sb.Engine(cfg)
-    base = initial_state(cfg, ENSEMBLE)
+    from shhd_b200.initial import initial_state_device
     for m in range(cfg.batch):
-        # member m: seed m (the ensemble draws psi0 per member seed)
-        eng.set_state(initial_state(cfg, ENSEMBLE.replace("all equilibrium/gaussian seed 0 ", f"all equilibrium/gaussian seed {m} ")) if m else base, member=m)
+        # member m: seed m (the ensemble draws psi0 per member seed), generated on the device
+        initial_state_device(eng, ENSEMBLE.replace("all equilibrium/gaussian seed 0 ", f"all equilibrium/gaussian seed {m} "), member=m)
     eng.step(2)
     nb = max(3, min(args.steps, 50))
     stream = torch.cuda.ExternalStream(eng.stream)

@@ -803,9 +803,13 @@ __device__ __forceinline__ double2 column_dft(const StepPlan& P, const double2* 
                                               int ky) {
     const int npy = P.npy;
     const int t = gx / P.W, w = gx - t * P.W;
-    const long long kk = ((ky % npy) + npy) % npy;
+    const int kk = ((ky % npy) + npy) % npy;
+    // twiddle index kk * y mod npy, stepped by kk * 32 mod npy from lane to lane's next row
+    const int lane = threadIdx.x & 31;
+    int idx = static_cast<int>((static_cast<long long>(kk) * lane) % npy);
+    const int stride = static_cast<int>((static_cast<long long>(kk) * 32) % npy);
     double re = 0.0, im = 0.0;
-    for (int y = threadIdx.x & 31; y < npy; y += 32) {
+    for (int y = lane; y < npy; y += 32) {
         T xr, xi;
         if (pair_layout) {
             const T* e = plane + 4 * (static_cast<size_t>(t) * npy + y);
@@ -816,7 +820,9 @@ __device__ __forceinline__ double2 column_dft(const StepPlan& P, const double2* 
             xr = e[0];
             xi = e[1];
         }
-        const double2 tw = wtab[(kk * y) % npy];
+        const double2 tw = wtab[idx];
+        idx += stride;
+        if (idx >= npy) idx -= npy;
         re += static_cast<double>(xr) * tw.x - static_cast<double>(xi) * tw.y;
         im += static_cast<double>(xr) * tw.y + static_cast<double>(xi) * tw.x;
     }
