@@ -1004,10 +1004,11 @@ void launch_flux_line_taps(shhd_engine* e, const void* cur, int step_off, double
         const FluxLineArgs& L = e->fline[ax];
         const double2* k0 = nullptr;
         if (e->k0_u) k0 = cur == e->u ? e->k0_u : (cur == e->s1 ? e->k0_s1 : (cur == e->s2 ? e->k0_s2 : nullptr));
-        const long long threads = static_cast<long long>(e->P.batch) * L.nline * 32;
-        const dim3 g(static_cast<unsigned>((threads + kThreads - 1) / kThreads));
-        flux_line_tap_kernel<T><<<g, kThreads, 0, e->stream>>>(e->P, L, e->members_dev, static_cast<const T*>(e->i2), static_cast<const cplx<T>*>(cur),
-                                                                k0, e->rho0_dev, e->step_dev, step_off, weight, first, last, e->cfg.dt);
+        const dim3 g(static_cast<unsigned>((L.nline + kThreads / 32 - 1) / (kThreads / 32)), static_cast<unsigned>(e->P.batch));
+        const size_t smem = ax == 1 ? sizeof(double2) * e->P.npy : 0;
+        flux_line_tap_kernel<T><<<g, kThreads, smem, e->stream>>>(e->P, L, e->members_dev, static_cast<const T*>(e->i2),
+                                                                   static_cast<const cplx<T>*>(cur), k0, e->rho0_dev, e->step_dev, step_off, weight,
+                                                                   first, last, e->cfg.dt);
         check_cuda(cudaGetLastError(), "flux_line_tap launch");
     }
 }
@@ -2141,6 +2142,9 @@ int shhd_engine_flux_line_enable(shhd_engine* e, int axis) {
             const double ang = -2.0 * M_PI * n / P.npy;
             wt[n] = make_double2(std::cos(ang), std::sin(ang));
         }
+        if (axis == 1) raise_smem_limit(reinterpret_cast<const void*>(e->fp32 ? reinterpret_cast<const void*>(flux_line_tap_kernel<float>)
+                                                                                : reinterpret_cast<const void*>(flux_line_tap_kernel<double>)),
+                                         sizeof(double2) * P.npy);
         L.wtab = static_cast<const double2*>(dalloc(e, sizeof(double2) * P.npy));
         check_cuda(cudaMemcpyAsync(const_cast<double2*>(L.wtab), wt.data(), sizeof(double2) * P.npy, cudaMemcpyHostToDevice, e->stream), "upload");
         const size_t bytes = sizeof(double2) * e->cfg.batch * L.ncomp * L.nline;

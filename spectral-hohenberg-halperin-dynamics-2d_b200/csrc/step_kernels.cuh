@@ -920,7 +920,10 @@ __global__ void __launch_bounds__(kThreads) gk_tap_kernel(const StepPlan P, cons
 // the first noise draw's flux / sqrt(dt) (fcalculator.cc:496-700) and, in
 // incompressible dynamics, the projection pressure (buffer_flux.cc:196-226).
 // acc[member][comp][nline], comp = pi_xx, pi_xy, pi_yy, then Jpsi[a]_x,
-// Jpsi[a]_y; one warp per (member, line mode); the first stage overwrites
+// Jpsi[a]_y; one warp per line mode, 8 modes per block, grid (ceil(nline / 8),
+// batch); on the kx = 0 column every mode transforms the same column of each
+// product plane, so the block stages it once in shared memory (npy x 16 bytes);
+// the first stage overwrites
 // ---------------------------------------------------------------------------
 struct FluxLineArgs {
     double2* acc;
@@ -948,14 +951,15 @@ __global__ void __launch_bounds__(kThreads) flux_line_tap_kernel(const StepPlan 
                                                                  const double2* __restrict__ k0cur, const double* __restrict__ rho0,
                                                                  const unsigned long long* __restrict__ step_base, int step_off, double weight,
                                                                  int first, int last, double dt) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    extern __shared__ double2 col[];   // npy entries (kx = 0 column only)
     const int lane = threadIdx.x & 31;
-    if (warp >= P.batch * L.nline) return;
-    const int b = warp / L.nline, i = warp - b * L.nline;
+    const int b = blockIdx.y;
+    const int i = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+    const bool valid = i < L.nline;
     const MemberInfo mi = members[b];
-    if (!mi.active) return;
-    const int gx = L.axis == 0 ? i : 0;
-    const int ky = L.axis == 0 ? 0 : ky_of_j(i, P.nay);
+    if (!mi.active) return;            // block-uniform
+    const int gx = L.axis == 0 ? (valid ? i : 0) : 0;
+    const int ky = L.axis == 0 ? 0 : (valid ? ky_of_j(i, P.nay) : 0);
     const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky, k2 = kx * kx + kyv * kyv;
     const bool zero = gx == 0 && ky == 0;
     const size_t plane = static_cast<size_t>(P.hx) * P.npy * 2;
@@ -967,7 +971,34 @@ __global__ void __launch_bounds__(kThreads) flux_line_tap_kernel(const StepPlan 
         const cplx<T> v = cur[pos + f * fst];
         return make_double2(static_cast<double>(v.x), static_cast<double>(v.y));
     };
-    auto dft = [&](int o) { return column_dft<T>(P, L.wtab, L.pair_layout, base + o * plane, gx, ky); };
+    auto dft = [&](int o) {
+        if (L.axis == 0) return column_dft<T>(P, L.wtab, L.pair_layout, base + o * plane, gx, ky);
+        // kx = 0 column: stage column 0 of plane o once for the block, then one DFT per warp
+        const T* pl = base + o * plane;
+        __syncthreads();
+        for (int y = threadIdx.x; y < P.npy; y += blockDim.x) {
+            const T* e = L.pair_layout ? pl + 4 * static_cast<size_t>(y) : pl + 2 * static_cast<size_t>(y) * P.W;
+            col[y] = make_double2(static_cast<double>(e[0]), static_cast<double>(e[L.pair_layout ? 2 : 1]));
+        }
+        __syncthreads();
+        const int npy = P.npy;
+        const int kk = ((ky % npy) + npy) % npy;
+        int idx = static_cast<int>((static_cast<long long>(kk) * lane) % npy);
+        const int stride = static_cast<int>((static_cast<long long>(kk) * 32) % npy);
+        double re = 0.0, im = 0.0;
+        for (int y = lane; y < npy; y += 32) {
+            const double2 x = col[y], tw = L.wtab[idx];
+            re += x.x * tw.x - x.y * tw.y;
+            im += x.x * tw.y + x.y * tw.x;
+            idx += stride;
+            if (idx >= npy) idx -= npy;
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            re += __shfl_xor_sync(0xffffffffu, re, off);
+            im += __shfl_xor_sync(0xffffffffu, im, off);
+        }
+        return make_double2(re, im);
+    };
     double2 F[3 + 2 * kMaxOp];
     for (int c = 0; c < 3 + 2 * kMaxOp; ++c) F[c] = make_double2(0.0, 0.0);
     if (L.mom_on) {
@@ -1010,7 +1041,7 @@ __global__ void __launch_bounds__(kThreads) flux_line_tap_kernel(const StepPlan 
         if (L.o_px[a] >= 0) F[3 + 2 * a] = dadd(F[3 + 2 * a], dft(L.o_px[a]));
         if (L.o_py[a] >= 0) F[4 + 2 * a] = dadd(F[4 + 2 * a], dft(L.o_py[a]));
     }
-    if (lane != 0) return;
+    if (lane != 0 || !valid) return;
     double2* acc = L.acc + static_cast<size_t>(b) * L.ncomp * L.nline + i;
     for (int c = 0; c < L.ncomp; ++c) {
         double2& a = acc[static_cast<size_t>(c) * L.nline];

@@ -269,3 +269,44 @@ def test_fp32_static_fields_keep_their_k0_values_through_euler_swaps(te):
     assert got[1][0][0] == got[0][0][0] == u0[0, 0, 0]
     for k in ENERGY:
         assert _close(got[1][1][k], got[0][1][k], 1e-5, max(abs(v) for v in got[0][1].values())), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_measures_of_batched_members_equal_single_engines(precision):
+    """Every device measure reads its own member of a batched engine (the served-slot case)."""
+    import shhd_b200 as sb
+    from helpers import random_state, script
+    text = script(grid=(32, 32), length=(64.0, 64.0), nop=2, dt=0.01, noise=None)
+    ocfg = so.parse_script(text)
+    states = [random_state(ocfg, seed=s, rho0=1.0 + 0.1 * s) for s in (3, 8)]
+
+    def measure(eng, m):
+        return (eng.time_series_energies(m), eng.time_series_l2(m), eng.flux0_read(m), eng.profile_line(1, 0, m),
+                eng.profile_line(0, 1, m), eng.profile_velocity(1, 0, m), eng.flux_line(1, m))
+
+    def engine(batch):
+        cfg = sb.config_from_script(text)
+        cfg.precision = precision
+        cfg.batch = batch
+        e = sb.Engine(cfg)
+        e.flux0_enable()
+        e.flux_line_enable(1)
+        return e
+
+    with engine(2) as both:
+        for m, st in enumerate(states):
+            both.set_state(st, member=m)
+        both.step(2)
+        got = [measure(both, m) for m in range(2)]
+    for m, st in enumerate(states):
+        with engine(1) as one:
+            one.set_state(st)
+            one.step(2)
+            want = measure(one, 0)
+        for g, w in zip(got[m], want):
+            if isinstance(w, dict):
+                for k in w:
+                    assert np.allclose(g[k], w[k], rtol=1e-12, atol=0.0), (m, k)
+            else:
+                assert np.allclose(g, w, rtol=1e-12, atol=1e-300), m
