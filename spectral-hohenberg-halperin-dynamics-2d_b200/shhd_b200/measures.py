@@ -8,7 +8,9 @@
       tap (shhd_engine_flux0_*), enabled when a column asks for it: the last
       step's stage-weighted (0, 0) fluxes, as the reference's flux buffer holds.
   ave/profile (measure_ave_profile.cc:180-453): block or running averages of
-      field profiles over one axis (class AveProfile).
+      field and flux profiles over one axis (class AveProfile).
+  yokota_green_kubo (measure_yokota_green_kubo.cc:16-225): the stress
+      autocorrelation table, accumulated on the device (class YokotaGreenKubo).
   snapshot (measure_snapshot.cc:43-138): `<file>_step<step>.snapshot`, the step
       zero-padded to the digits of the script's total run steps; space physical
       (every field inverse-transformed on the padded grid, rows gy-major) or
@@ -152,8 +154,49 @@ class Snapshot:
         pass
 
 
+class YokotaGreenKubo:
+    """`measure <id> yokota_green_kubo on nevery N nblock B file F [mode diagonal|all]` over one
+    engine member (measure_yokota_green_kubo.cc:16-225): the device accumulates the stress
+    integrals (shhd_engine_gk_*); at every completed block the reference's table is rewritten,
+    `nsample tau mode_index kx ky S_mean` per (tau, mode)."""
+
+    def __init__(self, engine, file: str, nevery: int, nblock: int, mode: str = "diagonal", member: int = 0):
+        if nevery <= 0:
+            raise ValueError("yokota_green_kubo measure: nevery must be positive.")
+        if nblock <= 0:
+            raise ValueError("yokota_green_kubo measure: nblock must be positive.")
+        if nblock % nevery != 0:
+            raise ValueError("yokota_green_kubo measure: nblock must be divisible by nevery.")
+        if mode not in ("diagonal", "all"):
+            raise ValueError("yokota_green_kubo measure: mode must be diagonal|all.")
+        self.engine, self.file, self.nevery, self.nblock, self.member = engine, file, int(nevery), int(nblock), member
+        engine.gk_enable(self.nevery, self.nblock, mode)
+        self.modes = list(engine.gk_modes)
+        self.block_step = 0
+
+    def observe(self, step: int, time: float) -> None:
+        self.block_step += 1
+        if self.block_step < self.nblock:
+            return
+        self.block_step = 0
+        sums, nsample = self.engine.gk_read(self.member)
+        cfg = self.engine.cfg
+        lines = ["# nsample tau mode_index kx ky S_mean"]
+        for ti in range(sums.shape[0]):
+            tau = float((ti + 1) * self.nevery) * cfg.dt
+            for mi, (nx, ny) in enumerate(self.modes):
+                kx = 2.0 * 3.14159265358979323846 * float(nx) / cfg.lx
+                ky = 2.0 * 3.14159265358979323846 * float(ny) / cfg.ly
+                lines.append(f"{nsample} {_sci(tau)} {mi} {_sci(kx)} {_sci(ky)} {_sci(sums[ti, mi] / nsample)}")
+        with open(self.file, "w") as f:
+            f.write("\n".join(lines) + "\n")
+
+    def close(self) -> None:
+        pass
+
+
 def parse_measures(engine, script_text: str, member: int = 0) -> List[object]:
-    """The script's `measure` commands (time_series, snapshot, ave/profile) over one engine member."""
+    """The script's `measure` commands (time_series, snapshot, ave/profile, yokota_green_kubo) over one engine member."""
     total = sum(int(t[1]) for t in (ln.split("#", 1)[0].split() for ln in script_text.splitlines()) if len(t) >= 2 and t[0] == "run")
     out = []
     for raw in script_text.splitlines():
@@ -174,6 +217,8 @@ def parse_measures(engine, script_text: str, member: int = 0) -> List[object]:
             out.append(AveProfile(engine, kv["file"], kv["axis"], int(kv["nevery"]), int(kv["nblock"]), kv["average"], targets, member))
         elif kind == "snapshot":
             out.append(Snapshot(engine, kv["file"], int(kv["nevery"]), kv["space"], total, member))
+        elif kind == "yokota_green_kubo":
+            out.append(YokotaGreenKubo(engine, kv["file"], int(kv["nevery"]), int(kv["nblock"]), kv.get("mode", "diagonal"), member))
         else:
             raise NotImplementedError(f"measure style {kind}")
     return out
@@ -187,8 +232,8 @@ def run_script_measures(engine, script_text: str, member: int = 0) -> List[objec
     measures = parse_measures(engine, script_text, member)
     runs = [int(t[1]) for t in (ln.split("#", 1)[0].split() for ln in script_text.splitlines()) if len(t) >= 2 and t[0] == "run"]
     step = int(engine.get_info().step_index)
-    # ave/profile counts every step it observes: step one at a time while one is present
-    periods = [1] if any(isinstance(m, AveProfile) for m in measures) else [m.nevery for m in measures if m.nevery > 0]
+    # ave/profile and yokota_green_kubo count every step they observe: step one at a time while one is present
+    periods = [1] if any(isinstance(m, (AveProfile, YokotaGreenKubo)) for m in measures) else [m.nevery for m in measures]
     for n in runs:
         end = step + n
         while step < end:

@@ -297,3 +297,29 @@ FLUX_PROFILE_CASES = {
         "measure p1 ave/profile on axis y nevery 1 nblock 2 file @DIR@/py.dat average running target Jpsi[0]_y Jpsi[1]_x psi[1]",
     ]),
 }
+
+
+# Yokota-Green-Kubo measure cases.  eta = zeta = 0 leaves the momentum without
+# noise (j_sto returns early) and psi does not enter the momentum equations, so
+# pi_xy, and with it every S_mean the reference writes, is deterministic while
+# the measure still sees the positive kBT of `fix noise` it requires.  Grid
+# spacing 2 keeps phi4's gradient term inside SRK3's stability interval.
+def _gk_case(grid, length, lines, nsteps):
+    return _HEAD + "\n".join([
+        f"grid {grid[0]} {grid[1]}", f"length {length[0]} {length[1]}", "dealias 3/2", "order_parameters 1",
+        "timestep 0.01", "time_evolution srk3/compressible", "model thermo linear_eos cT 1",
+        "model free_energy phi4 a[0] -1 b[0] 1 u[0] 1", "model transport constant eta 0 zeta 0 M[0,0] 1",
+        "fix 1 all nonlinear on", "fix 2 all noise on seed 5 kBT 1e-3",
+        "set density equilibrium/gaussian kBT 1e-3 rho0 1 cT 1 seed 1",
+        "set momentum all equilibrium/gaussian/compressible kBT 1e-3 seed 2",
+        "set order_parameter all equilibrium/gaussian seed 3 kBT 1 k0 2 k2 0",
+    ] + lines + [f"run {nsteps}"]) + "\n"
+
+
+GK_CASES = {
+    "gk_diagonal": _gk_case((16, 16), (32.0, 32.0), [
+        "measure gk yokota_green_kubo on nevery 2 nblock 4 file @DIR@/gk.dat mode diagonal"], 8),
+    "gk_all_rect": _gk_case((16, 12), (32.0, 18.0), [
+        "measure gk yokota_green_kubo on nevery 1 nblock 3 file @DIR@/gk_all.dat mode all",
+        "measure ts time_series on nevery 1 file @DIR@/ts.dat target E_K pi_xy"], 6),
+}

@@ -26,7 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, HERE)
-from cases import CASES, FLUX_PROFILE_CASES, IC_CASES, MEASURE_CASES, PROFILE_CASES  # noqa: E402
+from cases import CASES, FLUX_PROFILE_CASES, GK_CASES, IC_CASES, MEASURE_CASES, PROFILE_CASES  # noqa: E402
 
 NSTEPS = 2
 
@@ -94,7 +94,7 @@ def main_measures() -> None:
     lib.shref_create.restype = ctypes.c_void_p
     lib.shref_last_error.restype = ctypes.c_char_p
     out = {}
-    for name, template in {**MEASURE_CASES, **PROFILE_CASES, **FLUX_PROFILE_CASES}.items():
+    for name, template in {**MEASURE_CASES, **PROFILE_CASES, **FLUX_PROFILE_CASES, **GK_CASES}.items():
         with tempfile.TemporaryDirectory() as tmp:
             script = template.replace("@DIR@", tmp)
             nsteps = int(script.rsplit("run ", 1)[1].split()[0])
