@@ -1762,12 +1762,14 @@ int shhd_engine_set_initial_field(shhd_engine* e, int member, int field, const s
         else
             initial_field_kernel<double><<<g, kThreads, 0, e->stream>>>(P, static_cast<double2*>(e->u), member, field, s, k0);
         check_cuda(cudaGetLastError(), "initial_field launch");
-        double2 v00{};  // the (0, 0) coefficient in FP64: the FP32 engines' copy, else the state itself
-        const void* src = k0 ? static_cast<const void*>(k0)
-                             : static_cast<const void*>(static_cast<const double2*>(e->u) + (static_cast<size_t>(member) * P.nfields + field) * modes);
-        check_cuda(cudaMemcpyAsync(&v00, src, sizeof(double2), cudaMemcpyDeviceToHost, e->stream), "k = 0 read");
+        double2 v00{};  // the density's (0, 0) coefficient in FP64 (FP32 engines' copy, else the state), as set_state takes it
+        if (field == 0) {
+            const void* src = k0 ? static_cast<const void*>(k0)
+                                 : static_cast<const void*>(static_cast<const double2*>(e->u) + static_cast<size_t>(member) * P.nfields * modes);
+            check_cuda(cudaMemcpyAsync(&v00, src, sizeof(double2), cudaMemcpyDeviceToHost, e->stream), "k = 0 read");
+        }
         check_cuda(cudaStreamSynchronize(e->stream), "initial_field sync");
-        if (field == 0) e->rho0_candidate[member] = v00.x / (static_cast<double>(e->cfg.nx) * e->cfg.ny);  // as set_state takes it
+        if (field == 0) e->rho0_candidate[member] = v00.x / (static_cast<double>(e->cfg.nx) * e->cfg.ny);
     });
 }
 
@@ -1970,16 +1972,10 @@ void energies(shhd_engine* e, int member, double* out) {
     check_cuda(cudaGetLastError(), "sum_partials launch");
     std::vector<double> v(nv);
     check_cuda(cudaMemcpyAsync(v.data(), sums, sizeof(double) * nv, cudaMemcpyDeviceToHost, e->stream), "energy read");
+    // rho(0, 0) in FP64: the FP32 engines' k = 0 copy (always allocated for them), else the FP64 state
     double2 rho00{};
     const void* src = k0 ? static_cast<const void*>(k0) : static_cast<const void*>(st);
-    if (k0 || !e->fp32) {
-        check_cuda(cudaMemcpyAsync(&rho00, src, sizeof(double2), cudaMemcpyDeviceToHost, e->stream), "rho(0) read");
-    } else {
-        float2 r{};
-        check_cuda(cudaMemcpyAsync(&r, src, sizeof(float2), cudaMemcpyDeviceToHost, e->stream), "rho(0) read");
-        check_cuda(cudaStreamSynchronize(e->stream), "energy sync");
-        rho00.x = r.x;
-    }
+    check_cuda(cudaMemcpyAsync(&rho00, src, sizeof(double2), cudaMemcpyDeviceToHost, e->stream), "rho(0) read");
     check_cuda(cudaStreamSynchronize(e->stream), "energy sync");
     const double rho0 = rho00.x / ng;
     const bool comp = c.mode == SHHD_COMPRESSIBLE, incomp = c.mode == SHHD_INCOMPRESSIBLE;
