@@ -446,9 +446,13 @@ def run_measures(sb, torch, world):
     eng.flux_line_enable(1)
     out["steps_per_s_with_k0_and_flux_line_y_taps"] = rate()
     out["flux_line_read_ms"] = wall_ms(lambda: eng.flux_line(1))
+    eng.flux_tap_schedule(0, 10, 0)
+    eng.flux_tap_schedule(2, 10, 0)
+    out["steps_per_s_with_both_taps_every_10_steps"] = rate()
     out["what"] = ("1024^2 (3/2 -> 1536^2), N = 2, FP32 engine: wall time per measure call (E_T..E_C with the physical-space "
                    "transforms; L2 columns; one spectral profile line; the compressible vx profile over x); step rate "
-                   "without taps, with the k = 0 flux tap, and with the kx = 0 flux-line tap added (1535 modes, every flux)")
+                   "without taps, with the k = 0 flux tap, with the kx = 0 flux-line tap added (1535 modes, every flux), and with both "
+                   "taps recording every 10th step (a measure sampling every 10 steps)")
     eng.close()
     return out
 

@@ -318,6 +318,13 @@ int shhd_engine_profile_velocity(shhd_engine* engine, int member, int component,
  * in the order of shhd_engine_profile_line.  Refused with replayed (external)
  * noise when the noise is on.  Enabling drops captured graphs. */
 int shhd_engine_flux_line_enable(shhd_engine* engine, int axis);
+
+/* Which steps an enabled flux tap records (tap 0: the k = 0 fluxes, 1: the
+ * ky = 0 line, 2: the kx = 0 line): the steps whose engine step index after
+ * the step is phase modulo period (default every step).  A measure that
+ * samples every nevery steps needs no other; the others cost one early-exit
+ * launch per stage.  Changing it drops captured graphs. */
+int shhd_engine_flux_tap_schedule(shhd_engine* engine, int tap, int64_t period, int64_t phase);
 int shhd_engine_flux_line_read(shhd_engine* engine, int axis, int member, double* out, size_t n);
 
 /* Spectral L2 columns of the time-series measure (measure_time_series.cc:

@@ -986,14 +986,14 @@ void launch_gk_tap(shhd_engine* e, const void* cur, int step_off, double weight,
 }
 
 template <typename T>
-void launch_flux0_tap(shhd_engine* e, const void* cur, double weight, int first) {
+void launch_flux0_tap(shhd_engine* e, const void* cur, int step_off, double weight, int first) {
     if (!e->flux0_on) return;
     const double2* k0 = nullptr;
     if (e->k0_u) k0 = cur == e->u ? e->k0_u : (cur == e->s1 ? e->k0_s1 : (cur == e->s2 ? e->k0_s2 : nullptr));
     const long long threads = static_cast<long long>(e->P.batch) * e->flux0.ncol * 32;
     const dim3 g(static_cast<unsigned>((threads + kThreads - 1) / kThreads));
     flux0_tap_kernel<T><<<g, kThreads, 0, e->stream>>>(e->P, e->flux0, e->members_dev, static_cast<const T*>(e->i2),
-                                                       static_cast<const cplx<T>*>(cur), k0, weight, first);
+                                                       static_cast<const cplx<T>*>(cur), k0, weight, first, e->step_dev, step_off);
     check_cuda(cudaGetLastError(), "flux0_tap launch");
 }
 
@@ -1032,7 +1032,7 @@ void record_steps(shhd_engine* e, int nsteps) {
                 launch_col_forward<T>(e, A);
                 // stage flux weights 1/6, 1/6, 2/3 (time_integrator_srk3_compressible.h:15-21)
                 launch_gk_tap<T>(e, cur[k], s, k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0, k == 2);
-                launch_flux0_tap<T>(e, cur[k], k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0);
+                launch_flux0_tap<T>(e, cur[k], s, k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0);
                 launch_flux_line_taps<T>(e, cur[k], s, k == 2 ? 2.0 / 3.0 : 1.0 / 6.0, k == 0, k == 2);
             }
         } else {
@@ -1041,7 +1041,7 @@ void record_steps(shhd_engine* e, int nsteps) {
             A.step_off = s;
             launch_col_forward<T>(e, A);
             launch_gk_tap<T>(e, e->u, s, 1.0, 1, 1);
-            launch_flux0_tap<T>(e, e->u, 1.0, 1);
+            launch_flux0_tap<T>(e, e->u, s, 1.0, 1);
             launch_flux_line_taps<T>(e, e->u, s, 1.0, 1, 1);
             std::swap(e->u, e->s1);
             std::swap(e->k0_u, e->k0_s1);
@@ -2080,6 +2080,8 @@ int shhd_engine_flux0_enable(shhd_engine* e) {
         // j_det records the linear pressure flux whenever it runs with cT^2 != 0 (fcalculator.cc:110-136)
         F.pressure = e->cfg.mode != SHHD_QUIESCENT && P.cT2 != 0.0;
         F.pair_layout = e->pair_path ? 1 : 0;
+        F.period = 1;
+        F.phase = 0;
         const size_t bytes = sizeof(double) * e->cfg.batch * F.ncol;
         F.acc = static_cast<double*>(dalloc(e, bytes));
         check_cuda(cudaMemsetAsync(F.acc, 0, bytes, e->stream), "memset");
@@ -2133,6 +2135,8 @@ int shhd_engine_flux_line_enable(shhd_engine* e, int axis) {
         }
         L.noise_j = P.noise_j;
         L.incompressible = c.mode == SHHD_INCOMPRESSIBLE;
+        L.period = 1;
+        L.phase = 0;
         std::vector<double2> wt(P.npy);
         for (int n = 0; n < P.npy; ++n) {
             const double ang = -2.0 * M_PI * n / P.npy;
@@ -2150,6 +2154,24 @@ int shhd_engine_flux_line_enable(shhd_engine* e, int axis) {
         e->fline[axis] = L;
         e->fline_on[axis] = true;
         drop_graphs(e);  // captured graphs do not hold the tap yet
+    });
+}
+
+int shhd_engine_flux_tap_schedule(shhd_engine* e, int tap, int64_t period, int64_t phase) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (period < 1) throw Failure(SHHD_EINVAL, "the tap period must be positive");
+        long long* per = nullptr;
+        long long* ph = nullptr;
+        if (tap == 0 && e->flux0_on) { per = &e->flux0.period; ph = &e->flux0.phase; }
+        if ((tap == 1 || tap == 2) && e->fline_on[tap - 1]) { per = &e->fline[tap - 1].period; ph = &e->fline[tap - 1].phase; }
+        if (!per) throw Failure(SHHD_EINVAL, "tap " + std::to_string(tap) + " is not enabled");
+        const long long p = period, q = ((phase % period) + period) % period;
+        if (*per != p || *ph != q) {
+            *per = p;
+            *ph = q;
+            drop_graphs(e);  // captured graphs hold the schedule as a launch argument
+        }
     });
 }
 

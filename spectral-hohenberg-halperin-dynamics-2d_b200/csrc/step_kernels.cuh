@@ -925,6 +925,13 @@ __global__ void __launch_bounds__(kThreads) gk_tap_kernel(const StepPlan P, cons
 // product plane, so the block stages it once in shared memory (npy x 16 bytes);
 // the first stage overwrites
 // ---------------------------------------------------------------------------
+// the engine step index after the current step is on a tap's schedule
+__device__ __forceinline__ bool tap_scheduled(const unsigned long long* step_base, int step_off, long long period, long long phase) {
+    if (period <= 1) return true;
+    const long long s = static_cast<long long>(*step_base) + step_off + 1 - phase;
+    return ((s % period) + period) % period == 0;
+}
+
 struct FluxLineArgs {
     double2* acc;
     int axis, nline, ncomp;
@@ -939,6 +946,7 @@ struct FluxLineArgs {
     int o_mu[kMaxOp], o_px[kMaxOp], o_py[kMaxOp];
     int noise_j;                  // the momentum noise flux
     int incompressible;
+    long long period, phase;      // record the steps s (engine step index after the step) with s = phase mod period
 };
 
 __device__ __forceinline__ double2 cmi(double2 a) { return make_double2(a.y, -a.x); }  // -i a
@@ -952,6 +960,7 @@ __global__ void __launch_bounds__(kThreads) flux_line_tap_kernel(const StepPlan 
                                                                  const unsigned long long* __restrict__ step_base, int step_off, double weight,
                                                                  int first, int last, double dt) {
     extern __shared__ double2 col[];   // npy entries (kx = 0 column only)
+    if (!tap_scheduled(step_base, step_off, L.period, L.phase)) return;  // grid-uniform
     const int lane = threadIdx.x & 31;
     const int b = blockIdx.y;
     const int i = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
@@ -1099,12 +1108,16 @@ struct Flux0Args {
     int o[3 + 2 * kMaxOp];        // product plane of each column in I2 (-1: no advective term)
     int pressure;                 // cT^2 rho(0) on pi_xx and pi_yy
     int pair_layout;              // I2 element (re_2t, re_2t+1, im_2t, im_2t+1) with W = 2
+    long long period, phase;      // record the steps s (engine step index after the step) with s = phase mod period
 };
+
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads) flux0_tap_kernel(const StepPlan P, const Flux0Args F, const MemberInfo* __restrict__ members,
                                                              const T* __restrict__ i2, const cplx<T>* __restrict__ cur,
-                                                             const double2* __restrict__ k0cur, double weight, int first) {
+                                                             const double2* __restrict__ k0cur, double weight, int first,
+                                                             const unsigned long long* __restrict__ step_base, int step_off) {
+    if (!tap_scheduled(step_base, step_off, F.period, F.phase)) return;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= P.batch * F.ncol) return;

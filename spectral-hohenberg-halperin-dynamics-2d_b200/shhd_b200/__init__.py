@@ -126,7 +126,7 @@ EXPORTED = (
     "shhd_engine_gk_enable", "shhd_engine_gk_read", "shhd_engine_l2_sums", "shhd_engine_set_gaussian_field",
     "shhd_engine_set_initial_field", "shhd_engine_check_transverse", "shhd_engine_energies",
     "shhd_engine_flux0_enable", "shhd_engine_flux0_read", "shhd_engine_profile_line", "shhd_engine_profile_velocity",
-    "shhd_engine_flux_line_enable", "shhd_engine_flux_line_read",
+    "shhd_engine_flux_line_enable", "shhd_engine_flux_line_read", "shhd_engine_flux_tap_schedule",
 )
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
@@ -179,6 +179,7 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_profile_velocity.argtypes = [vp, i, i, i, dp, sz]
     lib.shhd_engine_flux_line_enable.argtypes = [vp, i]
     lib.shhd_engine_flux_line_read.argtypes = [vp, i, i, dp, sz]
+    lib.shhd_engine_flux_tap_schedule.argtypes = [vp, i, ctypes.c_int64, ctypes.c_int64]
     return lib
 
 
@@ -331,9 +332,29 @@ class Engine:
         _check(lib.shhd_engine_energies(self._h, int(member), _dptr(raw), raw.size))
         return {"E_T": float(raw[0]), "E_K": float(raw[1]), "E_psi": float(raw[2]), "E_C": float(raw[3])}
 
-    def flux0_enable(self) -> None:
-        """Record the k = 0 flux columns of every step from now on (drops captured graphs)."""
+    def flux0_enable(self, every: int = 1, phase: int = 0) -> None:
+        """Record the k = 0 flux columns from now on, on the steps s = phase mod every (see flux_tap_request)."""
         _check(lib.shhd_engine_flux0_enable(self._h))
+        self.flux_tap_request(0, every, phase)
+
+    def flux_tap_request(self, tap: int, every: int, phase: int) -> None:
+        """Ask tap 0 (k = 0), 1 (ky = 0 line) or 2 (kx = 0 line) to record the steps s = phase mod every
+        (s: the engine step index after the step).  Requests accumulate: the tap records every step any
+        request needs (period gcd(every, every', phase - phase'))."""
+        import math
+        sched = self.__dict__.setdefault("_tap_schedules", {})
+        ph = phase % every
+        if tap in sched:
+            p0, q0 = sched[tap]
+            g = math.gcd(math.gcd(p0, every), abs(ph - q0))
+            self.flux_tap_schedule(tap, g, q0)
+        else:
+            self.flux_tap_schedule(tap, every, ph)
+
+    def flux_tap_schedule(self, tap: int, every: int, phase: int) -> None:
+        """Set the steps a tap records (s = phase mod every), replacing earlier requests."""
+        self.__dict__.setdefault("_tap_schedules", {})[tap] = (int(every), int(phase) % int(every))
+        _check(lib.shhd_engine_flux_tap_schedule(self._h, int(tap), int(every), int(phase)))
 
     def flux0_read(self, member: int = 0) -> dict:
         """The last step's k = 0 flux columns: pi_xx, pi_xy, pi_yy, Jpsi[a]_x, Jpsi[a]_y."""
@@ -361,9 +382,11 @@ class Engine:
         _check(lib.shhd_engine_profile_velocity(self._h, int(member), int(component), int(axis), _dptr(raw), raw.size))
         return raw
 
-    def flux_line_enable(self, axis: int) -> None:
-        """Record the step's flux buffer along the ky = 0 row (axis 0) or kx = 0 column (axis 1)."""
+    def flux_line_enable(self, axis: int, every: int = 1, phase: int = 0) -> None:
+        """Record the step's flux buffer along the ky = 0 row (axis 0) or kx = 0 column (axis 1), on the
+        steps s = phase mod every (see flux_tap_request)."""
         _check(lib.shhd_engine_flux_line_enable(self._h, int(axis)))
+        self.flux_tap_request(1 + int(axis), every, phase)
 
     def flux_line(self, axis: int, member: int = 0) -> dict:
         """The last step's fluxes along the line, {pi_xx, pi_xy, pi_yy, Jpsi[a]_x, Jpsi[a]_y: complex128}."""

@@ -54,7 +54,7 @@ class TimeSeries:
                 raise ValueError(f"unknown time_series target: {t}")
         self._flux = any(t in _PI or _JPSI.match(t) for t in targets)
         if self._flux:
-            engine.flux0_enable()
+            engine.flux0_enable(every=int(nevery), phase=0)   # observed at step % nevery == 0
         self.engine, self.file, self.nevery, self.targets, self.member = engine, file, int(nevery), list(targets), member
         self._out: Optional[TextIO] = None
 
@@ -325,7 +325,9 @@ class AveProfile:
         self._running = [None] * len(self.targets)
         self._out: Optional[TextIO] = None
         if any(kind == "flux" for _n, kind, _i, _s in self.targets):
-            engine.flux_line_enable(self.axis)
+            # sampled every nevery-th observed step, counted from the step the measure starts at
+            start = int(engine.get_info().step_index)
+            engine.flux_line_enable(self.axis, every=self.nevery, phase=start)
 
     def _reference_density(self) -> float:
         """Re rho(0) / Ng of the first sample that needs it (measure_ave_profile.cc:123-149)."""

@@ -46,8 +46,13 @@ class _HostEngine:
         ky = np.concatenate([np.arange(half), np.arange(-(half - 1), 0)])
         return field2d[ky % c.ny, 0].copy()
 
-    def flux_line_enable(self, axis):
+    def flux_line_enable(self, axis, every=1, phase=0):
         pass
+
+    def get_info(self):
+        class _Info:
+            step_index = 0
+        return _Info()
 
     def flux_line(self, axis, member=0):
         return {k: self._line(v, axis) for k, v in self.flux.items()}

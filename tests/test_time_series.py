@@ -310,3 +310,32 @@ def test_measures_of_batched_members_equal_single_engines(precision):
                     assert np.allclose(g[k], w[k], rtol=1e-12, atol=0.0), (m, k)
             else:
                 assert np.allclose(g, w, rtol=1e-12, atol=1e-300), m
+
+
+@pytest.mark.gpu
+def test_scheduled_flux_taps_record_the_sampled_steps():
+    """A tap asked for every n-th step records, on those steps, what an always-on tap records
+    (direct launches and graph replays alike); requests from two measures merge to their gcd."""
+    import shhd_b200 as sb
+    from helpers import random_state, script
+    text = script(grid=(32, 32), length=(64.0, 64.0), nop=1, dt=0.01, noise="kBT 0.002 seed 4")
+    u0 = random_state(so.parse_script(text), seed=6)
+    cfg = sb.config_from_script(text)
+    with sb.Engine(cfg) as every, sb.Engine(cfg) as sched:
+        for e in (every, sched):
+            e.set_state(u0)
+        every.flux0_enable()
+        every.flux_line_enable(1)
+        sched.flux0_enable(every=3)
+        sched.flux_line_enable(1, every=4, phase=2)
+        sched.set_graph_chunk(2)
+        for step in range(1, 11):
+            every.step(1)
+            sched.step(1)
+            if step % 3 == 0:
+                assert sched.flux0_read() == every.flux0_read(), step
+            if step % 4 == 2:
+                a, b = sched.flux_line(1), every.flux_line(1)
+                assert all(np.array_equal(a[k], b[k]) for k in a), step
+        sched.flux_tap_request(0, 2, 0)      # merged with every=3, phase 0: every step
+        assert sched._tap_schedules[0] == (1, 0)
