@@ -926,10 +926,13 @@ void ensure_rho0(shhd_engine* e) {
 template <typename T>
 void prepare_static(shhd_engine* e) {
     if (e->n_static == 0) return;
-    dim3 grid(e->n_static, e->P.batch);
+    // about 1024 blocks per field (at least one kx = 0 line each, so block 0 holds that line)
+    const size_t fstride = static_cast<size_t>(e->P.hx) * e->P.kyn;
+    const size_t chunk = std::max<size_t>({static_cast<size_t>(e->P.kyn), (fstride + 1023) / 1024, static_cast<size_t>(kThreads)});
+    dim3 grid(static_cast<unsigned>((fstride + chunk - 1) / chunk), e->n_static, e->P.batch);
     LaunchScope scope(e, 3, static_cast<double>(sizeof(cplx<T>)) * e->P.batch * e->n_static * 3.0 * e->P.hx * e->P.kyn);
     prepare_static_kernel<T><<<grid, kThreads, 0, e->stream>>>(e->P, e->static_dev, static_cast<cplx<T>*>(e->u), static_cast<cplx<T>*>(e->s1),
-                                                             static_cast<cplx<T>*>(e->s2), e->k0_u, e->k0_s1, e->k0_s2);
+                                                             static_cast<cplx<T>*>(e->s2), e->k0_u, e->k0_s1, e->k0_s2, static_cast<int>(chunk));
     check_cuda(cudaGetLastError(), "prepare_static launch");
 }
 

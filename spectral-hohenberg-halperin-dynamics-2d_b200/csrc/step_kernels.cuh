@@ -1549,38 +1549,43 @@ __global__ void advance_step_kernel(unsigned long long* step, unsigned long long
 
 // ---------------------------------------------------------------------------
 // fields the integrator only copies: symmetrise the kx = 0 line once and
-// mirror them into the stage buffers   (grid: fields x batch)
+// mirror them into the stage buffers   (grid: chunks x fields x batch; chunk >= Ky elements
+// per block, block 0 of a field first symmetrises its kx = 0 line)
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(kThreads) prepare_static_kernel(const StepPlan P, const int* __restrict__ fields, cplx<T>* u, cplx<T>* s1,
-                                                                 cplx<T>* s2, double2* k0u, double2* k0s1, double2* k0s2) {
+                                                                 cplx<T>* s2, double2* k0u, double2* k0s1, double2* k0s2, int chunk) {
     using C = cplx<T>;
-    const int f = fields[blockIdx.x], b = blockIdx.y;
+    const int f = fields[blockIdx.y], b = blockIdx.z;
     const size_t fstride = static_cast<size_t>(P.hx) * P.kyn;
     C* uf = u + (static_cast<size_t>(b) * P.nfields + f) * fstride;
-    const int half = P.nay / 2;
-    if (threadIdx.x == 0) {
-        uf[0].y = T(0);
-        if (k0u) {  // FP32 engines: the FP64 k = 0 copy of the static field follows it into every buffer
-            const size_t q = static_cast<size_t>(b) * P.nfields + f;
-            const double2 v = make_double2(k0u[q].x, 0.0);
-            k0u[q] = v;
-            k0s1[q] = v;
-            k0s2[q] = v;
+    if (blockIdx.x == 0) {  // the kx = 0 line (the first Ky elements, inside this block's chunk)
+        const int half = P.nay / 2;
+        if (threadIdx.x == 0) {
+            uf[0].y = T(0);
+            if (k0u) {  // FP32 engines: the FP64 k = 0 copy of the static field follows it into every buffer
+                const size_t q = static_cast<size_t>(b) * P.nfields + f;
+                const double2 v = make_double2(k0u[q].x, 0.0);
+                k0u[q] = v;
+                k0s1[q] = v;
+                k0s2[q] = v;
+            }
         }
+        for (int ky = 1 + threadIdx.x; ky < half; ky += blockDim.x) {
+            const int jn = P.kyn - ky;  // j of -ky
+            const C a = uf[ky];
+            const C c = uf[jn];
+            const C pj = mk(static_cast<T>(0.5) * (a.x + c.x), static_cast<T>(0.5) * (a.y - c.y));
+            uf[ky] = pj;
+            uf[jn] = cconj(pj);
+        }
+        __syncthreads();
     }
-    for (int ky = 1 + threadIdx.x; ky < half; ky += blockDim.x) {
-        const int jn = P.kyn - ky;  // j of -ky
-        const C a = uf[ky];
-        const C c = uf[jn];
-        const C pj = mk(static_cast<T>(0.5) * (a.x + c.x), static_cast<T>(0.5) * (a.y - c.y));
-        uf[ky] = pj;
-        uf[jn] = cconj(pj);
-    }
-    __syncthreads();
     C* a1 = s1 + (static_cast<size_t>(b) * P.nfields + f) * fstride;
     C* a2 = s2 + (static_cast<size_t>(b) * P.nfields + f) * fstride;
-    for (size_t e = threadIdx.x; e < fstride; e += blockDim.x) {
+    const size_t e0 = static_cast<size_t>(blockIdx.x) * chunk;
+    const size_t e1 = e0 + chunk < fstride ? e0 + chunk : fstride;
+    for (size_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
         const C v = uf[e];
         a1[e] = v;
         a2[e] = v;
