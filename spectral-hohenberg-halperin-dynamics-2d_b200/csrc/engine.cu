@@ -926,9 +926,11 @@ void ensure_rho0(shhd_engine* e) {
 template <typename T>
 void prepare_static(shhd_engine* e) {
     if (e->n_static == 0) return;
-    // about 1024 blocks per field (at least one kx = 0 line each, so block 0 holds that line)
+    // about 2048 blocks over all static fields and members (a chunk holds at least one kx = 0 line,
+    // so block 0 of a field holds that line)
     const size_t fstride = static_cast<size_t>(e->P.hx) * e->P.kyn;
-    const size_t chunk = std::max<size_t>({static_cast<size_t>(e->P.kyn), (fstride + 1023) / 1024, static_cast<size_t>(kThreads)});
+    const size_t total = fstride * e->n_static * e->P.batch;
+    const size_t chunk = std::max<size_t>({static_cast<size_t>(e->P.kyn), (total + 2047) / 2048, static_cast<size_t>(kThreads)});
     dim3 grid(static_cast<unsigned>((fstride + chunk - 1) / chunk), e->n_static, e->P.batch);
     LaunchScope scope(e, 3, static_cast<double>(sizeof(cplx<T>)) * e->P.batch * e->n_static * 3.0 * e->P.hx * e->P.kyn);
     prepare_static_kernel<T><<<grid, kThreads, 0, e->stream>>>(e->P, e->static_dev, static_cast<cplx<T>*>(e->u), static_cast<cplx<T>*>(e->s1),
