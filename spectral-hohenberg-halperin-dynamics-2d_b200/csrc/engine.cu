@@ -639,7 +639,8 @@ void build_plan(shhd_engine* e) {
         constexpr int FX = decltype(fx)::value;
         if constexpr (FX != 0) {
             const int gsz = e->fp32 ? row_group<float, FX>() : row_group<double, FX>();
-            const size_t rb = static_cast<size_t>(P.n_in + kThreads / gsz) * FX * cs;
+            const int nt = e->fp32 ? row_block<float, FX>() : row_block<double, FX>();
+            const size_t rb = static_cast<size_t>(P.n_in + nt / gsz) * FX * cs;  // inputs + one work line per group
             if (rb <= smem_cap) {
                 e->row_fixed = true;
                 e->smem_row = rb;
@@ -839,7 +840,7 @@ void launch_row(shhd_engine* e) {
         constexpr int FX = decltype(fx)::value;
         if constexpr (FX != 0) {
             if (e->row_fixed) {
-                row_pass_fixed<T, FX><<<grid, kThreads, e->smem_row, e->stream>>>(
+                row_pass_fixed<T, FX><<<grid, row_block<T, FX>(), e->smem_row, e->stream>>>(
                     P, e->members_dev, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
                     e->err_dev);
                 return;

@@ -19,7 +19,14 @@ namespace shhd {
 template <typename T, int N>
 __host__ __device__ constexpr int row_group() {
     constexpr int g = (sizeof(T) == 4 ? N / 24 : N / 12);
+    // lines of 48 KB or more leave room for one CTA per SM: give each line a 512-thread block
+    if constexpr (N * 2 * sizeof(T) >= 49152) return 512;
     return g <= 32 ? 32 : (g <= 64 ? 64 : (g <= 128 ? 128 : 256));
+}
+// threads per block of the compile-time row kernel
+template <typename T, int N>
+__host__ __device__ constexpr int row_block() {
+    return row_group<T, N>() > kThreads ? row_group<T, N>() : kThreads;
 }
 // column tile width for the compile-time column kernels (columns per CTA, one group each)
 template <typename T, int N>
@@ -179,14 +186,15 @@ __global__ void __launch_bounds__(kThreads) col_inverse_fixed(const StepPlan P, 
 // row pass (compile-time NX): I1 -> C2R -> products -> R2C -> I2   (grid: row pairs x batch)
 // ---------------------------------------------------------------------------
 template <typename T, int NX>
-__global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, const MemberInfo* __restrict__ members,
+__global__ void __launch_bounds__(row_block<T, NX>(), (row_block<T, NX>() > kThreads ? 1 : 2)) row_pass_fixed(const StepPlan P, const MemberInfo* __restrict__ members,
                                                            const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
                                                            const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
                                                            int* __restrict__ err) {
     if (!members[blockIdx.y].active) return;
     using C = cplx<T>;
     constexpr int G = row_group<T, NX>();
-    constexpr int NG = kThreads / G;
+    constexpr int NT = row_block<T, NX>();   // threads per block
+    constexpr int NG = NT / G;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* lines = reinterpret_cast<C*>(smem_raw);          // [n_in][NX] physical row pairs
     C* work = lines + static_cast<size_t>(P.n_in) * NX;  // [NG][NX] one product line per group
@@ -202,11 +210,11 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, 
     const size_t slot_stride = static_cast<size_t>(P.ntiles) * npy * W;
     const int nload = P.n_in * hx;
     constexpr int U = 4;
-    for (int e0 = threadIdx.x; e0 < nload; e0 += kThreads * U) {
+    for (int e0 = threadIdx.x; e0 < nload; e0 += NT * U) {
         C a[U], c[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int e = e0 + u * kThreads;
+            const int e = e0 + u * NT;
             if (e < nload) {
                 const int s = e / hx, k = e - s * hx;
                 const int t = k >> P.logw, w = k & (W - 1);
@@ -217,7 +225,7 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, 
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int e = e0 + u * kThreads;
+            const int e = e0 + u * NT;
             if (e < nload) {
                 const int s = e / hx, k = e - s * hx;
                 C* z = lines + static_cast<size_t>(s) * NX;
@@ -229,7 +237,7 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, 
         }
     }
     const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
-    for (int e = threadIdx.x; e < P.n_in * nzero; e += kThreads) {
+    for (int e = threadIdx.x; e < P.n_in * nzero; e += NT) {
         const int s = e / nzero, k = hx + (e - s * nzero);
         lines[static_cast<size_t>(s) * NX + sw7(k)] = czero<C>();
     }
@@ -247,7 +255,7 @@ __global__ void __launch_bounds__(kThreads, 2) row_pass_fixed(const StepPlan P, 
     if (P.need_v && comp) {
         // zero-density check, then rho is replaced by 1/rho (its only use is v = j / rho)
         int bad = 0;
-        for (int x = threadIdx.x; x < NX; x += kThreads) {
+        for (int x = threadIdx.x; x < NX; x += NT) {
             C* pr = lines + static_cast<size_t>(s_rho) * NX + x;
             const C rho = *pr;
             if (rho.x == T(0) || (has1 && rho.y == T(0))) bad = 1;
