@@ -232,6 +232,7 @@ struct shhd_engine {
     int npos = 16;
     bool col_fixed = false;       // compile-time column kernels (group per column)
     bool row_fixed = false;       // compile-time row kernel (group per line)
+    int row_nt = 256;             // its threads per block (512: two line groups, for lines of 48 KB or more)
     bool pair_path = false;       // FP32 pair-line kernels (compile-time sizes up to 1536)
     int family_override = -1;     // -1 choose, 0 never the pair-line kernels, 1 pair-line where valid
     size_t tw_bytes = 0;
@@ -639,10 +640,16 @@ void build_plan(shhd_engine* e) {
         constexpr int FX = decltype(fx)::value;
         if constexpr (FX != 0) {
             const int gsz = e->fp32 ? row_group<float, FX>() : row_group<double, FX>();
-            const int nt = e->fp32 ? row_block<float, FX>() : row_block<double, FX>();
-            const size_t rb = static_cast<size_t>(P.n_in + nt / gsz) * FX * cs;  // inputs + one work line per group
-            if (rb <= smem_cap) {
+            const bool big = e->fp32 ? row_big_lines<float, FX>() : row_big_lines<double, FX>();
+            const size_t rb = static_cast<size_t>(P.n_in + kThreads / gsz) * FX * cs;  // inputs + one work line per group
+            const size_t rb2 = static_cast<size_t>(P.n_in + 2) * FX * cs;              // two groups, two work lines
+            if (big && rb2 <= smem_cap) {
                 e->row_fixed = true;
+                e->row_nt = 2 * kThreads;
+                e->smem_row = rb2;
+            } else if (rb <= smem_cap) {
+                e->row_fixed = true;
+                e->row_nt = kThreads;
                 e->smem_row = rb;
             }
         }
@@ -770,7 +777,13 @@ void set_smem_attrs(shhd_engine* e) {
         constexpr int FX = decltype(fx)::value;
         if constexpr (FX != 0) {
             if (e->row_fixed) {
-                setattr(reinterpret_cast<const void*>(row_pass_fixed<T, FX>), e->smem_row);
+                if constexpr (row_big_lines<T, FX>()) {
+                    if (e->row_nt == 2 * kThreads) {
+                        setattr(reinterpret_cast<const void*>(row_pass_fixed<T, FX, 2 * kThreads>), e->smem_row);
+                        return;
+                    }
+                }
+                setattr(reinterpret_cast<const void*>(row_pass_fixed<T, FX, kThreads>), e->smem_row);
                 return;
             }
         }
@@ -840,7 +853,15 @@ void launch_row(shhd_engine* e) {
         constexpr int FX = decltype(fx)::value;
         if constexpr (FX != 0) {
             if (e->row_fixed) {
-                row_pass_fixed<T, FX><<<grid, row_block<T, FX>(), e->smem_row, e->stream>>>(
+                if constexpr (row_big_lines<T, FX>()) {
+                    if (e->row_nt == 2 * kThreads) {
+                        row_pass_fixed<T, FX, 2 * kThreads><<<grid, 2 * kThreads, e->smem_row, e->stream>>>(
+                            P, e->members_dev, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2),
+                            static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev, e->err_dev);
+                        return;
+                    }
+                }
+                row_pass_fixed<T, FX, kThreads><<<grid, kThreads, e->smem_row, e->stream>>>(
                     P, e->members_dev, static_cast<const cplx<T>*>(e->i1), static_cast<cplx<T>*>(e->i2), static_cast<const cplx<T>*>(e->tw_x), e->rho0_dev,
                     e->err_dev);
                 return;

@@ -19,14 +19,13 @@ namespace shhd {
 template <typename T, int N>
 __host__ __device__ constexpr int row_group() {
     constexpr int g = (sizeof(T) == 4 ? N / 24 : N / 12);
-    // lines of 48 KB or more leave room for one CTA per SM: give each line a 512-thread block
-    if constexpr (N * 2 * sizeof(T) >= 49152) return 512;
     return g <= 32 ? 32 : (g <= 64 ? 64 : (g <= 128 ? 128 : 256));
 }
-// threads per block of the compile-time row kernel
+// lines of 48 KB or more (FP32 6144, FP64 3072) allow one CTA per SM: the row pass may then run
+// two line groups in a 512-thread block, two transform chains side by side
 template <typename T, int N>
-__host__ __device__ constexpr int row_block() {
-    return row_group<T, N>() > kThreads ? row_group<T, N>() : kThreads;
+__host__ __device__ constexpr bool row_big_lines() {
+    return N * 2 * sizeof(T) >= 49152 && row_group<T, N>() == kThreads;
 }
 // column tile width for the compile-time column kernels (columns per CTA, one group each)
 template <typename T, int N>
@@ -37,15 +36,17 @@ __host__ __device__ constexpr int col_width() {
 
 __device__ __forceinline__ uint32_t sw7(uint32_t y) { return y ^ ((y >> 3) & 7u); }
 
-template <int G>
+// synchronise one line group of G threads in a block of NT threads: the warp, the whole block, or
+// the group's own named barrier (id bid = 1 + group index; barrier 0 is __syncthreads)
+template <int G, int NT = kThreads>
 __device__ __forceinline__ void group_sync(int bid) {
     if constexpr (G == 32) __syncwarp();
-    else if constexpr (G == kThreads) __syncthreads();
+    else if constexpr (G == NT) __syncthreads();
     else asm volatile("bar.sync %0, %1;" ::"r"(bid), "n"(G) : "memory");
 }
 
 // one in-place stage of a group transform of a line (element y at sw7(y))
-template <int N, int R, int P, int TWOFF, int G, int DIR, typename C>
+template <int N, int R, int P, int TWOFF, int G, int DIR, int NT, typename C>
 __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt, int bid) {
     constexpr int NR = N / R;
     constexpr int B = (NR + G - 1) / G;
@@ -65,7 +66,7 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
             }
         }
     }
-    group_sync<G>(bid);
+    group_sync<G, NT>(bid);
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int bi = gt + i * G;
@@ -102,23 +103,23 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
             }
         }
     }
-    group_sync<G>(bid);
+    group_sync<G, NT>(bid);
 }
 
-template <int N, int G, int DIR, int S, typename C>
+template <int N, int G, int DIR, int NT, int S, typename C>
 __device__ __forceinline__ void gstages(C* line, const C* tw, int gt, int bid) {
     constexpr CPlan cp = FixedPlan<N>::c;
     if constexpr (S < cp.ns) {
-        gstage<N, cp.r[S], cp.p[S], cp.twoff[S], G, DIR>(line, tw, gt, bid);
-        gstages<N, G, DIR, S + 1>(line, tw, gt, bid);
+        gstage<N, cp.r[S], cp.p[S], cp.twoff[S], G, DIR, NT>(line, tw, gt, bid);
+        gstages<N, G, DIR, NT, S + 1>(line, tw, gt, bid);
     }
 }
 
-// in-place transform of one line by the calling group; the caller has
+// in-place transform of one line by the calling group of a block of NT threads; the caller has
 // synchronised the group (or CTA) after writing the line
-template <int N, int G, int DIR, typename C>
+template <int N, int G, int DIR, int NT = kThreads, typename C>
 __device__ __forceinline__ void gfft(C* line, const C* tw, int gt, int bid) {
-    gstages<N, G, DIR, 0>(line, tw, gt, bid);
+    gstages<N, G, DIR, NT, 0>(line, tw, gt, bid);
 }
 
 // contiguous [y][w] tile (global) -> [w][sw7(y)] lines (shared); all loads of a
@@ -185,16 +186,15 @@ __global__ void __launch_bounds__(kThreads) col_inverse_fixed(const StepPlan P, 
 // ---------------------------------------------------------------------------
 // row pass (compile-time NX): I1 -> C2R -> products -> R2C -> I2   (grid: row pairs x batch)
 // ---------------------------------------------------------------------------
-template <typename T, int NX>
-__global__ void __launch_bounds__(row_block<T, NX>(), (row_block<T, NX>() > kThreads ? 1 : 2)) row_pass_fixed(const StepPlan P, const MemberInfo* __restrict__ members,
+template <typename T, int NX, int NT>
+__global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(const StepPlan P, const MemberInfo* __restrict__ members,
                                                            const cplx<T>* __restrict__ i1, cplx<T>* __restrict__ i2,
                                                            const cplx<T>* __restrict__ tw, const double* __restrict__ rho0_member,
                                                            int* __restrict__ err) {
     if (!members[blockIdx.y].active) return;
     using C = cplx<T>;
     constexpr int G = row_group<T, NX>();
-    constexpr int NT = row_block<T, NX>();   // threads per block
-    constexpr int NG = NT / G;
+    constexpr int NG = NT / G;                // line groups per block (NT threads)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* lines = reinterpret_cast<C*>(smem_raw);          // [n_in][NX] physical row pairs
     C* work = lines + static_cast<size_t>(P.n_in) * NX;  // [NG][NX] one product line per group
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(row_block<T, NX>(), (row_block<T, NX>() > kThr
         lines[static_cast<size_t>(s) * NX + sw7(k)] = czero<C>();
     }
     __syncthreads();
-    for (int s = g; s < P.n_in; s += NG) gfft<NX, G, +1>(lines + static_cast<size_t>(s) * NX, tw, gt, bid);
+    for (int s = g; s < P.n_in; s += NG) gfft<NX, G, +1, NT>(lines + static_cast<size_t>(s) * NX, tw, gt, bid);
     __syncthreads();
 
     // 2. velocity: v = j / rho (compressible) or j / rho0 (fcalculator_workspace.cc:115-142);
@@ -292,8 +292,8 @@ __global__ void __launch_bounds__(row_block<T, NX>(), (row_block<T, NX>() > kThr
             if (!has1) val.y = T(0);
             z[x] = val;
         }
-        group_sync<G>(bid);
-        gfft<NX, G, -1>(z, tw, gt, bid);
+        group_sync<G, NT>(bid);
+        gfft<NX, G, -1, NT>(z, tw, gt, bid);
         C* dst = i2 + i2_member + static_cast<size_t>(o) * P.ntiles * npy * W;
         for (int k = gt; k < hx; k += G) {
             const C zk = z[sw7(k)];
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(row_block<T, NX>(), (row_block<T, NX>() > kThr
             q[0] = g0;
             if (has1) q[W] = g1;
         }
-        group_sync<G>(bid);
+        group_sync<G, NT>(bid);
     }
 }
 
