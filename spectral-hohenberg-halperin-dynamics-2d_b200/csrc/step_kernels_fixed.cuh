@@ -35,6 +35,13 @@ __host__ __device__ constexpr int col_width() {
 }
 
 __device__ __forceinline__ uint32_t sw7(uint32_t y) { return y ^ ((y >> 3) & 7u); }
+// shared-memory slot of element y in a line: SB = 3 is sw7 (bank-conflict free for 16-byte elements in
+// the transform stages); SB = 4 XORs four bits, which 8-byte elements need to spread a warp's stores of
+// the radix-8 stages with spans 1 and 8 over all 16 bank pairs
+template <int SB>
+__device__ __forceinline__ uint32_t swz(uint32_t y) {
+    return y ^ ((y >> SB) & ((1u << SB) - 1u));
+}
 
 // synchronise one line group of G threads in a block of NT threads: the warp, the whole block, or
 // the group's own named barrier (id bid = 1 + group index; barrier 0 is __syncthreads)
@@ -46,23 +53,24 @@ __device__ __forceinline__ void group_sync(int bid) {
 }
 
 // one in-place stage of a group transform of a line (element y at sw7(y))
-template <int N, int R, int P, int TWOFF, int G, int DIR, int NT, typename C>
+template <int N, int R, int P, int TWOFF, int G, int DIR, int NT, int SB, typename C>
 __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt, int bid) {
     constexpr int NR = N / R;
     constexpr int B = (NR + G - 1) / G;
     constexpr int ROW = tw_row(R);
+    constexpr int SPAN = 1 << (2 * SB);  // adding a multiple of SPAN leaves the swizzled bits alone
     C v[B][R];
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int bi = gt + i * G;
         if (NR % G == 0 || bi < NR) {
-            if constexpr (NR % 64 == 0) {
-                const uint32_t s0 = sw7(bi);
+            if constexpr (NR % SPAN == 0) {
+                const uint32_t s0 = swz<SB>(bi);
 #pragma unroll
                 for (int q = 0; q < R; ++q) v[i][q] = line[s0 + q * NR];
             } else {
 #pragma unroll
-                for (int q = 0; q < R; ++q) v[i][q] = line[sw7(bi + q * NR)];
+                for (int q = 0; q < R; ++q) v[i][q] = line[swz<SB>(bi + q * NR)];
             }
         }
     }
@@ -82,10 +90,13 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
             }
             bfly<R, DIR>(v[i]);
             const int j = (bi - k) * R + k;
-            if constexpr (P % 64 == 0) {
-                const uint32_t s0 = sw7(j);
+            if constexpr (P % SPAN == 0) {
+                const uint32_t s0 = swz<SB>(j);
 #pragma unroll
                 for (int q = 0; q < R; ++q) line[s0 + q * P] = v[i][q];
+            } else if constexpr (SB != 3) {
+#pragma unroll
+                for (int q = 0; q < R; ++q) line[swz<SB>(j + q * P)] = v[i][q];
             } else if constexpr (R == 8 && P == 1) {
                 // j = 8 bi: sw7(j + q) = 8 bi + (q ^ (bi & 7))
                 C* o = line + 8 * bi;
@@ -106,20 +117,20 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
     group_sync<G, NT>(bid);
 }
 
-template <int N, int G, int DIR, int NT, int S, typename C>
+template <int N, int G, int DIR, int NT, int SB, int S, typename C>
 __device__ __forceinline__ void gstages(C* line, const C* tw, int gt, int bid) {
     constexpr CPlan cp = FixedPlan<N>::c;
     if constexpr (S < cp.ns) {
-        gstage<N, cp.r[S], cp.p[S], cp.twoff[S], G, DIR, NT>(line, tw, gt, bid);
-        gstages<N, G, DIR, NT, S + 1>(line, tw, gt, bid);
+        gstage<N, cp.r[S], cp.p[S], cp.twoff[S], G, DIR, NT, SB>(line, tw, gt, bid);
+        gstages<N, G, DIR, NT, SB, S + 1>(line, tw, gt, bid);
     }
 }
 
-// in-place transform of one line by the calling group of a block of NT threads; the caller has
-// synchronised the group (or CTA) after writing the line
-template <int N, int G, int DIR, int NT = kThreads, typename C>
+// in-place transform of one line by the calling group of a block of NT threads, elements at
+// swz<SB>(y); the caller has synchronised the group (or CTA) after writing the line
+template <int N, int G, int DIR, int NT = kThreads, int SB = 3, typename C>
 __device__ __forceinline__ void gfft(C* line, const C* tw, int gt, int bid) {
-    gstages<N, G, DIR, NT, 0>(line, tw, gt, bid);
+    gstages<N, G, DIR, NT, SB, 0>(line, tw, gt, bid);
 }
 
 // contiguous [y][w] tile (global) -> [w][sw7(y)] lines (shared); all loads of a
@@ -195,6 +206,7 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
     using C = cplx<T>;
     constexpr int G = row_group<T, NX>();
     constexpr int NG = NT / G;                // line groups per block (NT threads)
+    constexpr int SB = sizeof(T) == 4 ? 4 : 3;  // line swizzle (swz<SB>) for this element size
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* lines = reinterpret_cast<C*>(smem_raw);          // [n_in][NX] physical row pairs
     C* work = lines + static_cast<size_t>(P.n_in) * NX;  // [NG][NX] one product line per group
@@ -231,18 +243,18 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
                 C* z = lines + static_cast<size_t>(s) * NX;
                 C av = a[u], cv = c[u];
                 if (k == 0) { av.y = 0; cv.y = 0; }  // C2R uses the real part of the kx = 0 entry
-                z[sw7(k)] = mk(av.x - cv.y, av.y + cv.x);
-                if (k > 0) z[sw7(NX - k)] = mk(av.x + cv.y, cv.x - av.y);
+                z[swz<SB>(k)] = mk(av.x - cv.y, av.y + cv.x);
+                if (k > 0) z[swz<SB>(NX - k)] = mk(av.x + cv.y, cv.x - av.y);
             }
         }
     }
     const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
     for (int e = threadIdx.x; e < P.n_in * nzero; e += NT) {
         const int s = e / nzero, k = hx + (e - s * nzero);
-        lines[static_cast<size_t>(s) * NX + sw7(k)] = czero<C>();
+        lines[static_cast<size_t>(s) * NX + swz<SB>(k)] = czero<C>();
     }
     __syncthreads();
-    for (int s = g; s < P.n_in; s += NG) gfft<NX, G, +1, NT>(lines + static_cast<size_t>(s) * NX, tw, gt, bid);
+    for (int s = g; s < P.n_in; s += NG) gfft<NX, G, +1, NT, SB>(lines + static_cast<size_t>(s) * NX, tw, gt, bid);
     __syncthreads();
 
     // 2. velocity: v = j / rho (compressible) or j / rho0 (fcalculator_workspace.cc:115-142);
@@ -293,11 +305,11 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
             z[x] = val;
         }
         group_sync<G, NT>(bid);
-        gfft<NX, G, -1, NT>(z, tw, gt, bid);
+        gfft<NX, G, -1, NT, SB>(z, tw, gt, bid);
         C* dst = i2 + i2_member + static_cast<size_t>(o) * P.ntiles * npy * W;
         for (int k = gt; k < hx; k += G) {
-            const C zk = z[sw7(k)];
-            const C zn = cconj(z[sw7(k == 0 ? 0 : NX - k)]);
+            const C zk = z[swz<SB>(k)];
+            const C zn = cconj(z[swz<SB>(k == 0 ? 0 : NX - k)]);
             const C g0 = mk(static_cast<T>(0.5) * (zk.x + zn.x), static_cast<T>(0.5) * (zk.y + zn.y));
             const C d = csub(zk, zn);
             const C g1 = mk(static_cast<T>(0.5) * d.y, static_cast<T>(-0.5) * d.x);

@@ -74,6 +74,8 @@ SCRIPTS = {
     "euler_quiescent_n3_64": script(grid=(64, 64), length=(64.0, 64.0), nop=3, dt=0.01, te="euler/quiescent", cT=None, eta=0.0,
                                     zeta=0.0, nonlinear=None, fe="quadratic", a=0.7),
     "srk3_comp_n0_128_none": script(grid=(128, 128), length=(128.0, 128.0), nop=0, dt=0.05, dealias="none"),
+    # rows of 96 compute points, columns of 72: no pair-line family, so FP32 runs the compile-time row pass
+    "srk3_comp_n2_64x48": script(grid=(64, 48), length=(128.0, 96.0), nop=2, dt=0.01),
     "srk3_comp_n1_two_40": script(grid=(40, 40), length=(40.0, 40.0), nop=1, dt=0.01, dealias="two"),
     # compile-time transform sizes (3/2 rule): 256 -> 384, 512 -> 768
     "srk3_comp_n2_256": script(grid=(256, 256), length=(512.0, 512.0), nop=2, dt=0.01),
