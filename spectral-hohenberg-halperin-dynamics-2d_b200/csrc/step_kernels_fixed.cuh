@@ -81,12 +81,17 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
         if (NR % G == 0 || bi < NR) {
             const int k = bi % P;
             if constexpr (P > 1) {
-                const C* t = tw + TWOFF + k * ROW;
+                // one load of w^k per butterfly; its powers by a product tree at most three roundings deep
+                C w[R];
+                w[1] = __ldg(tw + TWOFF + k * ROW);
+                if constexpr (R > 2) w[2] = cmul(w[1], w[1]);
+                if constexpr (R > 3) w[3] = cmul(w[2], w[1]);
+                if constexpr (R > 4) w[4] = cmul(w[2], w[2]);
+                if constexpr (R > 5) w[5] = cmul(w[4], w[1]);
+                if constexpr (R > 6) w[6] = cmul(w[3], w[3]);
+                if constexpr (R > 7) w[7] = cmul(w[4], w[3]);
 #pragma unroll
-                for (int q = 1; q < R; ++q) {
-                    const C w = __ldg(t + q - 1);
-                    v[i][q] = DIR < 0 ? cmul(v[i][q], w) : cmulc(v[i][q], w);
-                }
+                for (int q = 1; q < R; ++q) v[i][q] = DIR < 0 ? cmul(v[i][q], w[q]) : cmulc(v[i][q], w[q]);
             }
             bfly<R, DIR>(v[i]);
             const int j = (bi - k) * R + k;
