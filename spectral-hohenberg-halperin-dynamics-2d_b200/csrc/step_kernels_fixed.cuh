@@ -60,10 +60,12 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
     constexpr int ROW = tw_row(R);
     constexpr int SPAN = 1 << (2 * SB);  // adding a multiple of SPAN leaves the swizzled bits alone
     C v[B][R];
+    C wk[B];  // w^k of each butterfly, loaded before the barrier so its latency overlaps the wait
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int bi = gt + i * G;
         if (NR % G == 0 || bi < NR) {
+            if constexpr (P > 1) wk[i] = __ldg(tw + TWOFF + (bi % P) * ROW);
             if constexpr (NR % SPAN == 0) {
                 const uint32_t s0 = swz<SB>(bi);
 #pragma unroll
@@ -83,7 +85,7 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
             if constexpr (P > 1) {
                 // one load of w^k per butterfly; its powers by a product tree at most three roundings deep
                 C w[R];
-                w[1] = __ldg(tw + TWOFF + k * ROW);
+                w[1] = wk[i];
                 if constexpr (R > 2) w[2] = cmul(w[1], w[1]);
                 if constexpr (R > 3) w[3] = cmul(w[2], w[1]);
                 if constexpr (R > 4) w[4] = cmul(w[2], w[2]);
