@@ -284,14 +284,16 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
         __syncthreads();
     }
 
-    // 3. products -> forward transform -> keep kx < Hx; output o belongs to group o % NG
+    // 3. products -> forward transform -> keep kx < Hx; output o belongs to group o % NG.  In the
+    //    two-group block the outputs left over after the last full round of groups run on the whole
+    //    block, so no group idles through a transform (three outputs: one round of two, then one)
     const size_t i2_member = static_cast<size_t>(b) * P.n_out * P.ntiles * npy * W;
-    C* z = work + static_cast<size_t>(g) * NX;
-    for (int o = g; o < P.n_out; o += NG) {
+    auto one_output = [&](auto gg, int o, C* z, int tid, int barid) {
+        constexpr int GG = decltype(gg)::value;
         const int kind = P.out_kind[o], arg = P.out_arg[o];
         const int s_psi = (kind == OUT_MU || kind == OUT_PSIVX || kind == OUT_PSIVY) ? P.in_slot[1 + arg] : -1;
         const bool use_v = (kind != OUT_MU);
-        for (int x = gt; x < NX; x += G) {
+        for (int x = tid; x < NX; x += GG) {
             const C psi = s_psi >= 0 ? lines[static_cast<size_t>(s_psi) * NX + x] : czero<C>();
             C jx = czero<C>(), jy = czero<C>(), vx = czero<C>(), vy = czero<C>();
             if (use_v) {
@@ -311,10 +313,10 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
             if (!has1) val.y = T(0);
             z[x] = val;
         }
-        group_sync<G, NT>(bid);
-        gfft<NX, G, -1, NT, SB>(z, tw, gt, bid);
+        group_sync<GG, NT>(barid);
+        gfft<NX, GG, -1, NT, SB>(z, tw, tid, barid);
         C* dst = i2 + i2_member + static_cast<size_t>(o) * P.ntiles * npy * W;
-        for (int k = gt; k < hx; k += G) {
+        for (int k = tid; k < hx; k += GG) {
             const C zk = z[swz<SB>(k)];
             const C zn = cconj(z[swz<SB>(k == 0 ? 0 : NX - k)]);
             const C g0 = mk(static_cast<T>(0.5) * (zk.x + zn.x), static_cast<T>(0.5) * (zk.y + zn.y));
@@ -325,7 +327,16 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
             q[0] = g0;
             if (has1) q[W] = g1;
         }
-        group_sync<G, NT>(bid);
+        group_sync<GG, NT>(barid);
+    };
+    constexpr bool kBlockTail = NT > kThreads && NG == 2;
+    const int n_rounds = kBlockTail ? (P.n_out / NG) * NG : P.n_out;
+    for (int o = g; o < n_rounds; o += NG) one_output(std::integral_constant<int, G>{}, o, work + static_cast<size_t>(g) * NX, gt, bid);
+    if constexpr (kBlockTail) {
+        if (n_rounds < P.n_out) {
+            __syncthreads();  // every group is done with its work line
+            for (int o = n_rounds; o < P.n_out; ++o) one_output(std::integral_constant<int, NT>{}, o, work, threadIdx.x, 0);
+        }
     }
 }
 
