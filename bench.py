@@ -102,6 +102,27 @@ def dist_setup():
     return world, rank, local
 
 
+def launch_plan(gpus: int, env) -> str:
+    """How `bench.py --gpus N` runs: "run" (this process is one of the N ranks, or N = 1),
+    "spawn" (N > 1 and no launcher: re-execute under torch.distributed.run with N ranks).
+    A launcher whose world size differs from --gpus is an error, so an N-GPU number is never
+    a silent 1-GPU run."""
+    if gpus < 1:
+        raise SystemExit(f"bench.py: --gpus must be >= 1 (got {gpus})")
+    if "WORLD_SIZE" in env:
+        world = int(env["WORLD_SIZE"])
+        if world != gpus:
+            raise SystemExit(f"bench.py: --gpus {gpus} but the launcher started {world} ranks (WORLD_SIZE)")
+        return "run"
+    return "spawn" if gpus > 1 else "run"
+
+
+def spawn_command(argv, gpus: int, port: int):
+    """torch.distributed.run command line that starts `gpus` ranks of this script on this node."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}", "--master-addr=127.0.0.1",
+            f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+
+
 def init_group(world, local, backend):
     import torch
     import torch.distributed as dist
@@ -400,6 +421,8 @@ def run_b200(args):
                     "what": "set_state(host pinned) + step(1) + get_state(host) through the C ABI every step"},
             "e2e_resident": {"value": resident_value, "unit": UNIT, "what": f"set_state + step({args.steps}) + get_state, one host call"},
             "gpu_launches": launches,
+            "warnings": ([] if peak_kind == "measured" else
+                         [f"MEASURED_PEAKS.json absent: roofline.peak is the fallback {peak:.0f} GB/s, not a measured peak"]),
             "clocks": clk,
             "autotune": tuning,
         }
@@ -730,6 +753,12 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if launch_plan(args.gpus, os.environ) == "spawn":
+        import socket
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            port = s.getsockname()[1]
+        raise SystemExit(subprocess.call(spawn_command(sys.argv[1:], args.gpus, port)))
     if args.impl == "reference":
         run_reference(args)
     else:

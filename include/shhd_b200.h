@@ -385,11 +385,12 @@ const void* shhd_engine_state_device(const shhd_engine* engine);
  * into the library, which each GPU that loads the library holds until the
  * process exits.  A configuration that needs more is rejected with SHHD_EINVAL
  * and a message giving the size it needs (32 MiB covers, for example, a 256^2
- * grid with 3/2 padding, two order parameters and advection in FP64).  The
- * first call on a device looks up that device's address of the array; make
- * that first call before any stream capture.  All calls share the one array,
- * so calls whose work overlaps on the GPU (other streams or host threads)
- * race: serialise them. */
+ * grid with 3/2 padding, two order parameters and advection in FP64).  Each
+ * call looks up the current device's address of the array.  The call is
+ * synchronous: it waits on `stream` for its input checks and again for its
+ * result before returning.  All calls share the one array, which keeps the
+ * last call's contents, so calls whose work overlaps on the GPU (other
+ * streams or host threads) race: serialise them. */
 #define SHHD_NOALLOC_SCRATCH_BYTES (32u << 20)
 int shhd_rhs_noalloc(const shhd_config* cfg, const double* state_dev, double* rhs_dev, size_t n_doubles, void* stream);
 

@@ -1170,6 +1170,9 @@ void sync_and_check(shhd_engine* e) {
     if (err != 0) {
         check_cuda(cudaMemset(e->err_dev, 0, sizeof(int)), "error flag reset");
         if (err & ERR_ZERO_DENSITY) throw Failure(SHHD_ENUMERIC, "compressible velocity encountered zero density.");
+        if (err & ERR_NONFINITE)
+            throw Failure(SHHD_ENUMERIC, "state is not finite (NaN or Inf) after a step: the integration diverged "
+                                         "(timestep outside the stability interval of the stiffest mode, or a state too far from the model's range).");
     }
 }
 
@@ -2394,21 +2397,14 @@ namespace {
 constexpr size_t kNoAllocAlign = 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SHHD_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_base[kNoAllocMaxDevices] = {};
-
-// device address of the scratch array on the current device; the first call on
-// a device looks it up (the array's host-side name is not a device address)
-unsigned char* noalloc_base(int device) {
-    if (device < 0 || device >= kNoAllocMaxDevices) throw Failure(SHHD_EUNSUPPORTED, "device ordinal beyond the supported range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_base[device]) {
-        void* p = nullptr;
-        check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress of the static scratch");
-        g_noalloc_base[device] = static_cast<unsigned char*>(p);
-    }
-    return g_noalloc_base[device];
+// device address of the scratch array on the current device, looked up on every
+// call (cheap beside the call's two stream waits), so a context created anew
+// after cudaDeviceReset is never handed a stale address; the array's host-side
+// name is not a device address
+unsigned char* noalloc_base() {
+    void* p = nullptr;
+    check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress of the static scratch");
+    return static_cast<unsigned char*>(p);
 }
 
 // carves aligned regions out of the scratch array; sizes only, when base is null
@@ -2529,7 +2525,7 @@ extern "C" int shhd_rhs_noalloc(const shhd_config* cfg, const double* state_dev,
         check_device_buffer(state_dev, e.device, "state_dev");
         check_device_buffer(rhs_dev, e.device, "rhs_dev");
         e.stream = static_cast<cudaStream_t>(stream);
-        unsigned char* base = noalloc_base(e.device);
+        unsigned char* base = noalloc_base();
         if (e.fp32) {
             set_smem_attrs<float>(&e);
             rhs_noalloc<float>(&e, state_dev, rhs_dev, base);

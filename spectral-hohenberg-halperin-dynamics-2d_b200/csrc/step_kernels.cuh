@@ -37,7 +37,15 @@ constexpr int kMaxSine = 8;
 
 enum OutKind : int { OUT_MU = 0, OUT_PSIVX, OUT_PSIVY, OUT_GRAD, OUT_VX, OUT_VY, OUT_PXX, OUT_PXY, OUT_PYY };
 enum GroupKind : int { GROUP_PSI = 0, GROUP_MOMENTUM = 1 };
-enum ErrBits : int { ERR_ZERO_DENSITY = 1 };
+enum ErrBits : int { ERR_ZERO_DENSITY = 1, ERR_NONFINITE = 2 };
+
+// A diverging integration leaves NaN or Inf in the state: the state writes test each new
+// value and one lane per warp raises ERR_NONFINITE (all 32 lanes must call this)
+template <typename V>
+__device__ __forceinline__ bool nonfinite2(V v) { return !isfinite(v.x + v.y); }
+__device__ __forceinline__ void report_nonfinite(int* err, bool bad) {
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, ERR_NONFINITE);
+}
 
 struct SineSrc {
     int field;     // state field index
@@ -729,13 +737,17 @@ __global__ void __launch_bounds__(kThreads) col_forward_kernel(const StepPlan P,
         }
         // write the state
         C* dst = A.next + mbase + f * fstride;
+        bool bad = false;
         for (int p = threadIdx.x; p < npos_total; p += blockDim.x) {
             const int w = fdiv(p, P.div_kyn);
             const int j = p - w * kyn;
             const int ky = ky_of_j(j, nay);
             const int y = ky >= 0 ? ky : ky + npy;
-            dst[static_cast<size_t>(w) * kyn + j] = stage_buf[sw(y, mask) * W + w];
+            const C v = stage_buf[sw(y, mask) * W + w];
+            bad |= nonfinite2(v);
+            dst[static_cast<size_t>(w) * kyn + j] = v;
         }
+        report_nonfinite(A.err, bad);
         // y-inverse of the new field for the next stage (scaled by 1/(Nx Ny) on the way out)
         const int slot = P.in_slot[f];
         if (A.fused_inverse && slot >= 0) {

@@ -449,10 +449,14 @@ __global__ void __launch_bounds__(kThreads, 2) col_forward_fixed(const StepPlan 
             }
             group_sync<G>(bid);
         }
+        bool bad = false;
         for (int j = gt; j < kyn; j += G) {
             const int ky = ky_of_j(j, nay);
-            dst[j] = line[sw7(ky >= 0 ? ky : ky + NY)];
+            const C v = line[sw7(ky >= 0 ? ky : ky + NY)];
+            bad |= nonfinite2(v);
+            dst[j] = v;
         }
+        report_nonfinite(A.err, bad);
         const int slot = P.in_slot[f];
         if (A.fused_inverse && slot >= 0) {
             group_sync<G>(bid);

@@ -804,16 +804,20 @@ __global__ void __launch_bounds__(kThreads, 2) pcol_forward(const StepPlan P, co
         wfield[nwf] = P.nop + 2; wsrc[nwf++] = acc1;
         if (comp) { wfield[nwf] = 0; wsrc[nwf++] = acc2; }
     }
+    bool bad = false;
     for (int q = 0; q < nwf; ++q) {
         float2* dst = A.next + static_cast<size_t>(b) * P.nfields * fstride + static_cast<size_t>(wfield[q]) * fstride;
         for (int e = threadIdx.x; e < CP * kyn; e += kThreads) {
             const int c = fdiv(e, P.div_kyn), j = e - c * kyn;
             const PC v = ld_pc(wsrc[q] + e);
             const size_t gx = static_cast<size_t>(2 * (t0 + c));
-            dst[gx * kyn + j] = pc_col(v, 0);
-            dst[(gx + 1) * kyn + j] = pc_col(v, 1);
+            const float2 v0 = pc_col(v, 0), v1 = pc_col(v, 1);
+            bad |= nonfinite2(make_float2(v0.x + v0.y, v1.x + v1.y));
+            dst[gx * kyn + j] = v0;
+            dst[(gx + 1) * kyn + j] = v1;
         }
     }
+    report_nonfinite(A.err, bad);
 
     // y-inverse (DIT) of each new field the next stage transforms: the gather of
     // the new modes from the per-mode arrays is fused into its first stage, the

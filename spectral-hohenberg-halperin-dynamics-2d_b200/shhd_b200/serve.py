@@ -4,9 +4,13 @@ Jobs of mixed grid, component count and mode arrive over time.  Jobs whose
 configurations differ only in temperature and seed share a *bucket*: one
 batched engine whose members are slots.  A job is admitted into a free slot
 as soon as it has arrived and a slot (or HBM for a new bucket engine) is
-free; every scheduling round enqueues one chunk of steps on each bucket with
-active slots, each bucket on its own CUDA stream, so buckets overlap on the
-device; finished jobs are read back and their slots reused.
+free; a bucket whose slots are all free gives its HBM back when another shape
+needs it.  Each bucket keeps one chunk of steps in flight on its own CUDA
+stream, so buckets overlap on the device; the loop polls each chunk's event,
+reads finished jobs back and reuses their slots.  A job that no empty server
+could hold is refused up front (AdmissionError), so the loop never waits for
+room that cannot appear.  partition_jobs / serve_distributed split a stream
+over ranks (one server per GPU) with a single gather of statistics at the end.
 
 A job's result does not depend on what else is running: its noise is keyed by
 (server seed, job key) at the job's own step count (engine step index minus
@@ -64,9 +68,17 @@ def _noisy(cfg: Config) -> bool:
     return bool(cfg.noise_momentum or cfg.noise_order_parameter)
 
 
+def _torch_event(engine):
+    """A CUDA event recorded on the engine's stream after its enqueued work."""
+    import torch
+    ev = torch.cuda.Event()
+    ev.record(torch.cuda.ExternalStream(engine.stream))
+    return ev
+
+
 class _Bucket:
     def __init__(self, cfg: Config, slots: int, precision: int, seed: int, graph_chunk: int = 0,
-                 green_kubo: Optional[Tuple[int, int]] = None):
+                 green_kubo: Optional[Tuple[int, int]] = None, engine_factory=Engine):
         c = cfg.copy()
         c.batch = slots
         c.precision = precision
@@ -74,7 +86,8 @@ class _Bucket:
         c.member_offset = 0
         if _noisy(cfg):
             c.kBT = 1.0  # members carry sqrt(kBT_job) as their amplitude factor
-        self.engine = Engine(c)
+        self.engine = engine_factory(c)
+        self.device_bytes = int(self.engine.get_info().device_bytes)
         if graph_chunk > 0:
             self.engine.set_graph_chunk(graph_chunk)
         self.green_kubo = green_kubo
@@ -84,6 +97,7 @@ class _Bucket:
         self.remaining = [0] * slots
         self.step_index = 0
         self.noisy = _noisy(cfg)
+        self.inflight: Optional[Tuple[int, object]] = None   # (steps, completion event) of the enqueued chunk
         for m in range(slots):
             self.engine.set_member(m, key=0, active=False)
 
@@ -112,19 +126,38 @@ class _Bucket:
         return any(j is not None for j in self.slots)
 
 
+class AdmissionError(RuntimeError):
+    """A job that no empty server could hold (its bucket of one slot exceeds the HBM budget)."""
+
+
 class Server:
+    """Continuous batching of trajectory jobs within a device-memory budget.
+
+    `hbm_budget` caps the device bytes of the bucket engines (default: 80% of the free
+    memory).  A bucket whose slots are all free is destroyed, and its bytes returned to the
+    budget, when a job needs room for a new bucket.  A job that would not fit even into an
+    empty server is refused with AdmissionError before anything runs.  `engine_factory`
+    (default: the engine) and `event_factory` (default: a CUDA event on the engine's stream)
+    are the only device-facing parts; tests of the scheduling replace them."""
+
     def __init__(self, precision: int = FP32, seed: int = 20240601, max_slots: int = 32, chunk: int = 25,
-                 hbm_budget: Optional[int] = None, graphs: bool = True):
-        import torch
+                 hbm_budget: Optional[int] = None, graphs: bool = True, engine_factory=Engine, event_factory=_torch_event):
         self.graphs = graphs
         self.precision = precision
         self.seed = seed
         self.max_slots = max_slots
         self.chunk = chunk
-        free, _total = torch.cuda.mem_get_info()
-        self.budget = int(0.8 * free) if hbm_budget is None else int(hbm_budget)
+        self.engine_factory = engine_factory
+        self.event_factory = event_factory
+        if hbm_budget is None:
+            import torch
+            free, _total = torch.cuda.mem_get_info()
+            hbm_budget = int(0.8 * free)
+        self.budget = int(hbm_budget)
         self.used = 0
         self.buckets: Dict[bytes, List[_Bucket]] = {}
+        self.buckets_created = 0
+        self.buckets_released = 0
         self._member_bytes: Dict[bytes, int] = {}
 
     def _per_member_bytes(self, key: bytes, cfg: Config) -> int:
@@ -132,9 +165,31 @@ class Server:
             c = cfg.copy()
             c.batch = 1
             c.precision = self.precision
-            with Engine(c) as probe:
+            probe = self.engine_factory(c)
+            try:
                 self._member_bytes[key] = int(probe.get_info().device_bytes) + probe.info.state_doubles * 8
+            finally:
+                probe.close()
         return self._member_bytes[key]
+
+    def _release_idle(self) -> int:
+        """Destroy bucket engines with no job and nothing in flight; return the bytes freed."""
+        freed = 0
+        for key in list(self.buckets):
+            keep = []
+            for b in self.buckets[key]:
+                if b.active() or b.inflight is not None:
+                    keep.append(b)
+                else:
+                    b.engine.close()
+                    freed += b.device_bytes
+                    self.buckets_released += 1
+            if keep:
+                self.buckets[key] = keep
+            else:
+                del self.buckets[key]
+        self.used -= freed
+        return freed
 
     def _slot_for(self, job: Job) -> Optional[Tuple[_Bucket, int]]:
         key = bucket_key(job.config, job.green_kubo)
@@ -143,16 +198,52 @@ class Server:
             if m is not None:
                 return b, m
         per = self._per_member_bytes(key, job.config)
+        if self.budget - self.used < per:
+            self._release_idle()
         slots = min(self.max_slots, (self.budget - self.used) // per)
         if slots < 1:
             return None
-        b = _Bucket(job.config, int(slots), self.precision, self.seed, self.chunk if self.graphs else 0, job.green_kubo)
-        self.used += int(b.engine.get_info().device_bytes)
+        b = _Bucket(job.config, int(slots), self.precision, self.seed, self.chunk if self.graphs else 0, job.green_kubo,
+                    engine_factory=self.engine_factory)
+        self.used += b.device_bytes
+        self.buckets_created += 1
         self.buckets.setdefault(key, []).append(b)
         return b, 0
 
+    def _check_admissible(self, jobs: List[Job]) -> None:
+        for job in jobs:
+            per = self._per_member_bytes(bucket_key(job.config, job.green_kubo), job.config)
+            if per > self.budget:
+                raise AdmissionError(f"job {job.key} needs {per} bytes of device memory for one slot, more than the "
+                                     f"server's budget of {self.budget} bytes")
+
+    def _finish_chunk(self, b: _Bucket, now: float) -> int:
+        n, _ev = b.inflight
+        b.inflight = None
+        b.engine.synchronize()   # returns at once; raises the engine's device error word (zero density)
+        b.step_index += n
+        done = 0
+        for m, job in enumerate(b.slots):
+            if job is None:
+                continue
+            b.remaining[m] -= n
+            if b.remaining[m] == 0:
+                job.result = b.engine.get_state(m)
+                if b.green_kubo is not None:
+                    job.gk_sums, job.gk_blocks = b.engine.gk_read(m, reset=True)
+                job.finished = now
+                b.engine.set_member(m, key=0, active=False)
+                b.slots[m] = None
+                done += 1
+        return done
+
     def run(self, jobs: List[Job]) -> Dict[str, float]:
-        """Serve `jobs` (arrival times relative to now) until all have finished."""
+        """Serve `jobs` (arrival times relative to now) until all have finished.
+
+        Each bucket has at most one chunk in flight; chunks of different buckets overlap on the
+        device (one stream per engine), and a finished chunk is noticed by polling its event, so
+        one slow bucket does not hold back the admissions and launches of the others."""
+        self._check_admissible(jobs)
         future = sorted(jobs, key=lambda j: j.arrival)
         pending: List[Job] = []
         t0 = time.perf_counter()
@@ -169,34 +260,31 @@ class Server:
                 else:
                     slot[0].admit(slot[1], job, now)
             pending = still
-            stepped = []
+            inflight = []
             for group in self.buckets.values():
                 for b in group:
-                    if not b.active():
-                        continue
-                    n = min(self.chunk, min(r for j, r in zip(b.slots, b.remaining) if j is not None))
-                    b.engine.step_async(n)
-                    stepped.append((b, n))
-            if not stepped:
+                    if b.inflight is None and b.active():
+                        n = min(self.chunk, min(r for j, r in zip(b.slots, b.remaining) if j is not None))
+                        b.engine.step_async(n)
+                        b.inflight = (n, self.event_factory(b.engine))
+                    if b.inflight is not None:
+                        inflight.append(b)
+            if not inflight:
+                if pending and not future:
+                    # every bucket is idle, so _slot_for released them all and still found no room
+                    raise AdmissionError(f"{len(pending)} jobs cannot be admitted into an empty server "
+                                         f"(budget {self.budget} bytes)")
                 if future:
                     time.sleep(max(0.0, min(0.002, future[0].arrival - (time.perf_counter() - t0))))
                 continue
-            for b, n in stepped:
-                b.engine.synchronize()
-                b.step_index += n
-                now = time.perf_counter() - t0
-                for m, job in enumerate(b.slots):
-                    if job is None:
-                        continue
-                    b.remaining[m] -= n
-                    if b.remaining[m] == 0:
-                        job.result = b.engine.get_state(m)
-                        if b.green_kubo is not None:
-                            job.gk_sums, job.gk_blocks = b.engine.gk_read(m, reset=True)
-                        job.finished = now
-                        b.engine.set_member(m, key=0, active=False)
-                        b.slots[m] = None
-                        done += 1
+            ready = [b for b in inflight if b.inflight[1].query()]
+            if not ready:
+                # nothing finished yet: wait for the oldest chunk rather than spin
+                inflight[0].inflight[1].synchronize()
+                ready = [inflight[0]]
+            now = time.perf_counter() - t0
+            for b in ready:
+                done += self._finish_chunk(b, now)
         makespan = time.perf_counter() - t0
         lat = np.array([j.latency for j in jobs])
         return {
@@ -205,7 +293,8 @@ class Server:
             "steps_per_s": float(sum(j.nsteps for j in jobs) / makespan),
             "p50_s": float(np.percentile(lat, 50)),
             "p99_s": float(np.percentile(lat, 99)),
-            "buckets": sum(len(v) for v in self.buckets.values()),
+            "buckets": self.buckets_created,
+            "buckets_released": self.buckets_released,
         }
 
     def close(self) -> None:
@@ -213,6 +302,56 @@ class Server:
             for b in group:
                 b.engine.close()
         self.buckets.clear()
+        self.used = 0
+
+
+def job_cost(job: Job) -> float:
+    """Relative device work of a job: steps x compute-grid points x fields."""
+    c = job.config
+    return float(job.nsteps) * c.nx * c.ny * (c.num_order_parameters + 3)
+
+
+def partition_jobs(jobs: List[Job], world: int) -> List[List[Job]]:
+    """Split a stream's jobs over `world` ranks (one server per GPU): longest job first onto
+    the least-loaded rank.  Deterministic, so every rank computes the same split."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    load = [0.0] * world
+    parts: List[List[Job]] = [[] for _ in range(world)]
+    for job in sorted(jobs, key=lambda j: (-job_cost(j), j.key)):
+        r = min(range(world), key=lambda i: (load[i], i))
+        parts[r].append(job)
+        load[r] += job_cost(job)
+    for p in parts:
+        p.sort(key=lambda j: j.arrival)
+    return parts
+
+
+def serve_distributed(server: Server, jobs: List[Job], rank: int, world: int, group=None) -> Dict[str, float]:
+    """Serve this rank's share of `jobs` (partition_jobs) and combine the ranks' statistics:
+    aggregate steps/s over the slowest rank's makespan, p50/p99 over every job's latency.
+    The exchange is one all_gather of (makespan, steps, latencies) after the run, no
+    per-step collective."""
+    import torch.distributed as dist
+    mine = partition_jobs(jobs, world)[rank]
+    stats = server.run(mine) if mine else {"makespan_s": 0.0}
+    local = {"makespan_s": stats["makespan_s"], "steps": sum(j.nsteps for j in mine), "latency": [j.latency for j in mine],
+             "jobs": len(mine)}
+    if world > 1:
+        gathered: List[dict] = [None] * world  # type: ignore[list-item]
+        dist.all_gather_object(gathered, local, group=group)
+    else:
+        gathered = [local]
+    makespan = max(g["makespan_s"] for g in gathered)
+    lat = np.array([x for g in gathered for x in g["latency"]])
+    return {
+        "jobs": sum(g["jobs"] for g in gathered),
+        "jobs_per_rank": [g["jobs"] for g in gathered],
+        "makespan_s": makespan,
+        "steps_per_s": float(sum(g["steps"] for g in gathered) / makespan) if makespan > 0 else 0.0,
+        "p50_s": float(np.percentile(lat, 50)),
+        "p99_s": float(np.percentile(lat, 99)),
+    }
 
 
 def run_alone(job: Job, precision: int, seed: int) -> np.ndarray:

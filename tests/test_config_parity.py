@@ -1,0 +1,181 @@
+"""Parity at the benchmark configurations' full sizes, against the reference's own code (GPU).
+
+The reference checker (oracle/_ref/libshhd_ref.so: the reference's unmodified src/*.cc on
+single-rank MPI / heFFTe shims) runs here on the host cores beside the engine: it builds the
+initial state from the script's own `set` lines, steps with its own integrator and records
+the stochastic right-hand sides it drew; the engine replays that noise
+(shhd_engine_set_external_noise) from the same initial state.  Tolerances are those of the
+FP64 / FP32 bounds: relative L2 over the whole state <= 1e-12 (FP64) and <= 1e-5 (FP32).
+
+  * 128^2, N = 0 compressible, 3/2 rule (192^2), equilibrium initial density and momentum
+    (seed 1), kBT 1e-4, SRK3 dt 0.05, noise on: 5 steps.
+  * 1024^2, N = 2 compressible phi4 with advection (3/2 rule: 1536^2, the FP32 pair-line
+    kernels), kBT 1e-3, SRK3 dt 0.01: 2 steps.
+  * 4096^2 incompressible turbulence (6144^2), kBT = 0, FP32 against the FP64 engine (itself
+    pinned to the oracle): a deterministic trajectory of 3 steps.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import shhd_oracle as so
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libshhd_ref.so")
+TOL64 = 1e-12
+TOL32 = 1e-5
+
+PLAIN_128 = """dimension 2
+grid 128 128
+length 128 128
+dealias 3/2
+order_parameters 0
+timestep 0.05
+time_evolution srk3/compressible
+model thermo linear_eos cT 1
+model transport constant eta 1 zeta 1
+fix 1 all nonlinear on
+fix 2 all noise on seed 1 kBT 1e-4
+set density equilibrium/gaussian kBT 1e-4 rho0 1 cT 1 seed 1
+set momentum all equilibrium/gaussian/compressible kBT 1e-4 seed 1
+run 2000
+"""
+
+HH_1024 = """dimension 2
+grid 1024 1024
+length 2048 2048
+dealias 3/2
+order_parameters 2
+timestep 0.01
+time_evolution srk3/compressible
+model thermo linear_eos cT 1
+model free_energy phi4 a[0] -1 b[0] 1 u[0] 1 a[1] -1 b[1] 1 u[1] 1
+model transport constant eta 1 zeta 1 M[0,0] 1 M[1,1] 1
+fix 1 all nonlinear on
+fix 2 all noise on seed 7 kBT 1e-3
+set density uniform value 1.0
+set order_parameter all equilibrium/gaussian seed 7 kBT 0.0400782395901117 k0 1 k2 0
+run 10000
+"""
+
+TURB_4096_DET = """dimension 2
+grid 4096 4096
+length 4096 4096
+dealias 3/2
+order_parameters 0
+timestep 0.001
+time_evolution srk3/incompressible
+model transport constant eta 1e-4 zeta 0
+fix 1 momentum nonlinear on
+run 2000
+"""
+
+
+class Reference:
+    """The reference's own solver for one script (its initial state, steps and drawn noise)."""
+
+    def __init__(self, text):
+        if not os.path.exists(REF_LIB):
+            pytest.skip("reference checker not built (oracle/_ref)")
+        lib = ctypes.CDLL(REF_LIB)
+        lib.shref_create.restype = ctypes.c_void_p
+        lib.shref_last_error.restype = ctypes.c_char_p
+        self.lib = lib
+        self.h = ctypes.c_void_p(lib.shref_create(text.encode()))
+        if not self.h.value:
+            raise RuntimeError(lib.shref_last_error().decode())
+        info = (ctypes.c_long * 10)()
+        dinfo = (ctypes.c_double * 4)()
+        lib.shref_info(self.h, info, dinfo)
+        self.shape = (info[4], info[1], info[0] // 2 + 1)
+
+    def state(self):
+        u = np.zeros(self.shape, complex)
+        self.lib.shref_get_state(self.h, u.ctypes.data_as(ctypes.c_void_p))
+        return u
+
+    def step(self):
+        """One step; returns the (sto_a, sto_b) right-hand sides the reference drew."""
+        noise = np.zeros((2,) + self.shape, complex)
+        if self.lib.shref_step(self.h, 1, noise.ctypes.data_as(ctypes.c_void_p)) != 0:
+            raise RuntimeError(self.lib.shref_last_error().decode())
+        return noise
+
+    def close(self):
+        self.lib.shref_destroy(self.h)
+
+
+def _engine(sb, text, precision, external_noise):
+    cfg = sb.config_from_script(text)
+    cfg.precision = precision
+    cfg.noise_source = sb.NOISE_EXTERNAL if external_noise else sb.NOISE_PHILOX
+    return sb.Engine(cfg)
+
+
+def _replay(text, nsteps):
+    """The reference's initial state, its states after each step and the noise of each step."""
+    ref = Reference(text)
+    u0 = ref.state()
+    states, noises = [], []
+    for _ in range(nsteps):
+        noises.append(ref.step())
+        states.append(ref.state())
+    ref.close()
+    return u0, states, noises
+
+
+@pytest.mark.parametrize("text,nsteps", [(PLAIN_128, 5), (HH_1024, 2)], ids=["plain_128", "hh_1024"])
+def test_reference_trajectory_with_its_noise(text, nsteps):
+    import shhd_b200 as sb
+    u0, states, noises = _replay(text, nsteps)
+    for precision, tol in ((sb.FP64, TOL64), (sb.FP32, TOL32)):
+        with _engine(sb, text, precision, True) as eng:
+            eng.set_state(u0)
+            for s in range(nsteps):
+                eng.set_external_noise(noises[s][0], noises[s][1])
+                eng.step(1)
+                err = so.rel_l2(eng.get_state(), states[s])
+                assert err < tol, f"precision {precision} step {s}: rel L2 {err:.3e}"
+
+
+def test_reference_rhs_at_1024():
+    """The deterministic right-hand side of the 1024^2 N = 2 workload at the reference's own
+    initial state, FP64 and FP32 (the pair-line kernels of the benchmark)."""
+    import shhd_b200 as sb
+    ref = Reference(HH_1024)
+    u0 = ref.state()
+    want = np.zeros(ref.shape, complex)
+    assert ref.lib.shref_rhs(ref.h, ctypes.c_double(0.0), want.ctypes.data_as(ctypes.c_void_p)) == 0
+    ref.close()
+    for precision, tol in ((sb.FP64, TOL64), (sb.FP32, TOL32)):
+        with _engine(sb, HH_1024, precision, False) as eng:
+            eng.set_state(u0)
+            err = so.rel_l2(eng.rhs(), want)
+        assert err < tol, f"precision {precision}: rel L2 {err:.3e}"
+
+
+def test_turbulence_4096_fp32_tracks_fp64():
+    """4096^2 incompressible (6144^2 transforms) with kBT = 0: the FP32 trajectory stays within
+    1e-5 of the FP64 one over 3 steps, from the random-vorticity initial momentum generated on
+    the device."""
+    import shhd_b200 as sb
+    from shhd_b200.initial import initial_state_device
+    init = TURB_4096_DET.replace("run 2000", "set density uniform value 1.0\n"
+                                 "set momentum all random_vorticity n0 8 sigma 2 urms 1 seed 11\nrun 2000")
+    out = {}
+    for precision in (sb.FP64, sb.FP32):
+        with _engine(sb, init, precision, False) as eng:
+            if precision == sb.FP64:
+                initial_state_device(eng, init)
+                u0 = eng.get_state()
+            else:
+                eng.set_state(u0)
+            eng.step(3)
+            out[precision] = eng.get_state()
+    err = so.rel_l2(out[sb.FP32], out[sb.FP64])
+    assert err < TOL32, f"rel L2 {err:.3e}"
+    assert so.rel_l2(out[sb.FP64], u0) > 1e-9  # the state moved

@@ -84,8 +84,13 @@ SCRIPTS = {
 }
 
 
+# fixed seed per time evolution, so every run draws the same inputs
+SEEDS = {"euler/compressible": 11, "srk3/compressible": 12, "euler/incompressible": 21, "srk3/incompressible": 22,
+         "euler/quiescent": 31, "srk3/quiescent": 32}
+
+
 def _state_for(cfg):
-    return random_state(cfg, seed=hash(cfg.time_evolution) % 1000, amp=0.05, transverse=(cfg.mode == "incompressible"))
+    return random_state(cfg, seed=SEEDS[cfg.time_evolution], amp=0.05, transverse=(cfg.mode == "incompressible"))
 
 
 @pytest.mark.parametrize("name", sorted(SCRIPTS))
@@ -289,3 +294,31 @@ def test_rhs_with_512_thread_row_groups(sb, name):
         eng.set_state(u)
         got = eng.rhs()
     assert so.rel_l2(got, want) < (TOL64 if precision == 0 else TOL32_6144), name
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_divergence_is_reported(sb, precision):
+    """At grid spacing 1 the phi4 gradient term puts the highest active modes at
+    lambda dt = -M k^2 (a + b k^2) dt ~ -3.7 at dt = 0.01, outside SRK3's stability interval,
+    so the state overflows; the step call reports the non-finite state instead of returning it."""
+    text = script(grid=(64, 64), length=(64.0, 64.0), nop=2, dt=0.01)
+    cfg = so.parse_script(text)
+    u0 = random_state(cfg, seed=6)
+    with make_engine(sb, text, precision) as eng:
+        eng.set_state(u0)
+        eng.step(5)                       # still finite early on
+        with pytest.raises(sb.ShhdError) as ei:
+            for _ in range(40):
+                eng.step(100)
+        assert ei.value.code == sb.SHHD_ENUMERIC
+        assert "not finite" in str(ei.value)
+
+
+def test_stable_run_reports_nothing(sb):
+    """The same model at grid spacing 2 stays inside the stability interval: no report."""
+    text = script(grid=(64, 64), length=(128.0, 128.0), nop=2, dt=0.01, noise="kBT 0.001 seed 4")
+    cfg = so.parse_script(text)
+    with make_engine(sb, text, 1) as eng:
+        eng.set_state(random_state(cfg, seed=6))
+        eng.step(2000)
+        assert np.all(np.isfinite(eng.get_state()))

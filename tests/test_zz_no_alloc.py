@@ -6,8 +6,9 @@ reserved its device memory up front.  shhd_rhs_noalloc serves them: the caller
 passes device buffers it already owns, and every intermediate lives in a
 fixed array compiled into the library.  These tests call it through the C ABI
 and check it against shhd_engine_rhs (the engine entry point, which allocates)
-on consecutive calls, so that anything left in the shared array by one call
-would show up in the next.  This file is collected last on purpose.
+and against the FP64 oracle's right-hand side, on consecutive calls, so that
+anything left in the shared array by one call would show up in the next.
+This file is collected last on purpose.
 """
 import ctypes
 
@@ -30,6 +31,8 @@ CASES = [
     # incompressible: uses the reference density of the input state
     dict(grid=(64, 64), length=(64.0, 64.0), nop=0, dt=0.01, te="srk3/incompressible", cT=None, eta=0.05, zeta=0.0,
          nonlinear="momentum"),
+    # quiescent: psi only, the physical chemical potential is the one product
+    dict(grid=(64, 64), length=(128.0, 128.0), nop=1, dt=0.02, te="srk3/quiescent", cT=None, eta=0.0, zeta=0.0, nonlinear=None),
 ]
 
 
@@ -73,6 +76,25 @@ def test_noalloc_rhs_matches_engine_on_consecutive_calls(precision):
             assert np.all(np.isfinite(got))
             err = so.rel_l2(got, want)
             assert err < tol, f"case {ci} call {call}: rel L2 {err:.3e}"
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_noalloc_rhs_matches_oracle(precision):
+    """The same calls against the FP64 oracle's deterministic RHS directly (not only the engine)."""
+    import torch
+    import shhd_b200 as sb
+    tol = TOL64 if precision == 0 else TOL32
+    for ci, kw in enumerate(CASES):
+        text = script(**kw)
+        cfg = sb.config_from_script(text)
+        cfg.precision = precision
+        ocfg = so.parse_script(text)
+        for call, seed in enumerate((41 + ci, 53 + ci)):
+            u = random_state(ocfg, seed=seed, rho0=1.0 + 0.5 * call, transverse=ocfg.mode == "incompressible")
+            want = so.Oracle(ocfg).rhs(u)
+            got = _noalloc(sb, torch, cfg, u)
+            err = so.rel_l2(got, want)
+            assert err < tol, f"case {ci} call {call}: rel L2 {err:.3e} against the oracle"
 
 
 def test_noalloc_rhs_on_a_caller_stream():
