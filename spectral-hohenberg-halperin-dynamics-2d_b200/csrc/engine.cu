@@ -22,6 +22,7 @@
 #include "step_kernels.cuh"
 #include "step_kernels_fixed.cuh"
 #include "step_kernels_pair.cuh"
+#include "step_reg.h"
 
 using namespace shhd;
 
@@ -234,7 +235,11 @@ struct shhd_engine {
     bool row_fixed = false;       // compile-time row kernel (group per line)
     int row_nt = 256;             // its threads per block (512: two line groups, for lines of 48 KB or more)
     bool pair_path = false;       // FP32 pair-line kernels (compile-time sizes up to 1536)
-    int family_override = -1;     // -1 choose, 0 never the pair-line kernels, 1 pair-line where valid
+    bool reg_row = false;         // register-resident row pass on 1536-point rows (pair-line layout)
+    int family_override = -1;     // -1 choose, 0 never the pair-line kernels, 1 pair-line where valid,
+                                  // 2 pair-line with the register-resident row pass where valid
+    void* tw_reg = nullptr;       // twiddles of the register-resident transforms (FP32 engines with 1536-point rows)
+    size_t smem_rrow = 0;
     size_t tw_bytes = 0;
     size_t smem_col_inv = 0;
     size_t smem_col = 0, smem_row = 0;
@@ -292,7 +297,7 @@ void* dalloc(shhd_engine* e, size_t bytes) {
 void free_engine(shhd_engine* e) {
     for (void* p : {static_cast<void*>(e->k0_u), static_cast<void*>(e->k0_s1), static_cast<void*>(e->k0_s2)})
         if (p) cudaFree(p);
-    for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->ref_stage,
+    for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->tw_reg, e->ref_stage,
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
                     static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch), e->meas.tw_x, e->meas.tw_y, e->meas.i1,
@@ -718,6 +723,13 @@ void build_plan(shhd_engine* e) {
             plan_row_pairs(P);
         }
     }
+    // register-resident row pass (1536-point rows of the pair-line layout)
+    e->reg_row = false;
+    if (e->pair_path && e->family_override == 2 && c.nx == kRegRowN && c.ny % 2 == 0 && P.rp_canon && rrow_rounds(P) >= 2 &&
+        rrow_rounds(P) <= 4) {
+        e->smem_rrow = rrow_smem_bytes(P);
+        e->reg_row = e->smem_rrow <= smem_cap;
+    }
 
     e->state_elems = static_cast<size_t>(P.nfields) * P.hx * P.kyn;
     e->i1_elems = static_cast<size_t>(P.n_in) * P.hx * c.ny;
@@ -835,6 +847,11 @@ void launch_row(shhd_engine* e) {
     dim3 grid((P.npy + 1) / 2, P.batch);
     LaunchScope scope(e, 1, static_cast<double>(sizeof(cplx<T>)) * P.batch * (P.n_in + P.n_out) * static_cast<double>(P.hx) * P.npy);
     if constexpr (std::is_same<T, float>::value) {
+        if (e->pair_path && e->reg_row && e->tw_reg) {
+            launch_rrow_pass(P, P.batch, e->smem_rrow, e->stream, e->members_dev, e->i1, e->i2, e->tw_reg, e->rho0_dev, e->err_dev);
+            check_cuda(cudaGetLastError(), "row_pass launch");
+            return;
+        }
         if (e->pair_path) {
             with_pair_size(P.npx, [&](auto fx) {
                 constexpr int FX = decltype(fx)::value;
@@ -1287,6 +1304,13 @@ void init_device(shhd_engine* e) {
     e->tw_bytes = twx.size() + twy.size();
     check_cuda(cudaMemcpyAsync(e->tw_x, twx.data(), twx.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
     check_cuda(cudaMemcpyAsync(e->tw_y, twy.data(), twy.size(), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+    if (e->fp32 && e->cfg.nx == kRegRowN) {
+        std::vector<float> t(reg_twiddle_floats());
+        reg_twiddles(t.data());
+        e->tw_reg = dalloc(e, t.size() * sizeof(float));
+        check_cuda(cudaMemcpyAsync(e->tw_reg, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, e->stream), "twiddle upload");
+        check_cuda(cudaStreamSynchronize(e->stream), "twiddle upload");
+    }
     e->rho0_dev = static_cast<double*>(dalloc(e, sizeof(double) * B));
     check_cuda(cudaMemsetAsync(e->rho0_dev, 0, sizeof(double) * B, e->stream), "memset");
     e->err_dev = static_cast<int*>(dalloc(e, sizeof(int)));
@@ -1571,7 +1595,7 @@ void apply_family(shhd_engine* e, int family) {
     check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
     drop_graphs(e);
     e->family_override = family;
-    e->pair_path = e->col_fixed = e->row_fixed = false;
+    e->pair_path = e->col_fixed = e->row_fixed = e->reg_row = false;
     build_plan(e);
     for (void* p : {e->tw_x, e->tw_y})
         if (p) cudaFree(p);
@@ -1624,6 +1648,10 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
             probe.pair_path = probe.col_fixed = probe.row_fixed = false;
             build_plan(&probe);
             if (probe.pair_path) families.push_back(1);
+            probe.family_override = 2;
+            probe.pair_path = probe.col_fixed = probe.row_fixed = probe.reg_row = false;
+            build_plan(&probe);
+            if (probe.reg_row && e->tw_reg) families.push_back(2);
         }
         int chunk_trial = trial_steps;
         if (e->cfg.integrator == SHHD_EULER && chunk_trial % 2) ++chunk_trial;
@@ -2321,6 +2349,21 @@ int shhd_engine_gk_read(shhd_engine* e, int member, double* sums, size_t n, int6
         if (nsample) *nsample = done - e->gk_sample_base[member];
         if (reset) e->gk_sample_base[member] = done;
     });
+}
+
+int shhd_engine_set_family(shhd_engine* e, int family) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (family < -1 || family > 2) throw Failure(SHHD_EINVAL, "kernel family must be -1, 0, 1 or 2");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        if (e->fp32) apply_family<float>(e, family);
+        else apply_family<double>(e, family);
+    });
+}
+
+int shhd_engine_family(const shhd_engine* e) {
+    if (!e) return -1;
+    return e->reg_row ? 2 : (e->pair_path ? 1 : 0);
 }
 
 int shhd_engine_set_graph_chunk(shhd_engine* e, int chunk) {

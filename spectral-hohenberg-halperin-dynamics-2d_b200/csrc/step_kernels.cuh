@@ -1260,7 +1260,7 @@ __device__ __forceinline__ void ic_vorticity(const IcSpec& s, int gx, int ky, do
     uy = make_double2(ay * om.y, -ay * om.x);   // -(i kx / k^2) omega
 }
 
-__device__ double2 ic_value(const IcSpec& s, int gx, int ky) {
+__device__ inline double2 ic_value(const IcSpec& s, int gx, int ky) {
     const double kx = 2.0 * 3.14159265358979323846 * gx / s.lx, kyv = 2.0 * 3.14159265358979323846 * ky / s.ly;
     const double k2 = kx * kx + kyv * kyv;
     const bool zero = gx == 0 && ky == 0;
@@ -1321,7 +1321,7 @@ __global__ void __launch_bounds__(kThreads) initial_field_kernel(const StepPlan 
 
 // block sums of w (|u_x|^2 + |u_y|^2) of the random-vorticity shell over the active modes, w = 2 off the
 // kx = 0 line; partial[blockIdx.x].  grid: ceil(Hx * Ky / 256)
-__global__ void __launch_bounds__(kThreads) vorticity_norm_kernel(const StepPlan P, const IcSpec s, double* __restrict__ partial) {
+static __global__ void __launch_bounds__(kThreads) vorticity_norm_kernel(const StepPlan P, const IcSpec s, double* __restrict__ partial) {
     __shared__ double red[kThreads / 32];
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
@@ -1344,7 +1344,7 @@ __global__ void __launch_bounds__(kThreads) vorticity_norm_kernel(const StepPlan
 }
 
 // out[v] = sum over i < n of partial[i * nv + v] in a fixed order (deterministic); grid: nv blocks of kThreads
-__global__ void __launch_bounds__(kThreads) sum_partials_kernel(const double* __restrict__ partial, int n, int nv, double* __restrict__ out) {
+static __global__ void __launch_bounds__(kThreads) sum_partials_kernel(const double* __restrict__ partial, int n, int nv, double* __restrict__ out) {
     __shared__ double red[kThreads];
     const int v = blockIdx.x;
     double t = 0.0;
@@ -1360,7 +1360,7 @@ __global__ void __launch_bounds__(kThreads) sum_partials_kernel(const double* __
 
 // the incompressible check on two momentum specs, in FP64 (initial_condition.cc:7-40): sets *bad when
 // |k . j| > 1e-10 + 1e-10 |k| |j| at an active mode k != 0.  grid: ceil(Hx * Ky / 256)
-__global__ void __launch_bounds__(kThreads) transverse_check_kernel(const StepPlan P, const IcSpec sx, const IcSpec sy, int* __restrict__ bad) {
+static __global__ void __launch_bounds__(kThreads) transverse_check_kernel(const StepPlan P, const IcSpec sx, const IcSpec sy, int* __restrict__ bad) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= P.hx * P.kyn) return;
     const int gx = e / P.kyn, j = e - gx * P.kyn;
@@ -1546,7 +1546,7 @@ __global__ void __launch_bounds__(kThreads) profile_velocity_row_kernel(const St
 }
 
 // out[x] = sum over the row pairs of partial[pair][x] in a fixed order; grid: ceil(npx / 256)
-__global__ void __launch_bounds__(kThreads) column_sums_kernel(const double* __restrict__ partial, int npairs, int npx, double* __restrict__ out) {
+static __global__ void __launch_bounds__(kThreads) column_sums_kernel(const double* __restrict__ partial, int npairs, int npx, double* __restrict__ out) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= npx) return;
     double t = 0.0;
@@ -1556,8 +1556,8 @@ __global__ void __launch_bounds__(kThreads) column_sums_kernel(const double* __r
 
 // step counter of the call: set from the host at the start of a call, advanced
 // by the last node of a captured step graph
-__global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }
-__global__ void advance_step_kernel(unsigned long long* step, unsigned long long by) { *step += by; }
+static __global__ void set_step_kernel(unsigned long long* step, unsigned long long value) { *step = value; }
+static __global__ void advance_step_kernel(unsigned long long* step, unsigned long long by) { *step += by; }
 
 // ---------------------------------------------------------------------------
 // fields the integrator only copies: symmetrise the kx = 0 line once and
@@ -1622,7 +1622,7 @@ __global__ void __launch_bounds__(kThreads) ref_to_active_kernel(const StepPlan 
 }
 
 // flags a nonzero entry outside the active modes; grid: (ceil(npy*ref_hx / 256), nfields)
-__global__ void __launch_bounds__(kThreads) check_inactive_kernel(const StepPlan P, int ref_hx, const double2* __restrict__ ref,
+static __global__ void __launch_bounds__(kThreads) check_inactive_kernel(const StepPlan P, int ref_hx, const double2* __restrict__ ref,
                                                                   int* __restrict__ bad) {
     const int f = blockIdx.y;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;

@@ -370,6 +370,166 @@ __device__ __forceinline__ float2 pin(const ulonglong2* in, int nx, int s, int s
     return (s & 1) ? make_float2(f2_hi(e.x), f2_hi(e.y)) : make_float2(f2_lo(e.x), f2_lo(e.y));
 }
 
+// products of one output pair of the row pass (two outputs per pair-line), evaluated at one
+// position of a row pair's physical input lines: `in` is the row pair's first input line, `sp`
+// the position's swizzled slot.  Each product is a combination of the terms psi^3, psi vx,
+// psi vy, vx, vy, jx vx, jx vy, jy vy (fcalculator.cc:226-239, 366-367, 447-451,
+// model_free_energy_phi4.cc:47-55) with per-output coefficients, or, outside the canonical
+// input layouts, product_value per row.
+struct RowProduct {
+    int ka, aa, kb, ab, psa, psb, mode;
+    bool need_j, use_psi;
+    float inv_rho0;
+    u64 IR0;
+    u64 C[8];
+};
+
+__device__ __forceinline__ RowProduct row_product(const StepPlan& P, int pi, float inv_rho0) {
+    RowProduct R;
+    const int oa = P.rp_a[pi], ob = P.rp_b[pi];
+    R.ka = P.out_kind[oa];
+    R.aa = P.out_arg[oa];
+    R.kb = ob >= 0 ? P.out_kind[ob] : -1;
+    R.ab = ob >= 0 ? P.out_arg[ob] : 0;
+    R.psa = (R.ka == OUT_MU || R.ka == OUT_PSIVX || R.ka == OUT_PSIVY) ? P.in_slot[1 + R.aa] : -1;
+    R.psb = (R.kb == OUT_MU || R.kb == OUT_PSIVX || R.kb == OUT_PSIVY) ? P.in_slot[1 + R.ab] : -1;
+    R.need_j = (R.ka != OUT_MU) || (R.kb >= 0 && R.kb != OUT_MU);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) R.C[q] = f2_pack(P.rp_coef[pi][q][0], P.rp_coef[pi][q][1]);
+    R.use_psi = R.psa >= 0 || R.psb >= 0;
+    R.mode = P.rp_mode[pi];
+    R.inv_rho0 = inv_rho0;
+    R.IR0 = f2_splat(inv_rho0);
+    return R;
+}
+
+// canonical input roles: psi of A and B from their slots, (jx, jy) and (vx, vy) lines
+template <int NX>
+__device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProduct& R, const ulonglong2* in, int sp) {
+    const u64* C = R.C;
+    const int mode = R.mode;
+    if (mode != 0) {  // outputs that are elementwise products of whole lines
+        if (mode == 1 || mode == 2) {
+            const ulonglong2 J = in[P.rp_jline * NX + sp];
+            const ulonglong2 V = P.rp_vline >= 0 ? in[P.rp_vline * NX + sp] : make_ulonglong2(f2_mul(J.x, R.IR0), f2_mul(J.y, R.IR0));
+            if (mode == 1) return PC{V.x, V.y};
+            return PC{f2_mul(J.x, V.x), f2_mul(J.y, V.y)};
+        }
+        const ulonglong2 S = in[(R.psa >> 1) * NX + sp];
+        if (mode == 3) {
+            const u64 q0 = f2_mul(f2_mul(S.x, S.x), f2_mul(S.x, C[0]));
+            const u64 q1 = f2_mul(f2_mul(S.y, S.y), f2_mul(S.y, C[0]));
+            return PC{q0, q1};
+        }
+        const ulonglong2 J = in[P.rp_jline * NX + sp];
+        const ulonglong2 V = P.rp_vline >= 0 ? in[P.rp_vline * NX + sp] : make_ulonglong2(f2_mul(J.x, R.IR0), f2_mul(J.y, R.IR0));
+        const u64 v0 = mode == 4 ? f2_splat(f2_lo(V.x)) : f2_splat(f2_hi(V.x));
+        const u64 v1 = mode == 4 ? f2_splat(f2_lo(V.y)) : f2_splat(f2_hi(V.y));
+        const u64 cc = mode == 4 ? C[1] : C[2];
+        return PC{f2_mul(f2_mul(S.x, cc), v0), f2_mul(f2_mul(S.y, cc), v1)};
+    }
+    u64 out[2] = {0ull, 0ull};
+    float jxr[2] = {0.f, 0.f}, jyr[2] = {0.f, 0.f}, vxr[2] = {0.f, 0.f}, vyr[2] = {0.f, 0.f};
+    if (R.need_j) {
+        const ulonglong2 J = in[P.rp_jline * NX + sp];
+        ulonglong2 V;
+        if (P.rp_vline >= 0) V = in[P.rp_vline * NX + sp];
+        else V = make_ulonglong2(f2_mul(J.x, R.IR0), f2_mul(J.y, R.IR0));
+        jxr[0] = f2_lo(J.x); jyr[0] = f2_hi(J.x); jxr[1] = f2_lo(J.y); jyr[1] = f2_hi(J.y);
+        vxr[0] = f2_lo(V.x); vyr[0] = f2_hi(V.x); vxr[1] = f2_lo(V.y); vyr[1] = f2_hi(V.y);
+    }
+    float2 pa = make_float2(0.f, 0.f), pb = pa;
+    if (R.psa >= 0) pa = pin(in, NX, R.psa, sp);
+    if (R.psb >= 0) pb = pin(in, NX, R.psb, sp);
+#pragma unroll
+    for (int row = 0; row < 2; ++row) {
+        const u64 VX = f2_splat(vxr[row]), VY = f2_splat(vyr[row]);
+        const u64 JX = f2_splat(jxr[row]), JY = f2_splat(jyr[row]);
+        u64 o = f2_fma(C[4], VY, f2_mul(C[3], VX));                          // c3 vx + c4 vy
+        o = f2_fma(f2_mul(C[5], JX), VX, o);                                 // + c5 jx vx
+        o = f2_fma(f2_fma(C[6], JX, f2_mul(C[7], JY)), VY, o);               // + (c6 jx + c7 jy) vy
+        if (R.use_psi) {
+            const u64 PS = row ? f2_pack(pa.y, pb.y) : f2_pack(pa.x, pb.x);
+            u64 in2 = f2_fma(C[1], VX, f2_mul(C[2], VY));                    // c1 vx + c2 vy
+            in2 = f2_fma(f2_mul(C[0], PS), PS, in2);                         // + c0 psi^2
+            o = f2_fma(PS, in2, o);                                          // psi (...)
+        }
+        out[row] = o;
+    }
+    return PC{out[0], out[1]};
+}
+
+// any input layout: product_value per row (rho replaced by 1 / rho in compressible dynamics)
+template <int NX>
+__device__ __forceinline__ PC row_product_general(const StepPlan& P, const RowProduct& R, const ulonglong2* in, int sp) {
+    const int s_rho = P.in_slot[0];
+    const int s_jx = P.in_slot[P.nop + 1];
+    const int s_jy = P.in_slot[P.nop + 2];
+    const bool comp = (P.mode == 0);
+    float2 jx = make_float2(0.f, 0.f), jy = jx, vx = jx, vy = jx;
+    if (R.need_j) {
+        jx = pin(in, NX, s_jx, sp);
+        jy = pin(in, NX, s_jy, sp);
+        if (comp) {
+            const float2 ir = pin(in, NX, s_rho, sp);
+            vx = make_float2(jx.x * ir.x, jx.y * ir.y);
+            vy = make_float2(jy.x * ir.x, jy.y * ir.y);
+        } else {
+            vx = make_float2(jx.x * R.inv_rho0, jx.y * R.inv_rho0);
+            vy = make_float2(jy.x * R.inv_rho0, jy.y * R.inv_rho0);
+        }
+    }
+    const float2 pa = R.psa >= 0 ? pin(in, NX, R.psa, sp) : make_float2(0.f, 0.f);
+    const float2 pb = R.psb >= 0 ? pin(in, NX, R.psb, sp) : make_float2(0.f, 0.f);
+    const float a0 = product_value<float>(P, R.ka, R.aa, pa.x, jx.x, jy.x, vx.x, vy.x);
+    const float a1 = product_value<float>(P, R.ka, R.aa, pa.y, jx.y, jy.y, vx.y, vy.y);
+    float b0 = 0.f, b1 = 0.f;
+    if (R.kb >= 0) {
+        b0 = product_value<float>(P, R.kb, R.ab, pb.x, jx.x, jy.x, vx.x, vy.x);
+        b1 = product_value<float>(P, R.kb, R.ab, pb.y, jx.y, jy.y, vx.y, vy.y);
+    }
+    return PC{f2_pack(a0, b0), f2_pack(a1, b1)};
+}
+
+// velocity inputs after the x-inverse of a row pair's input lines (`inl`, `nl` row pairs of
+// `nip` lines of NX).  Canonical layout: (rho, jx), (jy, -) become (jx, jy), (vx, vy)
+// (compressible, with the zero-density check of fcalculator_workspace.cc:122-133); otherwise
+// rho is replaced by 1 / rho in place.  Threads tid < nthreads stride over the positions.
+template <int NX>
+__device__ __forceinline__ void row_velocity_prep(const StepPlan& P, ulonglong2* inl, int nl, int nip, int tid, int nthreads, int* err) {
+    int bad = 0;
+    const int s_rho = P.in_slot[0];
+    if (P.rp_prep) {
+        const int m = P.rp_jline;
+        for (int e = tid; e < nl * NX; e += nthreads) {
+            const int r = e / NX, x = e - r * NX;
+            ulonglong2* pj = inl + (static_cast<size_t>(r) * nip + m) * NX + x;
+            const ulonglong2 rj = pj[0], jy = pj[NX];
+            const float r0 = f2_lo(rj.x), r1 = f2_lo(rj.y);
+            if (r0 == 0.f || r1 == 0.f) bad = 1;
+            const u64 ir = f2_pack(1.f / r0, 1.f / r1);                       // (1/rho_row0, 1/rho_row1)
+            const u64 jx = f2_pack(f2_hi(rj.x), f2_hi(rj.y)), jyv = f2_pack(f2_lo(jy.x), f2_lo(jy.y));
+            const u64 vx = f2_mul(jx, ir), vy = f2_mul(jyv, ir);              // per row
+            pj[0] = make_ulonglong2(f2_pack(f2_lo(jx), f2_lo(jyv)), f2_pack(f2_hi(jx), f2_hi(jyv)));
+            pj[NX] = make_ulonglong2(f2_pack(f2_lo(vx), f2_lo(vy)), f2_pack(f2_hi(vx), f2_hi(vy)));
+        }
+    } else {
+        for (int e = tid; e < nl * NX; e += nthreads) {
+            const int r = e / NX, x = e - r * NX;
+            ulonglong2* pe = inl + (static_cast<size_t>(r) * nip + (s_rho >> 1)) * NX + x;
+            ulonglong2 v = *pe;
+            const int h = s_rho & 1;
+            const float r0 = h ? f2_hi(v.x) : f2_lo(v.x), r1 = h ? f2_hi(v.y) : f2_lo(v.y);
+            if (r0 == 0.f || r1 == 0.f) bad = 1;
+            const float i0 = 1.f / r0, i1v = 1.f / r1;
+            if (h) { v.x = f2_pack(f2_lo(v.x), i0); v.y = f2_pack(f2_lo(v.y), i1v); }
+            else { v.x = f2_pack(i0, f2_hi(v.x)); v.y = f2_pack(i1v, f2_hi(v.y)); }
+            *pe = v;
+        }
+    }
+    if (bad) atomicOr(err, ERR_ZERO_DENSITY);
+}
+
 template <int NX>
 __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const MemberInfo* __restrict__ members,
                                                       const ulonglong2* __restrict__ i1, ulonglong2* __restrict__ i2,
@@ -429,145 +589,23 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
     __syncthreads();
     pdif_range<NX, 0, pp.m, +1>(inl, RP * nip, tw);
 
-    // 2. velocity inputs.  Canonical layout: (rho, jx), (jy, -) become (jx, jy), (vx, vy)
-    //    (compressible; zero-density check) or v = j / rho0 later (incompressible).
-    //    Otherwise rho is replaced by 1 / rho in place.
-    const int s_rho = P.in_slot[0];
-    const int s_jx = P.in_slot[P.nop + 1];
-    const int s_jy = P.in_slot[P.nop + 2];
+    // 2. velocity inputs (compressible: v = j / rho with the zero-density check; otherwise
+    //    v = j / rho0 in the products)
     const bool comp = (P.mode == 0);
     const float inv_rho0 = (P.need_v && !comp) ? static_cast<float>(1.0 / rho0_member[b]) : 0.f;
     if (P.need_v && comp) {
-        int bad = 0;
-        if (P.rp_prep) {
-            const int m = P.rp_jline;
-            for (int e = threadIdx.x; e < RP * NX; e += kThreads) {
-                const int r = e / NX, x = e - r * NX;
-                ulonglong2* pj = inl + (static_cast<size_t>(r) * nip + m) * NX + x;
-                const ulonglong2 rj = pj[0], jy = pj[NX];
-                const float r0 = f2_lo(rj.x), r1 = f2_lo(rj.y);
-                if (r0 == 0.f || r1 == 0.f) bad = 1;
-                const u64 ir = f2_pack(1.f / r0, 1.f / r1);                       // (1/rho_row0, 1/rho_row1)
-                const u64 jx = f2_pack(f2_hi(rj.x), f2_hi(rj.y)), jyv = f2_pack(f2_lo(jy.x), f2_lo(jy.y));
-                const u64 vx = f2_mul(jx, ir), vy = f2_mul(jyv, ir);              // per row
-                pj[0] = make_ulonglong2(f2_pack(f2_lo(jx), f2_lo(jyv)), f2_pack(f2_hi(jx), f2_hi(jyv)));
-                pj[NX] = make_ulonglong2(f2_pack(f2_lo(vx), f2_lo(vy)), f2_pack(f2_hi(vx), f2_hi(vy)));
-            }
-        } else {
-            for (int e = threadIdx.x; e < RP * NX; e += kThreads) {
-                const int r = e / NX, x = e - r * NX;
-                ulonglong2* pe = inl + (static_cast<size_t>(r) * nip + (s_rho >> 1)) * NX + x;
-                ulonglong2 v = *pe;
-                const int h = s_rho & 1;
-                const float r0 = h ? f2_hi(v.x) : f2_lo(v.x), r1 = h ? f2_hi(v.y) : f2_lo(v.y);
-                if (r0 == 0.f || r1 == 0.f) bad = 1;
-                const float i0 = 1.f / r0, i1v = 1.f / r1;
-                if (h) { v.x = f2_pack(f2_lo(v.x), i0); v.y = f2_pack(f2_lo(v.y), i1v); }
-                else { v.x = f2_pack(i0, f2_hi(v.x)); v.y = f2_pack(i1v, f2_hi(v.y)); }
-                *pe = v;
-            }
-        }
-        if (bad) atomicOr(err, ERR_ZERO_DENSITY);
+        row_velocity_prep<NX>(P, inl, RP, nip, threadIdx.x, kThreads, err);
         __syncthreads();
     }
 
     // 3. per output pair: products fused into the first DIT stage, the rest of
     //    the forward transform, then the untangling of the two rows (kx < Hx)
     const u64 HALF = f2_splat(0.5f);
-    const u64 IR0 = f2_splat(inv_rho0);
     for (int pi = 0; pi < P.rp_n; ++pi) {
         const int oa = P.rp_a[pi], ob = P.rp_b[pi];
-        const int ka = P.out_kind[oa], aa = P.out_arg[oa];
-        const int kb = ob >= 0 ? P.out_kind[ob] : -1, ab = ob >= 0 ? P.out_arg[ob] : 0;
-        const int psa = (ka == OUT_MU || ka == OUT_PSIVX || ka == OUT_PSIVY) ? P.in_slot[1 + aa] : -1;
-        const int psb = (kb == OUT_MU || kb == OUT_PSIVX || kb == OUT_PSIVY) ? P.in_slot[1 + ab] : -1;
-        const bool need_j = (ka != OUT_MU) || (kb >= 0 && kb != OUT_MU);
-        u64 C[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) C[q] = f2_pack(P.rp_coef[pi][q][0], P.rp_coef[pi][q][1]);
-        const bool use_psi = psa >= 0 || psb >= 0;
-        // canonical roles: psi of A and B from their slots, (jx, jy) and (vx, vy) lines
-        const int mode = P.rp_mode[pi];
-        auto product_canon = [&](int r, int p) -> PC {
-            const ulonglong2* in = inl + static_cast<size_t>(r) * nip * NX;
-            const int sp = psw(p);
-            if (mode != 0) {  // outputs that are elementwise products of whole lines
-                if (mode == 1 || mode == 2) {
-                    const ulonglong2 J = in[P.rp_jline * NX + sp];
-                    const ulonglong2 V = P.rp_vline >= 0 ? in[P.rp_vline * NX + sp] : make_ulonglong2(f2_mul(J.x, IR0), f2_mul(J.y, IR0));
-                    if (mode == 1) return PC{V.x, V.y};
-                    return PC{f2_mul(J.x, V.x), f2_mul(J.y, V.y)};
-                }
-                const ulonglong2 S = in[(psa >> 1) * NX + sp];
-                if (mode == 3) {
-                    const u64 q0 = f2_mul(f2_mul(S.x, S.x), f2_mul(S.x, C[0]));
-                    const u64 q1 = f2_mul(f2_mul(S.y, S.y), f2_mul(S.y, C[0]));
-                    return PC{q0, q1};
-                }
-                const ulonglong2 J = in[P.rp_jline * NX + sp];
-                const ulonglong2 V = P.rp_vline >= 0 ? in[P.rp_vline * NX + sp] : make_ulonglong2(f2_mul(J.x, IR0), f2_mul(J.y, IR0));
-                const u64 v0 = mode == 4 ? f2_splat(f2_lo(V.x)) : f2_splat(f2_hi(V.x));
-                const u64 v1 = mode == 4 ? f2_splat(f2_lo(V.y)) : f2_splat(f2_hi(V.y));
-                const u64 cc = mode == 4 ? C[1] : C[2];
-                return PC{f2_mul(f2_mul(S.x, cc), v0), f2_mul(f2_mul(S.y, cc), v1)};
-            }
-            u64 out[2] = {0ull, 0ull};
-            float jxr[2] = {0.f, 0.f}, jyr[2] = {0.f, 0.f}, vxr[2] = {0.f, 0.f}, vyr[2] = {0.f, 0.f};
-            if (need_j) {
-                const ulonglong2 J = in[P.rp_jline * NX + sp];
-                ulonglong2 V;
-                if (P.rp_vline >= 0) V = in[P.rp_vline * NX + sp];
-                else V = make_ulonglong2(f2_mul(J.x, IR0), f2_mul(J.y, IR0));
-                jxr[0] = f2_lo(J.x); jyr[0] = f2_hi(J.x); jxr[1] = f2_lo(J.y); jyr[1] = f2_hi(J.y);
-                vxr[0] = f2_lo(V.x); vyr[0] = f2_hi(V.x); vxr[1] = f2_lo(V.y); vyr[1] = f2_hi(V.y);
-            }
-            float2 pa = make_float2(0.f, 0.f), pb = pa;
-            if (psa >= 0) pa = pin(in, NX, psa, sp);
-            if (psb >= 0) pb = pin(in, NX, psb, sp);
-#pragma unroll
-            for (int row = 0; row < 2; ++row) {
-                const u64 VX = f2_splat(vxr[row]), VY = f2_splat(vyr[row]);
-                const u64 JX = f2_splat(jxr[row]), JY = f2_splat(jyr[row]);
-                u64 o = f2_fma(C[4], VY, f2_mul(C[3], VX));                          // c3 vx + c4 vy
-                o = f2_fma(f2_mul(C[5], JX), VX, o);                                 // + c5 jx vx
-                o = f2_fma(f2_fma(C[6], JX, f2_mul(C[7], JY)), VY, o);               // + (c6 jx + c7 jy) vy
-                if (use_psi) {
-                    const u64 PS = row ? f2_pack(pa.y, pb.y) : f2_pack(pa.x, pb.x);
-                    u64 in2 = f2_fma(C[1], VX, f2_mul(C[2], VY));                    // c1 vx + c2 vy
-                    in2 = f2_fma(f2_mul(C[0], PS), PS, in2);                         // + c0 psi^2
-                    o = f2_fma(PS, in2, o);                                          // psi (...)
-                }
-                out[row] = o;
-            }
-            return PC{out[0], out[1]};
-        };
-        auto product = [&](int r, int p) -> PC {
-            const ulonglong2* in = inl + static_cast<size_t>(r) * nip * NX;
-            const int sp = psw(p);
-            float2 jx = make_float2(0.f, 0.f), jy = jx, vx = jx, vy = jx;
-            if (need_j) {
-                jx = pin(in, NX, s_jx, sp);
-                jy = pin(in, NX, s_jy, sp);
-                if (comp) {
-                    const float2 ir = pin(in, NX, s_rho, sp);
-                    vx = make_float2(jx.x * ir.x, jx.y * ir.y);
-                    vy = make_float2(jy.x * ir.x, jy.y * ir.y);
-                } else {
-                    vx = make_float2(jx.x * inv_rho0, jx.y * inv_rho0);
-                    vy = make_float2(jy.x * inv_rho0, jy.y * inv_rho0);
-                }
-            }
-            const float2 pa = psa >= 0 ? pin(in, NX, psa, sp) : make_float2(0.f, 0.f);
-            const float2 pb = psb >= 0 ? pin(in, NX, psb, sp) : make_float2(0.f, 0.f);
-            const float a0 = product_value<float>(P, ka, aa, pa.x, jx.x, jy.x, vx.x, vy.x);
-            const float a1 = product_value<float>(P, ka, aa, pa.y, jx.y, jy.y, vx.y, vy.y);
-            float b0 = 0.f, b1 = 0.f;
-            if (kb >= 0) {
-                b0 = product_value<float>(P, kb, ab, pb.x, jx.x, jy.x, vx.x, vy.x);
-                b1 = product_value<float>(P, kb, ab, pb.y, jx.y, jy.y, vx.y, vy.y);
-            }
-            return PC{f2_pack(a0, b0), f2_pack(a1, b1)};
-        };
+        const RowProduct R = row_product(P, pi, inv_rho0);
+        auto product_canon = [&](int r, int p) -> PC { return row_product_canon<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, psw(p)); };
+        auto product = [&](int r, int p) -> PC { return row_product_general<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, psw(p)); };
         const SmemIO wio{work, NX};
         if (P.rp_canon) pstage_io<NX, pp.m - 1, -1, true>(RP, tw, product_canon, wio);
         else pstage_io<NX, pp.m - 1, -1, true>(RP, tw, product, wio);

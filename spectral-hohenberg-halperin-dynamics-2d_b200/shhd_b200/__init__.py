@@ -127,7 +127,10 @@ EXPORTED = (
     "shhd_engine_set_initial_field", "shhd_engine_check_transverse", "shhd_engine_energies",
     "shhd_engine_flux0_enable", "shhd_engine_flux0_read", "shhd_engine_profile_line", "shhd_engine_profile_velocity",
     "shhd_engine_flux_line_enable", "shhd_engine_flux_line_read", "shhd_engine_flux_tap_schedule",
+    "shhd_engine_set_family", "shhd_engine_family",
 )
+
+FAMILY_NAMES = {0: "single-line", 1: "pair-line", 2: "pair-line + register row pass"}
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
 
@@ -165,6 +168,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_sk_accumulate.argtypes = [vp, i]
     lib.shhd_engine_sk_read.argtypes = [vp, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
     lib.shhd_engine_autotune.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), dp]
+    lib.shhd_engine_set_family.argtypes = [vp, i]
+    lib.shhd_engine_family.argtypes = [vp]
     lib.shhd_engine_gk_enable.argtypes = [vp, i, i, i]
     lib.shhd_engine_gk_read.argtypes = [vp, i, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
     lib.shhd_engine_l2_sums.argtypes = [vp, i, dp, sz]
@@ -305,10 +310,18 @@ class Engine:
     def autotune(self, trial_steps: int = 3) -> dict:
         """Time the valid kernel families x {direct, graph} on the current state; keep the fastest."""
         fam, chunk = ctypes.c_int(), ctypes.c_int()
-        ms = np.full(4, np.nan)
+        ms = np.full(6, np.nan)
         _check(lib.shhd_engine_autotune(self._h, int(trial_steps), ctypes.byref(fam), ctypes.byref(chunk), _dptr(ms)))
-        return {"family": "pair-line" if fam.value == 1 else "single-line", "graph_chunk": chunk.value,
+        return {"family": FAMILY_NAMES[fam.value], "graph_chunk": chunk.value,
                 "ms_per_step": [None if np.isnan(x) else float(x) for x in ms]}
+
+    def set_family(self, family: int) -> None:
+        """Kernel family: -1 default, 0 single-line, 1 pair-line, 2 pair-line with the register row pass."""
+        _check(lib.shhd_engine_set_family(self._h, int(family)))
+
+    @property
+    def family(self) -> int:
+        return int(lib.shhd_engine_family(self._h))
 
     def set_gaussian_field(self, member: int, field: int, seed: int, channel: int, mean: float, s0: float,
                            c0: float = 1.0, c2: float = 0.0, c4: float = 0.0) -> None:

@@ -11,8 +11,8 @@ FP64 / FP32 bounds: relative L2 over the whole state <= 1e-12 (FP64) and <= 1e-5
     (seed 1), kBT 1e-4, SRK3 dt 0.05, noise on: 5 steps.
   * 1024^2, N = 2 compressible phi4 with advection (3/2 rule: 1536^2, the FP32 pair-line
     kernels), kBT 1e-3, SRK3 dt 0.01: 2 steps.
-  * 4096^2 incompressible turbulence (6144^2), kBT = 0, FP32 against the FP64 engine (itself
-    pinned to the oracle): a deterministic trajectory of 3 steps.
+  * 4096^2 incompressible turbulence (6144^2), kBT = 0, FP32 against the reference: a
+    deterministic trajectory of 2 steps.
 """
 import ctypes
 import os
@@ -132,14 +132,17 @@ def _replay(text, nsteps):
 def test_reference_trajectory_with_its_noise(text, nsteps):
     import shhd_b200 as sb
     u0, states, noises = _replay(text, nsteps)
-    for precision, tol in ((sb.FP64, TOL64), (sb.FP32, TOL32)):
+    # FP64; FP32 in each kernel family valid for the size (1536-point rows: pair-line and the
+    # register-resident row pass)
+    for precision, tol, family in ((sb.FP64, TOL64, -1), (sb.FP32, TOL32, 1), (sb.FP32, TOL32, 2)):
         with _engine(sb, text, precision, True) as eng:
+            eng.set_family(family)
             eng.set_state(u0)
             for s in range(nsteps):
                 eng.set_external_noise(noises[s][0], noises[s][1])
                 eng.step(1)
                 err = so.rel_l2(eng.get_state(), states[s])
-                assert err < tol, f"precision {precision} step {s}: rel L2 {err:.3e}"
+                assert err < tol, f"precision {precision} family {eng.family} step {s}: rel L2 {err:.3e}"
 
 
 def test_reference_rhs_at_1024():
@@ -151,31 +154,29 @@ def test_reference_rhs_at_1024():
     want = np.zeros(ref.shape, complex)
     assert ref.lib.shref_rhs(ref.h, ctypes.c_double(0.0), want.ctypes.data_as(ctypes.c_void_p)) == 0
     ref.close()
-    for precision, tol in ((sb.FP64, TOL64), (sb.FP32, TOL32)):
+    for precision, tol, family in ((sb.FP64, TOL64, -1), (sb.FP32, TOL32, 1), (sb.FP32, TOL32, 2)):
         with _engine(sb, HH_1024, precision, False) as eng:
+            eng.set_family(family)
             eng.set_state(u0)
             err = so.rel_l2(eng.rhs(), want)
-        assert err < tol, f"precision {precision}: rel L2 {err:.3e}"
+            fam = eng.family
+        assert err < tol, f"precision {precision} family {fam}: rel L2 {err:.3e}"
 
 
-def test_turbulence_4096_fp32_tracks_fp64():
-    """4096^2 incompressible (6144^2 transforms) with kBT = 0: the FP32 trajectory stays within
-    1e-5 of the FP64 one over 3 steps, from the random-vorticity initial momentum generated on
-    the device."""
+def test_turbulence_4096_fp32_against_reference():
+    """4096^2 incompressible turbulence (6144^2 transforms) with kBT = 0: two deterministic
+    steps of the FP32 engine from the reference's random-vorticity initial momentum stay within
+    1e-5 of the reference's own FP64 trajectory.  (A step moves the state by ~1e-6 of its norm at
+    dt = 1e-3, so the FP32 rounding of the stored state alone is a few percent of one step's
+    increment: the bound is on the state, as for every FP32 trajectory.)"""
     import shhd_b200 as sb
-    from shhd_b200.initial import initial_state_device
-    init = TURB_4096_DET.replace("run 2000", "set density uniform value 1.0\n"
+    text = TURB_4096_DET.replace("run 2000", "set density uniform value 1.0\n"
                                  "set momentum all random_vorticity n0 8 sigma 2 urms 1 seed 11\nrun 2000")
-    out = {}
-    for precision in (sb.FP64, sb.FP32):
-        with _engine(sb, init, precision, False) as eng:
-            if precision == sb.FP64:
-                initial_state_device(eng, init)
-                u0 = eng.get_state()
-            else:
-                eng.set_state(u0)
-            eng.step(3)
-            out[precision] = eng.get_state()
-    err = so.rel_l2(out[sb.FP32], out[sb.FP64])
-    assert err < TOL32, f"rel L2 {err:.3e}"
-    assert so.rel_l2(out[sb.FP64], u0) > 1e-9  # the state moved
+    u0, states, _ = _replay(text, 2)
+    with _engine(sb, text, sb.FP32, False) as eng:
+        eng.set_state(u0)
+        for s in range(2):
+            eng.step(1)
+            u = eng.get_state()
+            err = so.rel_l2(u, states[s])
+            assert err < TOL32, f"step {s}: rel L2 {err:.3e}"
