@@ -18,6 +18,8 @@
  * flux buffer, as Project::run_steps does (project.h:127-143);
  * shref_finalize closes their files.
  */
+#include "ref_harness.h"
+
 #include "domain.h"
 #include "fcalculator.h"
 #include "fcalculator_dynamics_mode.h"
@@ -217,6 +219,18 @@ int guarded(F&& f) {
 }
 
 } // namespace
+
+bool shref_view(void* handle, RefRunView& out) {
+    if (!handle) return false;
+    RefRun* r = static_cast<RefRun*>(handle);
+    out.params = &r->params;
+    out.domain = r->domain.get();
+    out.thermodynamics = r->thermo.get();
+    out.free_energy = r->free_energy.get();
+    out.transport = r->transport.get();
+    out.state = r->state.get();
+    return true;
+}
 
 extern "C" {
 

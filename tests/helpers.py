@@ -81,3 +81,15 @@ def script(grid=(32, 32), length=(32.0, 32.0), dealias="3/2", nop=2, dt=0.01, te
         lines.append(extra)
     lines.append("run 1")
     return "\n".join(lines) + "\n"
+
+
+def fp32_transform_rhs(cfg: so.Config, state: np.ndarray) -> np.ndarray:
+    """The oracle's RHS with both transforms in single precision (scipy's pocketfft in float32,
+    correctly rounded twiddles), everything else in FP64: the error an FP32 transform pipeline
+    cannot avoid, to which the engine's FP32 error is compared at large sizes."""
+    import scipy.fft as sf
+    o = so.Oracle(cfg)
+    g = o.geo
+    g.backward = lambda f: sf.irfft2(np.asarray(f).astype(np.complex64), s=(g.ny, g.nx), axes=(-2, -1), workers=8).astype(np.float64)
+    g.forward = lambda p: sf.rfft2(np.asarray(p).astype(np.float32), axes=(-2, -1), workers=8).astype(np.complex128)
+    return o.rhs(state)

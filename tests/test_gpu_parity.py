@@ -279,13 +279,14 @@ BIG_LINES = {
 
 
 # FP32 at 6144^2: the incompressible RHS -i k . (j j / rho0) weights the white FP32 round-off of the
-# transforms by k up to a k_max four times the 1536^2 one; the 256-thread row groups give the same
-# 2.9e-5 bit for bit, so the bound here is size, not the grouping
-TOL32_6144 = 5e-5
+# transforms by k up to a k_max four times the 1536^2 one.  The oracle itself with single-precision
+# transforms (correctly rounded twiddles, FP64 products) lands at the same ~3e-5 on this state, so
+# above 1e-5 the bound is that FP32 floor: the engine must stay within 10% of it.
 
 
 @pytest.mark.parametrize("name", sorted(BIG_LINES))
 def test_rhs_with_512_thread_row_groups(sb, name):
+    from helpers import fp32_transform_rhs
     precision, text = BIG_LINES[name]
     ocfg = so.parse_script(text)
     u = random_state(ocfg, seed=31, transverse=(ocfg.mode == "incompressible"))
@@ -293,7 +294,13 @@ def test_rhs_with_512_thread_row_groups(sb, name):
     with make_engine(sb, text, precision) as eng:
         eng.set_state(u)
         got = eng.rhs()
-    assert so.rel_l2(got, want) < (TOL64 if precision == 0 else TOL32_6144), name
+    err = so.rel_l2(got, want)
+    if precision == 0:
+        assert err < TOL64, name
+    else:
+        floor = so.rel_l2(fp32_transform_rhs(ocfg, u), want)
+        print(f"{name}: engine FP32 rel L2 {err:.3e}, FP32-transform oracle {floor:.3e}")
+        assert err < max(TOL32, 1.1 * floor), f"{name}: {err:.3e} (FP32-transform floor {floor:.3e})"
 
 
 @pytest.mark.parametrize("precision", [0, 1])
