@@ -59,13 +59,19 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
     constexpr int B = (NR + G - 1) / G;
     constexpr int ROW = tw_row(R);
     constexpr int SPAN = 1 << (2 * SB);  // adding a multiple of SPAN leaves the swizzled bits alone
+    // FP32 reads w^k, w^2k, w^3k exactly (the table row holds every power) and forms the higher
+    // powers at most two roundings deep; FP64 reads w^k alone, its products being far below FP32
+    constexpr int NL = (sizeof(C) == 8) ? (R - 1 < 3 ? R - 1 : 3) : 1;
     C v[B][R];
-    C wk[B];  // w^k of each butterfly, loaded before the barrier so its latency overlaps the wait
+    C wk[B][NL];  // the loaded powers of each butterfly, before the barrier so their latency overlaps the wait
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int bi = gt + i * G;
         if (NR % G == 0 || bi < NR) {
-            if constexpr (P > 1) wk[i] = __ldg(tw + TWOFF + (bi % P) * ROW);
+            if constexpr (P > 1) {
+#pragma unroll
+                for (int l = 0; l < NL; ++l) wk[i][l] = __ldg(tw + TWOFF + (bi % P) * ROW + l);
+            }
             if constexpr (NR % SPAN == 0) {
                 const uint32_t s0 = swz<SB>(bi);
 #pragma unroll
@@ -83,15 +89,24 @@ __device__ __forceinline__ void gstage(C* line, const C* __restrict__ tw, int gt
         if (NR % G == 0 || bi < NR) {
             const int k = bi % P;
             if constexpr (P > 1) {
-                // one load of w^k per butterfly; its powers by a product tree at most three roundings deep
                 C w[R];
-                w[1] = wk[i];
-                if constexpr (R > 2) w[2] = cmul(w[1], w[1]);
-                if constexpr (R > 3) w[3] = cmul(w[2], w[1]);
-                if constexpr (R > 4) w[4] = cmul(w[2], w[2]);
-                if constexpr (R > 5) w[5] = cmul(w[4], w[1]);
-                if constexpr (R > 6) w[6] = cmul(w[3], w[3]);
-                if constexpr (R > 7) w[7] = cmul(w[4], w[3]);
+                if constexpr (NL == 1) {
+                    // one load of w^k per butterfly; its powers by a product tree at most three roundings deep
+                    w[1] = wk[i][0];
+                    if constexpr (R > 2) w[2] = cmul(w[1], w[1]);
+                    if constexpr (R > 3) w[3] = cmul(w[2], w[1]);
+                    if constexpr (R > 4) w[4] = cmul(w[2], w[2]);
+                    if constexpr (R > 5) w[5] = cmul(w[4], w[1]);
+                    if constexpr (R > 6) w[6] = cmul(w[3], w[3]);
+                    if constexpr (R > 7) w[7] = cmul(w[4], w[3]);
+                } else {
+#pragma unroll
+                    for (int l = 0; l < NL; ++l) w[l + 1] = wk[i][l];
+                    if constexpr (R > 4) w[4] = cmul(w[2], w[2]);
+                    if constexpr (R > 5) w[5] = cmul(w[2], w[3]);
+                    if constexpr (R > 6) w[6] = cmul(w[3], w[3]);
+                    if constexpr (R > 7) w[7] = cmul(w[3], w[4]);
+                }
 #pragma unroll
                 for (int q = 1; q < R; ++q) v[i][q] = DIR < 0 ? cmul(v[i][q], w[q]) : cmulc(v[i][q], w[q]);
             }

@@ -192,11 +192,19 @@ class Server:
         return freed
 
     def _slot_for(self, job: Job) -> Optional[Tuple[_Bucket, int]]:
+        """A free slot of an idle bucket of the job's shape, or a new bucket.  A bucket with a
+        chunk in flight admits nothing: its step count and the slots' remaining steps are
+        settled when the chunk completes, so the job waits for that (rather than a new bucket)."""
         key = bucket_key(job.config, job.green_kubo)
+        busy_room = False
         for b in self.buckets.get(key, []):
             m = b.free_slot()
             if m is not None:
-                return b, m
+                if b.inflight is None:
+                    return b, m
+                busy_room = True
+        if busy_room:
+            return None
         per = self._per_member_bytes(key, job.config)
         if self.budget - self.used < per:
             self._release_idle()

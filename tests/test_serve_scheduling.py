@@ -178,3 +178,20 @@ def test_served_stream_partitioned_over_two_ranks():
         assert out[0][1] == out[1][1] and sum(out[0][1]) == 7
         assert out[0][2] and out[1][2]
         assert sorted(out[0][3] + out[1][3]) == list(range(7))
+
+
+def test_jobs_arriving_while_chunks_are_in_flight():
+    """Arrivals land while their bucket's chunk is in flight (two shapes, so while the oldest chunk
+    is waited for the other bucket's stays in flight; slow events): each job still takes exactly
+    its own step count, counted from its own admission."""
+    from shhd_b200 import serve
+    FakeEngine.live = []
+    jobs = [serve.Job(key=k, config=_cfg((64, 128)[k % 2]), state=np.zeros(1), nsteps=60 + 7 * k, arrival=0.00002 * k)
+            for k in range(12)]
+    srv = serve.Server(precision=1, seed=1, hbm_budget=10 ** 9, max_slots=4, chunk=5, engine_factory=FakeEngine,
+                       event_factory=lambda eng: FakeEvent(40))
+    stats = srv.run(jobs)
+    assert stats["jobs"] == 12
+    for j in jobs:
+        assert int(j.result[0]) == j.nsteps, (j.key, int(j.result[0]), j.nsteps)
+    srv.close()
