@@ -282,16 +282,17 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
-def dram_traffic_from_profiles():
-    """Per-launch DRAM bytes of each kernel from the committed ncu summary, if present."""
+def dram_traffic_from_profiles(workload: str):
+    """Per-launch DRAM bytes of each kernel on `workload` from the committed ncu summary (lines
+    'kernel workload bytes'), if present."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     out = {}
     if os.path.exists(path):
         for line in open(path):
             t = line.split("#", 1)[0].split()
-            if len(t) == 2:
+            if len(t) == 3 and t[1] == workload:
                 try:
-                    out[t[0]] = float(t[1])
+                    out[t[0]] = float(t[2])
                 except ValueError:
                     pass
     return out
@@ -324,8 +325,13 @@ def run_b200(args):
     eng = sb.Engine(cfg)
     eng.set_state(u0)
     stream = torch.cuda.ExternalStream(eng.stream)
-    # kernel family and graph replay chosen by timing them on this state (state restored)
-    tuning = eng.autotune(3)
+    # kernel family and graph replay chosen by timing them on this state (state restored), or the
+    # family given on the command line (profiling one family)
+    if args.family is None:
+        tuning = eng.autotune(3)
+    else:
+        eng.set_family(args.family)
+        tuning = {"family": sb.FAMILY_NAMES[eng.family], "graph_chunk": 0, "forced": True}
 
     # warm-up
     eng.step(args.warmup)
@@ -363,7 +369,8 @@ def run_b200(args):
     t_ms, n_l, by = kst[dom]
     achieved = (by / n_l) / (t_ms / n_l * 1e-3) / 1e9
     peak, peak_kind = measured_peak_gbs()
-    traffic = dram_traffic_from_profiles().get(dom)
+    # the summary holds the pair-line kernels' capture; another family has no captured traffic
+    traffic = dram_traffic_from_profiles("hh1024_fp32").get(dom) if args.precision == "fp32" and tuning.get("family") == "pair-line" else None
     step_bytes = sum(v[2] for v in kst.values()) / kprof_steps
     step_ms_profiled = sum(v[0] for v in kst.values()) / kprof_steps
     kernels = {k: {"ms_per_launch": (v[0] / v[1]) if v[1] else None, "launches_per_step": v[1] / kprof_steps,
@@ -414,6 +421,7 @@ def run_b200(args):
             "dtype": "f32" if args.precision == "fp32" else "f64", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas x{world}"),
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": "profiles/dram_traffic.txt (ncu dram__bytes_read.sum + dram__bytes_write.sum, mean per launch)",
                          "algorithmic_bytes_per_launch": by / n_l, "step_GBps": step_bytes / (step_ms_profiled * 1e-3) / 1e9},
             "kernels": kernels,
             "cpu_baseline": cpu,
@@ -774,6 +782,8 @@ def main():
     ap.add_argument("--precision", choices=("fp32", "fp64"), default="fp32")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--family", type=int, choices=(0, 1, 2), default=None,
+                    help="kernel family instead of the autotuner's choice (0 single-line, 1 pair-line, 2 register row pass)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
