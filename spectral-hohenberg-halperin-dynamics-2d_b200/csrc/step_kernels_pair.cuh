@@ -646,8 +646,14 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
 // Shared memory: CP work pair-lines, then three per-mode arrays [CP][Ky]
 // (accumulators / new values: psi or jx, jy, rho), two columns per element.
 // ---------------------------------------------------------------------------
+// blocks per SM the column forward is compiled for: its 74 KB of shared memory allow three, and at
+// 384 points and up the register budget of three (85) holds it without spilling more than 40 B
 template <int NY>
-__global__ void __launch_bounds__(kThreads, 2) pcol_forward(const StepPlan P, const StageArgs<float> A, const float2* __restrict__ tw) {
+__host__ __device__ constexpr int pcol_forward_blocks() { return NY >= 384 ? 3 : 2; }
+
+template <int NY>
+__global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forward(const StepPlan P, const StageArgs<float> A,
+                                                                                 const float2* __restrict__ tw) {
     constexpr int CP = kPairMaxN / NY;
     constexpr PPlan pp = PairPlan<NY>::c;
     extern __shared__ __align__(16) unsigned char smem_raw[];
