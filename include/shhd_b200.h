@@ -209,22 +209,25 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * pair-line kernels and the single-line kernels; otherwise the one family)
  * with direct launches and as one replayed graph, on the engine's current
  * state, then restores the state, step counter and time and keeps the fastest
- * combination.  *family: 2 register row pass, 1 pair-line, 0 other; *graph_chunk: the chosen
+ * combination.  *family: 3 split row pass, 2 register row pass, 1 pair-line, 0 other; *graph_chunk: the chosen
  * chunk (0 = direct launches); ms_per_step (optional): the measured ms per
  * step of each candidate in order (family 0 direct, family 0 graph, family 1
- * direct, family 1 graph, family 2 direct, family 2 graph).  Family 2 is the
- * pair-line family with the register-resident row pass, valid for FP32
- * engines whose compute rows have 1536 points.  Allocates a temporary copy of
- * the state. */
+ * direct, family 1 graph, family 2 direct, family 2 graph, family 3 direct,
+ * family 3 graph).  Family 2 is the pair-line family with the
+ * register-resident row pass, valid for FP32 engines whose compute rows have
+ * 1536 points; family 3 the pair-line family with the row pass split into an
+ * inverse and a forward kernel over a physical-row buffer (allocated while the
+ * family is selected).  Allocates a temporary copy of the state. */
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
 /* Select the kernel family (no reference counterpart): -1 the default choice,
  * 0 never the pair-line kernels, 1 pair-line where valid, 2 pair-line with the
- * register-resident row pass where valid (otherwise as 1).  Results agree
- * across families within the precision's tolerance.  Drops captured graphs. */
+ * register-resident row pass where valid, 3 pair-line with the split row pass
+ * where valid (otherwise as 1).  Results agree across families within the
+ * precision's tolerance.  Drops captured graphs. */
 int shhd_engine_set_family(shhd_engine* engine, int family);
 
-/* The family the engine launches: 2, 1 or 0 as above. */
+/* The family the engine launches: 3, 2, 1 or 0 as above. */
 int shhd_engine_family(const shhd_engine* engine);
 
 /* Initial conditions generated on the device: the reference's `set` styles

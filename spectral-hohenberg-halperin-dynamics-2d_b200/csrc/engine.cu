@@ -237,8 +237,12 @@ struct shhd_engine {
     bool pair_path = false;       // FP32 pair-line kernels (compile-time sizes up to 1536)
     bool reg_row = false;         // register-resident row pass on 1536-point rows (pair-line layout)
     int family_override = -1;     // -1 choose, 0 never the pair-line kernels, 1 pair-line where valid,
-                                  // 2 pair-line with the register-resident row pass where valid
+                                  // 2 pair-line with the register-resident row pass where valid,
+                                  // 3 pair-line with the split row pass where valid
     void* tw_reg = nullptr;       // twiddles of the register-resident transforms (FP32 engines with 1536-point rows)
+    bool split_row = false;       // pair-line row pass split in two kernels over a physical-row buffer (family 3)
+    void* phys = nullptr;         // that buffer, [member][row pair][input pair-line][npx] pair elements
+    size_t phys_bytes = 0;
     size_t smem_rrow = 0;
     size_t tw_bytes = 0;
     size_t smem_col_inv = 0;
@@ -297,7 +301,7 @@ void* dalloc(shhd_engine* e, size_t bytes) {
 void free_engine(shhd_engine* e) {
     for (void* p : {static_cast<void*>(e->k0_u), static_cast<void*>(e->k0_s1), static_cast<void*>(e->k0_s2)})
         if (p) cudaFree(p);
-    for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->tw_reg, e->ref_stage,
+    for (void* p : {e->u, e->s1, e->s2, e->i1, e->i2, e->ext_a, e->ext_b, e->det, e->tw_x, e->tw_y, e->tw_reg, e->phys, e->ref_stage,
                     static_cast<void*>(e->rho0_dev), static_cast<void*>(e->err_dev), static_cast<void*>(e->static_dev),
                     static_cast<void*>(e->members_dev),
                     static_cast<void*>(e->flag_dev), static_cast<void*>(e->ic_scratch), e->meas.tw_x, e->meas.tw_y, e->meas.i1,
@@ -723,6 +727,8 @@ void build_plan(shhd_engine* e) {
             plan_row_pairs(P);
         }
     }
+    // split row pass (every pair-line size)
+    e->split_row = e->pair_path && e->family_override == 3 && split_row_supported(c.nx) && c.ny % 2 == 0;
     // register-resident row pass (1536-point rows of the pair-line layout)
     e->reg_row = false;
     if (e->pair_path && e->family_override == 2 && c.nx == kRegRowN && c.ny % 2 == 0 && P.rp_canon && rrow_rounds(P) >= 2 &&
@@ -847,6 +853,11 @@ void launch_row(shhd_engine* e) {
     dim3 grid((P.npy + 1) / 2, P.batch);
     LaunchScope scope(e, 1, static_cast<double>(sizeof(cplx<T>)) * P.batch * (P.n_in + P.n_out) * static_cast<double>(P.hx) * P.npy);
     if constexpr (std::is_same<T, float>::value) {
+        if (e->pair_path && e->split_row && e->phys) {
+            launch_split_row(P, P.batch, e->stream, e->members_dev, e->i1, e->phys, e->i2, e->tw_x, e->rho0_dev, e->err_dev);
+            check_cuda(cudaGetLastError(), "row_pass launch");
+            return;
+        }
         if (e->pair_path && e->reg_row && e->tw_reg) {
             launch_rrow_pass(P, P.batch, e->smem_rrow, e->stream, e->members_dev, e->i1, e->i2, e->tw_reg, e->rho0_dev, e->err_dev);
             check_cuda(cudaGetLastError(), "row_pass launch");
@@ -1595,8 +1606,18 @@ void apply_family(shhd_engine* e, int family) {
     check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
     drop_graphs(e);
     e->family_override = family;
-    e->pair_path = e->col_fixed = e->row_fixed = e->reg_row = false;
+    e->pair_path = e->col_fixed = e->row_fixed = e->reg_row = e->split_row = false;
     build_plan(e);
+    // the split row pass's physical-row buffer exists only while that family is selected
+    if (e->split_row && !e->phys) {
+        e->phys_bytes = split_phys_member_elems(e->P) * e->cfg.batch * 16;
+        e->phys = dalloc(e, e->phys_bytes);
+    } else if (!e->split_row && e->phys) {
+        cudaFree(e->phys);
+        e->phys = nullptr;
+        e->device_bytes -= e->phys_bytes;
+        e->phys_bytes = 0;
+    }
     for (void* p : {e->tw_x, e->tw_y})
         if (p) cudaFree(p);
     e->device_bytes -= e->tw_bytes;
@@ -1652,6 +1673,10 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
             probe.pair_path = probe.col_fixed = probe.row_fixed = probe.reg_row = false;
             build_plan(&probe);
             if (probe.reg_row && e->tw_reg) families.push_back(2);
+            probe.family_override = 3;
+            probe.pair_path = probe.col_fixed = probe.row_fixed = probe.reg_row = probe.split_row = false;
+            build_plan(&probe);
+            if (probe.split_row) families.push_back(3);
         }
         int chunk_trial = trial_steps;
         if (e->cfg.integrator == SHHD_EULER && chunk_trial % 2) ++chunk_trial;
@@ -2354,7 +2379,7 @@ int shhd_engine_gk_read(shhd_engine* e, int member, double* sums, size_t n, int6
 int shhd_engine_set_family(shhd_engine* e, int family) {
     return guarded([&] {
         if (!e) throw Failure(SHHD_EINVAL, "null engine");
-        if (family < -1 || family > 2) throw Failure(SHHD_EINVAL, "kernel family must be -1, 0, 1 or 2");
+        if (family < -1 || family > 3) throw Failure(SHHD_EINVAL, "kernel family must be -1, 0, 1, 2 or 3");
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         if (e->fp32) apply_family<float>(e, family);
         else apply_family<double>(e, family);
@@ -2363,7 +2388,7 @@ int shhd_engine_set_family(shhd_engine* e, int family) {
 
 int shhd_engine_family(const shhd_engine* e) {
     if (!e) return -1;
-    return e->reg_row ? 2 : (e->pair_path ? 1 : 0);
+    return e->split_row ? 3 : (e->reg_row ? 2 : (e->pair_path ? 1 : 0));
 }
 
 int shhd_engine_set_graph_chunk(shhd_engine* e, int chunk) {

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "step_kernels_reg.cuh"
+#include "step_kernels_split.cuh"
 #include "step_reg.h"
 
 namespace shhd {
@@ -51,6 +52,37 @@ void launch_rrow_pass(const StepPlan& P, int batch, size_t smem, cudaStream_t st
         case 2: rrow_pass1536<2><<<grid, kRegThreads, smem, stream>>>(P, members, a, o, t, rho0, err); break;
         case 3: rrow_pass1536<3><<<grid, kRegThreads, smem, stream>>>(P, members, a, o, t, rho0, err); break;
         default: rrow_pass1536<4><<<grid, kRegThreads, smem, stream>>>(P, members, a, o, t, rho0, err); break;
+    }
+}
+
+size_t split_phys_member_elems(const StepPlan& P) { return phys_member_elems(P); }
+
+bool split_row_supported(int nx) { return is_pair_size(nx); }
+
+namespace {
+template <int NX>
+void launch_split(const StepPlan& P, int batch, cudaStream_t s, const MemberInfo* members, const void* i1, void* phys, void* i2,
+                  const void* tw, const double* rho0, int* err) {
+    constexpr int RP = kPairMaxN / NX;
+    const size_t smem = static_cast<size_t>(RP) * NX * sizeof(ulonglong2);
+    const int nip = (P.n_in + 1) / 2;
+    dim3 g1(P.npy / 2 / RP, nip, batch), g2(P.npy / 2 / RP, P.rp_n, batch);
+    prow_inverse<NX><<<g1, kThreads, smem, s>>>(P, members, static_cast<const ulonglong2*>(i1), static_cast<ulonglong2*>(phys),
+                                                static_cast<const float2*>(tw), err);
+    prow_forward<NX><<<g2, kThreads, smem, s>>>(P, members, static_cast<const ulonglong2*>(phys), static_cast<ulonglong2*>(i2),
+                                                static_cast<const float2*>(tw), rho0);
+}
+}  // namespace
+
+void launch_split_row(const StepPlan& P, int batch, cudaStream_t stream, const MemberInfo* members, const void* i1, void* phys, void* i2,
+                      const void* tw, const double* rho0, int* err) {
+    switch (P.npx) {
+        case 96: launch_split<96>(P, batch, stream, members, i1, phys, i2, tw, rho0, err); break;
+        case 192: launch_split<192>(P, batch, stream, members, i1, phys, i2, tw, rho0, err); break;
+        case 384: launch_split<384>(P, batch, stream, members, i1, phys, i2, tw, rho0, err); break;
+        case 768: launch_split<768>(P, batch, stream, members, i1, phys, i2, tw, rho0, err); break;
+        case 1536: launch_split<1536>(P, batch, stream, members, i1, phys, i2, tw, rho0, err); break;
+        default: throw std::runtime_error("split row pass: unsupported row length " + std::to_string(P.npx));
     }
 }
 

@@ -26,4 +26,11 @@ size_t rrow_smem_bytes(const StepPlan& P);
 void launch_rrow_pass(const StepPlan& P, int batch, size_t smem, cudaStream_t stream, const MemberInfo* members, const void* i1, void* i2,
                       const void* tw, const double* rho0, int* err);
 
+// split row pass of the pair-line sizes 96 ... 1536 (kernel family 3): the physical-row buffer
+// it needs (pair elements per member), and the launch of its two kernels
+size_t split_phys_member_elems(const StepPlan& P);
+bool split_row_supported(int nx);
+void launch_split_row(const StepPlan& P, int batch, cudaStream_t stream, const MemberInfo* members, const void* i1, void* phys, void* i2,
+                      const void* tw, const double* rho0, int* err);
+
 }  // namespace shhd
