@@ -702,6 +702,8 @@ void build_plan(shhd_engine* e) {
     P.npos = e->npos;
     P.div_w = make_fastdiv(W);
     P.div_kyn = make_fastdiv(P.kyn);
+    P.kyp = (P.kyn + 7) & ~7;
+    P.div_kyp = make_fastdiv(P.kyp);
     P.div_npy = make_fastdiv(c.ny);
     P.div_hx = make_fastdiv(P.hx);
 
@@ -711,7 +713,7 @@ void build_plan(shhd_engine* e) {
         const int cp = kPairMaxN / c.ny, rp = kPairMaxN / c.nx;
         const int nip = (P.n_in + 1) / 2;
         const size_t row_b = static_cast<size_t>(rp) * (nip + 1) * c.nx * 16;
-        const size_t col_b = static_cast<size_t>(cp) * c.ny * 16 + 3ull * cp * P.kyn * 16;  // lines, 3 per-mode arrays
+        const size_t col_b = static_cast<size_t>(cp) * c.ny * 16 + 3ull * cp * ((P.kyn + 7) & ~7) * 16;  // lines, 3 per-mode arrays
         if ((P.hx / 2) % cp == 0 && (c.ny / 2) % rp == 0 && row_b <= smem_cap && col_b <= smem_cap) {
             e->pair_path = true;
             e->col_fixed = e->row_fixed = false;
@@ -1918,6 +1920,8 @@ void build_measure_plan(shhd_engine* e) {
     P.fx.swz = swizzle_mask(c.nx, e->fp32 ? 16 : 8, 1);
     P.div_w = make_fastdiv(W);
     P.div_kyn = make_fastdiv(P.kyn);
+    P.kyp = (P.kyn + 7) & ~7;
+    P.div_kyp = make_fastdiv(P.kyp);
     P.div_npy = make_fastdiv(c.ny);
     P.div_hx = make_fastdiv(P.hx);
     // row pass: at most 3 input lines and row_lb ping-pong lines

@@ -94,6 +94,8 @@ struct StepPlan {
     // transforms
     FftPlan fy, fx;
     FastDiv div_w, div_kyn, div_npy, div_hx;
+    int kyp;                       // kyn rounded up to a multiple of 8: the pair-line column forward's per-mode row stride
+    FastDiv div_kyp;
     int twx_count, twy_count;      // shared-memory twiddle entries for the row / column transforms
     int logw;                      // log2(W)
     int row_lb;                    // max lines per row transform call

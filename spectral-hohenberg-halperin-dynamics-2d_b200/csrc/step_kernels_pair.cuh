@@ -530,6 +530,45 @@ __device__ __forceinline__ void row_velocity_prep(const StepPlan& P, ulonglong2*
     if (bad) atomicOr(err, ERR_ZERO_DENSITY);
 }
 
+// Z staging of one item (input pair-line ip, tile t) of a row pair (rows y0, y0 + 1): the two
+// slots' I1 values at columns k = 2t, 2t + 1 (pz_load), then Z[k] = X0[k] + i X1[k] and the
+// Hermitian mirror Z[N - k] = conj X0[k] + i conj X1[k], kx = 0 keeping the real parts only
+// (pz_store).  Callers load kZBatch items per thread before storing any, so that many I1 reads
+// are in flight at once.
+constexpr int kZBatch = 4;
+struct ZItem {
+    ulonglong2 a0, a1, b0, b1;
+};
+__device__ __forceinline__ ZItem pz_load(const ulonglong2* i1m, size_t plane, int npy, int n_in, int ip, int t, int y0) {
+    const int sa = 2 * ip, sb = 2 * ip + 1;
+    const ulonglong2* pa = i1m + static_cast<size_t>(sa) * plane + static_cast<size_t>(t) * npy + y0;
+    ZItem z;
+    z.a0 = ld_stream(pa);
+    z.a1 = ld_stream(pa + 1);
+    z.b0 = z.b1 = make_ulonglong2(0ull, 0ull);
+    if (sb < n_in) {
+        const ulonglong2* pb = i1m + static_cast<size_t>(sb) * plane + static_cast<size_t>(t) * npy + y0;
+        z.b0 = ld_stream(pb);
+        z.b1 = ld_stream(pb + 1);
+    }
+    return z;
+}
+template <int NX>
+__device__ __forceinline__ void pz_store(ulonglong2* line, int t, const ZItem& z) {
+#pragma unroll
+    for (int w = 0; w < 2; ++w) {
+        const int k = 2 * t + w;
+        // X0, X1 of fields a and b at column k
+        float xa0r = w ? f2_hi(z.a0.x) : f2_lo(z.a0.x), xa0i = w ? f2_hi(z.a0.y) : f2_lo(z.a0.y);
+        float xa1r = w ? f2_hi(z.a1.x) : f2_lo(z.a1.x), xa1i = w ? f2_hi(z.a1.y) : f2_lo(z.a1.y);
+        float xb0r = w ? f2_hi(z.b0.x) : f2_lo(z.b0.x), xb0i = w ? f2_hi(z.b0.y) : f2_lo(z.b0.y);
+        float xb1r = w ? f2_hi(z.b1.x) : f2_lo(z.b1.x), xb1i = w ? f2_hi(z.b1.y) : f2_lo(z.b1.y);
+        if (k == 0) { xa0i = 0.f; xa1i = 0.f; xb0i = 0.f; xb1i = 0.f; }
+        st_pc(line + psw(k), PC{f2_pack(xa0r - xa1i, xb0r - xb1i), f2_pack(xa0i + xa1r, xb0i + xb1r)});
+        if (k > 0) st_pc(line + psw(NX - k), PC{f2_pack(xa0r + xa1i, xb0r + xb1i), f2_pack(xa1r - xa0i, xb1r - xb0i)});
+    }
+}
+
 template <int NX>
 __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const MemberInfo* __restrict__ members,
                                                       const ulonglong2* __restrict__ i1, ulonglong2* __restrict__ i2,
@@ -551,32 +590,26 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
     // 1. Z[k] = X0[k] + i X1[k] (rows y0, y0 + 1) with the Hermitian mirror Z[N - k]
     //    = conj X0[k] + i conj X1[k]; kx = 0 keeps the real parts only
     {
-        const int per_r = nip * hp;
-        for (int e = threadIdx.x; e < RP * per_r; e += kThreads) {
-            const int r = e / per_r, rem = e - r * per_r;
-            const int ip = rem / hp, t = rem - ip * hp;
-            const int y0 = 2 * (pair0 + r);
-            const int sa = 2 * ip, sb = 2 * ip + 1;
-            const ulonglong2* pa = i1m + static_cast<size_t>(sa) * plane + static_cast<size_t>(t) * npy + y0;
-            const ulonglong2 a0 = ld_stream(pa), a1 = ld_stream(pa + 1);
-            ulonglong2 b0 = make_ulonglong2(0ull, 0ull), b1 = b0;
-            if (sb < P.n_in) {
-                const ulonglong2* pb = i1m + static_cast<size_t>(sb) * plane + static_cast<size_t>(t) * npy + y0;
-                b0 = ld_stream(pb);
-                b1 = ld_stream(pb + 1);
-            }
-            ulonglong2* line = inl + (static_cast<size_t>(r) * nip + ip) * NX;
+        const int per_r = nip * hp, nz = RP * per_r;
+        for (int e0 = threadIdx.x; e0 < nz; e0 += kZBatch * kThreads) {
+            ZItem z[kZBatch];
 #pragma unroll
-            for (int w = 0; w < 2; ++w) {
-                const int k = 2 * t + w;
-                // X0, X1 of fields a and b at column k
-                float xa0r = w ? f2_hi(a0.x) : f2_lo(a0.x), xa0i = w ? f2_hi(a0.y) : f2_lo(a0.y);
-                float xa1r = w ? f2_hi(a1.x) : f2_lo(a1.x), xa1i = w ? f2_hi(a1.y) : f2_lo(a1.y);
-                float xb0r = w ? f2_hi(b0.x) : f2_lo(b0.x), xb0i = w ? f2_hi(b0.y) : f2_lo(b0.y);
-                float xb1r = w ? f2_hi(b1.x) : f2_lo(b1.x), xb1i = w ? f2_hi(b1.y) : f2_lo(b1.y);
-                if (k == 0) { xa0i = 0.f; xa1i = 0.f; xb0i = 0.f; xb1i = 0.f; }
-                st_pc(line + psw(k), PC{f2_pack(xa0r - xa1i, xb0r - xb1i), f2_pack(xa0i + xa1r, xb0i + xb1r)});
-                if (k > 0) st_pc(line + psw(NX - k), PC{f2_pack(xa0r + xa1i, xb0r + xb1i), f2_pack(xa1r - xa0i, xb1r - xb0i)});
+            for (int u = 0; u < kZBatch; ++u) {
+                const int e = e0 + u * kThreads;
+                if (e < nz) {
+                    const int r = e / per_r, rem = e - r * per_r;
+                    const int ip = rem / hp, t = rem - ip * hp;
+                    z[u] = pz_load(i1m, plane, npy, P.n_in, ip, t, 2 * (pair0 + r));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kZBatch; ++u) {
+                const int e = e0 + u * kThreads;
+                if (e < nz) {
+                    const int r = e / per_r, rem = e - r * per_r;
+                    const int ip = rem / hp, t = rem - ip * hp;
+                    pz_store<NX>(inl + (static_cast<size_t>(r) * nip + ip) * NX, t, z[u]);
+                }
             }
         }
         const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
@@ -643,9 +676,20 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
 
 // ---------------------------------------------------------------------------
 // column forward + epilogue (grid: column-pair tiles x groups x batch).
-// Shared memory: CP work pair-lines, then three per-mode arrays [CP][Ky]
-// (accumulators / new values: psi or jx, jy, rho), two columns per element.
+// Shared memory: CP work pair-lines, then three per-mode arrays [CP][Kp]
+// (accumulators / new values: psi or jx, jy, rho), two columns per element,
+// Kp = Ky rounded up to a multiple of 8.
 // ---------------------------------------------------------------------------
+// slot of mode j in a column's per-mode row.  The last DIF stage (and the first stage of the
+// fused inverse) reaches the modes in digit-reversed order: at 384 points and up the eight
+// threads of a quarter warp then touch modes 3 * 8 ... 3 * 64 apart, all in one 16-byte bank
+// group of a plain row, so there the low three bits are XORed with bits 3..5.  Eight
+// consecutive modes from a multiple of 8 stay in their own eight slots either way.
+template <int NY>
+__device__ __forceinline__ int pmode_slot(int c, int j, int kyp) {
+    return c * kyp + (NY >= 384 ? (j ^ ((j >> 3) & 7)) : j);
+}
+
 // blocks per SM the column forward is compiled for: its 74 KB of shared memory allow three, and at
 // 384 points and up the register budget of three (85) holds it without spilling more than 40 B
 template <int NY>
@@ -657,11 +701,11 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
     constexpr int CP = kPairMaxN / NY;
     constexpr PPlan pp = PairPlan<NY>::c;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int kyn = P.kyn, nay = P.nay, half = nay / 2;
+    const int kyn = P.kyn, kyp = P.kyp, nay = P.nay, half = nay / 2;
     ulonglong2* lines = reinterpret_cast<ulonglong2*>(smem_raw);       // [CP][NY]
-    ulonglong2* acc0 = lines + CP * NY;                                  // [CP][Ky]
-    ulonglong2* acc1 = acc0 + CP * kyn;
-    ulonglong2* acc2 = acc1 + CP * kyn;
+    ulonglong2* acc0 = lines + CP * NY;                                  // [CP][Kp], slots pmode_slot
+    ulonglong2* acc1 = acc0 + CP * kyp;
+    ulonglong2* acc2 = acc1 + CP * kyp;
     const int t0 = blockIdx.x * CP, grp = blockIdx.y, b = blockIdx.z;
     const int gkind = P.group_kind[grp], alpha = P.group_alpha[grp];
     const bool comp = (P.mode == 0);
@@ -684,7 +728,7 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
         if (gkind == GROUP_PSI) fetch(1 + alpha);
         else { fetch(P.nop + 1); fetch(P.nop + 2); fetch(0); }
     }
-    for (int e = threadIdx.x; e < CP * kyn; e += kThreads) {
+    for (int e = threadIdx.x; e < CP * kyp; e += kThreads) {
         st_pc(acc0 + e, pc_zero());
         st_pc(acc1 + e, pc_zero());
     }
@@ -716,8 +760,9 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
             const float gx0 = static_cast<float>(2 * (t0 + l));
             const u64 KX = f2_pack(kxu * gx0, kxu * (gx0 + 1.f));
             const u64 KY = f2_splat(kyv);
-            ulonglong2* q0 = acc0 + l * kyn + j;
-            ulonglong2* q1 = acc1 + l * kyn + j;
+            const int sj = pmode_slot<NY>(l, j, kyp);
+            ulonglong2* q0 = acc0 + sj;
+            ulonglong2* q1 = acc1 + sj;
             // -i v = (v.im, -v.re): a += beta (-i v) -> a.re += beta v.im, a.im -= beta v.re
             switch (kind) {
                 case OUT_MU: {  // a0 += -M k^2 v
@@ -783,11 +828,13 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
     __syncthreads();
 
     // epilogue per mode (natural order, coalesced state access): results replace the accumulators
-    for (int e = threadIdx.x; e < CP * kyn; e += kThreads) {
-        const int c = fdiv(e, P.div_kyn), j = e - c * kyn;
+    for (int e = threadIdx.x; e < CP * kyp; e += kThreads) {
+        const int c = fdiv(e, P.div_kyp), j = e - c * kyp;
+        if (j >= kyn) continue;
+        const int sj = pmode_slot<NY>(c, j, kyp);
         const int t = t0 + c;
         const size_t mbase = static_cast<size_t>(b) * P.nfields * fstride + static_cast<size_t>(t) * 2 * kyn;
-        const PC u0 = ld_pc(acc0 + e);
+        const PC u0 = ld_pc(acc0 + sj);
         if (gkind == GROUP_PSI) {
             float2 r[2];
 #pragma unroll
@@ -796,9 +843,9 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
                 const PsiLoads<float> L = psi_loads<float>(P, A, alpha, m.pos, fstride);
                 r[w] = psi_epilogue<float>(P, A, alpha, m, kxu * static_cast<float>(m.gx), kyu * static_cast<float>(m.ky), pc_col(u0, w), mi, L, b);
             }
-            st_pc(acc0 + e, pc_make(r[0], r[1]));
+            st_pc(acc0 + sj, pc_make(r[0], r[1]));
         } else {
-            const PC u1 = ld_pc(acc1 + e);
+            const PC u1 = ld_pc(acc1 + sj);
             float2 r0[2], r1[2], r2[2];
 #pragma unroll
             for (int w = 0; w < 2; ++w) {
@@ -810,9 +857,9 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
                 momentum_epilogue<float>(P, A, m, kx, kyv, r0[w], r1[w], mi, L, b);
                 r2[w] = comp ? rho_epilogue<float>(P, A, m.pos, kx, kyv, fstride) : make_float2(0.f, 0.f);
             }
-            st_pc(acc0 + e, pc_make(r0[0], r0[1]));
-            st_pc(acc1 + e, pc_make(r1[0], r1[1]));
-            st_pc(acc2 + e, pc_make(r2[0], r2[1]));
+            st_pc(acc0 + sj, pc_make(r0[0], r0[1]));
+            st_pc(acc1 + sj, pc_make(r1[0], r1[1]));
+            st_pc(acc2 + sj, pc_make(r2[0], r2[1]));
         }
     }
     __syncthreads();
@@ -828,12 +875,14 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
                 v.y = f2_pack(0.f, f2_hi(v.y));
                 a[0] = v;
             } else {
-                ulonglong2 vp = a[ky], vn = a[kyn - ky];
+                ulonglong2* ap = a + pmode_slot<NY>(0, ky, kyp);
+                ulonglong2* an = a + pmode_slot<NY>(0, kyn - ky, kyp);
+                ulonglong2 vp = *ap, vn = *an;
                 const float pr = 0.5f * (f2_lo(vp.x) + f2_lo(vn.x)), pi = 0.5f * (f2_lo(vp.y) - f2_lo(vn.y));
                 vp.x = f2_pack(pr, f2_hi(vp.x)); vp.y = f2_pack(pi, f2_hi(vp.y));
                 vn.x = f2_pack(pr, f2_hi(vn.x)); vn.y = f2_pack(-pi, f2_hi(vn.y));
-                a[ky] = vp;
-                a[kyn - ky] = vn;
+                *ap = vp;
+                *an = vn;
             }
         }
         __syncthreads();
@@ -851,9 +900,10 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
     bool bad = false;
     for (int q = 0; q < nwf; ++q) {
         float2* dst = A.next + static_cast<size_t>(b) * P.nfields * fstride + static_cast<size_t>(wfield[q]) * fstride;
-        for (int e = threadIdx.x; e < CP * kyn; e += kThreads) {
-            const int c = fdiv(e, P.div_kyn), j = e - c * kyn;
-            const PC v = ld_pc(wsrc[q] + e);
+        for (int e = threadIdx.x; e < CP * kyp; e += kThreads) {
+            const int c = fdiv(e, P.div_kyp), j = e - c * kyp;
+            if (j >= kyn) continue;
+            const PC v = ld_pc(wsrc[q] + pmode_slot<NY>(c, j, kyp));
             const size_t gx = static_cast<size_t>(2 * (t0 + c));
             const float2 v0 = pc_col(v, 0), v1 = pc_col(v, 1);
             bad |= nonfinite2(make_float2(v0.x + v0.y, v1.x + v1.y));
@@ -876,7 +926,7 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
         pstage_io<NY, pp.m - 1, +1, true>(CP, tw, [&](int l, int p) {
             const int ky = pky_of_y(ppinv<NY>(p), NY);
             if (ky >= half || ky <= -half) return pc_zero();
-            return ld_pc(a + l * kyn + (ky >= 0 ? ky : ky + kyn));
+            return ld_pc(a + pmode_slot<NY>(l, ky >= 0 ? ky : ky + kyn, kyp));
         }, SmemIO{lines, NY});
         __syncthreads();
         pdit_range<NY, pp.m - 1, 1, +1>(lines, CP, tw);

@@ -14,7 +14,8 @@
 //                  and the untangling into I2.
 // Each block holds one line per row pair (24 KB at 1536 points), so many blocks share an SM
 // and their barrier chains overlap.  The physical rows (57 MB at the 1024^2 N = 2 workload)
-// are written once and read by each output pair that uses them, mostly from L2.
+// are written once and read by each output pair that uses them; at that size they do not stay
+// in L2 (63 MB of DRAM reads per forward launch), and the family is slower than prow_pass there.
 #pragma once
 
 #include "step_kernels_pair.cuh"
@@ -41,31 +42,26 @@ __global__ void __launch_bounds__(kThreads) prow_inverse(const StepPlan P, const
     const int ip = blockIdx.y, pair0 = blockIdx.x * RP;
     const size_t plane = static_cast<size_t>(P.ntiles) * npy;
     const ulonglong2* i1m = i1 + static_cast<size_t>(b) * P.n_in * plane;
-    const int sa = 2 * ip, sb = 2 * ip + 1;
 
     // Z[k] = X0[k] + i X1[k] (rows y0, y0 + 1) with the Hermitian mirror Z[N - k]; kx = 0 real parts
-    for (int e = threadIdx.x; e < RP * hp; e += kThreads) {
-        const int r = e / hp, t = e - r * hp;
-        const int y0 = 2 * (pair0 + r);
-        const ulonglong2* pa = i1m + static_cast<size_t>(sa) * plane + static_cast<size_t>(t) * npy + y0;
-        const ulonglong2 a0 = ld_stream(pa), a1 = ld_stream(pa + 1);
-        ulonglong2 b0 = make_ulonglong2(0ull, 0ull), b1 = b0;
-        if (sb < P.n_in) {
-            const ulonglong2* pb = i1m + static_cast<size_t>(sb) * plane + static_cast<size_t>(t) * npy + y0;
-            b0 = ld_stream(pb);
-            b1 = ld_stream(pb + 1);
-        }
-        ulonglong2* line = lines + static_cast<size_t>(r) * NX;
+    const int nz = RP * hp;
+    for (int e0 = threadIdx.x; e0 < nz; e0 += kZBatch * kThreads) {
+        ZItem z[kZBatch];
 #pragma unroll
-        for (int w = 0; w < 2; ++w) {
-            const int k = 2 * t + w;
-            float xa0r = w ? f2_hi(a0.x) : f2_lo(a0.x), xa0i = w ? f2_hi(a0.y) : f2_lo(a0.y);
-            float xa1r = w ? f2_hi(a1.x) : f2_lo(a1.x), xa1i = w ? f2_hi(a1.y) : f2_lo(a1.y);
-            float xb0r = w ? f2_hi(b0.x) : f2_lo(b0.x), xb0i = w ? f2_hi(b0.y) : f2_lo(b0.y);
-            float xb1r = w ? f2_hi(b1.x) : f2_lo(b1.x), xb1i = w ? f2_hi(b1.y) : f2_lo(b1.y);
-            if (k == 0) { xa0i = 0.f; xa1i = 0.f; xb0i = 0.f; xb1i = 0.f; }
-            st_pc(line + psw(k), PC{f2_pack(xa0r - xa1i, xb0r - xb1i), f2_pack(xa0i + xa1r, xb0i + xb1r)});
-            if (k > 0) st_pc(line + psw(NX - k), PC{f2_pack(xa0r + xa1i, xb0r + xb1i), f2_pack(xa1r - xa0i, xb1r - xb0i)});
+        for (int u = 0; u < kZBatch; ++u) {
+            const int e = e0 + u * kThreads;
+            if (e < nz) {
+                const int r = e / hp, t = e - r * hp;
+                z[u] = pz_load(i1m, plane, npy, P.n_in, ip, t, 2 * (pair0 + r));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kZBatch; ++u) {
+            const int e = e0 + u * kThreads;
+            if (e < nz) {
+                const int r = e / hp, t = e - r * hp;
+                pz_store<NX>(lines + static_cast<size_t>(r) * NX, t, z[u]);
+            }
         }
     }
     const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
