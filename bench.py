@@ -782,9 +782,9 @@ def main():
     ap.add_argument("--precision", choices=("fp32", "fp64"), default="fp32")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--family", type=int, choices=(0, 1, 2, 3), default=None,
+    ap.add_argument("--family", type=int, choices=(0, 1, 2, 3, 4), default=None,
                     help="kernel family instead of the autotuner's choice (0 single-line, 1 pair-line, 2 register row pass, "
-                         "3 split row pass)")
+                         "3 split row pass, 4 two-pair row pass)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -209,25 +209,29 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * pair-line kernels and the single-line kernels; otherwise the one family)
  * with direct launches and as one replayed graph, on the engine's current
  * state, then restores the state, step counter and time and keeps the fastest
- * combination.  *family: 3 split row pass, 2 register row pass, 1 pair-line, 0 other; *graph_chunk: the chosen
- * chunk (0 = direct launches); ms_per_step (optional): the measured ms per
- * step of each candidate in order (family 0 direct, family 0 graph, family 1
- * direct, family 1 graph, family 2 direct, family 2 graph, family 3 direct,
- * family 3 graph).  Family 2 is the pair-line family with the
- * register-resident row pass, valid for FP32 engines whose compute rows have
- * 1536 points; family 3 the pair-line family with the row pass split into an
- * inverse and a forward kernel over a physical-row buffer (allocated while the
- * family is selected).  Allocates a temporary copy of the state. */
+ * combination.  *family: 4 two-pair row pass, 3 split row pass, 2 register
+ * row pass, 1 pair-line, 0 other; *graph_chunk: the chosen chunk (0 = direct
+ * launches); ms_per_step (optional, room for 10): the measured ms per step of
+ * each valid candidate in order (family 0 direct, family 0 graph, family 1
+ * direct, family 1 graph, ... family 4 graph).  Family 2 is the pair-line
+ * family with the register-resident row pass, valid for FP32 engines whose
+ * compute rows have 1536 points; family 3 the pair-line family with the row
+ * pass split into an inverse and a forward kernel over a physical-row buffer
+ * (allocated while the family is selected); family 4 the pair-line family
+ * whose row pass transforms two output pairs at a time, valid for compressible
+ * dynamics whose last two input pair-lines are (rho, jx), (jy, -).  Allocates
+ * a temporary copy of the state. */
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
 /* Select the kernel family (no reference counterpart): -1 the default choice,
  * 0 never the pair-line kernels, 1 pair-line where valid, 2 pair-line with the
  * register-resident row pass where valid, 3 pair-line with the split row pass
- * where valid (otherwise as 1).  Results agree across families within the
- * precision's tolerance.  Drops captured graphs. */
+ * where valid, 4 pair-line with the two-pair row pass where valid (2, 3 and 4
+ * otherwise as 1).  Results agree across families within the precision's
+ * tolerance; families 1 and 4 agree bit for bit.  Drops captured graphs. */
 int shhd_engine_set_family(shhd_engine* engine, int family);
 
-/* The family the engine launches: 3, 2, 1 or 0 as above. */
+/* The family the engine launches: 4, 3, 2, 1 or 0 as above. */
 int shhd_engine_family(const shhd_engine* engine);
 
 /* Initial conditions generated on the device: the reference's `set` styles

@@ -238,9 +238,12 @@ struct shhd_engine {
     bool reg_row = false;         // register-resident row pass on 1536-point rows (pair-line layout)
     int family_override = -1;     // -1 choose, 0 never the pair-line kernels, 1 pair-line where valid,
                                   // 2 pair-line with the register-resident row pass where valid,
-                                  // 3 pair-line with the split row pass where valid
+                                  // 3 pair-line with the split row pass where valid,
+                                  // 4 pair-line with the two-pair row pass where valid
     void* tw_reg = nullptr;       // twiddles of the register-resident transforms (FP32 engines with 1536-point rows)
     bool split_row = false;       // pair-line row pass split in two kernels over a physical-row buffer (family 3)
+    bool dual_row = false;        // pair-line row pass over two output pairs at a time (family 4)
+    size_t smem_dual = 0;
     void* phys = nullptr;         // that buffer, [member][row pair][input pair-line][npx] pair elements
     size_t phys_bytes = 0;
     size_t smem_rrow = 0;
@@ -731,6 +734,12 @@ void build_plan(shhd_engine* e) {
     }
     // split row pass (every pair-line size)
     e->split_row = e->pair_path && e->family_override == 3 && split_row_supported(c.nx) && c.ny % 2 == 0;
+    // row pass over two output pairs at a time (compressible canonical layouts)
+    e->dual_row = false;
+    if (e->pair_path && e->family_override == 4 && c.ny % 2 == 0 && dual_row_supported(P)) {
+        e->smem_dual = dual_row_smem_bytes(P);
+        e->dual_row = e->smem_dual <= smem_cap;
+    }
     // register-resident row pass (1536-point rows of the pair-line layout)
     e->reg_row = false;
     if (e->pair_path && e->family_override == 2 && c.nx == kRegRowN && c.ny % 2 == 0 && P.rp_canon && rrow_rounds(P) >= 2 &&
@@ -857,6 +866,11 @@ void launch_row(shhd_engine* e) {
     if constexpr (std::is_same<T, float>::value) {
         if (e->pair_path && e->split_row && e->phys) {
             launch_split_row(P, P.batch, e->stream, e->members_dev, e->i1, e->phys, e->i2, e->tw_x, e->rho0_dev, e->err_dev);
+            check_cuda(cudaGetLastError(), "row_pass launch");
+            return;
+        }
+        if (e->pair_path && e->dual_row) {
+            launch_dual_row(P, P.batch, e->stream, e->members_dev, e->i1, e->i2, e->tw_x, e->err_dev);
             check_cuda(cudaGetLastError(), "row_pass launch");
             return;
         }
@@ -1608,7 +1622,7 @@ void apply_family(shhd_engine* e, int family) {
     check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
     drop_graphs(e);
     e->family_override = family;
-    e->pair_path = e->col_fixed = e->row_fixed = e->reg_row = e->split_row = false;
+    e->pair_path = e->col_fixed = e->row_fixed = e->reg_row = e->split_row = e->dual_row = false;
     build_plan(e);
     // the split row pass's physical-row buffer exists only while that family is selected
     if (e->split_row && !e->phys) {
@@ -1679,6 +1693,10 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
             probe.pair_path = probe.col_fixed = probe.row_fixed = probe.reg_row = probe.split_row = false;
             build_plan(&probe);
             if (probe.split_row) families.push_back(3);
+            probe.family_override = 4;
+            probe.pair_path = probe.col_fixed = probe.row_fixed = probe.reg_row = probe.split_row = probe.dual_row = false;
+            build_plan(&probe);
+            if (probe.dual_row) families.push_back(4);
         }
         int chunk_trial = trial_steps;
         if (e->cfg.integrator == SHHD_EULER && chunk_trial % 2) ++chunk_trial;
@@ -2383,7 +2401,7 @@ int shhd_engine_gk_read(shhd_engine* e, int member, double* sums, size_t n, int6
 int shhd_engine_set_family(shhd_engine* e, int family) {
     return guarded([&] {
         if (!e) throw Failure(SHHD_EINVAL, "null engine");
-        if (family < -1 || family > 3) throw Failure(SHHD_EINVAL, "kernel family must be -1, 0, 1, 2 or 3");
+        if (family < -1 || family > 4) throw Failure(SHHD_EINVAL, "kernel family must be -1, 0, 1, 2, 3 or 4");
         check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
         if (e->fp32) apply_family<float>(e, family);
         else apply_family<double>(e, family);
@@ -2392,7 +2410,7 @@ int shhd_engine_set_family(shhd_engine* e, int family) {
 
 int shhd_engine_family(const shhd_engine* e) {
     if (!e) return -1;
-    return e->split_row ? 3 : (e->reg_row ? 2 : (e->pair_path ? 1 : 0));
+    return e->dual_row ? 4 : (e->split_row ? 3 : (e->reg_row ? 2 : (e->pair_path ? 1 : 0)));
 }
 
 int shhd_engine_set_graph_chunk(shhd_engine* e, int chunk) {

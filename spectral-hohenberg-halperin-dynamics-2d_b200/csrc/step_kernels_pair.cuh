@@ -56,6 +56,14 @@ __device__ __forceinline__ ulonglong2 ld_stream(const ulonglong2* p) {
     asm("ld.global.L1::no_allocate.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p));
     return v;
 }
+// and written once: kept out of L1, so that the lines the scattered plane writes touch do not
+// evict the twiddles
+__device__ __forceinline__ void st_stream(ulonglong2* p, ulonglong2 v) {
+    asm volatile("st.global.L1::no_allocate.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(v.x), "l"(v.y) : "memory");
+}
+
+// entry i of a twiddle table
+__device__ __forceinline__ float2 tw_at(const float2* __restrict__ tw, int i) { return ld_tw2(tw + i); }
 
 // one position of two lines: re = (re_a, re_b), im = (im_a, im_b)
 struct PC {
@@ -84,10 +92,9 @@ __device__ __forceinline__ float2 pc_col(PC v, int half) {  // one line's comple
 __device__ __forceinline__ PC pc_make(float2 a, float2 b) { return PC{f2_pack(a.x, b.x), f2_pack(a.y, b.y)}; }
 
 // x_q *= w^q (q = 1..R-1, DIR < 0) or conj: from one table twiddle w, powers by a product tree
-// at most three roundings deep
-template <int R, int DIR>
-__device__ __forceinline__ void ptwiddle_pow(PC* v, float2 w1) {
-    float2 w[8];
+// at most three roundings deep (ptwiddle_powers), applied to a butterfly's values (ptwiddle_apply)
+template <int R>
+__device__ __forceinline__ void ptwiddle_powers(float2 w1, float2* w) {
     w[1] = w1;
     auto cm = [](float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
     if constexpr (R > 2) w[2] = cm(w1, w1);
@@ -98,8 +105,17 @@ __device__ __forceinline__ void ptwiddle_pow(PC* v, float2 w1) {
         w[6] = cm(w[4], w[2]);
         w[7] = cm(w[4], w[3]);
     }
+}
+template <int R, int DIR>
+__device__ __forceinline__ void ptwiddle_apply(PC* v, const float2* w) {
 #pragma unroll
     for (int q = 1; q < R; ++q) v[q] = pcmul<DIR>(v[q], f2_splat(w[q].x), f2_splat(w[q].y));
+}
+template <int R, int DIR>
+__device__ __forceinline__ void ptwiddle_pow(PC* v, float2 w1) {
+    float2 w[8];
+    ptwiddle_powers<R>(w1, w);
+    ptwiddle_apply<R, DIR>(v, w);
 }
 
 // ---------------------------------------------------------------------------
@@ -241,8 +257,8 @@ template <int N> __device__ __forceinline__ int ppinv(int p) {
 // value at natural slot index p (0 <= p < N) of line l.  DIF twiddles after
 // the butterfly, DIT before; the stage-s twiddle of butterfly j is w_L^(j q).
 // ---------------------------------------------------------------------------
-template <int N, int S, int DIR, bool DIT, typename Load, typename Store>
-__device__ __forceinline__ void pstage_io(int nl, const float2* __restrict__ tw, Load&& load, Store&& store) {
+template <int N, int S, int DIR, bool DIT, typename TW, typename Load, typename Store>
+__device__ __forceinline__ void pstage_io(int nl, TW tw, Load&& load, Store&& store) {
     constexpr PPlan pp = PairPlan<N>::c;
     constexpr int R = pp.r[S], ST = pp.s[S], L = R * ST, NB = N / R;
     const int tot = nl * NB;
@@ -255,11 +271,11 @@ __device__ __forceinline__ void pstage_io(int nl, const float2* __restrict__ tw,
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = load(l, base + q * ST);
         if constexpr (L > R) {
-            if constexpr (DIT) ptwiddle_pow<R, DIR>(v, ld_tw2(tw + pp.twoff[S] + j));
+            if constexpr (DIT) ptwiddle_pow<R, DIR>(v, tw_at(tw, pp.twoff[S] + j));
         }
         pbfly<R, DIR>(v);
         if constexpr (L > R) {
-            if constexpr (!DIT) ptwiddle_pow<R, DIR>(v, ld_tw2(tw + pp.twoff[S] + j));
+            if constexpr (!DIT) ptwiddle_pow<R, DIR>(v, tw_at(tw, pp.twoff[S] + j));
         }
 #pragma unroll
         for (int q = 0; q < R; ++q) store(l, base + q * ST, v[q]);
@@ -275,8 +291,8 @@ struct SmemIO {
 };
 
 // stages [S, E) in shared memory (DIF ascending, DIT descending), a barrier after each
-template <int N, int S, int E, int DIR>
-__device__ __forceinline__ void pdif_range(ulonglong2* lines, int nl, const float2* tw) {
+template <int N, int S, int E, int DIR, typename TW>
+__device__ __forceinline__ void pdif_range(ulonglong2* lines, int nl, TW tw) {
     if constexpr (S < E) {
         const SmemIO io{lines, N};
         pstage_io<N, S, DIR, false>(nl, tw, io, io);
@@ -284,8 +300,8 @@ __device__ __forceinline__ void pdif_range(ulonglong2* lines, int nl, const floa
         pdif_range<N, S + 1, E, DIR>(lines, nl, tw);
     }
 }
-template <int N, int S, int E, int DIR>
-__device__ __forceinline__ void pdit_range(ulonglong2* lines, int nl, const float2* tw) {
+template <int N, int S, int E, int DIR, typename TW>
+__device__ __forceinline__ void pdit_range(ulonglong2* lines, int nl, TW tw) {
     if constexpr (S > E) {
         const SmemIO io{lines, N};
         pstage_io<N, S - 1, DIR, true>(nl, tw, io, io);
@@ -355,7 +371,7 @@ __global__ void __launch_bounds__(kThreads) pcol_inverse(const StepPlan P, const
     const u64 sc = f2_splat(static_cast<float>(P.inv_scale));
     ulonglong2* dst = i1 + ((static_cast<size_t>(b) * P.n_in + slot) * P.ntiles + t0) * static_cast<size_t>(NY);
     pstage_io<NY, 0, +1, true>(CP, tw, SmemIO{lines, NY}, [&](int l, int p, PC v) {
-        st_pc(dst + static_cast<size_t>(l) * NY + p, PC{f2_mul(v.re, sc), f2_mul(v.im, sc)});
+        st_stream(dst + static_cast<size_t>(l) * NY + p, make_ulonglong2(f2_mul(v.re, sc), f2_mul(v.im, sc)));
     });
 }
 
@@ -403,15 +419,28 @@ __device__ __forceinline__ RowProduct row_product(const StepPlan& P, int pi, flo
     return R;
 }
 
-// canonical input roles: psi of A and B from their slots, (jx, jy) and (vx, vy) lines
+// (jx, jy) and (vx, vy) of the canonical layout at one position: J = ((jx, jy) of row y0,
+// (jx, jy) of row y0 + 1), V likewise
+struct JV {
+    ulonglong2 J, V;
+};
 template <int NX>
-__device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProduct& R, const ulonglong2* in, int sp) {
+__device__ __forceinline__ JV row_jv(const StepPlan& P, const RowProduct& R, const ulonglong2* in, int sp) {
+    const ulonglong2 J = in[P.rp_jline * NX + sp];
+    const ulonglong2 V = P.rp_vline >= 0 ? in[P.rp_vline * NX + sp] : make_ulonglong2(f2_mul(J.x, R.IR0), f2_mul(J.y, R.IR0));
+    return JV{J, V};
+}
+
+// canonical input roles: psi of A and B from their slots, (jx, jy) and (vx, vy) from get_jv()
+// (read where a product needs them)
+template <int NX, typename GetJV>
+__device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProduct& R, const ulonglong2* in, int sp, GetJV&& get_jv) {
     const u64* C = R.C;
     const int mode = R.mode;
     if (mode != 0) {  // outputs that are elementwise products of whole lines
         if (mode == 1 || mode == 2) {
-            const ulonglong2 J = in[P.rp_jline * NX + sp];
-            const ulonglong2 V = P.rp_vline >= 0 ? in[P.rp_vline * NX + sp] : make_ulonglong2(f2_mul(J.x, R.IR0), f2_mul(J.y, R.IR0));
+            const JV jv = get_jv();
+            const ulonglong2 J = jv.J, V = jv.V;
             if (mode == 1) return PC{V.x, V.y};
             return PC{f2_mul(J.x, V.x), f2_mul(J.y, V.y)};
         }
@@ -421,8 +450,7 @@ __device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProd
             const u64 q1 = f2_mul(f2_mul(S.y, S.y), f2_mul(S.y, C[0]));
             return PC{q0, q1};
         }
-        const ulonglong2 J = in[P.rp_jline * NX + sp];
-        const ulonglong2 V = P.rp_vline >= 0 ? in[P.rp_vline * NX + sp] : make_ulonglong2(f2_mul(J.x, R.IR0), f2_mul(J.y, R.IR0));
+        const ulonglong2 V = get_jv().V;
         const u64 v0 = mode == 4 ? f2_splat(f2_lo(V.x)) : f2_splat(f2_hi(V.x));
         const u64 v1 = mode == 4 ? f2_splat(f2_lo(V.y)) : f2_splat(f2_hi(V.y));
         const u64 cc = mode == 4 ? C[1] : C[2];
@@ -431,10 +459,8 @@ __device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProd
     u64 out[2] = {0ull, 0ull};
     float jxr[2] = {0.f, 0.f}, jyr[2] = {0.f, 0.f}, vxr[2] = {0.f, 0.f}, vyr[2] = {0.f, 0.f};
     if (R.need_j) {
-        const ulonglong2 J = in[P.rp_jline * NX + sp];
-        ulonglong2 V;
-        if (P.rp_vline >= 0) V = in[P.rp_vline * NX + sp];
-        else V = make_ulonglong2(f2_mul(J.x, R.IR0), f2_mul(J.y, R.IR0));
+        const JV jv = get_jv();
+        const ulonglong2 J = jv.J, V = jv.V;
         jxr[0] = f2_lo(J.x); jyr[0] = f2_hi(J.x); jxr[1] = f2_lo(J.y); jyr[1] = f2_hi(J.y);
         vxr[0] = f2_lo(V.x); vyr[0] = f2_hi(V.x); vxr[1] = f2_lo(V.y); vyr[1] = f2_hi(V.y);
     }
@@ -457,6 +483,10 @@ __device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProd
         out[row] = o;
     }
     return PC{out[0], out[1]};
+}
+template <int NX>
+__device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProduct& R, const ulonglong2* in, int sp) {
+    return row_product_canon<NX>(P, R, in, sp, [&] { return row_jv<NX>(P, R, in, sp); });
 }
 
 // any input layout: product_value per row (rho replaced by 1 / rho in compressible dynamics)
@@ -569,6 +599,94 @@ __device__ __forceinline__ void pz_store(ulonglong2* line, int t, const ZItem& z
     }
 }
 
+// row pass, first part: Z staging of the nip input pair-lines of a block's RP row pairs (from
+// pair0) and their x-inverse in place (DIF stages in shared memory, a barrier after each)
+template <int NX, typename TW>
+__device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2* __restrict__ i1m, size_t plane, ulonglong2* inl, int nip,
+                                            int pair0, TW tw) {
+    constexpr int RP = kPairMaxN / NX;
+    constexpr PPlan pp = PairPlan<NX>::c;
+    const int npy = P.npy, hx = P.hx, hp = hx >> 1;
+    // Z[k] = X0[k] + i X1[k] (rows y0, y0 + 1) with the Hermitian mirror Z[N - k]
+    // = conj X0[k] + i conj X1[k]; kx = 0 keeps the real parts only
+    const int per_r = nip * hp, nz = RP * per_r;
+    for (int e0 = threadIdx.x; e0 < nz; e0 += kZBatch * kThreads) {
+        ZItem z[kZBatch];
+#pragma unroll
+        for (int u = 0; u < kZBatch; ++u) {
+            const int e = e0 + u * kThreads;
+            if (e < nz) {
+                const int r = e / per_r, rem = e - r * per_r;
+                const int ip = rem / hp, t = rem - ip * hp;
+                z[u] = pz_load(i1m, plane, npy, P.n_in, ip, t, 2 * (pair0 + r));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kZBatch; ++u) {
+            const int e = e0 + u * kThreads;
+            if (e < nz) {
+                const int r = e / per_r, rem = e - r * per_r;
+                const int ip = rem / hp, t = rem - ip * hp;
+                pz_store<NX>(inl + (static_cast<size_t>(r) * nip + ip) * NX, t, z[u]);
+            }
+        }
+    }
+    const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
+    const int per_z = nip * nzero;
+    for (int e = threadIdx.x; e < RP * per_z; e += kThreads) {
+        const int l = e / nzero, k = hx + (e - l * nzero);
+        st_pc(inl + static_cast<size_t>(l) * NX + psw(k), pc_zero());
+    }
+    __syncthreads();
+    pdif_range<NX, 0, pp.m, +1>(inl, RP * nip, tw);
+}
+
+// row pass, last part: the untangling of transformed output pairs into I2.  One or two (nl)
+// output pairs of RP row pairs: pair q's line of row pair r at Wq.line + r * Wq.stride, its
+// outputs Wq.oa, Wq.ob (-1: none).  G0[k] = (Z[k] + conj Z[N-k]) / 2 (row y0),
+// G1[k] = -i (Z[k] - conj Z[N-k]) / 2 (row y0 + 1), for kx = k < Hx.
+struct OutLine {
+    const ulonglong2* line;
+    size_t stride;
+    int oa, ob;
+};
+template <int NX>
+__device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const OutLine W0, const OutLine W1, ulonglong2* __restrict__ i2m,
+                                              size_t plane, int pair0) {
+    constexpr int RP = kPairMaxN / NX;
+    const int npy = P.npy, hp = P.hx >> 1;
+    const u64 HALF = f2_splat(0.5f);
+    const int per_q = RP * hp;
+#pragma unroll 2
+    for (int e = threadIdx.x; e < nl * per_q; e += kThreads) {
+        const bool q = e >= per_q;
+        const OutLine W = q ? W1 : W0;
+        const int rem = q ? e - per_q : e;
+        const int r = rem / hp, t = rem - r * hp;
+        const ulonglong2* z = W.line + static_cast<size_t>(r) * W.stride;
+        const int y0 = 2 * (pair0 + r);
+        u64 g0r[2], g0i[2], g1r[2], g1i[2];
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            const int k = 2 * t + w;
+            const PC zk = ld_pc(z + psw(k));
+            const PC zn = ld_pc(z + psw(k == 0 ? 0 : NX - k));
+            g0r[w] = f2_mul(f2_add(zk.re, zn.re), HALF);
+            g0i[w] = f2_mul(f2_sub(zk.im, zn.im), HALF);
+            g1r[w] = f2_mul(f2_add(zk.im, zn.im), HALF);   //  (d.im) / 2, d = Z[k] - conj Z[N-k]
+            g1i[w] = f2_mul(f2_sub(zn.re, zk.re), HALF);   // -(d.re) / 2
+        }
+        ulonglong2* qa = i2m + static_cast<size_t>(W.oa) * plane + static_cast<size_t>(t) * npy + y0;
+        st_stream(qa, make_ulonglong2(f2_pack(f2_lo(g0r[0]), f2_lo(g0r[1])), f2_pack(f2_lo(g0i[0]), f2_lo(g0i[1]))));
+        st_stream(qa + 1, make_ulonglong2(f2_pack(f2_lo(g1r[0]), f2_lo(g1r[1])), f2_pack(f2_lo(g1i[0]), f2_lo(g1i[1]))));
+        if (W.ob >= 0) {
+            ulonglong2* qb = i2m + static_cast<size_t>(W.ob) * plane + static_cast<size_t>(t) * npy + y0;
+            st_stream(qb, make_ulonglong2(f2_pack(f2_hi(g0r[0]), f2_hi(g0r[1])), f2_pack(f2_hi(g0i[0]), f2_hi(g0i[1]))));
+            st_stream(qb + 1, make_ulonglong2(f2_pack(f2_hi(g1r[0]), f2_hi(g1r[1])), f2_pack(f2_hi(g1i[0]), f2_hi(g1i[1]))));
+        }
+    }
+}
+
 template <int NX>
 __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const MemberInfo* __restrict__ members,
                                                       const ulonglong2* __restrict__ i1, ulonglong2* __restrict__ i2,
@@ -581,46 +699,14 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
     const int nip = (P.n_in + 1) >> 1;
     ulonglong2* inl = reinterpret_cast<ulonglong2*>(smem_raw);          // [RP][nip][NX]
     ulonglong2* work = inl + static_cast<size_t>(RP) * nip * NX;        // [RP][NX]
-    const int npy = P.npy, hx = P.hx, hp = hx >> 1, b = blockIdx.y;
+    const int b = blockIdx.y;
     const int pair0 = blockIdx.x * RP;
-    const size_t plane = static_cast<size_t>(P.ntiles) * npy;           // one slot of I1 / I2 (pair elements)
+    const size_t plane = static_cast<size_t>(P.ntiles) * P.npy;         // one slot of I1 / I2 (pair elements)
     const ulonglong2* i1m = i1 + static_cast<size_t>(b) * P.n_in * plane;
     ulonglong2* i2m = i2 + static_cast<size_t>(b) * P.n_out * plane;
 
-    // 1. Z[k] = X0[k] + i X1[k] (rows y0, y0 + 1) with the Hermitian mirror Z[N - k]
-    //    = conj X0[k] + i conj X1[k]; kx = 0 keeps the real parts only
-    {
-        const int per_r = nip * hp, nz = RP * per_r;
-        for (int e0 = threadIdx.x; e0 < nz; e0 += kZBatch * kThreads) {
-            ZItem z[kZBatch];
-#pragma unroll
-            for (int u = 0; u < kZBatch; ++u) {
-                const int e = e0 + u * kThreads;
-                if (e < nz) {
-                    const int r = e / per_r, rem = e - r * per_r;
-                    const int ip = rem / hp, t = rem - ip * hp;
-                    z[u] = pz_load(i1m, plane, npy, P.n_in, ip, t, 2 * (pair0 + r));
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kZBatch; ++u) {
-                const int e = e0 + u * kThreads;
-                if (e < nz) {
-                    const int r = e / per_r, rem = e - r * per_r;
-                    const int ip = rem / hp, t = rem - ip * hp;
-                    pz_store<NX>(inl + (static_cast<size_t>(r) * nip + ip) * NX, t, z[u]);
-                }
-            }
-        }
-        const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
-        const int per_z = nip * nzero;
-        for (int e = threadIdx.x; e < RP * per_z; e += kThreads) {
-            const int l = e / nzero, k = hx + (e - l * nzero);
-            st_pc(inl + static_cast<size_t>(l) * NX + psw(k), pc_zero());
-        }
-    }
-    __syncthreads();
-    pdif_range<NX, 0, pp.m, +1>(inl, RP * nip, tw);
+    // 1. inputs: Z staging and x-inverse
+    prow_inputs<NX>(P, i1m, plane, inl, nip, pair0, tw);
 
     // 2. velocity inputs (compressible: v = j / rho with the zero-density check; otherwise
     //    v = j / rho0 in the products)
@@ -633,9 +719,7 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
 
     // 3. per output pair: products fused into the first DIT stage, the rest of
     //    the forward transform, then the untangling of the two rows (kx < Hx)
-    const u64 HALF = f2_splat(0.5f);
     for (int pi = 0; pi < P.rp_n; ++pi) {
-        const int oa = P.rp_a[pi], ob = P.rp_b[pi];
         const RowProduct R = row_product(P, pi, inv_rho0);
         auto product_canon = [&](int r, int p) -> PC { return row_product_canon<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, psw(p)); };
         auto product = [&](int r, int p) -> PC { return row_product_general<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, psw(p)); };
@@ -644,32 +728,8 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
         else pstage_io<NX, pp.m - 1, -1, true>(RP, tw, product, wio);
         __syncthreads();
         pdit_range<NX, pp.m - 1, 0, -1>(work, RP, tw);
-
-        // G0[k] = (Z[k] + conj Z[N-k]) / 2 (row y0), G1[k] = -i (Z[k] - conj Z[N-k]) / 2 (row y0 + 1)
-        for (int e = threadIdx.x; e < RP * hp; e += kThreads) {
-            const int r = e / hp, t = e - r * hp;
-            const ulonglong2* z = work + static_cast<size_t>(r) * NX;
-            const int y0 = 2 * (pair0 + r);
-            u64 g0r[2], g0i[2], g1r[2], g1i[2];
-#pragma unroll
-            for (int w = 0; w < 2; ++w) {
-                const int k = 2 * t + w;
-                const PC zk = ld_pc(z + psw(k));
-                const PC zn = ld_pc(z + psw(k == 0 ? 0 : NX - k));
-                g0r[w] = f2_mul(f2_add(zk.re, zn.re), HALF);
-                g0i[w] = f2_mul(f2_sub(zk.im, zn.im), HALF);
-                g1r[w] = f2_mul(f2_add(zk.im, zn.im), HALF);   //  (d.im) / 2, d = Z[k] - conj Z[N-k]
-                g1i[w] = f2_mul(f2_sub(zn.re, zk.re), HALF);   // -(d.re) / 2
-            }
-            ulonglong2* qa = i2m + static_cast<size_t>(oa) * plane + static_cast<size_t>(t) * npy + y0;
-            qa[0] = make_ulonglong2(f2_pack(f2_lo(g0r[0]), f2_lo(g0r[1])), f2_pack(f2_lo(g0i[0]), f2_lo(g0i[1])));
-            qa[1] = make_ulonglong2(f2_pack(f2_lo(g1r[0]), f2_lo(g1r[1])), f2_pack(f2_lo(g1i[0]), f2_lo(g1i[1])));
-            if (ob >= 0) {
-                ulonglong2* qb = i2m + static_cast<size_t>(ob) * plane + static_cast<size_t>(t) * npy + y0;
-                qb[0] = make_ulonglong2(f2_pack(f2_hi(g0r[0]), f2_hi(g0r[1])), f2_pack(f2_hi(g0i[0]), f2_hi(g0i[1])));
-                qb[1] = make_ulonglong2(f2_pack(f2_hi(g1r[0]), f2_hi(g1r[1])), f2_pack(f2_hi(g1i[0]), f2_hi(g1i[1])));
-            }
-        }
+        const OutLine W{work, static_cast<size_t>(NX), P.rp_a[pi], P.rp_b[pi]};
+        prow_untangle<NX>(P, 1, W, W, i2m, plane, pair0);
         __syncthreads();
     }
 }
@@ -932,7 +992,7 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
         pdit_range<NY, pp.m - 1, 1, +1>(lines, CP, tw);
         ulonglong2* dst = reinterpret_cast<ulonglong2*>(A.i1_next) + (static_cast<size_t>(b) * P.n_in + slot) * plane + static_cast<size_t>(t0) * NY;
         pstage_io<NY, 0, +1, true>(CP, tw, SmemIO{lines, NY}, [&](int l, int p, PC v) {
-            st_pc(dst + static_cast<size_t>(l) * NY + p, PC{f2_mul(v.re, sc), f2_mul(v.im, sc)});
+            st_stream(dst + static_cast<size_t>(l) * NY + p, make_ulonglong2(f2_mul(v.re, sc), f2_mul(v.im, sc)));
         });
     }
 }

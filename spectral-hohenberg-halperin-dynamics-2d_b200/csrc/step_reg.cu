@@ -4,6 +4,7 @@
 #include <stdexcept>
 #include <string>
 
+#include "step_kernels_dual.cuh"
 #include "step_kernels_reg.cuh"
 #include "step_kernels_split.cuh"
 #include "step_reg.h"
@@ -83,6 +84,50 @@ void launch_split_row(const StepPlan& P, int batch, cudaStream_t stream, const M
         case 768: launch_split<768>(P, batch, stream, members, i1, phys, i2, tw, rho0, err); break;
         case 1536: launch_split<1536>(P, batch, stream, members, i1, phys, i2, tw, rho0, err); break;
         default: throw std::runtime_error("split row pass: unsupported row length " + std::to_string(P.npx));
+    }
+}
+
+bool dual_row_supported(const StepPlan& P) {
+    // compressible canonical layout: (rho, jx), (jy, -) are the last two input pair-lines
+    return is_pair_size(P.npx) && P.rp_canon && P.rp_prep && P.rp_jline == (P.n_in + 1) / 2 - 2;
+}
+
+size_t dual_row_smem_bytes(const StepPlan& P) { return prow2_smem_bytes<kPairMaxN>((P.n_in + 1) / 2); }
+
+namespace {
+template <int NX>
+void launch_dual(const StepPlan& P, int batch, cudaStream_t s, const MemberInfo* members, const void* i1, void* i2, const void* tw, int* err) {
+    constexpr int RP = kPairMaxN / NX;
+    const size_t smem = prow2_smem_bytes<NX>((P.n_in + 1) / 2);
+    {
+        // raised once per device to the largest need (eight order parameters: six input pair-lines)
+        static std::mutex mu;
+        static std::set<int> done;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        std::lock_guard<std::mutex> lock(mu);
+        if (!done.count(dev)) {
+            const cudaError_t rc = cudaFuncSetAttribute(reinterpret_cast<const void*>(prow_pass2<NX>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        static_cast<int>(prow2_smem_bytes<NX>(6)));
+            if (rc != cudaSuccess) throw std::runtime_error(std::string("cudaFuncSetAttribute (two-pair row pass): ") + cudaGetErrorString(rc));
+            done.insert(dev);
+        }
+    }
+    dim3 grid(P.npy / 2 / RP, batch);
+    prow_pass2<NX><<<grid, kThreads, smem, s>>>(P, members, static_cast<const ulonglong2*>(i1), static_cast<ulonglong2*>(i2),
+                                                static_cast<const float2*>(tw), err);
+}
+}  // namespace
+
+void launch_dual_row(const StepPlan& P, int batch, cudaStream_t stream, const MemberInfo* members, const void* i1, void* i2,
+                     const void* tw, int* err) {
+    switch (P.npx) {
+        case 96: launch_dual<96>(P, batch, stream, members, i1, i2, tw, err); break;
+        case 192: launch_dual<192>(P, batch, stream, members, i1, i2, tw, err); break;
+        case 384: launch_dual<384>(P, batch, stream, members, i1, i2, tw, err); break;
+        case 768: launch_dual<768>(P, batch, stream, members, i1, i2, tw, err); break;
+        case 1536: launch_dual<1536>(P, batch, stream, members, i1, i2, tw, err); break;
+        default: throw std::runtime_error("two-pair row pass: unsupported row length " + std::to_string(P.npx));
     }
 }
 

@@ -33,4 +33,11 @@ bool split_row_supported(int nx);
 void launch_split_row(const StepPlan& P, int batch, cudaStream_t stream, const MemberInfo* members, const void* i1, void* phys, void* i2,
                       const void* tw, const double* rho0, int* err);
 
+// row pass over two output pairs at a time (kernel family 4): whether a plan has the input
+// layout it needs, its dynamic shared memory, and its launch
+bool dual_row_supported(const StepPlan& P);
+size_t dual_row_smem_bytes(const StepPlan& P);
+void launch_dual_row(const StepPlan& P, int batch, cudaStream_t stream, const MemberInfo* members, const void* i1, void* i2,
+                     const void* tw, int* err);
+
 }  // namespace shhd

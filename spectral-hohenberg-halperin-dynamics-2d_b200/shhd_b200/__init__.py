@@ -130,7 +130,8 @@ EXPORTED = (
     "shhd_engine_set_family", "shhd_engine_family",
 )
 
-FAMILY_NAMES = {0: "single-line", 1: "pair-line", 2: "pair-line + register row pass", 3: "pair-line + split row pass"}
+FAMILY_NAMES = {0: "single-line", 1: "pair-line", 2: "pair-line + register row pass", 3: "pair-line + split row pass",
+                4: "pair-line + two-pair row pass"}
 
 KERNEL_KINDS = ("col_inverse", "row_pass", "col_forward", "other")
 
@@ -310,14 +311,14 @@ class Engine:
     def autotune(self, trial_steps: int = 3) -> dict:
         """Time the valid kernel families x {direct, graph} on the current state; keep the fastest."""
         fam, chunk = ctypes.c_int(), ctypes.c_int()
-        ms = np.full(8, np.nan)
+        ms = np.full(10, np.nan)
         _check(lib.shhd_engine_autotune(self._h, int(trial_steps), ctypes.byref(fam), ctypes.byref(chunk), _dptr(ms)))
         return {"family": FAMILY_NAMES[fam.value], "graph_chunk": chunk.value,
                 "ms_per_step": [None if np.isnan(x) else float(x) for x in ms]}
 
     def set_family(self, family: int) -> None:
         """Kernel family: -1 default, 0 single-line, 1 pair-line, 2 pair-line with the register row pass,
-        3 pair-line with the split row pass."""
+        3 pair-line with the split row pass, 4 pair-line with the two-pair row pass."""
         _check(lib.shhd_engine_set_family(self._h, int(family)))
 
     @property

@@ -96,12 +96,12 @@ def test_autotune_restores_state_and_keeps_results(precision):
         e.set_state(u0)
         before = e.get_state()
         choice = e.autotune(2)
-        # FP32 at a 96-point compute grid: single-line, pair-line and split row pass, each
-        # direct and through graphs (the register row pass exists for 1536-point rows only)
-        assert choice["family"] in (("pair-line", "single-line", "pair-line + split row pass") if precision == 1
-                                    else ("single-line",))
+        # FP32 at a 96-point compute grid: single-line, pair-line, split and two-pair row passes,
+        # each direct and through graphs (the register row pass exists for 1536-point rows only)
+        fp32_families = ("pair-line", "single-line", "pair-line + split row pass", "pair-line + two-pair row pass")
+        assert choice["family"] in (fp32_families if precision == 1 else ("single-line",))
         timed = [x for x in choice["ms_per_step"] if x is not None]
-        assert len(timed) == (6 if precision == 1 else 2) and all(x > 0 for x in timed)
+        assert len(timed) == (8 if precision == 1 else 2) and all(x > 0 for x in timed)
         assert e.get_info().step_index == 0
         assert np.array_equal(e.get_state(), before)
         e.step(4)
