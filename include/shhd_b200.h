@@ -35,6 +35,7 @@ typedef struct shhd_engine shhd_engine;
 
 #define SHHD_MAX_ORDER_PARAMETERS 8
 #define SHHD_MAX_FORCES 8
+#define SHHD_MAX_FE_PARAMS 4      /* parameters of a free-energy plugin style */
 
 /* error codes */
 #define SHHD_OK 0
@@ -48,7 +49,7 @@ enum shhd_mode { SHHD_COMPRESSIBLE = 0, SHHD_INCOMPRESSIBLE = 1, SHHD_QUIESCENT 
 enum shhd_integrator { SHHD_EULER = 0, SHHD_SRK3 = 1 };
 enum shhd_precision { SHHD_FP64 = 0, SHHD_FP32 = 1 };
 enum shhd_noise_source { SHHD_NOISE_PHILOX = 0, SHHD_NOISE_EXTERNAL = 1 };
-enum shhd_free_energy { SHHD_FE_NONE = 0, SHHD_FE_PHI4 = 1, SHHD_FE_QUADRATIC = 2 };
+enum shhd_free_energy { SHHD_FE_NONE = 0, SHHD_FE_PHI4 = 1, SHHD_FE_QUADRATIC = 2, SHHD_FE_PLUGIN = 3 };
 
 typedef struct shhd_sine_force {
     int target;      /* 0 momentum, 1 order parameter */
@@ -74,7 +75,8 @@ typedef struct shhd_config {
     int mode;                   /* enum shhd_mode   (`time_evolution` */
     int integrator;             /* enum shhd_integrator  .../...) */
     int num_order_parameters;   /* `order_parameters` */
-    /* `model free_energy`: mu_a = (k0 + k2 k^2 + k4 k^4) psi_a (spectral) + u3 psi_a^3 (physical) */
+    /* `model free_energy`: mu_a = (k0 + k2 k^2 + k4 k^4) psi_a (spectral) + u3 psi_a^3 (physical;
+     * a plugin style's mu_a instead, fe_plugin below) */
     int free_energy;            /* enum shhd_free_energy */
     double mu_k0[SHHD_MAX_ORDER_PARAMETERS];
     double mu_k2[SHHD_MAX_ORDER_PARAMETERS];
@@ -101,6 +103,11 @@ typedef struct shhd_config {
     int noise_source;           /* enum shhd_noise_source */
     int batch;                  /* members advanced together (>= 1) */
     int member_offset;          /* first member id for the noise key */
+    /* free_energy == SHHD_FE_PLUGIN: the compiled-in style (1 ... shhd_free_energy_plugin_count(),
+     * include/shhd_b200_free_energy.cuh) and its parameters [parameter][order parameter]; the
+     * linear part is mu_k0, mu_k2 (keys a[], b[]) */
+    int fe_plugin;
+    double fe_param[SHHD_MAX_FE_PARAMS][SHHD_MAX_ORDER_PARAMETERS];
 } shhd_config;
 
 typedef struct shhd_info {
@@ -118,6 +125,16 @@ typedef struct shhd_info {
 
 /* Thread-local message of the last failure. */
 const char* shhd_last_error(void);
+
+/* Free-energy plugin styles compiled into this library (no reference counterpart as a call; it
+ * lists what FreeEnergyRegistry::register_free_energy_style registered,
+ * src/model_free_energy_registry.h:65-85): their number, and the name of style id (1-based;
+ * NULL when out of range).  Host only; needs no GPU. */
+int shhd_free_energy_plugin_count(void);
+const char* shhd_free_energy_plugin_name(int id);
+/* Script key of parameter k of style id ("u[]": one value per order parameter, written u[0],
+ * u[1], ...; "g": one value), or NULL when out of range. */
+const char* shhd_free_energy_plugin_key(int id, int k);
 
 /* Fill *cfg with the reference defaults (src/simulationinfo.h:35-98):
  * grid 128^2, L = 2 pi, no dealiasing, dt 0.005, srk3/compressible, N = 0,

@@ -22,6 +22,11 @@ relative to the reference project):
   * Euler / SRK3 stage updates ...... src/time_integrator_euler_*.h,
                                        src/time_integrator_srk3_*.h
 
+Free-energy plugin styles (``PLUGINS``) are the engine's own compile-time styles
+(its csrc/free_energy_plugins.h); the reference has only the registry seam they
+plug into (src/model_free_energy_registry.h:65-85), so their physical chemical
+potentials and densities are restated here from the engine's definitions.
+
 State layout is the reference's: complex128 array [field, gy, gx] with
 gx in [0, Nx/2] (Nx, Ny = compute grid), field order rho, psi_0..psi_{N-1},
 jx, jy.  Noise can come from (a) the reference's own draws replayed as
@@ -64,6 +69,34 @@ class GradientForce:
     amplitude: float
 
 
+# Free-energy plugin styles: name -> (mu(a, psi, par), density(psi, par), parameter keys); psi the
+# list of order-parameter fields, par {key without "[]": list of values}
+def _coupled_phi4_mu(a, psi, par):
+    others = sum(psi[b] * psi[b] for b in range(len(psi)) if b != a) if len(psi) > 1 else 0.0 * psi[a]
+    return par["u"][a] * psi[a] * psi[a] * psi[a] + par["g"][0] * psi[a] * others
+
+
+def _coupled_phi4_density(psi, par):
+    q = [p * p for p in psi]
+    s2, s4 = sum(q), sum(x * x for x in q)
+    return sum(0.25 * par["u"][b] * q[b] * q[b] for b in range(len(psi))) + 0.25 * par["g"][0] * (s2 * s2 - s4)
+
+
+def _phi6_mu(a, psi, par):
+    q = psi[a] * psi[a]
+    return psi[a] * q * (par["u"][a] + par["w"][a] * q)
+
+
+def _phi6_density(psi, par):
+    return sum((p * p) ** 2 * (0.25 * par["u"][b] + par["w"][b] * (p * p) / 6.0) for b, p in enumerate(psi))
+
+
+PLUGINS = {
+    "coupled_phi4": (_coupled_phi4_mu, _coupled_phi4_density, ("u[]", "g")),
+    "phi6": (_phi6_mu, _phi6_density, ("u[]", "w[]")),
+}
+
+
 @dataclasses.dataclass
 class Config:
     active: Tuple[int, int] = (128, 128)
@@ -74,7 +107,8 @@ class Config:
     time_evolution: str = "srk3/compressible"
     cT: float = 0.0
     has_thermo: bool = False
-    free_energy: str = "none"  # none | phi4 | quadratic
+    free_energy: str = "none"  # none | phi4 | quadratic | a PLUGINS name
+    plugin_par: dict = dataclasses.field(default_factory=dict)
     phi4_a: List[float] = dataclasses.field(default_factory=list)
     phi4_b: List[float] = dataclasses.field(default_factory=list)
     phi4_u: List[float] = dataclasses.field(default_factory=list)
@@ -115,17 +149,29 @@ class Config:
         return self.num_order_parameters + 3
 
     def mu_k0(self, a: int) -> float:
-        if self.free_energy == "phi4":
+        if self.free_energy == "phi4" or self.free_energy in PLUGINS:
             return self.phi4_a[a]
         if self.free_energy == "quadratic":
             return self.quad_a[a]
         return 0.0
 
     def mu_k2(self, a: int) -> float:
-        return self.phi4_b[a] if self.free_energy == "phi4" else 0.0
+        return self.phi4_b[a] if (self.free_energy == "phi4" or self.free_energy in PLUGINS) else 0.0
 
     def has_physical_mu(self) -> bool:
-        return self.free_energy == "phi4" and any(u != 0.0 for u in self.phi4_u)
+        return self.free_energy in PLUGINS or (self.free_energy == "phi4" and any(u != 0.0 for u in self.phi4_u))
+
+    def physical_mu(self, a: int, psi) -> np.ndarray:
+        """Physical chemical potential of order parameter a from the physical fields psi."""
+        if self.free_energy in PLUGINS:
+            return PLUGINS[self.free_energy][0](a, psi, self.plugin_par)
+        return self.phi4_u[a] * psi[a] * psi[a] * psi[a]
+
+    def physical_density(self, psi) -> np.ndarray:
+        """Free-energy density of the physical part."""
+        if self.free_energy in PLUGINS:
+            return PLUGINS[self.free_energy][1](psi, self.plugin_par)
+        return sum(0.25 * self.phi4_u[a] * p ** 4 for a, p in enumerate(psi))
 
 
 def parse_script(text: str) -> Config:
@@ -169,6 +215,17 @@ def parse_script(text: str) -> Config:
                 c.phi4_b = [0.0] * n_op
                 c.phi4_u = [0.0] * n_op
                 c.quad_a = [0.0] * n_op
+                if c.free_energy in PLUGINS:
+                    c.plugin_par = {key.rstrip("[]"): [0.0] * max(n_op, 1) for key in PLUGINS[c.free_energy][2]}
+                    for k, v in kv:
+                        m = re.fullmatch(r"(\w+)\[(\d+)\]", k)
+                        if m and m.group(1) in ("a", "b"):
+                            (c.phi4_a if m.group(1) == "a" else c.phi4_b)[int(m.group(2))] = float(v)
+                        elif m:
+                            c.plugin_par[m.group(1)][int(m.group(2))] = float(v)
+                        else:
+                            c.plugin_par[k][0] = float(v)
+                    continue
                 for k, v in kv:
                     m = re.fullmatch(r"([abu])\[(\d+)\]", k)
                     if m:
@@ -428,8 +485,7 @@ class Oracle:
                 p = need_phys()
                 has_mu = M != 0.0 and cfg.has_physical_mu()
                 if has_mu:
-                    psi = p["psi"]
-                    mu = cfg.phi4_u[a] * psi[a] * psi[a] * psi[a]
+                    mu = cfg.physical_mu(a, p["psi"])
                     mu_hat = g.forward(mu)
                     jxf = -1j * (M * kx) * mu_hat
                     jyf = -1j * (M * ky) * mu_hat
@@ -774,7 +830,7 @@ class Oracle:
         for a in range(n):
             out[f"Jpsi[{a}]_x"], out[f"Jpsi[{a}]_y"] = zero(), zero()
         p = self.physical_fields(state)
-        has_phys = cfg.free_energy == "phi4" and any(u != 0.0 for u in cfg.phi4_u)
+        has_phys = cfg.has_physical_mu()
         for a in range(n):
             M = cfg.mobility[a]
             adv = cfg.order_parameter_advection
@@ -788,7 +844,7 @@ class Oracle:
                 fy += np.where(act, -1j * (M * ky) * mu, 0.0)
             if adv or has_phys:
                 if M != 0.0 and has_phys:
-                    mu_p = g.forward(cfg.phi4_u[a] * p["psi"][a] ** 3)
+                    mu_p = g.forward(cfg.physical_mu(a, p["psi"]))
                     fx += np.where(act, -1j * (M * kx) * mu_p, 0.0)
                     fy += np.where(act, -1j * (M * ky) * mu_p, 0.0)
                 if adv:
@@ -1013,7 +1069,7 @@ def time_series_energies(cfg: Config, state: np.ndarray) -> Dict[str, float]:
         comp = 0.5 * cfg.cT * cfg.cT * cell / (g.grid_size * rho0) * float(np.sum(np.where(use, w * np.abs(state[0]) ** 2, 0.0)))
     free = 0.0
     for a in range(n):
-        if cfg.free_energy == "phi4":
+        if cfg.free_energy == "phi4" or cfg.free_energy in PLUGINS:
             k0, k2c, k4 = cfg.phi4_a[a], cfg.phi4_b[a], 0.0
         elif cfg.free_energy == "quadratic":
             k0, k2c, k4 = cfg.quad_a[a], 0.0, 0.0
@@ -1023,7 +1079,9 @@ def time_series_energies(cfg: Config, state: np.ndarray) -> Dict[str, float]:
             continue
         coef = k0 + k2c * g.k2 + k4 * g.k2 * g.k2
         free += 0.5 * cell / g.grid_size * float(np.sum(np.where(act, w * coef * np.abs(state[1 + a]) ** 2, 0.0)))
-    if cfg.free_energy == "phi4" and any(u != 0.0 for u in cfg.phi4_u):
+    if cfg.free_energy in PLUGINS and n > 0:
+        free += float(np.sum(cfg.physical_density([g.backward(state[1 + a]) for a in range(n)]) * cell))
+    elif cfg.free_energy == "phi4" and any(u != 0.0 for u in cfg.phi4_u):
         dens = np.zeros((g.ny, g.nx))
         for a in range(n):
             p = g.backward(state[1 + a])

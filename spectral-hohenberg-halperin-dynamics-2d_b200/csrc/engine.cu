@@ -386,6 +386,8 @@ void validate_config(const shhd_config& c) {
         if (c.mobility[a] < 0) throw Failure(SHHD_EINVAL, "transport coefficient requires nonnegative order parameter mobility.");
         if (c.mu_u3[a] < 0) throw Failure(SHHD_EINVAL, "phi4 free energy requires nonnegative u coefficient.");
     }
+    if (c.free_energy == SHHD_FE_PLUGIN && (c.fe_plugin < 1 || c.fe_plugin > plugin_count()))
+        throw Failure(SHHD_EINVAL, "free-energy plugin style " + std::to_string(c.fe_plugin) + " is not compiled into this library");
     if (c.batch < 1) throw Failure(SHHD_EINVAL, "batch must be >= 1");
     if (c.precision != SHHD_FP64 && c.precision != SHHD_FP32) throw Failure(SHHD_EINVAL, "unknown precision");
     if (c.n_sine_forces < 0 || c.n_sine_forces > SHHD_MAX_FORCES || c.n_gradient_forces < 0 || c.n_gradient_forces > SHHD_MAX_FORCES)
@@ -452,7 +454,9 @@ void plan_row_pairs(StepPlan& P) {
     // canonical input roles after the x-inverse
     const int s_rho = P.in_slot[0], s_jx = P.in_slot[P.nop + 1], s_jy = P.in_slot[P.nop + 2];
     P.rp_canon = 0; P.rp_prep = 0; P.rp_jline = -1; P.rp_vline = -1;
-    if (!P.need_v) {
+    if (P.fe_plugin) {
+        // plugin styles: mu from every order parameter, per row (row_product_general)
+    } else if (!P.need_v) {
         P.rp_canon = 1;
     } else if (P.mode == SHHD_COMPRESSIBLE) {
         if (s_rho >= 0 && s_rho % 2 == 0 && s_jx == s_rho + 1 && s_jy == s_rho + 2 && P.n_in == s_rho + 3) {
@@ -497,10 +501,17 @@ void build_plan(shhd_engine* e) {
     const int f_jx = nop + 1, f_jy = nop + 2;
 
     // ---- physics flags ----
-    const bool has_phys_mu = c.free_energy == SHHD_FE_PHI4 && [&] {
+    const bool plugin = c.free_energy == SHHD_FE_PLUGIN;
+    const bool has_phys_mu = plugin || (c.free_energy == SHHD_FE_PHI4 && [&] {
         for (int a = 0; a < nop; ++a) if (c.mu_u3[a] != 0.0) return true;
         return false;
-    }();
+    }());
+    P.fe_plugin = plugin ? c.fe_plugin : 0;
+    for (int k = 0; k < SHHD_MAX_FE_PARAMS; ++k)
+        for (int a = 0; a < kMaxOp; ++a) {
+            P.fe_param[k][a] = plugin ? c.fe_param[k][a] : 0.0;
+            P.fe_paramf[k][a] = static_cast<float>(P.fe_param[k][a]);
+        }
     const bool has_visc = c.eta != 0.0 || c.zeta != 0.0;
     P.cT2 = c.cT * c.cT; P.eta = c.eta; P.zeta = c.zeta;
     P.j_zero = quiet || !(P.cT2 != 0.0 || has_visc || c.momentum_advection);
@@ -563,7 +574,12 @@ void build_plan(shhd_engine* e) {
         P.group_kind[g] = GROUP_PSI;
         P.group_alpha[g] = a;
         if (P.psi_zero[a]) continue;
-        if (c.mobility[a] != 0.0 && has_phys_mu && P.mu_u3[a] != 0.0) { add_group_out(g, add_out(OUT_MU, a)); need[1 + a] = true; }
+        if (c.mobility[a] != 0.0 && has_phys_mu && (plugin || P.mu_u3[a] != 0.0)) {
+            add_group_out(g, add_out(OUT_MU, a));
+            need[1 + a] = true;
+            if (plugin)  // a plugin's mu_a may read every order parameter
+                for (int b = 0; b < nop; ++b) need[1 + b] = true;
+        }
         if (c.order_parameter_advection) {
             add_group_out(g, add_out(OUT_PSIVX, a));
             add_group_out(g, add_out(OUT_PSIVY, a));
@@ -1382,6 +1398,18 @@ extern "C" {
 
 const char* shhd_last_error(void) { return g_last_error.c_str(); }
 
+int shhd_free_energy_plugin_count(void) { return plugin_count(); }
+
+const char* shhd_free_energy_plugin_name(int id) {
+    PluginInfo info{};
+    return plugin_info(id, &info) ? info.name : nullptr;
+}
+
+const char* shhd_free_energy_plugin_key(int id, int k) {
+    PluginInfo info{};
+    return plugin_info(id, &info) && k >= 0 && k < info.n_params ? info.keys[k] : nullptr;
+}
+
 int shhd_engine_create(const shhd_config* cfg, shhd_engine** out) {
     if (!cfg || !out) {
         g_last_error = "null argument";
@@ -1942,9 +1970,11 @@ void build_measure_plan(shhd_engine* e) {
     P.div_kyp = make_fastdiv(P.kyp);
     P.div_npy = make_fastdiv(c.ny);
     P.div_hx = make_fastdiv(P.hx);
-    // row pass: at most 3 input lines and row_lb ping-pong lines
+    // row pass: at most 3 input lines (every order parameter for a plugin style's density) and
+    // row_lb ping-pong lines
+    const int nin = std::max(3, c.free_energy == SHHD_FE_PLUGIN ? c.num_order_parameters : 0);
     const size_t line = static_cast<size_t>(c.nx) * cs;
-    auto row_bytes = [&](int lb) { return static_cast<size_t>(P.twx_count) * cs + (3 + lb) * line; };
+    auto row_bytes = [&](int lb) { return static_cast<size_t>(P.twx_count) * cs + (nin + lb) * line; };
     int lb = 3;
     while (lb > 1 && row_bytes(lb) > 113 * 1024) --lb;
     if (row_bytes(lb) > smem_cap) throw Failure(SHHD_EUNSUPPORTED, "energy measure: compute grid too large for the row transform");
@@ -1958,7 +1988,7 @@ void build_measure_plan(shhd_engine* e) {
     M.tw_y = dalloc(e, twy.size() * cs);
     check_cuda(cudaMemcpyAsync(M.tw_x, twx.data(), twx.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
     check_cuda(cudaMemcpyAsync(M.tw_y, twy.data(), twy.size() * cs, cudaMemcpyHostToDevice, e->stream), "twiddle upload");
-    M.i1 = dalloc(e, 3 * static_cast<size_t>(P.hx) * c.ny * cs);
+    M.i1 = dalloc(e, static_cast<size_t>(nin) * P.hx * c.ny * cs);
     MemberInfo mi{};
     mi.active = 1;
     M.member = dalloc(e, sizeof(MemberInfo));
@@ -1983,6 +2013,9 @@ double physical_energy_sum(shhd_engine* e, const cplx<T>* st, int term, int fiel
         P.in_field[0] = 0;
         P.in_field[1] = P.nop + 1;
         P.in_field[2] = P.nop + 2;
+    } else if (term == 2) {  // a plugin style's density: every order parameter
+        P.n_in = P.nop;
+        for (int a = 0; a < P.nop; ++a) P.in_field[a] = 1 + a;
     } else {
         P.n_in = 1;
         P.in_field[0] = field;
@@ -2092,6 +2125,7 @@ void energies(shhd_engine* e, int member, double* out) {
         if (P.mu_k0[a] != 0.0 || P.mu_k2[a] != 0.0 || P.mu_k4[a] != 0.0) free_e += 0.5 * cell / ng * v[2 + a];
     for (int a = 0; a < nop; ++a)
         if (P.mu_u3[a] != 0.0) free_e += 0.25 * P.mu_u3[a] * physical_energy_sum<T>(e, st, 1, 1 + a) * cell;
+    if (P.fe_plugin && nop > 0) free_e += physical_energy_sum<T>(e, st, 2, 0) * cell;
     out[0] = kin + free_e + compress;
     out[1] = kin;
     out[2] = free_e;

@@ -122,11 +122,18 @@ void parse_model(ParseState& s, const Tokens& t) {
         if (action == "coeff") {
             if (!s.has_free_energy) throw std::runtime_error("model free_energy coeff requires model free_energy <type> first");
         } else {
-            if (action != "phi4" && action != "quadratic") throw std::runtime_error("Unknown free energy type: " + action);
+            // the reference's styles, then the plugin styles compiled into the library
+            int plugin = 0;
+            for (int id = 1; id <= shhd_free_energy_plugin_count(); ++id)
+                if (action == shhd_free_energy_plugin_name(id)) plugin = id;
+            if (action != "phi4" && action != "quadratic" && plugin == 0) throw std::runtime_error("Unknown free energy type: " + action);
             s.has_free_energy = true;
             s.free_energy_type = action;
-            c.free_energy = action == "phi4" ? SHHD_FE_PHI4 : SHHD_FE_QUADRATIC;
+            c.free_energy = action == "phi4" ? SHHD_FE_PHI4 : (action == "quadratic" ? SHHD_FE_QUADRATIC : SHHD_FE_PLUGIN);
+            c.fe_plugin = plugin;
             for (int a = 0; a < SHHD_MAX_ORDER_PARAMETERS; ++a) c.mu_k0[a] = c.mu_k2[a] = c.mu_k4[a] = c.mu_u3[a] = 0.0;
+            for (int k = 0; k < SHHD_MAX_FE_PARAMS; ++k)
+                for (int a = 0; a < SHHD_MAX_ORDER_PARAMETERS; ++a) c.fe_param[k][a] = 0.0;
         }
         for (const auto& p : kv) {
             int idx = -1;
@@ -144,12 +151,37 @@ void parse_model(ParseState& s, const Tokens& t) {
                 }
                 throw std::runtime_error("unknown phi4 free energy coefficient: " + p.first);
             }
-            if (indexed_key(p.first, "a", idx)) {
-                if (idx < 0 || idx >= nop) throw std::runtime_error("model free_energy quadratic coefficient index out of range: " + p.first);
-                c.mu_k0[idx] = v;
+            if (s.free_energy_type == "quadratic") {
+                if (indexed_key(p.first, "a", idx)) {
+                    if (idx < 0 || idx >= nop) throw std::runtime_error("model free_energy quadratic coefficient index out of range: " + p.first);
+                    c.mu_k0[idx] = v;
+                    continue;
+                }
+                throw std::runtime_error("unknown quadratic free energy coefficient: " + p.first);
+            }
+            // plugin style: linear a[], b[] as phi4, then the style's own keys
+            const std::string& st = s.free_energy_type;
+            if (indexed_key(p.first, "a", idx) || indexed_key(p.first, "b", idx)) {
+                if (idx < 0 || idx >= nop) throw std::runtime_error("model free_energy " + st + " coefficient index out of range: " + p.first);
+                (p.first[0] == 'a' ? c.mu_k0 : c.mu_k2)[idx] = v;
                 continue;
             }
-            throw std::runtime_error("unknown quadratic free energy coefficient: " + p.first);
+            bool known = false;
+            for (int k = 0; !known; ++k) {
+                const char* key = shhd_free_energy_plugin_key(c.fe_plugin, k);
+                if (!key) break;
+                const std::string ks(key);
+                if (ks.size() > 2 && ks.compare(ks.size() - 2, 2, "[]") == 0) {
+                    if (!indexed_key(p.first, ks.substr(0, ks.size() - 2), idx)) continue;
+                    if (idx < 0 || idx >= nop) throw std::runtime_error("model free_energy " + st + " coefficient index out of range: " + p.first);
+                    c.fe_param[k][idx] = v;
+                } else {
+                    if (p.first != ks) continue;
+                    c.fe_param[k][0] = v;
+                }
+                known = true;
+            }
+            if (!known) throw std::runtime_error("unknown " + st + " free energy coefficient: " + p.first);
         }
         return;
     }

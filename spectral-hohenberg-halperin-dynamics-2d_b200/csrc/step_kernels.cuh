@@ -22,6 +22,7 @@
 #include <stdint.h>
 
 #include "fft_core.cuh"
+#include "free_energy_plugins.h"
 #include "philox.cuh"
 
 namespace shhd {
@@ -75,6 +76,9 @@ struct StepPlan {
     int group_out[kMaxGroups][kMaxGroupOut];
     // physics
     double mobility[kMaxOp], mu_k0[kMaxOp], mu_k2[kMaxOp], mu_k4[kMaxOp], mu_u3[kMaxOp];
+    int fe_plugin;                 // free-energy plugin style (0: none; its mu replaces u3 psi^3)
+    double fe_param[SHHD_MAX_FE_PARAMS][kMaxOp];
+    float fe_paramf[SHHD_MAX_FE_PARAMS][kMaxOp];
     int psi_zero[kMaxOp];          // psi_det early return (fcalculator.cc:93-95)
     int psi_linear[kMaxOp];        // linear mu term present (fcalculator.cc:158-160)
     double grad_ax[kMaxOp], grad_ay[kMaxOp];  // summed -A per direction (gradient forces)
@@ -190,6 +194,61 @@ __global__ void __launch_bounds__(kThreads) col_inverse_kernel(const StepPlan P,
         const int w = e - y * W;
         dst[e] = cscale(buf[sw(y, mask) * W + w], sc);
     }
+}
+
+// ---------------------------------------------------------------------------
+// free-energy plugin styles (free_energy_plugins.h): the physical chemical potential and the
+// free-energy density at one point, from the plan's style and parameters
+// ---------------------------------------------------------------------------
+template <typename T>
+struct PluginParams {
+    const StepPlan& P;
+    __device__ __forceinline__ T operator()(int k, int b) const {
+        if constexpr (sizeof(T) == sizeof(float)) return P.fe_paramf[k][b];
+        else return P.fe_param[k][b];
+    }
+};
+template <typename T>
+__device__ __forceinline__ T plugin_mu(const StepPlan& P, int a, T psi_a, const T* psi) {
+    const PluginParams<T> par{P};
+    switch (P.fe_plugin) {
+#define SHHD_MU(ID, S) \
+    case ID: return S::template mu<T>(a, psi_a, psi, P.nop, par);
+        SHHD_FREE_ENERGY_PLUGINS(SHHD_MU)
+#undef SHHD_MU
+        default: return T(0);
+    }
+}
+template <typename T>
+__device__ __forceinline__ T plugin_density(const StepPlan& P, const T* psi) {
+    const PluginParams<T> par{P};
+    switch (P.fe_plugin) {
+#define SHHD_DENSITY(ID, S) \
+    case ID: return S::template density<T>(psi, P.nop, par);
+        SHHD_FREE_ENERGY_PLUGINS(SHHD_DENSITY)
+#undef SHHD_DENSITY
+        default: return T(0);
+    }
+}
+// plugin mu_a of both rows of a row pair at one position: get(slot) returns the position's
+// (row y0, row y0 + 1) values of an input slot; every order parameter is an input
+template <typename T, typename Get>
+__device__ __forceinline__ void plugin_mu_rows(const StepPlan& P, int a, Get&& get, T& mu0, T& mu1) {
+    T p0[kMaxOp], p1[kMaxOp];
+    T a0 = T(0), a1 = T(0);
+#pragma unroll
+    for (int b = 0; b < kMaxOp; ++b) {
+        p0[b] = T(0);
+        p1[b] = T(0);
+        if (b < P.nop) {
+            const auto v = get(P.in_slot[1 + b]);
+            p0[b] = v.x;
+            p1[b] = v.y;
+            if (b == a) { a0 = v.x; a1 = v.y; }
+        }
+    }
+    mu0 = plugin_mu<T>(P, a, a0, p0);
+    mu1 = plugin_mu<T>(P, a, a1, p1);
 }
 
 // ---------------------------------------------------------------------------
@@ -313,6 +372,8 @@ __global__ void __launch_bounds__(kThreads) row_pass_kernel(const StepPlan P, co
                 }
                 C val = mk(product_value<T>(P, kind, arg, psi.x, jx.x, jy.x, vx.x, vy.x),
                            product_value<T>(P, kind, arg, psi.y, jx.y, jy.y, vx.y, vy.y));
+                if (kind == OUT_MU && P.fe_plugin)
+                    plugin_mu_rows<T>(P, arg, [&](int s) { return lines[static_cast<size_t>(s) * npx + x]; }, val.x, val.y);
                 if (!has1) val.y = T(0);  // odd row count: the last pair holds one row
                 dst[x] = val;
             }
@@ -1448,11 +1509,25 @@ __global__ void __launch_bounds__(kThreads) energy_row_kernel(const StepPlan P, 
             const C rho = lines[x], jx = lines[npx + x], jy = lines[2 * npx + x];
             acc += 0.5 * (static_cast<double>(jx.x) * jx.x + static_cast<double>(jy.x) * jy.x) / static_cast<double>(rho.x);
             if (has1) acc += 0.5 * (static_cast<double>(jx.y) * jx.y + static_cast<double>(jy.y) * jy.y) / static_cast<double>(rho.y);
-        } else {
+        } else if (term == 1) {
             const C p = lines[x];
             const double a = static_cast<double>(p.x) * p.x, b = static_cast<double>(p.y) * p.y;
             acc += a * a;
             if (has1) acc += b * b;
+        } else {  // plugin free-energy density; lines hold the order parameters in order
+            double p0[kMaxOp], p1[kMaxOp];
+#pragma unroll
+            for (int b = 0; b < kMaxOp; ++b) {
+                p0[b] = 0.0;
+                p1[b] = 0.0;
+                if (b < P.n_in) {
+                    const C v = lines[static_cast<size_t>(b) * npx + x];
+                    p0[b] = v.x;
+                    p1[b] = v.y;
+                }
+            }
+            acc += plugin_density<double>(P, p0);
+            if (has1) acc += plugin_density<double>(P, p1);
         }
     }
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);

@@ -325,6 +325,8 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
             }
             C val = mk(product_value<T>(P, kind, arg, psi.x, jx.x, jy.x, vx.x, vy.x),
                        product_value<T>(P, kind, arg, psi.y, jx.y, jy.y, vx.y, vy.y));
+            if (kind == OUT_MU && P.fe_plugin)
+                plugin_mu_rows<T>(P, arg, [&](int s) { return lines[static_cast<size_t>(s) * NX + x]; }, val.x, val.y);
             if (!has1) val.y = T(0);
             z[x] = val;
         }

@@ -511,12 +511,17 @@ __device__ __forceinline__ PC row_product_general(const StepPlan& P, const RowPr
     }
     const float2 pa = R.psa >= 0 ? pin(in, NX, R.psa, sp) : make_float2(0.f, 0.f);
     const float2 pb = R.psb >= 0 ? pin(in, NX, R.psb, sp) : make_float2(0.f, 0.f);
-    const float a0 = product_value<float>(P, R.ka, R.aa, pa.x, jx.x, jy.x, vx.x, vy.x);
-    const float a1 = product_value<float>(P, R.ka, R.aa, pa.y, jx.y, jy.y, vx.y, vy.y);
+    float a0 = product_value<float>(P, R.ka, R.aa, pa.x, jx.x, jy.x, vx.x, vy.x);
+    float a1 = product_value<float>(P, R.ka, R.aa, pa.y, jx.y, jy.y, vx.y, vy.y);
     float b0 = 0.f, b1 = 0.f;
     if (R.kb >= 0) {
         b0 = product_value<float>(P, R.kb, R.ab, pb.x, jx.x, jy.x, vx.x, vy.x);
         b1 = product_value<float>(P, R.kb, R.ab, pb.y, jx.y, jy.y, vx.y, vy.y);
+    }
+    if (P.fe_plugin) {  // plugin styles: mu from every order parameter at the position
+        auto get = [&](int s) { return pin(in, NX, s, sp); };
+        if (R.ka == OUT_MU) plugin_mu_rows<float>(P, R.aa, get, a0, a1);
+        if (R.kb == OUT_MU) plugin_mu_rows<float>(P, R.ab, get, b0, b1);
     }
     return PC{f2_pack(a0, b0), f2_pack(a1, b1)};
 }

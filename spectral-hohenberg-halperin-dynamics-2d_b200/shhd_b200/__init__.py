@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libshhd_b200.so")
 
 MAX_OP = 8
 MAX_FORCES = 8
+MAX_FE_PARAMS = 4
 
 SHHD_OK = 0
 SHHD_EINVAL = -1
@@ -71,6 +72,7 @@ class Config(ctypes.Structure):
         ("n_gradient_forces", ctypes.c_int), ("gradient_forces", GradientForce * MAX_FORCES),
         ("precision", ctypes.c_int), ("noise_source", ctypes.c_int),
         ("batch", ctypes.c_int), ("member_offset", ctypes.c_int),
+        ("fe_plugin", ctypes.c_int), ("fe_param", (ctypes.c_double * MAX_OP) * MAX_FE_PARAMS),
     ]
 
     def copy(self) -> "Config":
@@ -128,6 +130,7 @@ EXPORTED = (
     "shhd_engine_flux0_enable", "shhd_engine_flux0_read", "shhd_engine_profile_line", "shhd_engine_profile_velocity",
     "shhd_engine_flux_line_enable", "shhd_engine_flux_line_read", "shhd_engine_flux_tap_schedule",
     "shhd_engine_set_family", "shhd_engine_family",
+    "shhd_free_energy_plugin_count", "shhd_free_energy_plugin_name", "shhd_free_energy_plugin_key",
 )
 
 FAMILY_NAMES = {0: "single-line", 1: "pair-line", 2: "pair-line + register row pass", 3: "pair-line + split row pass",
@@ -171,6 +174,11 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_autotune.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), dp]
     lib.shhd_engine_set_family.argtypes = [vp, i]
     lib.shhd_engine_family.argtypes = [vp]
+    lib.shhd_free_energy_plugin_count.argtypes = []
+    lib.shhd_free_energy_plugin_name.argtypes = [i]
+    lib.shhd_free_energy_plugin_name.restype = ctypes.c_char_p
+    lib.shhd_free_energy_plugin_key.argtypes = [i, i]
+    lib.shhd_free_energy_plugin_key.restype = ctypes.c_char_p
     lib.shhd_engine_gk_enable.argtypes = [vp, i, i, i]
     lib.shhd_engine_gk_read.argtypes = [vp, i, dp, sz, ctypes.POINTER(ctypes.c_int64), i]
     lib.shhd_engine_l2_sums.argtypes = [vp, i, dp, sz]
@@ -201,6 +209,18 @@ def default_config() -> Config:
     c = Config()
     _check(lib.shhd_config_default(ctypes.byref(c)))
     return c
+
+
+def free_energy_plugins() -> dict:
+    """The free-energy plugin styles compiled into the library: {name: (id, [parameter keys])}."""
+    out = {}
+    for sid in range(1, lib.shhd_free_energy_plugin_count() + 1):
+        keys, k = [], 0
+        while (key := lib.shhd_free_energy_plugin_key(sid, k)) is not None:
+            keys.append(key.decode())
+            k += 1
+        out[lib.shhd_free_energy_plugin_name(sid).decode()] = (sid, keys)
+    return out
 
 
 def config_from_script(text: str) -> Config:
