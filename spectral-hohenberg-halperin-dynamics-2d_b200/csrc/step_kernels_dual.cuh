@@ -2,18 +2,16 @@
 // dynamics with the canonical (rho, jx), (jy, -) input pair-lines.
 //
 // prow_pass transforms one output pair at a time through one work line: every pair is a chain
-// of barriers (products with the first stage, the remaining stages, the untangling), its
-// radix-8 stages run by 192 of the 256 threads, each thread reading the pair's inputs and
-// forming its twiddle powers alone.  prow_pass2 keeps 1 / rho in an 8-byte slot per position
-// instead of (vx, vy) in a full line, which frees the (jy, -) line after the velocity
-// preparation as a second work line.  Each thread then
-//   - reads a position's inputs once and evaluates the products of two output pairs from them,
-//   - runs the same butterfly of both lines with one set of twiddle powers,
-//   - untangles both lines in one pass,
-// so the forward transforms take half as many barrier chains.  Each output's arithmetic is
-// prow_pass's, operation for operation (v = j * (1 / rho), one rounding either way).
+// of barriers (products with the first stage, the remaining stages, the untangling) whose
+// radix-8 stages keep 192 of its 256 threads busy, at 16 warps per SM (two blocks).
+// prow_pass2 keeps 1 / rho in an 8-byte slot per position instead of (vx, vy) in a full line,
+// which frees the (jy, -) line after the velocity preparation as a second work line, and runs
+// 384 threads (two blocks per SM: 24 warps): the two output pairs of a round are the two lines
+// of one stage, 2 x 192 radix-8 butterflies, one per thread, so the forward transforms take
+// half as many barrier chains with every thread busy in their radix-8 stages.  Each output's
+// arithmetic is prow_pass's, operation for operation (v = j * (1 / rho), one rounding either way).
 // Shared memory per row pair: nip input pair-lines, one more work line and NX 1 / rho slots
-// (110.6 KB at 1536 points with three input pair-lines: two blocks per SM).
+// (110.6 KB at 1536 points with three input pair-lines); registers at most 85 per thread.
 #pragma once
 
 #include "step_kernels_pair.cuh"
@@ -25,62 +23,28 @@ constexpr size_t prow2_smem_bytes(int nip) {
     return static_cast<size_t>(kPairMaxN / NX) * NX * ((nip + 1) * sizeof(ulonglong2) + sizeof(u64));
 }
 
-// one stage of two lines (line l of A at a + l * as, of B at b + l * bs): the same butterfly
-// of both, with one set of twiddle powers
-template <int N, int S, int DIR, bool DIT, typename TW>
-__device__ __forceinline__ void pstage2(int nl, ulonglong2* a, size_t as, ulonglong2* b, size_t bs, TW tw) {
-    constexpr PPlan pp = PairPlan<N>::c;
-    constexpr int R = pp.r[S], ST = pp.s[S], L = R * ST, NB = N / R;
-#pragma unroll 1
-    for (int bi = threadIdx.x; bi < nl * NB; bi += kThreads) {
-        const int l = bi / NB, i = bi - l * NB;
-        const int j = i & (ST - 1);
-        const int base = (i >> pp.lg[S]) * L + j;
-        ulonglong2* la = a + l * as;
-        ulonglong2* lb = b + l * bs;
-        PC va[R], vb[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            va[q] = ld_pc(la + psw(base + q * ST));
-            vb[q] = ld_pc(lb + psw(base + q * ST));
-        }
-        float2 w[8];
-        if constexpr (L > R) ptwiddle_powers<R>(tw_at(tw, pp.twoff[S] + j), w);
-        if constexpr (DIT && L > R) {
-            ptwiddle_apply<R, DIR>(va, w);
-            ptwiddle_apply<R, DIR>(vb, w);
-        }
-        pbfly<R, DIR>(va);
-        pbfly<R, DIR>(vb);
-        if constexpr (!DIT && L > R) {
-            ptwiddle_apply<R, DIR>(va, w);
-            ptwiddle_apply<R, DIR>(vb, w);
-        }
-#pragma unroll
-        for (int q = 0; q < R; ++q) {
-            st_pc(la + psw(base + q * ST), va[q]);
-            st_pc(lb + psw(base + q * ST), vb[q]);
-        }
-    }
-}
-// DIT stages S - 1 down to E of two lines, a barrier after each
-template <int N, int S, int E, int DIR, typename TW>
-__device__ __forceinline__ void pdit2_range(int nl, ulonglong2* a, size_t as, ulonglong2* b, size_t bs, TW tw) {
-    if constexpr (S > E) {
-        pstage2<N, S - 1, DIR, true>(nl, a, as, b, bs, tw);
-        __syncthreads();
-        pdit2_range<N, S - 1, E, DIR>(nl, a, as, b, bs, tw);
-    }
-}
+// block size of the two-pair row pass
+constexpr int kDualThreads = 384;
+
+// the two work lines of a round as lines l = 2 r + q of one stage: output pair q of row pair r
+struct DualIO {
+    ulonglong2* a;
+    size_t as;
+    ulonglong2* b;
+    size_t bs;
+    __device__ __forceinline__ ulonglong2* line(int l) const { return (l & 1) ? b + (l >> 1) * bs : a + (l >> 1) * as; }
+    __device__ __forceinline__ PC operator()(int l, int p) const { return ld_pc(line(l) + psw(p)); }
+    __device__ __forceinline__ void operator()(int l, int p, PC v) const { st_pc(line(l) + psw(p), v); }
+};
 
 template <int NX>
-__global__ void __launch_bounds__(kThreads, 2) prow_pass2(const StepPlan P, const MemberInfo* __restrict__ members,
-                                                       const ulonglong2* __restrict__ i1, ulonglong2* __restrict__ i2,
-                                                       const float2* __restrict__ tw, int* __restrict__ err) {
+__global__ void __launch_bounds__(kDualThreads, 2) prow_pass2(const StepPlan P, const MemberInfo* __restrict__ members,
+                                                           const ulonglong2* __restrict__ i1, ulonglong2* __restrict__ i2,
+                                                           const float2* __restrict__ tw, int* __restrict__ err) {
     if (!members[blockIdx.y].active) return;
+    constexpr int NT = kDualThreads;
     constexpr int RP = kPairMaxN / NX;
     constexpr PPlan pp = PairPlan<NX>::c;
-    constexpr int RL = pp.r[pp.m - 1], NBL = NX / RL;  // first forward stage: radix, butterflies (stride 1, no twiddles)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nip = (P.n_in + 1) >> 1;
     const int m = P.rp_jline;                                            // (rho, jx); (jy, -) is line m + 1 = nip - 1
@@ -95,13 +59,13 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass2(const StepPlan P, cons
     ulonglong2* i2m = i2 + static_cast<size_t>(b) * P.n_out * plane;
 
     // 1. inputs: Z staging and x-inverse
-    prow_inputs<NX>(P, i1m, plane, inl, nip, pair0, tw);
+    prow_inputs<NX, NT>(P, i1m, plane, inl, nip, pair0, tw);
 
     // 2. (rho, jx), (jy, -) -> (jx, jy) in line m and 1 / rho per position, with the
     //    zero-density check of fcalculator_workspace.cc:122-133
     {
         int bad = 0;
-        for (int e = threadIdx.x; e < RP * NX; e += kThreads) {
+        for (int e = threadIdx.x; e < RP * NX; e += NT) {
             const int r = e / NX, x = e - r * NX;
             ulonglong2* pj = inl + (static_cast<size_t>(r) * nip + m) * NX + x;
             const ulonglong2 rj = pj[0], jy = pj[NX];
@@ -120,49 +84,32 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass2(const StepPlan P, cons
         return JV{J, make_ulonglong2(f2_mul(J.x, f2_splat(f2_lo(ir))), f2_mul(J.y, f2_splat(f2_hi(ir))))};
     };
 
-    // 3. output pairs two at a time: both pairs' products from one read of a position's inputs,
-    //    fused into the first DIT stage; both lines' remaining stages; both untangled
+    // 3. output pairs two at a time, as the two lines of each stage: products fused into the
+    //    first DIT stage (stride 1, no twiddles), the remaining stages, both untangled
+    const DualIO io{worka, as, workb, bs};
     int pi = 0;
     for (; pi + 1 < P.rp_n; pi += 2) {
-        const RowProduct RA = row_product(P, pi, 0.f), RB = row_product(P, pi + 1, 0.f);
-#pragma unroll 1
-        for (int bi = threadIdx.x; bi < RP * NBL; bi += kThreads) {
-            const int r = bi / NBL, i = bi - r * NBL;
-            const ulonglong2* in = inl + static_cast<size_t>(r) * nip * NX;
-            PC va[RL], vb[RL];
-#pragma unroll
-            for (int q = 0; q < RL; ++q) {
-                const int sp = psw(i * RL + q);
-                const JV jv = jv_at(r, sp);
-                va[q] = row_product_canon<NX>(P, RA, in, sp, [&] { return jv; });
-                vb[q] = row_product_canon<NX>(P, RB, in, sp, [&] { return jv; });
-            }
-            pbfly<RL, -1>(va);
-            pbfly<RL, -1>(vb);
-            ulonglong2* la = worka + r * as;
-            ulonglong2* lb = workb + r * bs;
-#pragma unroll
-            for (int q = 0; q < RL; ++q) {
-                st_pc(la + psw(i * RL + q), va[q]);
-                st_pc(lb + psw(i * RL + q), vb[q]);
-            }
-        }
+        pstage_io<NX, pp.m - 1, -1, true, NT>(2 * RP, tw, [&](int l, int p) -> PC {
+            const int r = l >> 1, sp = psw(p);
+            const RowProduct R = row_product(P, pi + (l & 1), 0.f);
+            return row_product_canon<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, sp, [&] { return jv_at(r, sp); });
+        }, io);
         __syncthreads();
-        pdit2_range<NX, pp.m - 1, 0, -1>(RP, worka, as, workb, bs, tw);
-        prow_untangle<NX>(P, 2, OutLine{worka, as, P.rp_a[pi], P.rp_b[pi]}, OutLine{workb, bs, P.rp_a[pi + 1], P.rp_b[pi + 1]},
-                          i2m, plane, pair0);
+        pdit_range_io<NX, pp.m - 1, 0, -1, NT>(io, 2 * RP, tw);
+        prow_untangle<NX, NT>(P, 2, OutLine{worka, as, P.rp_a[pi], P.rp_b[pi]}, OutLine{workb, bs, P.rp_a[pi + 1], P.rp_b[pi + 1]},
+                              i2m, plane, pair0);
         __syncthreads();
     }
     if (pi < P.rp_n) {  // an odd last pair: line B alone
         const RowProduct R = row_product(P, pi, 0.f);
-        pstage_io<NX, pp.m - 1, -1, true>(RP, tw, [&](int r, int p) -> PC {
+        pstage_io<NX, pp.m - 1, -1, true, NT>(RP, tw, [&](int r, int p) -> PC {
             const int sp = psw(p);
             return row_product_canon<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, sp, [&] { return jv_at(r, sp); });
         }, SmemIO{workb, NX});
         __syncthreads();
-        pdit_range<NX, pp.m - 1, 0, -1>(workb, RP, tw);
+        pdit_range<NX, pp.m - 1, 0, -1, NT>(workb, RP, tw);
         const OutLine W{workb, bs, P.rp_a[pi], P.rp_b[pi]};
-        prow_untangle<NX>(P, 1, W, W, i2m, plane, pair0);
+        prow_untangle<NX, NT>(P, 1, W, W, i2m, plane, pair0);
     }
 }
 

@@ -62,6 +62,16 @@ __device__ __forceinline__ void st_stream(ulonglong2* p, ulonglong2 v) {
     asm volatile("st.global.L1::no_allocate.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(v.x), "l"(v.y) : "memory");
 }
 
+// a row pair's two elements of a transform plane (rows y0, y0 + 1: 32 bytes, 32-byte aligned as
+// y0, the row count and the plane sizes are even) in one access: the row pass reaches each plane
+// row pair by row pair, 32 bytes per column tile, so that each 32-byte sector is touched once
+__device__ __forceinline__ void ld_stream2(const ulonglong2* p, ulonglong2& a, ulonglong2& b) {
+    asm("ld.global.L1::no_allocate.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a.x), "=l"(a.y), "=l"(b.x), "=l"(b.y) : "l"(p));
+}
+__device__ __forceinline__ void st_stream2(ulonglong2* p, ulonglong2 a, ulonglong2 b) {
+    asm volatile("st.global.L1::no_allocate.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(a.x), "l"(a.y), "l"(b.x), "l"(b.y) : "memory");
+}
+
 // entry i of a twiddle table
 __device__ __forceinline__ float2 tw_at(const float2* __restrict__ tw, int i) { return ld_tw2(tw + i); }
 
@@ -257,13 +267,13 @@ template <int N> __device__ __forceinline__ int ppinv(int p) {
 // value at natural slot index p (0 <= p < N) of line l.  DIF twiddles after
 // the butterfly, DIT before; the stage-s twiddle of butterfly j is w_L^(j q).
 // ---------------------------------------------------------------------------
-template <int N, int S, int DIR, bool DIT, typename TW, typename Load, typename Store>
+template <int N, int S, int DIR, bool DIT, int NT = kThreads, typename TW, typename Load, typename Store>
 __device__ __forceinline__ void pstage_io(int nl, TW tw, Load&& load, Store&& store) {
     constexpr PPlan pp = PairPlan<N>::c;
     constexpr int R = pp.r[S], ST = pp.s[S], L = R * ST, NB = N / R;
     const int tot = nl * NB;
 #pragma unroll 2
-    for (int b = threadIdx.x; b < tot; b += kThreads) {
+    for (int b = threadIdx.x; b < tot; b += NT) {
         const int l = b / NB, i = b - l * NB;
         const int j = i & (ST - 1);
         const int base = (i >> pp.lg[S]) * L + j;
@@ -291,22 +301,33 @@ struct SmemIO {
 };
 
 // stages [S, E) in shared memory (DIF ascending, DIT descending), a barrier after each
-template <int N, int S, int E, int DIR, typename TW>
+template <int N, int S, int E, int DIR, int NT = kThreads, typename TW>
 __device__ __forceinline__ void pdif_range(ulonglong2* lines, int nl, TW tw) {
     if constexpr (S < E) {
         const SmemIO io{lines, N};
-        pstage_io<N, S, DIR, false>(nl, tw, io, io);
+        pstage_io<N, S, DIR, false, NT>(nl, tw, io, io);
         __syncthreads();
-        pdif_range<N, S + 1, E, DIR>(lines, nl, tw);
+        pdif_range<N, S + 1, E, DIR, NT>(lines, nl, tw);
     }
 }
-template <int N, int S, int E, int DIR, typename TW>
+template <int N, int S, int E, int DIR, int NT = kThreads, typename TW>
 __device__ __forceinline__ void pdit_range(ulonglong2* lines, int nl, TW tw) {
     if constexpr (S > E) {
         const SmemIO io{lines, N};
-        pstage_io<N, S - 1, DIR, true>(nl, tw, io, io);
+        pstage_io<N, S - 1, DIR, true, NT>(nl, tw, io, io);
         __syncthreads();
-        pdit_range<N, S - 1, E, DIR>(lines, nl, tw);
+        pdit_range<N, S - 1, E, DIR, NT>(lines, nl, tw);
+    }
+}
+
+// DIT stages S - 1 down to E of the lines an IO object reaches (load(l, p) / store(l, p, v) for
+// line l < nl), a barrier after each
+template <int N, int S, int E, int DIR, int NT, typename IO, typename TW>
+__device__ __forceinline__ void pdit_range_io(const IO& io, int nl, TW tw) {
+    if constexpr (S > E) {
+        pstage_io<N, S - 1, DIR, true, NT>(nl, tw, io, io);
+        __syncthreads();
+        pdit_range_io<N, S - 1, E, DIR, NT>(io, nl, tw);
     }
 }
 
@@ -578,13 +599,11 @@ __device__ __forceinline__ ZItem pz_load(const ulonglong2* i1m, size_t plane, in
     const int sa = 2 * ip, sb = 2 * ip + 1;
     const ulonglong2* pa = i1m + static_cast<size_t>(sa) * plane + static_cast<size_t>(t) * npy + y0;
     ZItem z;
-    z.a0 = ld_stream(pa);
-    z.a1 = ld_stream(pa + 1);
+    ld_stream2(pa, z.a0, z.a1);
     z.b0 = z.b1 = make_ulonglong2(0ull, 0ull);
     if (sb < n_in) {
         const ulonglong2* pb = i1m + static_cast<size_t>(sb) * plane + static_cast<size_t>(t) * npy + y0;
-        z.b0 = ld_stream(pb);
-        z.b1 = ld_stream(pb + 1);
+        ld_stream2(pb, z.b0, z.b1);
     }
     return z;
 }
@@ -606,7 +625,7 @@ __device__ __forceinline__ void pz_store(ulonglong2* line, int t, const ZItem& z
 
 // row pass, first part: Z staging of the nip input pair-lines of a block's RP row pairs (from
 // pair0) and their x-inverse in place (DIF stages in shared memory, a barrier after each)
-template <int NX, typename TW>
+template <int NX, int NT = kThreads, typename TW>
 __device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2* __restrict__ i1m, size_t plane, ulonglong2* inl, int nip,
                                             int pair0, TW tw) {
     constexpr int RP = kPairMaxN / NX;
@@ -615,11 +634,11 @@ __device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2*
     // Z[k] = X0[k] + i X1[k] (rows y0, y0 + 1) with the Hermitian mirror Z[N - k]
     // = conj X0[k] + i conj X1[k]; kx = 0 keeps the real parts only
     const int per_r = nip * hp, nz = RP * per_r;
-    for (int e0 = threadIdx.x; e0 < nz; e0 += kZBatch * kThreads) {
+    for (int e0 = threadIdx.x; e0 < nz; e0 += kZBatch * NT) {
         ZItem z[kZBatch];
 #pragma unroll
         for (int u = 0; u < kZBatch; ++u) {
-            const int e = e0 + u * kThreads;
+            const int e = e0 + u * NT;
             if (e < nz) {
                 const int r = e / per_r, rem = e - r * per_r;
                 const int ip = rem / hp, t = rem - ip * hp;
@@ -628,7 +647,7 @@ __device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2*
         }
 #pragma unroll
         for (int u = 0; u < kZBatch; ++u) {
-            const int e = e0 + u * kThreads;
+            const int e = e0 + u * NT;
             if (e < nz) {
                 const int r = e / per_r, rem = e - r * per_r;
                 const int ip = rem / hp, t = rem - ip * hp;
@@ -638,12 +657,12 @@ __device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2*
     }
     const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
     const int per_z = nip * nzero;
-    for (int e = threadIdx.x; e < RP * per_z; e += kThreads) {
+    for (int e = threadIdx.x; e < RP * per_z; e += NT) {
         const int l = e / nzero, k = hx + (e - l * nzero);
         st_pc(inl + static_cast<size_t>(l) * NX + psw(k), pc_zero());
     }
     __syncthreads();
-    pdif_range<NX, 0, pp.m, +1>(inl, RP * nip, tw);
+    pdif_range<NX, 0, pp.m, +1, NT>(inl, RP * nip, tw);
 }
 
 // row pass, last part: the untangling of transformed output pairs into I2.  One or two (nl)
@@ -655,7 +674,7 @@ struct OutLine {
     size_t stride;
     int oa, ob;
 };
-template <int NX>
+template <int NX, int NT = kThreads>
 __device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const OutLine W0, const OutLine W1, ulonglong2* __restrict__ i2m,
                                               size_t plane, int pair0) {
     constexpr int RP = kPairMaxN / NX;
@@ -663,7 +682,7 @@ __device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const O
     const u64 HALF = f2_splat(0.5f);
     const int per_q = RP * hp;
 #pragma unroll 2
-    for (int e = threadIdx.x; e < nl * per_q; e += kThreads) {
+    for (int e = threadIdx.x; e < nl * per_q; e += NT) {
         const bool q = e >= per_q;
         const OutLine W = q ? W1 : W0;
         const int rem = q ? e - per_q : e;
@@ -682,12 +701,12 @@ __device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const O
             g1i[w] = f2_mul(f2_sub(zn.re, zk.re), HALF);   // -(d.re) / 2
         }
         ulonglong2* qa = i2m + static_cast<size_t>(W.oa) * plane + static_cast<size_t>(t) * npy + y0;
-        st_stream(qa, make_ulonglong2(f2_pack(f2_lo(g0r[0]), f2_lo(g0r[1])), f2_pack(f2_lo(g0i[0]), f2_lo(g0i[1]))));
-        st_stream(qa + 1, make_ulonglong2(f2_pack(f2_lo(g1r[0]), f2_lo(g1r[1])), f2_pack(f2_lo(g1i[0]), f2_lo(g1i[1]))));
+        st_stream2(qa, make_ulonglong2(f2_pack(f2_lo(g0r[0]), f2_lo(g0r[1])), f2_pack(f2_lo(g0i[0]), f2_lo(g0i[1]))),
+                   make_ulonglong2(f2_pack(f2_lo(g1r[0]), f2_lo(g1r[1])), f2_pack(f2_lo(g1i[0]), f2_lo(g1i[1]))));
         if (W.ob >= 0) {
             ulonglong2* qb = i2m + static_cast<size_t>(W.ob) * plane + static_cast<size_t>(t) * npy + y0;
-            st_stream(qb, make_ulonglong2(f2_pack(f2_hi(g0r[0]), f2_hi(g0r[1])), f2_pack(f2_hi(g0i[0]), f2_hi(g0i[1]))));
-            st_stream(qb + 1, make_ulonglong2(f2_pack(f2_hi(g1r[0]), f2_hi(g1r[1])), f2_pack(f2_hi(g1i[0]), f2_hi(g1i[1]))));
+            st_stream2(qb, make_ulonglong2(f2_pack(f2_hi(g0r[0]), f2_hi(g0r[1])), f2_pack(f2_hi(g0i[0]), f2_hi(g0i[1]))),
+                       make_ulonglong2(f2_pack(f2_hi(g1r[0]), f2_hi(g1r[1])), f2_pack(f2_hi(g1i[0]), f2_hi(g1i[1]))));
         }
     }
 }

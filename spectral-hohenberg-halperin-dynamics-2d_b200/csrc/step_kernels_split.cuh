@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kThreads) prow_forward(const StepPlan P, const
     constexpr PPlan pp = PairPlan<NX>::c;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ulonglong2* work = reinterpret_cast<ulonglong2*>(smem_raw);  // [RP][NX]
-    const int npy = P.npy, hx = P.hx, hp = hx >> 1;
+    const int npy = P.npy;
     const int nip = (P.n_in + 1) >> 1;
     const int pi = blockIdx.y, pair0 = blockIdx.x * RP;
     const size_t plane = static_cast<size_t>(P.ntiles) * npy;
@@ -129,32 +129,8 @@ __global__ void __launch_bounds__(kThreads) prow_forward(const StepPlan P, const
     __syncthreads();
     pdit_range<NX, pp.m - 1, 0, -1>(work, RP, tw);
 
-    // G0[k] = (Z[k] + conj Z[N-k]) / 2 (row y0), G1[k] = -i (Z[k] - conj Z[N-k]) / 2 (row y0 + 1)
-    const u64 HALF = f2_splat(0.5f);
-    for (int e = threadIdx.x; e < RP * hp; e += kThreads) {
-        const int r = e / hp, t = e - r * hp;
-        const ulonglong2* z = work + static_cast<size_t>(r) * NX;
-        const int y0 = 2 * (pair0 + r);
-        u64 g0r[2], g0i[2], g1r[2], g1i[2];
-#pragma unroll
-        for (int w = 0; w < 2; ++w) {
-            const int k = 2 * t + w;
-            const PC zk = ld_pc(z + psw(k));
-            const PC zn = ld_pc(z + psw(k == 0 ? 0 : NX - k));
-            g0r[w] = f2_mul(f2_add(zk.re, zn.re), HALF);
-            g0i[w] = f2_mul(f2_sub(zk.im, zn.im), HALF);
-            g1r[w] = f2_mul(f2_add(zk.im, zn.im), HALF);
-            g1i[w] = f2_mul(f2_sub(zn.re, zk.re), HALF);
-        }
-        ulonglong2* qa = i2m + static_cast<size_t>(oa) * plane + static_cast<size_t>(t) * npy + y0;
-        qa[0] = make_ulonglong2(f2_pack(f2_lo(g0r[0]), f2_lo(g0r[1])), f2_pack(f2_lo(g0i[0]), f2_lo(g0i[1])));
-        qa[1] = make_ulonglong2(f2_pack(f2_lo(g1r[0]), f2_lo(g1r[1])), f2_pack(f2_lo(g1i[0]), f2_lo(g1i[1])));
-        if (ob >= 0) {
-            ulonglong2* qb = i2m + static_cast<size_t>(ob) * plane + static_cast<size_t>(t) * npy + y0;
-            qb[0] = make_ulonglong2(f2_pack(f2_hi(g0r[0]), f2_hi(g0r[1])), f2_pack(f2_hi(g0i[0]), f2_hi(g0i[1])));
-            qb[1] = make_ulonglong2(f2_pack(f2_hi(g1r[0]), f2_hi(g1r[1])), f2_pack(f2_hi(g1i[0]), f2_hi(g1i[1])));
-        }
-    }
+    const OutLine W{work, static_cast<size_t>(NX), oa, ob};
+    prow_untangle<NX>(P, 1, W, W, i2m, plane, pair0);
 }
 
 }  // namespace shhd

@@ -114,7 +114,7 @@ void launch_dual(const StepPlan& P, int batch, cudaStream_t s, const MemberInfo*
         }
     }
     dim3 grid(P.npy / 2 / RP, batch);
-    prow_pass2<NX><<<grid, kThreads, smem, s>>>(P, members, static_cast<const ulonglong2*>(i1), static_cast<ulonglong2*>(i2),
+    prow_pass2<NX><<<grid, kDualThreads, smem, s>>>(P, members, static_cast<const ulonglong2*>(i1), static_cast<ulonglong2*>(i2),
                                                 static_cast<const float2*>(tw), err);
 }
 }  // namespace
