@@ -370,7 +370,8 @@ def run_b200(args):
     achieved = (by / n_l) / (t_ms / n_l * 1e-3) / 1e9
     peak, peak_kind = measured_peak_gbs()
     # the summary holds the pair-line kernels' capture; another family has no captured traffic
-    traffic = dram_traffic_from_profiles("hh1024_fp32").get(dom) if args.precision == "fp32" and tuning.get("family") == "pair-line" else None
+    # the committed capture covers the FP32 engine with the family it timed (hh1024_fp32_f<family>)
+    traffic = dram_traffic_from_profiles(f"hh1024_fp32_f{eng.family}").get(dom) if args.precision == "fp32" else None
     step_bytes = sum(v[2] for v in kst.values()) / kprof_steps
     step_ms_profiled = sum(v[0] for v in kst.values()) / kprof_steps
     kernels = {k: {"ms_per_launch": (v[0] / v[1]) if v[1] else None, "launches_per_step": v[1] / kprof_steps,
