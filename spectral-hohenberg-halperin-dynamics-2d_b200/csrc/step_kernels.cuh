@@ -196,6 +196,35 @@ __global__ void __launch_bounds__(kThreads) col_inverse_kernel(const StepPlan P,
     }
 }
 
+// a row pair's two elements of a transform plane (rows y0, y0 + 1: 32 bytes, 32-byte aligned when
+// y0, the row count and the plane sizes are even) in one access: the row passes reach each plane
+// row pair by row pair, 32 bytes per column tile, so that each 32-byte sector is touched once.
+// Read once and written once per kernel, so not allocated in L1.
+__device__ __forceinline__ void ld_stream2(const ulonglong2* p, ulonglong2& a, ulonglong2& b) {
+    asm("ld.global.L1::no_allocate.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a.x), "=l"(a.y), "=l"(b.x), "=l"(b.y) : "l"(p));
+}
+__device__ __forceinline__ void st_stream2(ulonglong2* p, ulonglong2 a, ulonglong2 b) {
+    asm volatile("st.global.L1::no_allocate.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(a.x), "l"(a.y), "l"(b.x), "l"(b.y) : "memory");
+}
+// complex value w of a 16-byte group (two FP32 complex, or one FP64), and its inverse
+__device__ __forceinline__ float2 c16_get(const ulonglong2& v, int w, float2) {
+    const unsigned long long q = w ? v.y : v.x;
+    return make_float2(__int_as_float(static_cast<int>(q & 0xffffffffull)), __int_as_float(static_cast<int>(q >> 32)));
+}
+__device__ __forceinline__ double2 c16_get(const ulonglong2& v, int, double2) {
+    return make_double2(__longlong_as_double(static_cast<long long>(v.x)), __longlong_as_double(static_cast<long long>(v.y)));
+}
+__device__ __forceinline__ void c16_set(ulonglong2& v, int w, float2 c) {
+    const unsigned long long q = static_cast<unsigned long long>(static_cast<unsigned int>(__float_as_int(c.x))) |
+                                 (static_cast<unsigned long long>(static_cast<unsigned int>(__float_as_int(c.y))) << 32);
+    if (w) v.y = q;
+    else v.x = q;
+}
+__device__ __forceinline__ void c16_set(ulonglong2& v, int, double2 c) {
+    v.x = static_cast<unsigned long long>(__double_as_longlong(c.x));
+    v.y = static_cast<unsigned long long>(__double_as_longlong(c.y));
+}
+
 // ---------------------------------------------------------------------------
 // free-energy plugin styles (free_energy_plugins.h): the physical chemical potential and the
 // free-energy density at one point, from the plan's style and parameters

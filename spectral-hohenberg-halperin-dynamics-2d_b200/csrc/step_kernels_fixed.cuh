@@ -242,9 +242,44 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
     //    loads are issued in batches of 4 per thread so several are in flight
     const size_t i1_member = static_cast<size_t>(b) * P.n_in * P.ntiles * npy * W;
     const size_t slot_stride = static_cast<size_t>(P.ntiles) * npy * W;
-    const int nload = P.n_in * hx;
     constexpr int U = 4;
-    for (int e0 = threadIdx.x; e0 < nload; e0 += NT * U) {
+    // a row pair of one column tile is one 32-byte sector when the tile is 16 bytes wide (FP32
+    // with two-column tiles, FP64 with one) and the row count is even: one 256-bit load per tile
+    constexpr int WC = 16 / static_cast<int>(sizeof(C));  // columns of such a tile
+    const bool wide = W == WC && has1 && (npy & 1) == 0;
+    const int nload = wide ? P.n_in * (hx / WC) : P.n_in * hx;
+    if (wide) {
+        const int ntile = hx / WC;
+        for (int e0 = threadIdx.x; e0 < nload; e0 += NT * U) {
+            ulonglong2 r0[U], r1[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * NT;
+                if (e < nload) {
+                    const int s = e / ntile, t = e - s * ntile;
+                    const C* p0 = i1 + i1_member + s * slot_stride + (static_cast<size_t>(t) * npy + y0) * WC;
+                    ld_stream2(reinterpret_cast<const ulonglong2*>(p0), r0[u], r1[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int e = e0 + u * NT;
+                if (e < nload) {
+                    const int s = e / ntile, t = e - s * ntile;
+                    C* z = lines + static_cast<size_t>(s) * NX;
+#pragma unroll
+                    for (int w = 0; w < WC; ++w) {
+                        const int k = t * WC + w;
+                        C av = c16_get(r0[u], w, C{}), cv = c16_get(r1[u], w, C{});
+                        if (k == 0) { av.y = 0; cv.y = 0; }  // C2R uses the real part of the kx = 0 entry
+                        z[swz<SB>(k)] = mk(av.x - cv.y, av.y + cv.x);
+                        if (k > 0) z[swz<SB>(NX - k)] = mk(av.x + cv.y, cv.x - av.y);
+                    }
+                }
+            }
+        }
+    }
+    for (int e0 = threadIdx.x; !wide && e0 < nload; e0 += NT * U) {
         C a[U], c[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -333,7 +368,7 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
         group_sync<GG, NT>(barid);
         gfft<NX, GG, -1, NT, SB>(z, tw, tid, barid);
         C* dst = i2 + i2_member + static_cast<size_t>(o) * P.ntiles * npy * W;
-        for (int k = tid; k < hx; k += GG) {
+        for (int k = tid; !wide && k < hx; k += GG) {
             const C zk = z[swz<SB>(k)];
             const C zn = cconj(z[swz<SB>(k == 0 ? 0 : NX - k)]);
             const C g0 = mk(static_cast<T>(0.5) * (zk.x + zn.x), static_cast<T>(0.5) * (zk.y + zn.y));
@@ -343,6 +378,19 @@ __global__ void __launch_bounds__(NT, (NT > kThreads ? 1 : 2)) row_pass_fixed(co
             C* q = dst + (static_cast<size_t>(t) * npy + y0) * W + w;
             q[0] = g0;
             if (has1) q[W] = g1;
+        }
+        for (int t = tid; wide && t < hx / WC; t += GG) {  // one 256-bit store per tile and row pair
+            ulonglong2 o0, o1;
+#pragma unroll
+            for (int w = 0; w < WC; ++w) {
+                const int k = t * WC + w;
+                const C zk = z[swz<SB>(k)];
+                const C zn = cconj(z[swz<SB>(k == 0 ? 0 : NX - k)]);
+                const C d = csub(zk, zn);
+                c16_set(o0, w, mk(static_cast<T>(0.5) * (zk.x + zn.x), static_cast<T>(0.5) * (zk.y + zn.y)));
+                c16_set(o1, w, mk(static_cast<T>(0.5) * d.y, static_cast<T>(-0.5) * d.x));
+            }
+            st_stream2(reinterpret_cast<ulonglong2*>(dst + (static_cast<size_t>(t) * npy + y0) * WC), o0, o1);
         }
         group_sync<GG, NT>(barid);
     };

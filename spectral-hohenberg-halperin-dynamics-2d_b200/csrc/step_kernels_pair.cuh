@@ -62,16 +62,6 @@ __device__ __forceinline__ void st_stream(ulonglong2* p, ulonglong2 v) {
     asm volatile("st.global.L1::no_allocate.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(v.x), "l"(v.y) : "memory");
 }
 
-// a row pair's two elements of a transform plane (rows y0, y0 + 1: 32 bytes, 32-byte aligned as
-// y0, the row count and the plane sizes are even) in one access: the row pass reaches each plane
-// row pair by row pair, 32 bytes per column tile, so that each 32-byte sector is touched once
-__device__ __forceinline__ void ld_stream2(const ulonglong2* p, ulonglong2& a, ulonglong2& b) {
-    asm("ld.global.L1::no_allocate.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a.x), "=l"(a.y), "=l"(b.x), "=l"(b.y) : "l"(p));
-}
-__device__ __forceinline__ void st_stream2(ulonglong2* p, ulonglong2 a, ulonglong2 b) {
-    asm volatile("st.global.L1::no_allocate.v4.u64 [%0], {%1, %2, %3, %4};" ::"l"(p), "l"(a.x), "l"(a.y), "l"(b.x), "l"(b.y) : "memory");
-}
-
 // entry i of a twiddle table
 __device__ __forceinline__ float2 tw_at(const float2* __restrict__ tw, int i) { return ld_tw2(tw + i); }
 
