@@ -26,6 +26,11 @@ constexpr size_t prow2_smem_bytes(int nip) {
 // block size of the two-pair row pass
 constexpr int kDualThreads = 384;
 
+// slot of position slot x in a row pair's 1 / rho array (8-byte entries): bit 3 flipped by bit 6.
+// The first forward stage at 1536 points reads positions 8 i + (q ^ (i & 7)) for consecutive
+// i, which put lanes i and i + 8 of a half warp in one bank pair of a plain array
+__device__ __forceinline__ int irho_slot(int x) { return x ^ ((x >> 3) & 8); }
+
 // the two work lines of a round as lines l = 2 r + q of one stage: output pair q of row pair r
 struct DualIO {
     ulonglong2* a;
@@ -71,7 +76,7 @@ __global__ void __launch_bounds__(kDualThreads, 2) prow_pass2(const StepPlan P, 
             const ulonglong2 rj = pj[0], jy = pj[NX];
             const float r0 = f2_lo(rj.x), r1 = f2_lo(rj.y);
             if (r0 == 0.f || r1 == 0.f) bad = 1;
-            irho[e] = f2_pack(1.f / r0, 1.f / r1);
+            irho[static_cast<size_t>(r) * NX + irho_slot(x)] = f2_pack(1.f / r0, 1.f / r1);
             pj[0] = make_ulonglong2(f2_pack(f2_hi(rj.x), f2_lo(jy.x)), f2_pack(f2_hi(rj.y), f2_lo(jy.y)));
         }
         if (bad) atomicOr(err, ERR_ZERO_DENSITY);
@@ -80,7 +85,7 @@ __global__ void __launch_bounds__(kDualThreads, 2) prow_pass2(const StepPlan P, 
     // (jx, jy) and (vx, vy) at slot sp of row pair r
     auto jv_at = [&](int r, int sp) {
         const ulonglong2 J = inl[(static_cast<size_t>(r) * nip + m) * NX + sp];
-        const u64 ir = irho[static_cast<size_t>(r) * NX + sp];
+        const u64 ir = irho[static_cast<size_t>(r) * NX + irho_slot(sp)];
         return JV{J, make_ulonglong2(f2_mul(J.x, f2_splat(f2_lo(ir))), f2_mul(J.y, f2_splat(f2_hi(ir))))};
     };
 

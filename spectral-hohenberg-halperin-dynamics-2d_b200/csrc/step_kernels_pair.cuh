@@ -780,7 +780,9 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
     ulonglong2* acc0 = lines + CP * NY;                                  // [CP][Kp], slots pmode_slot
     ulonglong2* acc1 = acc0 + CP * kyp;
     ulonglong2* acc2 = acc1 + CP * kyp;
-    const int t0 = blockIdx.x * CP, grp = blockIdx.y, b = blockIdx.z;
+    // the momentum group (the last, and the heaviest: five or six product fields and three
+    // updated fields) is launched first, so that the lighter order-parameter blocks fill the tail
+    const int t0 = blockIdx.x * CP, grp = P.n_groups - 1 - static_cast<int>(blockIdx.y), b = blockIdx.z;
     const int gkind = P.group_kind[grp], alpha = P.group_alpha[grp];
     const bool comp = (P.mode == 0);
     const MemberInfo mi = A.members[b];
