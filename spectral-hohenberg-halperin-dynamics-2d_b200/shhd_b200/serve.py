@@ -64,6 +64,9 @@ def bucket_key(cfg: Config, green_kubo: Optional[Tuple[int, int]] = None) -> byt
     return bytes(memoryview(c).cast("B")) + repr(green_kubo).encode()
 
 
+_POLL_S = 5e-5  # interval of the loop's event polling while every bucket has a chunk in flight
+
+
 def _noisy(cfg: Config) -> bool:
     return bool(cfg.noise_momentum or cfg.noise_order_parameter)
 
@@ -249,8 +252,10 @@ class Server:
         """Serve `jobs` (arrival times relative to now) until all have finished.
 
         Each bucket has at most one chunk in flight; chunks of different buckets overlap on the
-        device (one stream per engine), and a finished chunk is noticed by polling its event, so
-        one slow bucket does not hold back the admissions and launches of the others."""
+        device (one stream per engine), and a finished chunk is noticed by polling every event, so
+        one slow bucket does not hold back the admissions and launches of the others.  Buckets
+        stay with the server between runs (until another shape needs their memory), so a later
+        run reuses their engines."""
         self._check_admissible(jobs)
         future = sorted(jobs, key=lambda j: j.arrival)
         pending: List[Job] = []
@@ -287,9 +292,10 @@ class Server:
                 continue
             ready = [b for b in inflight if b.inflight[1].query()]
             if not ready:
-                # nothing finished yet: wait for the oldest chunk rather than spin
-                inflight[0].inflight[1].synchronize()
-                ready = [inflight[0]]
+                # nothing finished yet: poll again shortly (every bucket's event, and the arrivals),
+                # so that whichever chunk ends first has its bucket refilled at once
+                time.sleep(_POLL_S)
+                continue
             now = time.perf_counter() - t0
             for b in ready:
                 done += self._finish_chunk(b, now)
