@@ -746,6 +746,25 @@ void build_plan(shhd_engine* e) {
             e->smem_row = row_b;
             e->smem_col = col_b;
             plan_row_pairs(P);
+            // the density as a group of its own (compressible): its update needs no products, and
+            // the momentum blocks, the heaviest, lose a field; launch order momentum, order
+            // parameters, density (heaviest first, so that the light blocks fill the tail)
+            int gm = -1;
+            for (int g = 0; g < P.n_groups; ++g)
+                if (P.group_kind[g] == GROUP_MOMENTUM) gm = g;
+            if (P.mode == SHHD_COMPRESSIBLE && gm >= 0) {
+                const int g = P.n_groups++;
+                P.group_kind[g] = GROUP_RHO;
+                P.group_alpha[g] = 0;
+                P.group_nout[g] = 0;
+                P.rho_split = 1;
+            }
+            int k = 0;
+            if (gm >= 0) P.group_order[k++] = gm;
+            for (int g = 0; g < P.n_groups; ++g)
+                if (P.group_kind[g] == GROUP_PSI) P.group_order[k++] = g;
+            for (int g = 0; g < P.n_groups; ++g)
+                if (P.group_kind[g] == GROUP_RHO) P.group_order[k++] = g;
         }
     }
     // split row pass (every pair-line size)

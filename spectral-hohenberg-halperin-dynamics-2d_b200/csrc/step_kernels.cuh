@@ -33,11 +33,13 @@ constexpr int kMaxFields = kMaxOp + 3;
 constexpr int kMaxIn = kMaxOp + 3;
 constexpr int kMaxOut = 4 * kMaxOp + 5;
 constexpr int kMaxGroupOut = 8;
-constexpr int kMaxGroups = kMaxOp + 1;
+constexpr int kMaxGroups = kMaxOp + 2;
 constexpr int kMaxSine = 8;
 
 enum OutKind : int { OUT_MU = 0, OUT_PSIVX, OUT_PSIVY, OUT_GRAD, OUT_VX, OUT_VY, OUT_PXX, OUT_PXY, OUT_PYY };
-enum GroupKind : int { GROUP_PSI = 0, GROUP_MOMENTUM = 1 };
+// GROUP_RHO: the density alone (its RHS -i k.j needs no products), split from the momentum
+// group in the pair-line column kernel so that the heavy momentum blocks lose a field
+enum GroupKind : int { GROUP_PSI = 0, GROUP_MOMENTUM = 1, GROUP_RHO = 2 };
 enum ErrBits : int { ERR_ZERO_DENSITY = 1, ERR_NONFINITE = 2 };
 
 // A diverging integration leaves NaN or Inf in the state: the state writes test each new
@@ -74,6 +76,8 @@ struct StepPlan {
     int group_alpha[kMaxGroups];
     int group_nout[kMaxGroups];
     int group_out[kMaxGroups][kMaxGroupOut];
+    int group_order[kMaxGroups];   // pair-line column kernel: group of blockIdx.y (heaviest first)
+    int rho_split;                 // the density is its own group (GROUP_RHO), not the momentum group's
     // physics
     double mobility[kMaxOp], mu_k0[kMaxOp], mu_k2[kMaxOp], mu_k4[kMaxOp], mu_u3[kMaxOp];
     int fe_plugin;                 // free-energy plugin style (0: none; its mu replaces u3 psi^3)

@@ -780,9 +780,9 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
     ulonglong2* acc0 = lines + CP * NY;                                  // [CP][Kp], slots pmode_slot
     ulonglong2* acc1 = acc0 + CP * kyp;
     ulonglong2* acc2 = acc1 + CP * kyp;
-    // the momentum group (the last, and the heaviest: five or six product fields and three
-    // updated fields) is launched first, so that the lighter order-parameter blocks fill the tail
-    const int t0 = blockIdx.x * CP, grp = P.n_groups - 1 - static_cast<int>(blockIdx.y), b = blockIdx.z;
+    // groups in the plan's launch order: momentum (the heaviest: five or six product fields and
+    // two or three updated fields) first, so that the lighter blocks fill the tail
+    const int t0 = blockIdx.x * CP, grp = P.group_order[blockIdx.y], b = blockIdx.z;
     const int gkind = P.group_kind[grp], alpha = P.group_alpha[grp];
     const bool comp = (P.mode == 0);
     const MemberInfo mi = A.members[b];
@@ -802,7 +802,11 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
             if (base_used) prefetch_l2(A.base + col0 + static_cast<size_t>(f) * fstride, span);
         };
         if (gkind == GROUP_PSI) fetch(1 + alpha);
-        else { fetch(P.nop + 1); fetch(P.nop + 2); fetch(0); }
+        else {
+            fetch(P.nop + 1);
+            fetch(P.nop + 2);
+            if (gkind == GROUP_RHO || (comp && !P.rho_split)) fetch(0);
+        }
     }
     for (int e = threadIdx.x; e < CP * kyp; e += kThreads) {
         st_pc(acc0 + e, pc_zero());
@@ -920,7 +924,16 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
                 r[w] = psi_epilogue<float>(P, A, alpha, m, kxu * static_cast<float>(m.gx), kyu * static_cast<float>(m.ky), pc_col(u0, w), mi, L, b);
             }
             st_pc(acc0 + sj, pc_make(r[0], r[1]));
+        } else if (gkind == GROUP_RHO) {
+            float2 r[2];
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+                const ModeCtx m = mode_ctx<float>(P, mbase, t, w, j);
+                r[w] = rho_epilogue<float>(P, A, m.pos, kxu * static_cast<float>(m.gx), kyu * static_cast<float>(m.ky), fstride);
+            }
+            st_pc(acc0 + sj, pc_make(r[0], r[1]));
         } else {
+            const bool with_rho = comp && !P.rho_split;
             const PC u1 = ld_pc(acc1 + sj);
             float2 r0[2], r1[2], r2[2];
 #pragma unroll
@@ -931,17 +944,17 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
                 r0[w] = pc_col(u0, w);
                 r1[w] = pc_col(u1, w);
                 momentum_epilogue<float>(P, A, m, kx, kyv, r0[w], r1[w], mi, L, b);
-                r2[w] = comp ? rho_epilogue<float>(P, A, m.pos, kx, kyv, fstride) : make_float2(0.f, 0.f);
+                r2[w] = with_rho ? rho_epilogue<float>(P, A, m.pos, kx, kyv, fstride) : make_float2(0.f, 0.f);
             }
             st_pc(acc0 + sj, pc_make(r0[0], r0[1]));
             st_pc(acc1 + sj, pc_make(r1[0], r1[1]));
-            st_pc(acc2 + sj, pc_make(r2[0], r2[1]));
+            if (with_rho) st_pc(acc2 + sj, pc_make(r2[0], r2[1]));
         }
     }
     __syncthreads();
 
     // real-symmetry projection of the kx = 0 line (time_integrator.h:70-109): column 0 of tile 0
-    const int nres = (gkind == GROUP_PSI) ? 1 : (comp ? 3 : 2);
+    const int nres = (gkind != GROUP_MOMENTUM) ? 1 : ((comp && !P.rho_split) ? 3 : 2);
     if (t0 == 0 && !A.det_mode) {
         for (int e = threadIdx.x; e < nres * half; e += kThreads) {
             const int q = e / half, ky = e - q * half;
@@ -968,10 +981,11 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
     int wfield[3], nwf = 0;
     const ulonglong2* wsrc[3];
     if (gkind == GROUP_PSI) { wfield[nwf] = 1 + alpha; wsrc[nwf++] = acc0; }
+    else if (gkind == GROUP_RHO) { wfield[nwf] = 0; wsrc[nwf++] = acc0; }
     else {
         wfield[nwf] = P.nop + 1; wsrc[nwf++] = acc0;
         wfield[nwf] = P.nop + 2; wsrc[nwf++] = acc1;
-        if (comp) { wfield[nwf] = 0; wsrc[nwf++] = acc2; }
+        if (comp && !P.rho_split) { wfield[nwf] = 0; wsrc[nwf++] = acc2; }
     }
     bool bad = false;
     for (int q = 0; q < nwf; ++q) {
