@@ -33,6 +33,7 @@ __device__ __forceinline__ int irho_slot(int x) { return x ^ ((x >> 3) & 8); }
 
 // the two work lines of a round as lines l = 2 r + q of one stage: output pair q of row pair r
 struct DualIO {
+    static constexpr bool kSlots = true;
     ulonglong2* a;
     size_t as;
     ulonglong2* b;

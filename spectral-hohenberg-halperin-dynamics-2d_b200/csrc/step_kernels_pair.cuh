@@ -22,6 +22,8 @@
 // the product evaluation, the RHS accumulation and the gather of new modes.
 #pragma once
 
+#include <type_traits>
+
 #include "step_kernels_fixed.cuh"
 
 namespace shhd {
@@ -224,6 +226,18 @@ __host__ __device__ constexpr bool is_pair_size(int n) { return n == 96 || n == 
 // slot of position p in a line: low three bits XORed with bits 3..5
 __device__ __forceinline__ int psw(int p) { return p ^ ((p >> 3) & 7); }
 
+// psw(base + q ST) for the positions of one butterfly of a stage with stride ST, span L and radix
+// R, from psw(base) and the compile-time q where the stage's structure allows: strides that are
+// multiples of 64 leave bits 3..5 alone; at stride 8 of a 64-point span bits 3..5 of base are
+// zero and become q; at stride 1 of radix 8 the low three bits of base are zero
+template <int ST, int L, int R>
+__device__ __forceinline__ int psw_q(int base, int pswbase, int q) {
+    if constexpr (ST % 64 == 0) return pswbase + q * ST;
+    else if constexpr (ST == 8 && L == 64) return (base ^ q) + 8 * q;
+    else if constexpr (ST == 1 && R == 8) return pswbase ^ q;
+    else return psw(base + q * ST);
+}
+
 // digit-reversed position of natural index y, and its inverse
 template <int N> __device__ __forceinline__ int ppos(int y) {
     constexpr PPlan pp = PairPlan<N>::c;
@@ -257,6 +271,11 @@ template <int N> __device__ __forceinline__ int ppinv(int p) {
 // value at natural slot index p (0 <= p < N) of line l.  DIF twiddles after
 // the butterfly, DIT before; the stage-s twiddle of butterfly j is w_L^(j q).
 // ---------------------------------------------------------------------------
+// whether an IO object exposes line(l) for slot addressing (SmemIO and the like), or is a
+// load / store function of (line, position)
+template <typename T, typename = void> struct has_slots { static constexpr bool value = false; };
+template <typename T> struct has_slots<T, decltype(void(T::kSlots))> { static constexpr bool value = T::kSlots; };
+
 template <int N, int S, int DIR, bool DIT, int NT = kThreads, typename TW, typename Load, typename Store>
 __device__ __forceinline__ void pstage_io(int nl, TW tw, Load&& load, Store&& store) {
     constexpr PPlan pp = PairPlan<N>::c;
@@ -268,8 +287,16 @@ __device__ __forceinline__ void pstage_io(int nl, TW tw, Load&& load, Store&& st
         const int j = i & (ST - 1);
         const int base = (i >> pp.lg[S]) * L + j;
         PC v[R];
+        const int pb = psw(base);
+        (void)pb;
+        if constexpr (has_slots<std::decay_t<Load>>::value) {
+            const ulonglong2* ln = load.line(l);
 #pragma unroll
-        for (int q = 0; q < R; ++q) v[q] = load(l, base + q * ST);
+            for (int q = 0; q < R; ++q) v[q] = ld_pc(ln + psw_q<ST, L, R>(base, pb, q));
+        } else {
+#pragma unroll
+            for (int q = 0; q < R; ++q) v[q] = load(l, base + q * ST);
+        }
         if constexpr (L > R) {
             if constexpr (DIT) ptwiddle_pow<R, DIR>(v, tw_at(tw, pp.twoff[S] + j));
         }
@@ -277,15 +304,23 @@ __device__ __forceinline__ void pstage_io(int nl, TW tw, Load&& load, Store&& st
         if constexpr (L > R) {
             if constexpr (!DIT) ptwiddle_pow<R, DIR>(v, tw_at(tw, pp.twoff[S] + j));
         }
+        if constexpr (has_slots<std::decay_t<Store>>::value) {
+            ulonglong2* ln = store.line(l);
 #pragma unroll
-        for (int q = 0; q < R; ++q) store(l, base + q * ST, v[q]);
+            for (int q = 0; q < R; ++q) st_pc(ln + psw_q<ST, L, R>(base, pb, q), v[q]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < R; ++q) store(l, base + q * ST, v[q]);
+        }
     }
 }
 
 // shared-memory load/store of `lines` (line l at lines + l * N)
 struct SmemIO {
+    static constexpr bool kSlots = true;  // line(l) + slot: pstage_io forms the slots itself
     ulonglong2* lines;
     int n;
+    __device__ __forceinline__ ulonglong2* line(int l) const { return lines + l * n; }
     __device__ __forceinline__ PC operator()(int l, int p) const { return ld_pc(lines + l * n + psw(p)); }
     __device__ __forceinline__ void operator()(int l, int p, PC v) const { st_pc(lines + l * n + psw(p), v); }
 };
