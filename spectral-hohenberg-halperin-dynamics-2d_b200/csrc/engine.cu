@@ -481,6 +481,14 @@ void plan_row_pairs(StepPlan& P) {
         else if (ka == OUT_PSIVX && P.need_v) P.rp_mode[pi] = 4;
         else if (ka == OUT_PSIVY && P.need_v) P.rp_mode[pi] = 5;
     }
+    // one input slot and one output (psi -> u psi^3, e.g. quiescent dynamics with N = 1): a
+    // pair-line holds two row pairs of that slot instead of a slot and an empty half, both halves
+    // with the output's coefficients (blocks of two or more row pairs, i.e. rows of <= 768 points)
+    P.rp_pack = 0;
+    if (P.n_in == 1 && P.n_out == 1 && P.rp_n == 1 && P.rp_canon && P.rp_mode[0] == 3 && kPairMaxN / P.npx >= 2) {
+        P.rp_pack = 1;
+        for (int q = 0; q < 8; ++q) P.rp_coef[0][q][1] = P.rp_coef[0][q][0];
+    }
 }
 
 void build_plan(shhd_engine* e) {
@@ -769,6 +777,7 @@ void build_plan(shhd_engine* e) {
     }
     // split row pass (every pair-line size)
     e->split_row = e->pair_path && e->family_override == 3 && split_row_supported(c.nx) && c.ny % 2 == 0;
+    if (e->split_row) P.rp_pack = 0;  // the split kernels transform unpacked lines
     // row pass over two output pairs at a time (compressible canonical layouts); the default on
     // 1536-point rows, where it beats the pair-line row pass (105 against 113 us at 1024^2, N = 2;
     // on shorter rows, several row pairs per block, it is the slower one)

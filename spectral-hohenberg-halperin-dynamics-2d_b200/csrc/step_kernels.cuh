@@ -118,6 +118,8 @@ struct StepPlan {
     int rp_canon;                  // 1: roles below are valid (else the generic product path)
     int rp_prep;                   // 1: rewrite (rho, jx), (jy, -) into (jx, jy), (vx, vy)
     int rp_jline, rp_vline;        // line of (jx, jy) and of (vx, vy) (-1: v = j / rho0)
+    int rp_pack;                   // one input slot and one output (psi -> u psi^3): a pair-line holds two row
+                                   // pairs of that slot instead of two slots of one row pair
     int rp_mode[kMaxOut];          // 0 coefficient form; 1 (vx, vy); 2 (jx vx, jy vy);
                                    // 3 c0 psi^3, 4 c1 psi vx, 5 c2 psi vy with psi = (psi_a, psi_b) one line
 };

@@ -632,6 +632,15 @@ __device__ __forceinline__ ZItem pz_load(const ulonglong2* i1m, size_t plane, in
     }
     return z;
 }
+// the same for a packed plan: slot 0 of two row pairs (rows ya, ya + 1 and yb, yb + 1) as the
+// two halves
+__device__ __forceinline__ ZItem pz_load_rows(const ulonglong2* i1m, int npy, int t, int ya, int yb) {
+    const ulonglong2* p = i1m + static_cast<size_t>(t) * npy;
+    ZItem z;
+    ld_stream2(p + ya, z.a0, z.a1);
+    ld_stream2(p + yb, z.b0, z.b1);
+    return z;
+}
 template <int NX>
 __device__ __forceinline__ void pz_store(ulonglong2* line, int t, const ZItem& z) {
 #pragma unroll
@@ -649,16 +658,20 @@ __device__ __forceinline__ void pz_store(ulonglong2* line, int t, const ZItem& z
 }
 
 // row pass, first part: Z staging of the nip input pair-lines of a block's RP row pairs (from
-// pair0) and their x-inverse in place (DIF stages in shared memory, a barrier after each)
+// pair0) and their x-inverse in place (DIF stages in shared memory, a barrier after each).  A
+// packed plan (P.rp_pack, one input slot) stages RP / 2 lines, line r holding row pairs 2r and
+// 2r + 1 as its two halves.
 template <int NX, int NT = kThreads, typename TW>
 __device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2* __restrict__ i1m, size_t plane, ulonglong2* inl, int nip,
                                             int pair0, TW tw) {
     constexpr int RP = kPairMaxN / NX;
     constexpr PPlan pp = PairPlan<NX>::c;
     const int npy = P.npy, hx = P.hx, hp = hx >> 1;
+    const bool pack = P.rp_pack;
+    const int nlr = pack ? RP / 2 : RP;  // staged lines per input pair-line slot
     // Z[k] = X0[k] + i X1[k] (rows y0, y0 + 1) with the Hermitian mirror Z[N - k]
     // = conj X0[k] + i conj X1[k]; kx = 0 keeps the real parts only
-    const int per_r = nip * hp, nz = RP * per_r;
+    const int per_r = nip * hp, nz = nlr * per_r;
     for (int e0 = threadIdx.x; e0 < nz; e0 += kZBatch * NT) {
         ZItem z[kZBatch];
 #pragma unroll
@@ -667,7 +680,8 @@ __device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2*
             if (e < nz) {
                 const int r = e / per_r, rem = e - r * per_r;
                 const int ip = rem / hp, t = rem - ip * hp;
-                z[u] = pz_load(i1m, plane, npy, P.n_in, ip, t, 2 * (pair0 + r));
+                z[u] = pack ? pz_load_rows(i1m, npy, t, 2 * (pair0 + 2 * r), 2 * (pair0 + 2 * r + 1))
+                            : pz_load(i1m, plane, npy, P.n_in, ip, t, 2 * (pair0 + r));
             }
         }
 #pragma unroll
@@ -682,12 +696,12 @@ __device__ __forceinline__ void prow_inputs(const StepPlan& P, const ulonglong2*
     }
     const int nzero = NX - 2 * hx + 1;  // k in [hx, NX - hx]
     const int per_z = nip * nzero;
-    for (int e = threadIdx.x; e < RP * per_z; e += NT) {
+    for (int e = threadIdx.x; e < nlr * per_z; e += NT) {
         const int l = e / nzero, k = hx + (e - l * nzero);
         st_pc(inl + static_cast<size_t>(l) * NX + psw(k), pc_zero());
     }
     __syncthreads();
-    pdif_range<NX, 0, pp.m, +1, NT>(inl, RP * nip, tw);
+    pdif_range<NX, 0, pp.m, +1, NT>(inl, nlr * nip, tw);
 }
 
 // row pass, last part: the untangling of transformed output pairs into I2.  One or two (nl)
@@ -705,7 +719,9 @@ __device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const O
     constexpr int RP = kPairMaxN / NX;
     const int npy = P.npy, hp = P.hx >> 1;
     const u64 HALF = f2_splat(0.5f);
-    const int per_q = RP * hp;
+    // packed plan: line r holds row pairs 2r and 2r + 1 of the one output (halves a and b)
+    const bool pack = P.rp_pack;
+    const int per_q = (pack ? RP / 2 : RP) * hp;
 #pragma unroll 2
     for (int e = threadIdx.x; e < nl * per_q; e += NT) {
         const bool q = e >= per_q;
@@ -713,7 +729,7 @@ __device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const O
         const int rem = q ? e - per_q : e;
         const int r = rem / hp, t = rem - r * hp;
         const ulonglong2* z = W.line + static_cast<size_t>(r) * W.stride;
-        const int y0 = 2 * (pair0 + r);
+        const int y0 = 2 * (pair0 + (pack ? 2 * r : r));
         u64 g0r[2], g0i[2], g1r[2], g1i[2];
 #pragma unroll
         for (int w = 0; w < 2; ++w) {
@@ -728,8 +744,8 @@ __device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const O
         ulonglong2* qa = i2m + static_cast<size_t>(W.oa) * plane + static_cast<size_t>(t) * npy + y0;
         st_stream2(qa, make_ulonglong2(f2_pack(f2_lo(g0r[0]), f2_lo(g0r[1])), f2_pack(f2_lo(g0i[0]), f2_lo(g0i[1]))),
                    make_ulonglong2(f2_pack(f2_lo(g1r[0]), f2_lo(g1r[1])), f2_pack(f2_lo(g1i[0]), f2_lo(g1i[1]))));
-        if (W.ob >= 0) {
-            ulonglong2* qb = i2m + static_cast<size_t>(W.ob) * plane + static_cast<size_t>(t) * npy + y0;
+        if (W.ob >= 0 || pack) {
+            ulonglong2* qb = pack ? qa + 2 : i2m + static_cast<size_t>(W.ob) * plane + static_cast<size_t>(t) * npy + y0;
             st_stream2(qb, make_ulonglong2(f2_pack(f2_hi(g0r[0]), f2_hi(g0r[1])), f2_pack(f2_hi(g0i[0]), f2_hi(g0i[1]))),
                        make_ulonglong2(f2_pack(f2_hi(g1r[0]), f2_hi(g1r[1])), f2_pack(f2_hi(g1i[0]), f2_hi(g1i[1]))));
         }
@@ -768,15 +784,16 @@ __global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const
 
     // 3. per output pair: products fused into the first DIT stage, the rest of
     //    the forward transform, then the untangling of the two rows (kx < Hx)
+    const int nl = P.rp_pack ? RP / 2 : RP;  // lines per input / output pair-line
     for (int pi = 0; pi < P.rp_n; ++pi) {
         const RowProduct R = row_product(P, pi, inv_rho0);
         auto product_canon = [&](int r, int p) -> PC { return row_product_canon<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, psw(p)); };
         auto product = [&](int r, int p) -> PC { return row_product_general<NX>(P, R, inl + static_cast<size_t>(r) * nip * NX, psw(p)); };
         const SmemIO wio{work, NX};
-        if (P.rp_canon) pstage_io<NX, pp.m - 1, -1, true>(RP, tw, product_canon, wio);
-        else pstage_io<NX, pp.m - 1, -1, true>(RP, tw, product, wio);
+        if (P.rp_canon) pstage_io<NX, pp.m - 1, -1, true>(nl, tw, product_canon, wio);
+        else pstage_io<NX, pp.m - 1, -1, true>(nl, tw, product, wio);
         __syncthreads();
-        pdit_range<NX, pp.m - 1, 0, -1>(work, RP, tw);
+        pdit_range<NX, pp.m - 1, 0, -1>(work, nl, tw);
         const OutLine W{work, static_cast<size_t>(NX), P.rp_a[pi], P.rp_b[pi]};
         prow_untangle<NX>(P, 1, W, W, i2m, plane, pair0);
         __syncthreads();

@@ -106,3 +106,26 @@ def test_split_row_pass_zero_density_graphs_and_family_switch():
         e.set_state(u)
         e.step(2)
         assert np.all(np.isfinite(e.get_state()))
+
+
+@pytest.mark.parametrize("grid", [(64, 64), (256, 128), (512, 512)])
+def test_packed_row_pairs_match_unpacked(grid):
+    """One input slot and one output (quiescent, N = 1): the pair-line row pass packs two row
+    pairs into one pair-line; its results equal the split row pass's, which transforms the same
+    lines unpacked, bit for bit (each half's arithmetic is the same operations)."""
+    import shhd_b200 as sb
+    text = script(grid=grid, length=(2.0 * grid[0], 2.0 * grid[1]), nop=1, dt=0.02, te="srk3/quiescent", cT=None, eta=0.0,
+                  zeta=0.0, nonlinear=None).replace("run 1", "fix 9 all noise on seed 3 kBT 0.01\nrun 1")
+    ocfg = so.parse_script(text)
+    u = random_state(ocfg, seed=17, amp=0.3)
+    out = {}
+    for fam in (1, 3):
+        with _engine(sb, text, fam, batch=2) as e:
+            for m in range(2):
+                e.set_state(u, member=m)
+            out[fam, "rhs"] = e.rhs()
+            e.step(4)
+            out[fam, "state"] = e.get_state(1)
+    assert np.array_equal(out[1, "rhs"], out[3, "rhs"])
+    assert np.array_equal(out[1, "state"], out[3, "state"])
+    assert so.rel_l2(out[1, "rhs"], so.Oracle(ocfg).rhs(u)) < TOL32
