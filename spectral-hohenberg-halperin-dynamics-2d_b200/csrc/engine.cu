@@ -830,7 +830,10 @@ void set_smem_attrs(shhd_engine* e) {
             });
             with_pair_size(e->P.npx, [&](auto fx) {
                 constexpr int FX = decltype(fx)::value;
-                if constexpr (FX != 0) setattr(reinterpret_cast<const void*>(prow_pass<FX>), e->smem_row);
+                if constexpr (FX != 0) {
+                    setattr(reinterpret_cast<const void*>(prow_pass<FX, 2>), e->smem_row);
+                    setattr(reinterpret_cast<const void*>(prow_pass<FX, 3>), e->smem_row);
+                }
             });
             return;
         }
@@ -904,6 +907,10 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
     check_cuda(cudaGetLastError(), "col_inverse launch");
 }
 
+// dynamic shared memory per block up to which three pair-line row-pass blocks share an SM (228 KB,
+// less 1 KB reserved per block)
+constexpr size_t kRowThreeBlockSmem = 75 * 1024;
+
 template <typename T>
 void launch_row(shhd_engine* e) {
     const StepPlan& P = e->P;
@@ -931,9 +938,13 @@ void launch_row(shhd_engine* e) {
                 constexpr int FX = decltype(fx)::value;
                 if constexpr (FX != 0) {
                     dim3 pg(P.npy / 2 / (kPairMaxN / FX), P.batch);
-                    prow_pass<FX><<<pg, kThreads, e->smem_row, e->stream>>>(P, e->members_dev, static_cast<const ulonglong2*>(e->i1),
-                                                                           static_cast<ulonglong2*>(e->i2), static_cast<const float2*>(e->tw_x),
-                                                                           e->rho0_dev, e->err_dev);
+                    // registers for three blocks per SM where shared memory holds three (one or two
+                    // input pair-lines on rows of <= 768 points), else for two
+                    const bool three = e->smem_row <= kRowThreeBlockSmem;
+                    auto kern = three ? prow_pass<FX, 3> : prow_pass<FX, 2>;
+                    kern<<<pg, kThreads, e->smem_row, e->stream>>>(P, e->members_dev, static_cast<const ulonglong2*>(e->i1),
+                                                                   static_cast<ulonglong2*>(e->i2), static_cast<const float2*>(e->tw_x),
+                                                                   e->rho0_dev, e->err_dev);
                 }
             });
             check_cuda(cudaGetLastError(), "row_pass launch");

@@ -752,8 +752,10 @@ __device__ __forceinline__ void prow_untangle(const StepPlan& P, int nl, const O
     }
 }
 
-template <int NX>
-__global__ void __launch_bounds__(kThreads, 2) prow_pass(const StepPlan P, const MemberInfo* __restrict__ members,
+// MINB: blocks per SM the registers are budgeted for (2; 3 where shared memory allows more blocks,
+// e.g. one input pair-line on rows of <= 768 points)
+template <int NX, int MINB = 2>
+__global__ void __launch_bounds__(kThreads, MINB) prow_pass(const StepPlan P, const MemberInfo* __restrict__ members,
                                                       const ulonglong2* __restrict__ i1, ulonglong2* __restrict__ i2,
                                                       const float2* __restrict__ tw, const double* __restrict__ rho0_member,
                                                       int* __restrict__ err) {
