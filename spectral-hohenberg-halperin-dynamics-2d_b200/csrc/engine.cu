@@ -767,6 +767,10 @@ void build_plan(shhd_engine* e) {
                 P.group_nout[g] = 0;
                 P.rho_split = 1;
             }
+            // per-mode arrays a block uses: acc0 (every group), acc1 (momentum: jy), acc2 (momentum
+            // with the density unsplit); shared memory for what this plan's groups use
+            const int narr = gm < 0 ? 1 : (P.rho_split ? 2 : 3);
+            e->smem_col = static_cast<size_t>(cp) * c.ny * 16 + static_cast<size_t>(narr) * cp * ((P.kyn + 7) & ~7) * 16;
             int k = 0;
             if (gm >= 0) P.group_order[k++] = gm;
             for (int g = 0; g < P.n_groups; ++g)
@@ -826,6 +830,7 @@ void set_smem_attrs(shhd_engine* e) {
                 if constexpr (FY != 0) {
                     setattr(reinterpret_cast<const void*>(pcol_inverse<FY>), e->smem_col_inv);
                     setattr(reinterpret_cast<const void*>(pcol_forward<FY>), e->smem_col);
+                    if constexpr (FY >= 384) setattr(reinterpret_cast<const void*>(pcol_forward<FY, 4>), e->smem_col);
                 }
             });
             with_pair_size(e->P.npx, [&](auto fx) {
@@ -910,6 +915,8 @@ void launch_col_inverse(shhd_engine* e, const void* state) {
 // dynamic shared memory per block up to which three pair-line row-pass blocks share an SM (228 KB,
 // less 1 KB reserved per block)
 constexpr size_t kRowThreeBlockSmem = 75 * 1024;
+// and four column-forward blocks
+constexpr size_t kColFourBlockSmem = 56 * 1024;
 
 template <typename T>
 void launch_row(shhd_engine* e) {
@@ -994,7 +1001,12 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
                 constexpr int FY = decltype(fy)::value;
                 if constexpr (FY != 0) {
                     dim3 pg(P.ntiles / (kPairMaxN / FY), P.n_groups, P.batch);
-                    pcol_forward<FY><<<pg, kThreads, e->smem_col, e->stream>>>(P, A, static_cast<const float2*>(e->tw_y));
+                    // four blocks per SM where the shared memory holds four (one per-mode array per
+                    // column: order-parameter groups only) on columns of >= 384 points
+                    auto kern = pcol_forward<FY>;
+                    if constexpr (FY >= 384)
+                        if (e->smem_col <= kColFourBlockSmem) kern = pcol_forward<FY, 4>;
+                    kern<<<pg, kThreads, e->smem_col, e->stream>>>(P, A, static_cast<const float2*>(e->tw_y));
                 }
             });
             check_cuda(cudaGetLastError(), "col_forward launch");

@@ -823,8 +823,10 @@ __device__ __forceinline__ int pmode_slot(int c, int j, int kyp) {
 template <int NY>
 __host__ __device__ constexpr int pcol_forward_blocks() { return NY >= 384 ? 3 : 2; }
 
-template <int NY>
-__global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forward(const StepPlan P, const StageArgs<float> A,
+// MINB: blocks per SM the registers are budgeted for (pcol_forward_blocks, or 4 where the plan's
+// per-mode arrays are one per column: order-parameter groups only)
+template <int NY, int MINB = pcol_forward_blocks<NY>()>
+__global__ void __launch_bounds__(kThreads, MINB) pcol_forward(const StepPlan P, const StageArgs<float> A,
                                                                                  const float2* __restrict__ tw) {
     constexpr int CP = kPairMaxN / NY;
     constexpr PPlan pp = PairPlan<NY>::c;
@@ -864,7 +866,7 @@ __global__ void __launch_bounds__(kThreads, pcol_forward_blocks<NY>()) pcol_forw
     }
     for (int e = threadIdx.x; e < CP * kyp; e += kThreads) {
         st_pc(acc0 + e, pc_zero());
-        st_pc(acc1 + e, pc_zero());
+        if (gkind == GROUP_MOMENTUM) st_pc(acc1 + e, pc_zero());  // the only group with a second array
     }
 
     // y-forward of each product field of the group (DIF; global tile loads fused
