@@ -740,7 +740,7 @@ void build_plan(shhd_engine* e) {
         const int cp = kPairMaxN / c.ny, rp = kPairMaxN / c.nx;
         const int nip = (P.n_in + 1) / 2;
         const size_t row_b = static_cast<size_t>(rp) * (nip + 1) * c.nx * 16;
-        const size_t col_b = static_cast<size_t>(cp) * c.ny * 16 + 3ull * cp * ((P.kyn + 7) & ~7) * 16;  // lines, 3 per-mode arrays
+        const size_t col_b = static_cast<size_t>(cp) * c.ny * 16 + 3ull * cp * ((P.kyn + 7) & ~7) * 16;  // lines, at most 3 per-mode arrays
         if ((P.hx / 2) % cp == 0 && (c.ny / 2) % rp == 0 && row_b <= smem_cap && col_b <= smem_cap) {
             e->pair_path = true;
             e->col_fixed = e->row_fixed = false;

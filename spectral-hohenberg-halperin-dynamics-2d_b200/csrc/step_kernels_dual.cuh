@@ -11,7 +11,7 @@
 // half as many barrier chains with every thread busy in their radix-8 stages.  Each output's
 // arithmetic is prow_pass's, operation for operation (v = j * (1 / rho), one rounding either way).
 // Shared memory per row pair: nip input pair-lines, one more work line and NX 1 / rho slots
-// (110.6 KB at 1536 points with three input pair-lines); registers at most 85 per thread.
+// (110.6 KB at 1536 points with three input pair-lines); 80 registers per thread.
 #pragma once
 
 #include "step_kernels_pair.cuh"

@@ -804,9 +804,10 @@ __global__ void __launch_bounds__(kThreads, MINB) prow_pass(const StepPlan P, co
 
 // ---------------------------------------------------------------------------
 // column forward + epilogue (grid: column-pair tiles x groups x batch).
-// Shared memory: CP work pair-lines, then three per-mode arrays [CP][Kp]
-// (accumulators / new values: psi or jx, jy, rho), two columns per element,
-// Kp = Ky rounded up to a multiple of 8.
+// Shared memory: CP work pair-lines, then per-mode arrays [CP][Kp] (accumulators / new
+// values), two columns per element, Kp = Ky rounded up to a multiple of 8: acc0 for every
+// group (psi, jx or rho), acc1 for the momentum group's jy, acc2 for its rho when the density
+// shares the momentum group; the launch provides the arrays the plan's groups use.
 // ---------------------------------------------------------------------------
 // slot of mode j in a column's per-mode row.  The last DIF stage (and the first stage of the
 // fused inverse) reaches the modes in digit-reversed order: at 384 points and up the eight
@@ -818,8 +819,9 @@ __device__ __forceinline__ int pmode_slot(int c, int j, int kyp) {
     return c * kyp + (NY >= 384 ? (j ^ ((j >> 3) & 7)) : j);
 }
 
-// blocks per SM the column forward is compiled for: its 74 KB of shared memory allow three, and at
-// 384 points and up the register budget of three (85) holds it without spilling more than 40 B
+// blocks per SM the column forward is compiled for: its 41-74 KB of shared memory allow three,
+// and at 384 points and up the register budget of three (80) holds it without spilling more than
+// 40 B
 template <int NY>
 __host__ __device__ constexpr int pcol_forward_blocks() { return NY >= 384 ? 3 : 2; }
 
