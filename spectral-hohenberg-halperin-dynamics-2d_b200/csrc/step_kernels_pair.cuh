@@ -443,7 +443,7 @@ struct RowProduct {
     bool need_j, use_psi;
     float inv_rho0;
     u64 IR0;
-    u64 C[8];
+    int pi;                        // output pair: coefficient q is P.rp_coef[pi][q] (rp_coef below)
 };
 
 __device__ __forceinline__ RowProduct row_product(const StepPlan& P, int pi, float inv_rho0) {
@@ -456,8 +456,7 @@ __device__ __forceinline__ RowProduct row_product(const StepPlan& P, int pi, flo
     R.psa = (R.ka == OUT_MU || R.ka == OUT_PSIVX || R.ka == OUT_PSIVY) ? P.in_slot[1 + R.aa] : -1;
     R.psb = (R.kb == OUT_MU || R.kb == OUT_PSIVX || R.kb == OUT_PSIVY) ? P.in_slot[1 + R.ab] : -1;
     R.need_j = (R.ka != OUT_MU) || (R.kb >= 0 && R.kb != OUT_MU);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) R.C[q] = f2_pack(P.rp_coef[pi][q][0], P.rp_coef[pi][q][1]);
+    R.pi = pi;
     R.use_psi = R.psa >= 0 || R.psb >= 0;
     R.mode = P.rp_mode[pi];
     R.inv_rho0 = inv_rho0;
@@ -481,7 +480,8 @@ __device__ __forceinline__ JV row_jv(const StepPlan& P, const RowProduct& R, con
 // (read where a product needs them)
 template <int NX, typename GetJV>
 __device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProduct& R, const ulonglong2* in, int sp, GetJV&& get_jv) {
-    const u64* C = R.C;
+    // coefficient q of the pair (A, B), read where a product uses it
+    auto C = [&](int q) { return f2_pack(P.rp_coef[R.pi][q][0], P.rp_coef[R.pi][q][1]); };
     const int mode = R.mode;
     if (mode != 0) {  // outputs that are elementwise products of whole lines
         if (mode == 1 || mode == 2) {
@@ -492,14 +492,14 @@ __device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProd
         }
         const ulonglong2 S = in[(R.psa >> 1) * NX + sp];
         if (mode == 3) {
-            const u64 q0 = f2_mul(f2_mul(S.x, S.x), f2_mul(S.x, C[0]));
-            const u64 q1 = f2_mul(f2_mul(S.y, S.y), f2_mul(S.y, C[0]));
+            const u64 q0 = f2_mul(f2_mul(S.x, S.x), f2_mul(S.x, C(0)));
+            const u64 q1 = f2_mul(f2_mul(S.y, S.y), f2_mul(S.y, C(0)));
             return PC{q0, q1};
         }
         const ulonglong2 V = get_jv().V;
         const u64 v0 = mode == 4 ? f2_splat(f2_lo(V.x)) : f2_splat(f2_hi(V.x));
         const u64 v1 = mode == 4 ? f2_splat(f2_lo(V.y)) : f2_splat(f2_hi(V.y));
-        const u64 cc = mode == 4 ? C[1] : C[2];
+        const u64 cc = C(mode == 4 ? 1 : 2);
         return PC{f2_mul(f2_mul(S.x, cc), v0), f2_mul(f2_mul(S.y, cc), v1)};
     }
     u64 out[2] = {0ull, 0ull};
@@ -517,13 +517,13 @@ __device__ __forceinline__ PC row_product_canon(const StepPlan& P, const RowProd
     for (int row = 0; row < 2; ++row) {
         const u64 VX = f2_splat(vxr[row]), VY = f2_splat(vyr[row]);
         const u64 JX = f2_splat(jxr[row]), JY = f2_splat(jyr[row]);
-        u64 o = f2_fma(C[4], VY, f2_mul(C[3], VX));                          // c3 vx + c4 vy
-        o = f2_fma(f2_mul(C[5], JX), VX, o);                                 // + c5 jx vx
-        o = f2_fma(f2_fma(C[6], JX, f2_mul(C[7], JY)), VY, o);               // + (c6 jx + c7 jy) vy
+        u64 o = f2_fma(C(4), VY, f2_mul(C(3), VX));                          // c3 vx + c4 vy
+        o = f2_fma(f2_mul(C(5), JX), VX, o);                                 // + c5 jx vx
+        o = f2_fma(f2_fma(C(6), JX, f2_mul(C(7), JY)), VY, o);               // + (c6 jx + c7 jy) vy
         if (R.use_psi) {
             const u64 PS = row ? f2_pack(pa.y, pb.y) : f2_pack(pa.x, pb.x);
-            u64 in2 = f2_fma(C[1], VX, f2_mul(C[2], VY));                    // c1 vx + c2 vy
-            in2 = f2_fma(f2_mul(C[0], PS), PS, in2);                         // + c0 psi^2
+            u64 in2 = f2_fma(C(1), VX, f2_mul(C(2), VY));                    // c1 vx + c2 vy
+            in2 = f2_fma(f2_mul(C(0), PS), PS, in2);                         // + c0 psi^2
             o = f2_fma(PS, in2, o);                                          // psi (...)
         }
         out[row] = o;
