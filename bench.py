@@ -326,9 +326,10 @@ def run_b200(args):
     eng.set_state(u0)
     stream = torch.cuda.ExternalStream(eng.stream)
     # kernel family and graph replay chosen by timing them on this state (state restored), or the
-    # family given on the command line (profiling one family)
+    # family given on the command line (profiling one family); trials of 10 steps, the graph chunk
+    # a long run would replay
     if args.family is None:
-        tuning = eng.autotune(3)
+        tuning = eng.autotune(10)
     else:
         eng.set_family(args.family)
         tuning = {"family": sb.FAMILY_NAMES[eng.family], "graph_chunk": 0, "forced": True}
