@@ -647,7 +647,7 @@ def run_other_configs(sb, initial_state, torch, world):
         cfg.precision = prec
         eng = sb.Engine(cfg)
         initial_state_device(eng, text)
-        tuning = eng.autotune(3) if nsteps > 50 else None
+        tuning = eng.autotune(10) if nsteps > 50 else None
         eng.step(3)
         stream = torch.cuda.ExternalStream(eng.stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
