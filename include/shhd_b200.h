@@ -241,8 +241,7 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
 /* Select the kernel family (no reference counterpart): -1 the default choice
- * (4 where valid on 1536-point compute rows, else 1 where valid, else 0), 0
- * never the pair-line kernels,
+ * (1 where valid, else 0), 0 never the pair-line kernels,
  * 1 pair-line where valid, 2 pair-line with the
  * register-resident row pass where valid, 3 pair-line with the split row pass
  * where valid, 4 pair-line with the two-pair row pass where valid (2, 3 and 4

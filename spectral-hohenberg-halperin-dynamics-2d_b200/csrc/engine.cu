@@ -236,7 +236,7 @@ struct shhd_engine {
     int row_nt = 256;             // its threads per block (512: two line groups, for lines of 48 KB or more)
     bool pair_path = false;       // FP32 pair-line kernels (compile-time sizes up to 1536)
     bool reg_row = false;         // register-resident row pass on 1536-point rows (pair-line layout)
-    int family_override = -1;     // -1 choose (4 where valid on 1536-point rows, else 1, else 0), 0 never the pair-line kernels, 1 pair-line where valid,
+    int family_override = -1;     // -1 choose (1 where valid, else 0), 0 never the pair-line kernels, 1 pair-line where valid,
                                   // 2 pair-line with the register-resident row pass where valid,
                                   // 3 pair-line with the split row pass where valid,
                                   // 4 pair-line with the two-pair row pass where valid
@@ -782,12 +782,12 @@ void build_plan(shhd_engine* e) {
     // split row pass (every pair-line size)
     e->split_row = e->pair_path && e->family_override == 3 && split_row_supported(c.nx) && c.ny % 2 == 0;
     if (e->split_row) P.rp_pack = 0;  // the split kernels transform unpacked lines
-    // row pass over two output pairs at a time (compressible canonical layouts); the default on
-    // 1536-point rows, where it beats the pair-line row pass (105 against 113 us at 1024^2, N = 2;
-    // on shorter rows, several row pairs per block, it is the slower one)
+    // row pass over two output pairs at a time (compressible canonical layouts), when selected:
+    // level with the pair-line row pass on 1536-point rows (102.5 against 103 us at 1024^2, N = 2;
+    // 63 against 56 us with N = 0, where the pair-line kernel runs three blocks per SM), slower on
+    // shorter rows, so the default stays the pair-line row pass and the autotuner times both
     e->dual_row = false;
-    const bool dual_wanted = e->family_override == 4 || (e->family_override == -1 && c.nx == kPairMaxN);
-    if (e->pair_path && dual_wanted && c.ny % 2 == 0 && dual_row_supported(P)) {
+    if (e->pair_path && e->family_override == 4 && c.ny % 2 == 0 && dual_row_supported(P)) {
         e->smem_dual = dual_row_smem_bytes(P);
         e->dual_row = e->smem_dual <= smem_cap;
     }
