@@ -236,8 +236,12 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * pass split into an inverse and a forward kernel over a physical-row buffer
  * (allocated while the family is selected); family 4 the pair-line family
  * whose row pass transforms two output pairs at a time, valid for compressible
- * dynamics whose last two input pair-lines are (rho, jx), (jy, -).  Allocates
- * a temporary copy of the state. */
+ * dynamics whose last two input pair-lines are (rho, jx), (jy, -).  The
+ * families are timed at the rule's launch shapes; then, with the chosen family
+ * and chunk, the launch shapes of its pair-line kernels where shared memory
+ * leaves a choice (shhd_engine_set_launch_shape: row pass at 2 or 3 blocks per
+ * SM, column forward at 3 or 4), and the fastest is kept (read it back with
+ * shhd_engine_launch_shape).  Allocates a temporary copy of the state. */
 int shhd_engine_autotune(shhd_engine* engine, int trial_steps, int* family, int* graph_chunk, double* ms_per_step);
 
 /* Select the kernel family (no reference counterpart): -1 the default choice
@@ -251,6 +255,22 @@ int shhd_engine_set_family(shhd_engine* engine, int family);
 
 /* The family the engine launches: 4, 3, 2, 1 or 0 as above. */
 int shhd_engine_family(const shhd_engine* engine);
+
+/* Launch shapes of the pair-line stage kernels (no reference counterpart): the
+ * row pass compiled with registers for row_blocks blocks per SM (2 or 3), the
+ * column forward on columns of 384 points and more for col_blocks (3 or 4);
+ * 0 keeps the rule (row pass: 3 where shared memory holds three blocks;
+ * column forward: 4 where it holds four, on 1536-point columns and for plans
+ * without a momentum group).  Where shared memory holds fewer blocks than the
+ * registers are budgeted for, fewer run per SM; results do not depend on the
+ * shape.  Kept across shhd_engine_set_family; the autotuner sets its choice.
+ * Drops captured graphs. */
+int shhd_engine_set_launch_shape(shhd_engine* engine, int row_blocks, int col_blocks);
+
+/* The launch shapes the engine uses: *row_blocks 2 or 3 (0 when the row kernel
+ * is not the pair-line row pass), *col_blocks 2, 3 or 4 (0 without pair-line
+ * kernels); either pointer may be NULL. */
+int shhd_engine_launch_shape(const shhd_engine* engine, int* row_blocks, int* col_blocks);
 
 /* Initial conditions generated on the device: the reference's `set` styles
  * (initial_condition_*.cc), one field of one member per call, every active

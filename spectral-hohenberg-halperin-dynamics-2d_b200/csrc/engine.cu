@@ -240,6 +240,8 @@ struct shhd_engine {
                                   // 2 pair-line with the register-resident row pass where valid,
                                   // 3 pair-line with the split row pass where valid,
                                   // 4 pair-line with the two-pair row pass where valid
+    int row_blocks = 0;           // pair-line row pass compiled for 2 or 3 blocks per SM (0: by its shared memory)
+    int col_blocks = 0;           // pair-line column forward on >= 384-point columns for 3 or 4 blocks per SM (0: by rule)
     void* tw_reg = nullptr;       // twiddles of the register-resident transforms (FP32 engines with 1536-point rows)
     bool split_row = false;       // pair-line row pass split in two kernels over a physical-row buffer (family 3)
     bool dual_row = false;        // pair-line row pass over two output pairs at a time (family 4)
@@ -918,6 +920,31 @@ constexpr size_t kRowThreeBlockSmem = 75 * 1024;
 // and four column-forward blocks
 constexpr size_t kColFourBlockSmem = 56 * 1024;
 
+// launch shapes of the pair-line stage kernels: the variant whose registers are budgeted for
+// three row-pass blocks per SM (else two), and for four column-forward blocks (else three), each
+// as set (shhd_engine_set_launch_shape, the autotuner) or by rule.  The row rule takes three
+// where shared memory holds three (one or two input pair-lines on rows of <= 768 points); the
+// column rule four where shared memory holds four, on 1536-point columns and for
+// order-parameter-only plans (384 and 768 points with a momentum group run faster at three: 66
+// against 69 us and 58 against 62 us)
+bool row_three_blocks(const shhd_engine* e) {
+    return e->row_blocks ? e->row_blocks == 3 : e->smem_row <= kRowThreeBlockSmem;
+}
+
+bool col_four_blocks(const shhd_engine* e) {
+    const StepPlan& P = e->P;
+    if (P.npy < 384) return false;
+    if (e->col_blocks) return e->col_blocks == 4;
+    bool momentum = false;
+    for (int g = 0; g < P.n_groups; ++g) momentum |= P.group_kind[g] == GROUP_MOMENTUM;
+    return e->smem_col <= kColFourBlockSmem && (P.npy == kPairMaxN || !momentum);
+}
+
+// the pair-line row pass (not the split, two-pair or register one) is the row kernel
+bool pair_line_row(const shhd_engine* e) {
+    return e->pair_path && !e->split_row && !e->dual_row && !e->reg_row && e->P.n_out > 0;
+}
+
 template <typename T>
 void launch_row(shhd_engine* e) {
     const StepPlan& P = e->P;
@@ -945,10 +972,7 @@ void launch_row(shhd_engine* e) {
                 constexpr int FX = decltype(fx)::value;
                 if constexpr (FX != 0) {
                     dim3 pg(P.npy / 2 / (kPairMaxN / FX), P.batch);
-                    // registers for three blocks per SM where shared memory holds three (one or two
-                    // input pair-lines on rows of <= 768 points), else for two
-                    const bool three = e->smem_row <= kRowThreeBlockSmem;
-                    auto kern = three ? prow_pass<FX, 3> : prow_pass<FX, 2>;
+                    auto kern = row_three_blocks(e) ? prow_pass<FX, 3> : prow_pass<FX, 2>;
                     kern<<<pg, kThreads, e->smem_row, e->stream>>>(P, e->members_dev, static_cast<const ulonglong2*>(e->i1),
                                                                    static_cast<ulonglong2*>(e->i2), static_cast<const float2*>(e->tw_x),
                                                                    e->rho0_dev, e->err_dev);
@@ -1001,14 +1025,9 @@ void launch_col_forward(shhd_engine* e, const StageArgs<T>& A) {
                 constexpr int FY = decltype(fy)::value;
                 if constexpr (FY != 0) {
                     dim3 pg(P.ntiles / (kPairMaxN / FY), P.n_groups, P.batch);
-                    // four blocks per SM where the shared memory holds four, on 1536-point columns
-                    // and for order-parameter-only plans (384 and 768 points with a momentum group
-                    // run faster at three: 66 against 69 us and 58 against 62 us)
                     auto kern = pcol_forward<FY>;
                     if constexpr (FY >= 384) {
-                        bool momentum = false;
-                        for (int g = 0; g < P.n_groups; ++g) momentum |= P.group_kind[g] == GROUP_MOMENTUM;
-                        if (e->smem_col <= kColFourBlockSmem && (FY == kPairMaxN || !momentum)) kern = pcol_forward<FY, 4>;
+                        if (col_four_blocks(e)) kern = pcol_forward<FY, 4>;
                     }
                     kern<<<pg, kThreads, e->smem_col, e->stream>>>(P, A, static_cast<const float2*>(e->tw_y));
                 }
@@ -1786,30 +1805,56 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
         }
         int chunk_trial = trial_steps;
         if (e->cfg.integrator == SHHD_EULER && chunk_trial % 2) ++chunk_trial;
+        // ms per step of chunk_trial steps after as many untimed ones (warm-up and capture), from the saved state
+        auto trial = [&] {
+            drop_graphs(e);
+            enqueue(e, chunk_trial);
+            check_cuda(cudaEventRecord(a, e->stream), "cudaEventRecord");
+            enqueue(e, chunk_trial);
+            check_cuda(cudaEventRecord(b, e->stream), "cudaEventRecord");
+            sync_and_check(e);
+            float ms = 0.f;
+            check_cuda(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
+            restore();
+            return ms / chunk_trial;
+        };
+        // families at the rule's launch shapes
+        e->row_blocks = e->col_blocks = 0;
         double best = 1e300;
         int best_family = 0, best_chunk = 0, idx = 0;
         for (int fam : families) {
             apply_family<T>(e, fam);
             for (int chunk : {0, chunk_trial}) {
                 e->graph_chunk = chunk;
-                drop_graphs(e);
-                enqueue(e, chunk_trial);  // warm-up (and capture)
-                check_cuda(cudaEventRecord(a, e->stream), "cudaEventRecord");
-                enqueue(e, chunk_trial);
-                check_cuda(cudaEventRecord(b, e->stream), "cudaEventRecord");
-                sync_and_check(e);
-                float ms = 0.f;
-                check_cuda(cudaEventElapsedTime(&ms, a, b), "cudaEventElapsedTime");
-                const double per = ms / chunk_trial;
+                const double per = trial();
                 if (ms_out) ms_out[idx] = per;
                 ++idx;
                 if (per < best) { best = per; best_family = fam; best_chunk = chunk; }
-                restore();
             }
         }
         drop_graphs(e);
         apply_family<T>(e, best_family);
         e->graph_chunk = best_chunk;
+        // then the launch shapes of the chosen family's pair-line kernels: registers for three or
+        // two row-pass blocks per SM where shared memory holds three, for four or three
+        // column-forward blocks on >= 384-point columns where it holds four
+        std::vector<int> rows = {0}, cols = {0};
+        if (pair_line_row(e) && e->smem_row <= kRowThreeBlockSmem) rows = {2, 3};
+        if (e->pair_path && e->P.n_groups > 0 && e->P.npy >= 384 && e->smem_col <= kColFourBlockSmem) cols = {3, 4};
+        if (rows.size() * cols.size() > 1) {
+            double best_shape = 1e300;
+            int best_row = 0, best_col = 0;
+            for (int r : rows)
+                for (int c : cols) {
+                    e->row_blocks = r;
+                    e->col_blocks = c;
+                    const double per = trial();
+                    if (per < best_shape) { best_shape = per; best_row = r; best_col = c; }
+                }
+            e->row_blocks = best_row;
+            e->col_blocks = best_col;
+            drop_graphs(e);
+        }
         if (family_out) *family_out = best_family;
         if (chunk_out) *chunk_out = best_chunk;
     } catch (...) {
@@ -2503,6 +2548,28 @@ int shhd_engine_set_family(shhd_engine* e, int family) {
 int shhd_engine_family(const shhd_engine* e) {
     if (!e) return -1;
     return e->dual_row ? 4 : (e->split_row ? 3 : (e->reg_row ? 2 : (e->pair_path ? 1 : 0)));
+}
+
+int shhd_engine_set_launch_shape(shhd_engine* e, int row_blocks, int col_blocks) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (row_blocks != 0 && row_blocks != 2 && row_blocks != 3) throw Failure(SHHD_EINVAL, "row-pass blocks per SM must be 0, 2 or 3");
+        if (col_blocks != 0 && col_blocks != 3 && col_blocks != 4)
+            throw Failure(SHHD_EINVAL, "column-forward blocks per SM must be 0, 3 or 4");
+        check_cuda(cudaSetDevice(e->device), "cudaSetDevice");
+        check_cuda(cudaStreamSynchronize(e->stream), "stream synchronize");
+        drop_graphs(e);
+        e->row_blocks = row_blocks;
+        e->col_blocks = col_blocks;
+    });
+}
+
+int shhd_engine_launch_shape(const shhd_engine* e, int* row_blocks, int* col_blocks) {
+    return guarded([&] {
+        if (!e) throw Failure(SHHD_EINVAL, "null engine");
+        if (row_blocks) *row_blocks = pair_line_row(e) ? (row_three_blocks(e) ? 3 : 2) : 0;
+        if (col_blocks) *col_blocks = e->pair_path && e->P.n_groups > 0 ? (e->P.npy >= 384 ? (col_four_blocks(e) ? 4 : 3) : 2) : 0;
+    });
 }
 
 int shhd_engine_set_graph_chunk(shhd_engine* e, int chunk) {

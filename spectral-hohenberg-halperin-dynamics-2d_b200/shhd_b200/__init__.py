@@ -16,7 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from typing import Optional, Sequence
+from typing import Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -129,7 +129,7 @@ EXPORTED = (
     "shhd_engine_set_initial_field", "shhd_engine_check_transverse", "shhd_engine_energies",
     "shhd_engine_flux0_enable", "shhd_engine_flux0_read", "shhd_engine_profile_line", "shhd_engine_profile_velocity",
     "shhd_engine_flux_line_enable", "shhd_engine_flux_line_read", "shhd_engine_flux_tap_schedule",
-    "shhd_engine_set_family", "shhd_engine_family",
+    "shhd_engine_set_family", "shhd_engine_family", "shhd_engine_set_launch_shape", "shhd_engine_launch_shape",
     "shhd_free_energy_plugin_count", "shhd_free_energy_plugin_name", "shhd_free_energy_plugin_key",
 )
 
@@ -174,6 +174,8 @@ def _load() -> ctypes.CDLL:
     lib.shhd_engine_autotune.argtypes = [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), dp]
     lib.shhd_engine_set_family.argtypes = [vp, i]
     lib.shhd_engine_family.argtypes = [vp]
+    lib.shhd_engine_set_launch_shape.argtypes = [vp, i, i]
+    lib.shhd_engine_launch_shape.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.shhd_free_energy_plugin_count.argtypes = []
     lib.shhd_free_energy_plugin_name.argtypes = [i]
     lib.shhd_free_energy_plugin_name.restype = ctypes.c_char_p
@@ -329,12 +331,15 @@ class Engine:
         return out.reshape(self.cfg.active_nx // 2, self.cfg.active_ny - 1), int(cnt.value)
 
     def autotune(self, trial_steps: int = 3) -> dict:
-        """Time the valid kernel families x {direct, graph} on the current state; keep the fastest."""
+        """Time the valid kernel families x {direct, graph} on the current state, then the launch
+        shapes of the chosen family's pair-line kernels; keep the fastest."""
         fam, chunk = ctypes.c_int(), ctypes.c_int()
         ms = np.full(10, np.nan)
         _check(lib.shhd_engine_autotune(self._h, int(trial_steps), ctypes.byref(fam), ctypes.byref(chunk), _dptr(ms)))
+        row, col = self.launch_shape
         return {"family": FAMILY_NAMES[fam.value], "graph_chunk": chunk.value,
-                "ms_per_step": [None if np.isnan(x) else float(x) for x in ms]}
+                "ms_per_step": [None if np.isnan(x) else float(x) for x in ms],
+                "launch_shape": {"row_blocks": row, "col_blocks": col}}
 
     def set_family(self, family: int) -> None:
         """Kernel family: -1 default, 0 single-line, 1 pair-line, 2 pair-line with the register row pass,
@@ -344,6 +349,18 @@ class Engine:
     @property
     def family(self) -> int:
         return int(lib.shhd_engine_family(self._h))
+
+    def set_launch_shape(self, row_blocks: int = 0, col_blocks: int = 0) -> None:
+        """Blocks per SM the pair-line row pass (2 or 3) and column forward (3 or 4) are compiled
+        for; 0 keeps the rule."""
+        _check(lib.shhd_engine_set_launch_shape(self._h, int(row_blocks), int(col_blocks)))
+
+    @property
+    def launch_shape(self) -> Tuple[int, int]:
+        """(row-pass, column-forward) blocks per SM in use; 0 where the kernel is not a pair-line one."""
+        r, c = ctypes.c_int(), ctypes.c_int()
+        _check(lib.shhd_engine_launch_shape(self._h, ctypes.byref(r), ctypes.byref(c)))
+        return r.value, c.value
 
     def set_gaussian_field(self, member: int, field: int, seed: int, channel: int, mean: float, s0: float,
                            c0: float = 1.0, c2: float = 0.0, c4: float = 0.0) -> None:

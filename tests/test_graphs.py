@@ -106,3 +106,57 @@ def test_autotune_restores_state_and_keeps_results(precision):
         assert np.array_equal(e.get_state(), before)
         e.step(4)
         assert so.rel_l2(e.get_state(), ref) < (1e-12 if precision == 0 else 1e-5)
+
+
+SHAPES = {
+    # 384-point rows and columns, one input pair-line, no momentum group: both kernels have a choice
+    "quiescent_384": script(grid=(256, 256), length=(512.0, 512.0), nop=1, dt=0.02, te="srk3/quiescent", cT=None,
+                            eta=0.0, zeta=0.0, nonlinear=None, noise="kBT 0.05 seed 5"),
+    # 768-point rows and columns, compressible N = 2 (three input pair-lines, a momentum group)
+    "compressible_768": script(grid=(512, 512), length=(1024.0, 1024.0), nop=2, dt=0.01, noise="kBT 0.001 seed 3"),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SHAPES))
+def test_launch_shapes_give_identical_results(name):
+    """Every launch shape of the pair-line kernels runs the same code at another register budget:
+    the RHS and a noisy trajectory agree bit for bit with the rule's shape."""
+    import shhd_b200 as sb
+    text = SHAPES[name]
+    u0 = random_state(so.parse_script(text), seed=31)
+    out = {}
+    for shape in ((0, 0), (2, 3), (2, 4), (3, 3), (3, 4)):
+        with _engine(sb, text, sb.FP32) as e:
+            assert e.family == 1
+            e.set_launch_shape(*shape)
+            row, col = e.launch_shape
+            if shape != (0, 0):
+                assert (row, col) == shape
+            e.set_state(u0)
+            rhs = e.rhs()
+            e.step(4)
+            out[shape] = (rhs, e.get_state())
+    for shape, (rhs, state) in out.items():
+        assert np.all(np.isfinite(state))
+        assert np.array_equal(rhs, out[0, 0][0]), (name, shape)
+        assert np.array_equal(state, out[0, 0][1]), (name, shape)
+
+
+def test_launch_shape_rules_and_autotune():
+    import shhd_b200 as sb
+    with _engine(sb, SHAPES["quiescent_384"], sb.FP32) as e:
+        assert e.launch_shape == (3, 4)          # 1 input pair-line, no momentum group: both at the higher count
+        with pytest.raises(sb.ShhdError) as ei:
+            e.set_launch_shape(4, 0)
+        assert ei.value.code == sb.SHHD_EINVAL
+        with pytest.raises(sb.ShhdError):
+            e.set_launch_shape(0, 2)
+        e.set_state(random_state(so.parse_script(SHAPES["quiescent_384"]), seed=32))
+        choice = e.autotune(2)
+        assert e.launch_shape == (choice["launch_shape"]["row_blocks"], choice["launch_shape"]["col_blocks"])
+        if choice["family"] == "pair-line":
+            assert e.launch_shape[0] in (2, 3) and e.launch_shape[1] in (3, 4)
+    with _engine(sb, SHAPES["compressible_768"], sb.FP32) as e:
+        assert e.launch_shape[1] == 3            # momentum group on 768-point columns: three
+    with _engine(sb, SRK3, sb.FP64) as e:
+        assert e.launch_shape == (0, 0)          # no pair-line kernels
