@@ -445,7 +445,9 @@ const void* shhd_engine_state_device(const shhd_engine* engine);
  * grid with 3/2 padding, two order parameters and advection in FP64).  Each
  * call looks up the current device's address of the array.  The call is
  * synchronous: it waits on `stream` for its input checks and again for its
- * result before returning.  All calls share the one array, which keeps the
+ * result before returning, so it cannot be recorded into a CUDA graph; on a
+ * stream that is being captured it returns SHHD_EINVAL and enqueues nothing.
+ * All calls share the one array, which keeps the
  * last call's contents, so calls whose work overlaps on the GPU (other
  * streams or host threads) race: serialise them. */
 #define SHHD_NOALLOC_SCRATCH_BYTES (32u << 20)

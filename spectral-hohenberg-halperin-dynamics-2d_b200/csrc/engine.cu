@@ -2771,9 +2771,14 @@ extern "C" int shhd_rhs_noalloc(const shhd_config* cfg, const double* state_dev,
         if (n_doubles != ref_doubles(&e))
             throw Failure(SHHD_EINVAL, "state size mismatch: expected " + std::to_string(ref_doubles(&e)) + " doubles");
         check_cuda(cudaGetDevice(&e.device), "cudaGetDevice");
+        e.stream = static_cast<cudaStream_t>(stream);
+        // the call waits on its stream and reads results back: it cannot be recorded into a graph
+        cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+        check_cuda(cudaStreamIsCapturing(e.stream, &capture), "cudaStreamIsCapturing");
+        if (capture != cudaStreamCaptureStatusNone)
+            throw Failure(SHHD_EINVAL, "shhd_rhs_noalloc is synchronous and cannot run on a stream that is being captured");
         check_device_buffer(state_dev, e.device, "state_dev");
         check_device_buffer(rhs_dev, e.device, "rhs_dev");
-        e.stream = static_cast<cudaStream_t>(stream);
         unsigned char* base = noalloc_base();
         if (e.fp32) {
             set_smem_attrs<float>(&e);

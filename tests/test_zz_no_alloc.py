@@ -131,3 +131,30 @@ def test_noalloc_rejects_what_it_cannot_hold():
     rc = sb.lib.shhd_rhs_noalloc(ctypes.byref(c2), u.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p), u.size, None)
     assert rc == sb.SHHD_EINVAL
     assert "device memory" in sb.lib.shhd_last_error().decode() or "CUDA pointer" in sb.lib.shhd_last_error().decode()
+
+
+@pytest.mark.filterwarnings("ignore:The CUDA Graph is empty")
+def test_noalloc_refuses_a_capturing_stream():
+    """The call is synchronous: on a stream under graph capture it returns SHHD_EINVAL before
+    enqueuing anything, and the capture ends normally."""
+    import torch
+    import shhd_b200 as sb
+    text = script(**CASES[0])
+    cfg = sb.config_from_script(text)
+    state = random_state(so.parse_script(text), seed=71)
+    flat = np.ascontiguousarray(state, dtype=np.complex128).view(np.float64).ravel()
+    dev_in = torch.from_numpy(flat.copy()).to("cuda")
+    dev_out = torch.zeros_like(dev_in)
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    c = cfg.copy()
+    with torch.cuda.graph(graph, stream=side):
+        rc = sb.lib.shhd_rhs_noalloc(ctypes.byref(c), ctypes.c_void_p(dev_in.data_ptr()), ctypes.c_void_p(dev_out.data_ptr()),
+                                     flat.size, ctypes.c_void_p(side.cuda_stream))
+    assert rc == sb.SHHD_EINVAL
+    assert "cannot run on a stream that is being captured" in sb.lib.shhd_last_error().decode()
+    del graph
+    # the entry point still works afterwards
+    got = _noalloc(sb, torch, cfg, state)
+    assert so.rel_l2(got, so.Oracle(so.parse_script(text)).rhs(state)) < TOL64
