@@ -1142,8 +1142,7 @@ StageArgs<T> stage_args(shhd_engine* e, const void* cur, const void* base, void*
 template <typename T>
 void launch_gk_tap(shhd_engine* e, const void* cur, int step_off, double weight, int first, int last) {
     if (!e->gk_on) return;
-    const int warps = e->P.batch * e->gk.nmodes;
-    const dim3 g(static_cast<unsigned>((static_cast<long long>(warps) * 32 + kThreads - 1) / kThreads));
+    const dim3 g(static_cast<unsigned>(e->gk.nmodes), static_cast<unsigned>(e->P.batch));
     gk_tap_kernel<T><<<g, kThreads, 0, e->stream>>>(e->P, e->gk, e->members_dev, static_cast<const T*>(e->i2), static_cast<const cplx<T>*>(cur),
                                                     e->rho0_dev, e->step_dev, step_off, weight, first, last, e->cfg.dt);
     check_cuda(cudaGetLastError(), "gk_tap launch");

@@ -889,9 +889,10 @@ __global__ void __launch_bounds__(kThreads) structure_factor_kernel(const StepPl
 // flux pi_xy of each RHS evaluation at the selected modes, weighted by the
 // stage's flux weight into the step flux; after the last stage the first
 // draw's stochastic flux / sqrt(dt) is added and the block integral and its
-// normalised square are accumulated, all in FP64.  One warp per (member, mode);
-// the y-transform of the x-transformed product planes at the mode is a direct
-// DFT over the column (table w^n = e^{-2 pi i n / Np_y}).
+// normalised square are accumulated, all in FP64.  One block per (mode, member):
+// the y-transforms of the x-transformed product planes at the mode are direct
+// DFTs over the column (table w^n = e^{-2 pi i n / Np_y}), every plane in one
+// pass, each thread a strided set of rows, then a fixed-order block sum.
 // ---------------------------------------------------------------------------
 struct GkArgs {
     const int2* modes;          // (gx, ky) per selected mode
@@ -943,9 +944,22 @@ __device__ __forceinline__ double2 column_dft(const StepPlan& P, const double2* 
     return make_double2(re, im);
 }
 
+// one row's term of a column DFT: element y of column (t, w) of an I2 plane times the twiddle
 template <typename T>
-__device__ __forceinline__ double2 gk_column_dft(const StepPlan& P, const GkArgs& G, const T* plane, int gx, int ky) {
-    return column_dft<T>(P, G.wtab, G.pair_layout, plane, gx, ky);
+__device__ __forceinline__ void gk_dft_term(const T* plane, int pair_layout, int W, int npy, int t, int w, int y, double2 tw, double& re,
+                                            double& im) {
+    T xr, xi;
+    if (pair_layout) {
+        const T* e = plane + 4 * (static_cast<size_t>(t) * npy + y);
+        xr = e[w];
+        xi = e[2 + w];
+    } else {
+        const T* e = plane + 2 * ((static_cast<size_t>(t) * npy + y) * W + w);
+        xr = e[0];
+        xi = e[1];
+    }
+    re += static_cast<double>(xr) * tw.x - static_cast<double>(xi) * tw.y;
+    im += static_cast<double>(xr) * tw.y + static_cast<double>(xi) * tw.x;
 }
 
 template <typename T>
@@ -953,26 +967,59 @@ __global__ void __launch_bounds__(kThreads) gk_tap_kernel(const StepPlan P, cons
                                                           const T* __restrict__ i2, const cplx<T>* __restrict__ cur, const double* __restrict__ rho0,
                                                           const unsigned long long* __restrict__ step_base, int step_off, double weight,
                                                           int first_stage, int last_stage, double dt) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= P.batch * G.nmodes) return;
-    const int b = warp / G.nmodes, i = warp - b * G.nmodes;
+    const int i = blockIdx.x, b = blockIdx.y;
     const MemberInfo mi = members[b];
-    if (!mi.active) return;
+    if (!mi.active) return;  // the whole block
     const int gx = G.modes[i].x, ky = G.modes[i].y;
     const double kx = P.kx_unit * gx, kyv = P.ky_unit * ky;
     const size_t plane = static_cast<size_t>(P.hx) * P.npy * 2;  // scalars of one I2 plane
     const T* base = i2 + static_cast<size_t>(b) * P.n_out * plane;
+    const bool has_p = G.o_pxy >= 0, has_v = G.o_vx >= 0;
+    const T* pp = base + (has_p ? G.o_pxy : 0) * plane;
+    const T* pvx = base + (has_v ? G.o_vx : 0) * plane;
+    const T* pvy = base + (has_v ? G.o_vy : 0) * plane;
+    // column DFTs at ky: thread r sums rows r, r + kThreads, ... (twiddle index ky * y mod Np_y,
+    // stepped by ky * kThreads mod Np_y), every plane in the same pass
+    const int npy = P.npy;
+    const int t = gx / P.W, w = gx - t * P.W;
+    const int kk = ((ky % npy) + npy) % npy;
+    int idx = static_cast<int>((static_cast<long long>(kk) * threadIdx.x) % npy);
+    const int stride = static_cast<int>((static_cast<long long>(kk) * kThreads) % npy);
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // pxy, vx, vy (re, im)
+    for (int y = threadIdx.x; y < npy; y += kThreads) {
+        const double2 tw = G.wtab[idx];
+        idx += stride;
+        if (idx >= npy) idx -= npy;
+        if (has_p) gk_dft_term<T>(pp, G.pair_layout, P.W, npy, t, w, y, tw, acc[0], acc[1]);
+        if (has_v) {
+            gk_dft_term<T>(pvx, G.pair_layout, P.W, npy, t, w, y, tw, acc[2], acc[3]);
+            gk_dft_term<T>(pvy, G.pair_layout, P.W, npy, t, w, y, tw, acc[4], acc[5]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    __shared__ double part[kThreads / 32][6];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 6; ++q) part[wid][q] = acc[q];
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double v = part[0][q];
+        for (int k = 1; k < kThreads / 32; ++k) v += part[k][q];
+        acc[q] = v;
+    }
     double2 pxy = make_double2(0.0, 0.0);
-    if (G.o_pxy >= 0) pxy = gk_column_dft<T>(P, G, base + G.o_pxy * plane, gx, ky);
-    if (G.o_vx >= 0) {  // compressible viscous: -i eta (ky vx + kx vy) with v transformed from physical space
-        const double2 vx = gk_column_dft<T>(P, G, base + G.o_vx * plane, gx, ky);
-        const double2 vy = gk_column_dft<T>(P, G, base + G.o_vy * plane, gx, ky);
-        const double sr = kyv * vx.x + kx * vy.x, si = kyv * vx.y + kx * vy.y;
+    if (has_p) pxy = make_double2(acc[0], acc[1]);
+    if (has_v) {  // compressible viscous: -i eta (ky vx + kx vy) with v transformed from physical space
+        const double sr = kyv * acc[2] + kx * acc[4], si = kyv * acc[3] + kx * acc[5];
         pxy.x += P.eta * si;
         pxy.y -= P.eta * sr;
     }
-    if (lane != 0) return;
     if (G.incomp_visc) {  // incompressible viscous: v = j / rho0 of the stage state
         const int j = ky >= 0 ? ky : ky + P.kyn;
         const size_t fst = static_cast<size_t>(P.hx) * P.kyn;
