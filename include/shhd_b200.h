@@ -225,7 +225,8 @@ int shhd_engine_sk_read(shhd_engine* engine, double* out, size_t n_modes, int64_
  * kernel family valid for the configuration (FP32 compute sizes 96-1536: the
  * pair-line kernels and the single-line kernels; otherwise the one family)
  * with direct launches and as one replayed graph, on the engine's current
- * state, then restores the state, step counter and time and keeps the fastest
+ * state, then restores the state, step counter and time (and the accumulators
+ * of enabled per-step measures: Green-Kubo sums, flux taps) and keeps the fastest
  * combination.  *family: 4 two-pair row pass, 3 split row pass, 2 register
  * row pass, 1 pair-line, 0 other; *graph_chunk: the chosen chunk (0 = direct
  * launches); ms_per_step (optional, room for 10): the measured ms per step of

@@ -1763,6 +1763,24 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
     void* save_k0 = nullptr;
     check_cuda(cudaMalloc(&save, bytes), "autotune save buffer");
     if (k0b) check_cuda(cudaMalloc(&save_k0, k0b), "autotune save buffer");
+    // device buffers the per-stage measure taps accumulate into while trials step: saved with the
+    // state and restored after every trial, so that a measure's sums hold no trial steps
+    struct Kept { void* dev; size_t bytes; void* copy; };
+    std::vector<Kept> kept;
+    const size_t B = e->cfg.batch;
+    if (e->gk_on) {
+        const GkArgs& G = e->gk;
+        kept.push_back({G.sums, sizeof(double) * B * G.ntau * G.nmodes, nullptr});
+        kept.push_back({G.integral, sizeof(double2) * B * G.nmodes, nullptr});
+        kept.push_back({G.flux_step, sizeof(double2) * B * G.nmodes, nullptr});
+    }
+    if (e->flux0_on) kept.push_back({e->flux0.acc, sizeof(double) * B * e->flux0.ncol, nullptr});
+    for (int ax = 0; ax < 2; ++ax)
+        if (e->fline_on[ax]) kept.push_back({e->fline[ax].acc, sizeof(double2) * B * e->fline[ax].ncomp * e->fline[ax].nline, nullptr});
+    auto free_kept = [&] {
+        for (Kept& k : kept)
+            if (k.copy) cudaFree(k.copy);
+    };
     cudaEvent_t a = nullptr, b = nullptr;
     const int64_t step0 = e->step_index;
     const double time0 = e->time;
@@ -1773,12 +1791,17 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
     auto restore = [&] {
         check_cuda(cudaMemcpyAsync(e->u, save, bytes, cudaMemcpyDeviceToDevice, e->stream), "autotune restore");
         if (k0b) check_cuda(cudaMemcpyAsync(e->k0_u, save_k0, k0b, cudaMemcpyDeviceToDevice, e->stream), "autotune restore");
+        for (const Kept& k : kept) check_cuda(cudaMemcpyAsync(k.dev, k.copy, k.bytes, cudaMemcpyDeviceToDevice, e->stream), "autotune restore");
         e->step_index = step0;
         e->time = time0;
     };
     try {
         check_cuda(cudaMemcpyAsync(save, e->u, bytes, cudaMemcpyDeviceToDevice, e->stream), "autotune save");
         if (k0b) check_cuda(cudaMemcpyAsync(save_k0, e->k0_u, k0b, cudaMemcpyDeviceToDevice, e->stream), "autotune save");
+        for (Kept& k : kept) {
+            check_cuda(cudaMalloc(&k.copy, k.bytes), "autotune save buffer");
+            check_cuda(cudaMemcpyAsync(k.copy, k.dev, k.bytes, cudaMemcpyDeviceToDevice, e->stream), "autotune save");
+        }
         check_cuda(cudaEventCreate(&a), "cudaEventCreate");
         check_cuda(cudaEventCreate(&b), "cudaEventCreate");
         // candidates: kernel families valid for this configuration x {direct launches, one graph of trial_steps}
@@ -1861,6 +1884,7 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
         cudaStreamSynchronize(e->stream);
         cudaFree(save);
         if (save_k0) cudaFree(save_k0);
+        free_kept();
         if (a) cudaEventDestroy(a);
         if (b) cudaEventDestroy(b);
         throw;
@@ -1871,6 +1895,7 @@ void autotune(shhd_engine* e, int trial_steps, int* family_out, int* chunk_out, 
     e->profiling = prof;
     cudaFree(save);
     if (save_k0) cudaFree(save_k0);
+    free_kept();
     cudaEventDestroy(a);
     cudaEventDestroy(b);
 }

@@ -81,7 +81,7 @@ def _torch_event(engine):
 
 class _Bucket:
     def __init__(self, cfg: Config, slots: int, precision: int, seed: int, graph_chunk: int = 0,
-                 green_kubo: Optional[Tuple[int, int]] = None, engine_factory=Engine):
+                 green_kubo: Optional[Tuple[int, int]] = None, engine_factory=Engine, autotune: int = 0):
         c = cfg.copy()
         c.batch = slots
         c.precision = precision
@@ -91,8 +91,10 @@ class _Bucket:
             c.kBT = 1.0  # members carry sqrt(kBT_job) as their amplitude factor
         self.engine = engine_factory(c)
         self.device_bytes = int(self.engine.get_info().device_bytes)
+        self.graph_chunk = graph_chunk
         if graph_chunk > 0:
             self.engine.set_graph_chunk(graph_chunk)
+        self.autotune = autotune      # trial steps for timing the engine's kernels on its first job (0: no)
         self.green_kubo = green_kubo
         if green_kubo is not None:
             self.engine.gk_enable(*green_kubo)
@@ -121,6 +123,13 @@ class _Bucket:
         self.engine.set_member(m, key=job.key, step_origin=self.step_index, noise_scale=scale, active=True)
         if self.green_kubo is not None:
             self.engine.gk_read(m, reset=True)  # the slot's previous job's sums
+        if self.autotune:
+            # kernel family and launch shapes timed on the first job's state (state, step count and
+            # measure sums restored); the server's graph chunk is kept, since staggered slots need it
+            self.engine.autotune(self.autotune)
+            if self.graph_chunk > 0:
+                self.engine.set_graph_chunk(self.graph_chunk)
+            self.autotune = 0
         self.slots[m] = job
         self.remaining[m] = job.nsteps
         job.admitted = now
@@ -144,8 +153,10 @@ class Server:
     are the only device-facing parts; tests of the scheduling replace them."""
 
     def __init__(self, precision: int = FP32, seed: int = 20240601, max_slots: int = 32, chunk: int = 25,
-                 hbm_budget: Optional[int] = None, graphs: bool = True, engine_factory=Engine, event_factory=_torch_event):
+                 hbm_budget: Optional[int] = None, graphs: bool = True, engine_factory=Engine, event_factory=_torch_event,
+                 autotune: int = 0):
         self.graphs = graphs
+        self.autotune = autotune      # > 0: each new bucket engine autotunes (trials of this many steps) on its first job
         self.precision = precision
         self.seed = seed
         self.max_slots = max_slots
@@ -215,7 +226,7 @@ class Server:
         if slots < 1:
             return None
         b = _Bucket(job.config, int(slots), self.precision, self.seed, self.chunk if self.graphs else 0, job.green_kubo,
-                    engine_factory=self.engine_factory)
+                    engine_factory=self.engine_factory, autotune=self.autotune)
         self.used += b.device_bytes
         self.buckets_created += 1
         self.buckets.setdefault(key, []).append(b)

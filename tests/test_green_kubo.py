@@ -57,6 +57,31 @@ def test_green_kubo_matches_restatement(precision, name, text, selection):
     assert np.abs(sums - gk.sums).max() <= tol * scale, (name, precision, np.abs(sums - gk.sums).max() / scale)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_autotune_mid_run_leaves_the_measure_intact(precision):
+    """The autotuner's trial steps run the measure's taps; it restores their accumulators with the
+    state, so that an autotune in the middle of a block changes no sum."""
+    import shhd_b200 as sb
+    cfg = so.parse_script(COMP)
+    u0 = random_state(cfg, seed=14)
+    nevery, nblock, nsteps = 2, 6, 14
+    gk, uref = _oracle_gk(COMP, u0, nsteps, nevery, nblock, "diagonal")
+    c = sb.config_from_script(COMP)
+    c.precision = precision
+    with sb.Engine(c) as eng:
+        eng.set_state(u0)
+        eng.gk_enable(nevery, nblock, "diagonal")
+        eng.step(5)                    # inside the first block of 6
+        eng.autotune(2)
+        eng.step(nsteps - 5)
+        sums, blocks = eng.gk_read()
+        u = eng.get_state()
+    assert blocks == gk.nsample
+    assert so.rel_l2(u, uref) < (1e-12 if precision == 0 else 1e-5)
+    tol = 1e-10 if precision == 0 else 2e-4
+    assert np.abs(sums - gk.sums).max() <= tol * np.abs(gk.sums).max()
+
+
 def test_green_kubo_rejects_what_the_reference_rejects():
     import shhd_b200 as sb
     quiet = script(grid=(24, 24), length=(48.0, 48.0), nop=1, dt=0.01, te="srk3/quiescent", cT=None, eta=0.0, zeta=0.0,

@@ -50,7 +50,11 @@ class FakeEngine:
         return self.info
 
     def set_graph_chunk(self, n):
-        pass
+        self.chunks = getattr(self, "chunks", []) + [n]
+
+    def autotune(self, trial_steps):
+        # the real engine restores state and step count; here: record the call and what was active
+        self.tuned = getattr(self, "tuned", []) + [(trial_steps, int(self.active.sum()))]
 
     def gk_enable(self, *a):
         pass
@@ -194,4 +198,21 @@ def test_jobs_arriving_while_chunks_are_in_flight():
     assert stats["jobs"] == 12
     for j in jobs:
         assert int(j.result[0]) == j.nsteps, (j.key, int(j.result[0]), j.nsteps)
+    srv.close()
+
+
+def test_each_new_bucket_autotunes_once_on_its_first_job():
+    from shhd_b200 import serve
+    FakeEngine.live = []
+    jobs = [serve.Job(key=k, config=_cfg(g), state=np.zeros(1), nsteps=n, arrival=0.0)
+            for k, (g, n) in enumerate([(64, 30), (128, 20), (64, 10), (128, 25), (64, 5)])]
+    srv = _server(10 ** 9, max_slots=4, chunk=7, autotune=3)
+    srv.run(jobs)
+    engines = [e for e in FakeEngine.live if e.batch > 1 or getattr(e, "chunks", None)]
+    assert len(engines) == 2
+    for e in engines:
+        assert e.tuned == [(3, 1)]          # once, with the first job's slot active
+        assert e.chunks == [7, 7]           # the server's chunk set again after the autotuner's choice
+    for j in jobs:
+        assert int(j.result[0]) == j.nsteps
     srv.close()
