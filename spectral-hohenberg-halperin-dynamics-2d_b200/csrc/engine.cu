@@ -1153,8 +1153,7 @@ void launch_flux0_tap(shhd_engine* e, const void* cur, int step_off, double weig
     if (!e->flux0_on) return;
     const double2* k0 = nullptr;
     if (e->k0_u) k0 = cur == e->u ? e->k0_u : (cur == e->s1 ? e->k0_s1 : (cur == e->s2 ? e->k0_s2 : nullptr));
-    const long long threads = static_cast<long long>(e->P.batch) * e->flux0.ncol * 32;
-    const dim3 g(static_cast<unsigned>((threads + kThreads - 1) / kThreads));
+    const dim3 g(static_cast<unsigned>(e->flux0.ncol), static_cast<unsigned>(e->P.batch));
     flux0_tap_kernel<T><<<g, kThreads, 0, e->stream>>>(e->P, e->flux0, e->members_dev, static_cast<const T*>(e->i2),
                                                        static_cast<const cplx<T>*>(cur), k0, weight, first, e->step_dev, step_off);
     check_cuda(cudaGetLastError(), "flux0_tap launch");

@@ -1257,7 +1257,7 @@ __global__ void __launch_bounds__(kThreads) flux_line_tap_kernel(const StepPlan 
 // of the stage's x-transformed product planes, plus the linear pressure
 // cT^2 rho(0) on the diagonal; the gradient terms and the noise vanish at
 // k = 0.  The first stage of a step overwrites, so acc holds the last step's.
-// acc[member][3 + 2 nop]; one warp per (member, column)
+// acc[member][3 + 2 nop]; one block per (column, member)
 // ---------------------------------------------------------------------------
 struct Flux0Args {
     double* acc;
@@ -1274,22 +1274,27 @@ __global__ void __launch_bounds__(kThreads) flux0_tap_kernel(const StepPlan P, c
                                                              const T* __restrict__ i2, const cplx<T>* __restrict__ cur,
                                                              const double2* __restrict__ k0cur, double weight, int first,
                                                              const unsigned long long* __restrict__ step_base, int step_off) {
-    if (!tap_scheduled(step_base, step_off, F.period, F.phase)) return;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= P.batch * F.ncol) return;
-    const int b = warp / F.ncol, c = warp - b * F.ncol;
-    if (!members[b].active) return;
+    if (!tap_scheduled(step_base, step_off, F.period, F.phase)) return;  // grid-uniform
+    // one block per (column, member): strided rows per thread, then a fixed-order block sum
+    const int c = blockIdx.x, b = blockIdx.y;
+    if (!members[b].active) return;  // the whole block
     double v = 0.0;
     const int o = F.o[c];
     if (o >= 0) {
         const size_t plane = static_cast<size_t>(P.hx) * P.npy * 2;  // scalars of one I2 plane
         const T* base = i2 + (static_cast<size_t>(b) * P.n_out + o) * plane;
-        for (int y = lane; y < P.npy; y += 32)  // kx = 0: tile 0, slot 0, real part
+        for (int y = threadIdx.x; y < P.npy; y += kThreads)  // kx = 0: tile 0, slot 0, real part
             v += static_cast<double>(F.pair_layout ? base[4 * static_cast<size_t>(y)] : base[2 * static_cast<size_t>(y) * P.W]);
         for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+        __shared__ double part[kThreads / 32];
+        if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            v = part[0];
+            for (int k = 1; k < kThreads / 32; ++k) v += part[k];
+        }
     }
-    if (lane != 0) return;
+    if (threadIdx.x != 0) return;
     if (F.pressure && (c == 0 || c == 2)) {
         const size_t fst = static_cast<size_t>(P.hx) * P.kyn;
         const double r00 = k0cur ? k0cur[static_cast<size_t>(b) * P.nfields].x
