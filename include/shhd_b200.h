@@ -101,7 +101,7 @@ typedef struct shhd_config {
     /* engine options (no reference counterpart) */
     int precision;              /* enum shhd_precision */
     int noise_source;           /* enum shhd_noise_source */
-    int batch;                  /* members advanced together (>= 1) */
+    int batch;                  /* members advanced together (1 ... 65535) */
     int member_offset;          /* first member id for the noise key */
     /* free_energy == SHHD_FE_PLUGIN: the compiled-in style (1 ... shhd_free_energy_plugin_count(),
      * include/shhd_b200_free_energy.cuh) and its parameters [parameter][order parameter]; the

@@ -391,6 +391,8 @@ void validate_config(const shhd_config& c) {
     if (c.free_energy == SHHD_FE_PLUGIN && (c.fe_plugin < 1 || c.fe_plugin > plugin_count()))
         throw Failure(SHHD_EINVAL, "free-energy plugin style " + std::to_string(c.fe_plugin) + " is not compiled into this library");
     if (c.batch < 1) throw Failure(SHHD_EINVAL, "batch must be >= 1");
+    // members are a y or z grid dimension of the stage kernels
+    if (c.batch > 65535) throw Failure(SHHD_EINVAL, "batch must be <= 65535");
     if (c.precision != SHHD_FP64 && c.precision != SHHD_FP32) throw Failure(SHHD_EINVAL, "unknown precision");
     if (c.n_sine_forces < 0 || c.n_sine_forces > SHHD_MAX_FORCES || c.n_gradient_forces < 0 || c.n_gradient_forces > SHHD_MAX_FORCES)
         throw Failure(SHHD_EINVAL, "too many forces");

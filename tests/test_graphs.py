@@ -160,3 +160,13 @@ def test_launch_shape_rules_and_autotune():
         assert e.launch_shape[1] == 3            # momentum group on 768-point columns: three
     with _engine(sb, SRK3, sb.FP64) as e:
         assert e.launch_shape == (0, 0)          # no pair-line kernels
+
+
+def test_batch_above_the_grid_limit_is_refused():
+    """Members are a grid dimension of the stage kernels: more than 65535 is refused at creation."""
+    import shhd_b200 as sb
+    cfg = sb.config_from_script(SRK3)
+    cfg.batch = 65536
+    with pytest.raises(sb.ShhdError) as ei:
+        sb.Engine(cfg)
+    assert ei.value.code == sb.SHHD_EINVAL and "batch must be <= 65535" in str(ei.value)
